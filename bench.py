@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Benchmark: pair-column comparisons per second of the all-pairs distance path.
+
+One unit = one (i < j, column) comparison; an alignment of n sequences and L
+columns is n (n - 1) / 2 * L units.  A step is one pass of the path over one
+alignment: pack the resident bytes into bit planes, count every pair, apply the
+transform, post-process (mirror, diagonal, saturation fix-up).
+
+Default workload (one B200): DNA Kimura-2P, 10,000 x 10,000, tree-evolved
+synthetic alignment.  Output: one JSON line on rank 0.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+  python bench.py --impl reference ...   (the reference's threaded CPU path)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (generator, n, L, type, model)
+    "dna-k2p-10000x10000": ("tree_dna", 10000, 10000, "dna", "kim"),
+    "dna-jc-512x2000": ("iid_dna", 512, 2000, "dna", "jc"),
+    "dna-k2p-50000x1000": ("tree_dna", 50000, 1000, "dna", "kim"),
+    "protein-kimura-5000x1500": ("tree_protein", 5000, 1500, "protein", "kim"),
+}
+DEFAULT = "dna-k2p-10000x10000"
+# Algorithmic integer operations per pair per 32-column word:
+# (POPC, LOP3) of the counting kernel for each (type, model).
+OPS_PER_WORD = {("dna", "kim"): (3, 4), ("dna", "jc"): (2, 4), ("protein", "kim"): (2, 7),
+                ("protein", "jc"): (2, 7)}
+
+
+def make_alignment(name: str, seed: int = 0) -> np.ndarray:
+    from rapidnj_b200 import synth
+    gen, n, L, _, _ = WORKLOADS[name]
+    return getattr(synth, gen)(n, L, seed=seed)
+
+
+def units(n: int, L: int) -> float:
+    return n * (n - 1) / 2.0 * L
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- CPU baseline
+
+def cpu_reference(seqs: np.ndarray, model: str, type_: str, warmup: int, steps: int,
+                  budget_s: float = 12.0):
+    """The reference's threaded SSE path (oracle/_ref/ref_harness, built from the
+    reference sources) on all host cores, on a bounded sample of the workload:
+    the first n' sequences, n' chosen so one call takes about budget_s."""
+    from oracle import oracle
+    from rapidnj_b200 import synth
+    if not oracle.ref_available():
+        return None
+    cores = os.cpu_count() or 1
+    n, L = seqs.shape
+    t = "d" if type_ == "dna" else "p"
+
+    def run(rows: int, w: int, s: int):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "sample.fa")
+            synth.write_fasta(path, seqs[:rows])
+            p = subprocess.run([oracle.REF_HARNESS, "bench", path, "fa", t, "1", model, str(cores),
+                                str(w), str(s)], check=True, capture_output=True, text=True)
+            return json.loads(p.stdout.strip().splitlines()[-1])["step_s"]
+
+    probe_rows = min(n, 1024)
+    probe = run(probe_rows, 0, 1)[0]
+    rate = units(probe_rows, L) / max(probe, 1e-6)
+    rows = n
+    if units(n, L) / rate > budget_s:
+        rows = int((2.0 * budget_s * rate / L) ** 0.5)
+        rows = max(probe_rows, min(n, rows))
+    times = run(rows, warmup, steps)
+    mean = sum(times) / len(times)
+    return {"value": units(rows, L) / mean, "unit": "pair-columns/s", "cores": cores,
+            "kind": "reference",
+            "sample": f"first {rows} of {n} sequences x {L} columns, {len(times)} timed call(s) "
+                      f"of the reference driver (oracle/_ref/ref_harness, g++ -O3 -msse2, "
+                      f"{cores} threads)",
+            "step_s": times}
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def run_gpu(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+    from rapidnj_b200 import api
+
+    name = args.workload
+    gen, n, L, type_, model = WORKLOADS[name]
+    torch.cuda.set_device(local_rank)
+    seqs = make_alignment(name, seed=0)
+    typ = 0 if type_ == "dna" else 1
+    ctx = api.Context(local_rank)
+    ctx.set_profiling(True)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    d_chars = torch.from_numpy(seqs).cuda(local_rank)
+    out = torch.empty((n, n), dtype=torch.float32, device=f"cuda:{local_rank}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")  # > 126 MB L2
+    torch.cuda.synchronize()
+
+    def step():
+        aln = ctx.alignment(d_chars, typ)
+        ctx.distance_into(aln, model, out)
+        aln.close()
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank).start()
+    total_ms, count_ms = 0.0, []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        b.synchronize()
+        total_ms += a.elapsed_time(b)
+        count_ms.append(ctx.stage_times()[1])
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    W = units(n, L) * world
+    result = {"ms_per_step": ms_per_step, "value": W / (ms_per_step * 1e-3), "clocks": clk,
+              "count_ms": count_ms}
+
+    if rank == 0:
+        # Roofline of the dominant kernel (the tile count kernel) against the
+        # measured integer-pipe peak of this device.
+        popc_peak, lop3_peak = ctx.probe_int_peaks()
+        popc_w, lop3_w = OPS_PER_WORD[(type_, model)]
+        words = units(n, L) / 32.0
+        cnt = sum(count_ms) / len(count_ms)
+        achieved = popc_w * words / (cnt * 1e-3)
+        result["roofline"] = {
+            "bound": "int", "pipe": "POPC", "achieved": achieved / 1e12, "peak": popc_peak / 1e12,
+            "unit": "Tops/s", "frac": achieved / popc_peak,
+            "traffic": traffic_from_profiles(name),
+            "kernel": "count_tiles_kernel", "kernel_ms": cnt,
+            "lop3_frac": (lop3_w * words / (cnt * 1e-3)) / lop3_peak,
+            "peak_source": "rnj_probe_int_peaks, measured on this device in this run",
+            "ops_per_pair_word": {"popc": popc_w, "lop3": lop3_w},
+        }
+        result["e2e"] = run_e2e(ctx, seqs, typ, model, args)
+    ctx.close()
+    return result
+
+
+def run_e2e(ctx, seqs, typ, model, args):
+    """The same metric through the host-facing C ABI call (rnj_distance_matrix_host):
+    pinned host bytes in, a freshly allocated host n x n float matrix out, the
+    H2D and D2H copies and the host row copy inside the timed region."""
+    import torch
+    n, L = seqs.shape
+    pinned = torch.from_numpy(seqs).pin_memory()
+    host = pinned.numpy()
+    steps = max(1, min(args.steps, 5))
+    ctx.distance_matrix_host(host, model, typ)  # warm-up
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ctx.distance_matrix_host(host, model, typ)
+        times.append(time.perf_counter() - t0)
+    mean = sum(times) / len(times)
+    return {"value": units(n, L) / mean, "unit": "pair-columns/s", "h2d_bytes_per_step": n * L,
+            "d2h_bytes_per_step": n * n * 4, "ms_per_step": mean * 1e3, "steps": steps,
+            "call": "rnj_distance_matrix_host"}
+
+
+def traffic_from_profiles(name: str):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        return json.load(open(p)).get(name)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------- main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    gen, n, L, type_, model = WORKLOADS[args.workload]
+    config = {"workload": args.workload, "n": n, "L": L, "type": type_, "model": model,
+              "generator": gen, "seed": 0, "parallelism": f"tiles/{world}" if world > 1 else "single",
+              "l2": "256 MiB buffer written between timed steps (L2 flushed)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        seqs = make_alignment(args.workload)
+        cpu = cpu_reference(seqs, model, type_, args.warmup, args.steps, budget_s=8.0)
+        if cpu is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/ref_harness not built (needs the reference sources)"}))
+            return
+        line = {"impl": "reference", "metric": "pair-column comparisons/s", "value": cpu["value"],
+                "unit": "pair-columns/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * sum(cpu["step_s"]) / len(cpu["step_s"]),
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "u32", "data": "synthetic", "config": config,
+                "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cpu["value"], "unit": "pair-columns/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    res = run_gpu(args, rank, world, local_rank)
+    if rank == 0:
+        line = {"metric": "pair-column comparisons/s", "value": res["value"],
+                "unit": "pair-columns/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+                "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": config,
+                "roofline": res["roofline"], "e2e": res["e2e"], "clocks": res["clocks"],
+                "gpu_launches": 3 * args.steps}
+        if not args.no_cpu_baseline:
+            seqs = make_alignment(args.workload)
+            cpu = cpu_reference(seqs, model, type_, 0, 1)
+            line["cpu_baseline"] = ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                                    if cpu else None)
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,188 @@
+/*
+ * rnj.h -- C ABI of librnjgpu.so, the B200 (sm_100a) distance-estimation path of
+ * rapidNJ.
+ *
+ * The library replaces the all-pairs distance matrix that rapidNJ builds from an
+ * alignment (src/distanceCalculation/ of rapidNJ):
+ *   - DNA: Jukes-Cantor and Kimura two-parameter distances,
+ *   - protein: Jukes-Cantor and Kimura's protein distance (Dayhoff PAM table),
+ * with the reference's packing rules, per-pair counts, transforms and
+ * post-process (mirror, zero diagonal, saturated pairs -> 2 * max).
+ *
+ * Every entry point returns an rnj_status; on failure rnj_last_error() holds a
+ * message for the calling thread.  Nothing here calls exit().
+ *
+ * Objects (rnj_ctx, rnj_aln, rnj_mat, rnj_batch, rnj_server) are opaque.  A context
+ * owns one CUDA stream on one device and is not shared between host threads.
+ * Device pointers passed in or out are plain CUDA device addresses on the
+ * context's device.
+ */
+#ifndef RNJ_H
+#define RNJ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- constants */
+
+typedef enum {
+  RNJ_OK = 0,
+  RNJ_ERR_INVALID = 1,     /* bad argument */
+  RNJ_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  RNJ_ERR_NOMEM = 3,       /* device or pinned host allocation failed */
+  RNJ_ERR_IO = 4,          /* file could not be read / written */
+  RNJ_ERR_FORMAT = 5,      /* malformed alignment (ragged rows, < 2 sequences, ...) */
+  RNJ_ERR_TIMEOUT = 6,     /* a bounded device or host wait ran out */
+  RNJ_ERR_BUSY = 7,        /* admission refused (not enough free device memory) */
+  RNJ_ERR_UNSUPPORTED = 8, /* option not available in this build */
+  RNJ_ERR_NOTREADY = 9     /* request still running */
+} rnj_status;
+
+/* Sequence type; same values as InputType in rapidNJ src/stdinclude.h:26. */
+typedef enum { RNJ_DNA = 0, RNJ_PROTEIN = 1, RNJ_UNKNOWN = 2 } rnj_type;
+
+/* Evolution model (-a jc / -a kim, src/main.cpp:253-274). */
+typedef enum { RNJ_JC = 0, RNJ_KIMURA = 1 } rnj_model;
+
+/* Alignment flags. */
+enum {
+  /* Bit-string fast path, the CLI default (src/main.cpp:597).  Without it the
+   * counts follow the naive estimator used by -f
+   * (src/distanceCalculation/simpleDistanceCalculator.cpp:40-98). */
+  RNJ_FASTDIST = 1,
+  /* Reproduce the fast protein estimator's valid-site arithmetic for
+   * L % 128 == 0 (bitDistanceProtein.cpp:15-16,59), which subtracts 128 extra
+   * padding gaps and can wrap.  Off by default: the default counts are the
+   * correct ones, equal to the naive estimator's. */
+  RNJ_COMPAT_PROTEIN_WRAP = 2,
+  /* Compute every (row, column) pair in row order instead of the upper triangle
+   * plus mirror, as the disk-matrix driver does (KimuraDistance.cpp:308-354 with
+   * dm != NULL).  Only differs for the naive DNA estimator, whose counts are
+   * asymmetric. */
+  RNJ_FULL_ROWS = 4
+};
+
+typedef struct rnj_ctx rnj_ctx;
+typedef struct rnj_aln rnj_aln;
+typedef struct rnj_mat rnj_mat;
+
+/* ------------------------------------------------------------------ general */
+
+const char *rnj_version(void);
+const char *rnj_last_error(void);
+
+/* Context on CUDA device `device`.  Replaces initialiseDNA_gpu /
+ * initialiseProtein_gpu of the reference's CUDA glue (KimuraDistance.cpp:17-28). */
+int rnj_ctx_create(int device, rnj_ctx **out);
+int rnj_ctx_destroy(rnj_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t). */
+int rnj_ctx_stream(rnj_ctx *ctx, void **stream);
+int rnj_ctx_synchronize(rnj_ctx *ctx);
+
+/* Stage timing: when on, the library records CUDA events around its kernels
+ * (pack, count, transform/fix-up) on the context's stream;
+ * rnj_ctx_stage_times() synchronises and returns the last call's milliseconds
+ * per stage in ms[0..2]: pack, count (incl. a split-K transform), fix-up. */
+int rnj_ctx_set_profiling(rnj_ctx *ctx, int on);
+int rnj_ctx_stage_times(rnj_ctx *ctx, float *ms);
+
+/* Measured device-wide throughput of the two integer pipes the counting kernels
+ * run on: POPC and LOP3 operations per second (a short microbenchmark). */
+int rnj_probe_int_peaks(rnj_ctx *ctx, double *popc_per_s, double *lop3_per_s);
+
+/* Sequence type of an alignment from its first sequence: any byte >= 65 outside
+ * ACGTUN/acgtun makes it protein (dataloaderFasta.hpp:54-76). */
+int rnj_detect_type(const char *seq0, int L);
+
+/* --------------------------------------------------------- alignment upload */
+
+/* Packs n sequences of L bytes each into the device bit-plane layout.  Replaces
+ * the loader's packing (encodeDNASequence / encodeProteinSequence,
+ * dataloaderFasta.hpp:135-182) and storeDataDNA_gpu (KimuraDistance.cpp:19).
+ * `type` RNJ_UNKNOWN detects it from seqs[0].  `flags` is RNJ_FASTDIST |
+ * RNJ_COMPAT_PROTEIN_WRAP | RNJ_FULL_ROWS.  Bytes are the characters of the
+ * alignment as the reference's parsers keep them (33..126). */
+int rnj_aln_from_host(rnj_ctx *ctx, const char *const *seqs, int n, int L, int type,
+                      int flags, rnj_aln **out);
+/* Same, from one host buffer of n rows with stride ld >= L. */
+int rnj_aln_from_host_buffer(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
+                             int type, int flags, rnj_aln **out);
+/* Same, from a device buffer already on the context's device. */
+int rnj_aln_from_device(rnj_ctx *ctx, const void *d_chars, int n, int L, size_t ld,
+                        int type, int flags, rnj_aln **out);
+/* From the reference loader's packed arrays (dataloader::getBitStrings /
+ * getGapFilters / getBitStringsCount, dataloader.hpp:20-24): DNA 2-bit codes, 16
+ * sites per uint32 LSB first, with 01-per-valid-site gap filters; protein one
+ * resolved byte per site.  This is the entry the drop-in distance classes use on
+ * the fast path. */
+int rnj_aln_from_bitstrings(rnj_ctx *ctx, const unsigned int *const *bit_strings,
+                            const unsigned int *const *gap_filters, int n, int L,
+                            int bit_strings_count, int type, int flags, rnj_aln **out);
+int rnj_aln_info(const rnj_aln *aln, int *n, int *L, int *type);
+int rnj_aln_destroy(rnj_aln *aln);
+
+/* ---------------------------------------------------------------- distances */
+
+/* Full post-processed n x n float matrix on the device: the matrix that
+ * JCdistance::computeDistanceMatrix (JCdistance.cpp:24-44) and
+ * KimuraDistance::computeDistances (KimuraDistance.cpp:75-99) leave behind, and
+ * the replacement for computeDistancesDNA2_gpu / computeDistancesProtein_gpu
+ * (KimuraDistance.cpp:21,25). */
+int rnj_distance(rnj_ctx *ctx, rnj_aln *aln, int model, rnj_mat **out);
+/* Same into a caller-owned device buffer of n rows with stride ld (floats).
+ * max_out (host, may be NULL) receives the maximum distance; reading it
+ * synchronises the context's stream. */
+int rnj_distance_into(rnj_ctx *ctx, rnj_aln *aln, int model, float *d_out, size_t ld,
+                      float *max_out);
+/* Raw per-pair counts, the DistanceEstimate::computeDistance contract
+ * (DistanceEstimate.hpp:14): {ts, tv, valid} for DNA, {mismatch, 0, valid} for
+ * protein, as n*n*3 uint32 on the device, written for j > i (every pair with
+ * RNJ_FULL_ROWS; every other entry is set to zero).  The valid count is the
+ * correct one; RNJ_COMPAT_PROTEIN_WRAP only changes distances. */
+int rnj_counts_into(rnj_ctx *ctx, rnj_aln *aln, unsigned int *d_counts);
+
+int rnj_mat_info(rnj_mat *mat, int *n, float *max_distance);
+int rnj_mat_device_ptr(rnj_mat *mat, float **d_ptr, size_t *ld);
+/* Copies rows [row0, row0 + nrows) into host arrays rows[0..nrows) of n floats
+ * each (for example rows allocated with new distType[n], which the join loops
+ * later delete[]).  Uses pinned staging and `threads` host threads (<= 0: all
+ * online cores) for the final copy. */
+int rnj_mat_copy_rows(rnj_ctx *ctx, rnj_mat *mat, int row0, int nrows, float **rows,
+                      int threads);
+int rnj_mat_destroy(rnj_mat *mat);
+
+/* One call, host in / host out: pack, distances, copy into out (n*n floats,
+ * row-major).  max_out may be NULL. */
+int rnj_distance_matrix_host(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
+                             int type, int model, int flags, float *out, float *max_out);
+
+/* ------------------------------------------------------- alignment files */
+
+/* A parsed multiple alignment on the host: names and n*L bytes (row-major). */
+typedef struct rnj_msa rnj_msa;
+
+/* Reads a single-line FASTA ("fa") or Stockholm ("sth") alignment with the
+ * reference loaders' rules (dataloaderFasta.hpp:78-133,201-276;
+ * dataloaderStockholm.hpp:79-120,185-307): characters <= 32 are dropped from
+ * sequence lines, every sequence must have the first one's length.  format
+ * NULL picks by file extension as main.cpp:646-683 does. */
+int rnj_msa_read(const char *path, const char *format, rnj_msa **out);
+int rnj_msa_info(const rnj_msa *msa, int *n, int *L, int *detected_type);
+const char *rnj_msa_name(const rnj_msa *msa, int i);
+const char *rnj_msa_chars(const rnj_msa *msa);
+int rnj_msa_destroy(rnj_msa *msa);
+
+/* Writes the "-o m" text matrix of main.cpp:212-221 ("\t<n>", then per row the
+ * name, a tab and n values printed with six fixed decimals, each followed by a
+ * space).  rows[i] are n floats; path NULL writes to stdout. */
+int rnj_write_matrix_text(const char *path, const char *const *names, const float *const *rows,
+                          int n, int threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RNJ_H */

@@ -1,0 +1,255 @@
+"""Python face of the C ABI: contexts, packed alignments, distance matrices.
+
+Everything here forwards to librnjgpu.so; device buffers may be torch CUDA
+tensors (passed by data pointer).  Host arrays are numpy.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+from ._native import (RNJ_COMPAT_PROTEIN_WRAP, RNJ_DNA, RNJ_FASTDIST, RNJ_FULL_ROWS, RNJ_JC,
+                      RNJ_KIMURA, RNJ_PROTEIN, RNJ_UNKNOWN, check)
+
+MODELS = {"jc": RNJ_JC, "kim": RNJ_KIMURA, RNJ_JC: RNJ_JC, RNJ_KIMURA: RNJ_KIMURA}
+TYPES = {None: RNJ_UNKNOWN, "d": RNJ_DNA, "p": RNJ_PROTEIN, "dna": RNJ_DNA, "protein": RNJ_PROTEIN,
+         RNJ_DNA: RNJ_DNA, RNJ_PROTEIN: RNJ_PROTEIN, RNJ_UNKNOWN: RNJ_UNKNOWN}
+
+
+def flags_of(fastdist: bool = True, compat_wrap: bool = False, full_rows: bool = False) -> int:
+    return ((RNJ_FASTDIST if fastdist else 0) | (RNJ_COMPAT_PROTEIN_WRAP if compat_wrap else 0)
+            | (RNJ_FULL_ROWS if full_rows else 0))
+
+
+def detect_type(seq0: bytes) -> int:
+    return N.lib().rnj_detect_type(seq0, len(seq0))
+
+
+def version() -> str:
+    return N.lib().rnj_version().decode()
+
+
+class Alignment:
+    """A packed alignment on the device (rnj_aln)."""
+
+    def __init__(self, ctx: "Context", handle: int):
+        self.ctx = ctx
+        self.handle = ctypes.c_void_p(handle)
+        n, L, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(N.lib().rnj_aln_info(self.handle, ctypes.byref(n), ctypes.byref(L), ctypes.byref(t)))
+        self.n, self.L, self.type = n.value, L.value, t.value
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().rnj_aln_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Matrix:
+    """A post-processed distance matrix on the device (rnj_mat)."""
+
+    def __init__(self, ctx: "Context", handle: int):
+        self.ctx = ctx
+        self.handle = ctypes.c_void_p(handle)
+        n = ctypes.c_int()
+        check(N.lib().rnj_mat_info(self.handle, ctypes.byref(n), None))
+        self.n = n.value
+
+    @property
+    def max(self) -> float:
+        m = ctypes.c_float()
+        check(N.lib().rnj_mat_info(self.handle, None, ctypes.byref(m)))
+        return m.value
+
+    def device_ptr(self):
+        p, ld = ctypes.c_void_p(), ctypes.c_size_t()
+        check(N.lib().rnj_mat_device_ptr(self.handle, ctypes.byref(p), ctypes.byref(ld)))
+        return p.value, ld.value
+
+    def copy_rows(self, rows, row0: int = 0, threads: int = 0) -> None:
+        """Copies len(rows) rows starting at row0 into host float32 arrays."""
+        ptrs = (ctypes.c_void_p * len(rows))(*[r.ctypes.data for r in rows])
+        check(N.lib().rnj_mat_copy_rows(self.ctx.handle, self.handle, row0, len(rows), ptrs, threads))
+
+    def to_numpy(self, threads: int = 0) -> np.ndarray:
+        out = np.empty((self.n, self.n), dtype=np.float32)
+        self.copy_rows([out[i] for i in range(self.n)], 0, threads)
+        return out
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().rnj_mat_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """One device, one CUDA stream (rnj_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_ctx_create(device, ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        check(N.lib().rnj_ctx_stream(self.handle, ctypes.byref(s)))
+        return s.value or 0
+
+    def synchronize(self) -> None:
+        check(N.lib().rnj_ctx_synchronize(self.handle))
+
+    def set_profiling(self, on: bool = True) -> None:
+        check(N.lib().rnj_ctx_set_profiling(self.handle, int(on)))
+
+    def stage_times(self):
+        """(pack_ms, count_ms, fixup_ms) of the last call, profiling on."""
+        ms = (ctypes.c_float * 3)()
+        check(N.lib().rnj_ctx_stage_times(self.handle, ms))
+        return tuple(ms)
+
+    def probe_int_peaks(self):
+        """(POPC ops/s, LOP3 ops/s) measured on this device."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(N.lib().rnj_probe_int_peaks(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    # --- alignments
+    def alignment(self, seqs, type_=None, fastdist: bool = True, compat_wrap: bool = False,
+                  full_rows: bool = False) -> Alignment:
+        """Packs an alignment from a host (n, L) uint8 array or a CUDA uint8 tensor."""
+        flags = flags_of(fastdist, compat_wrap, full_rows)
+        t = TYPES[type_]
+        h = ctypes.c_void_p()
+        if hasattr(seqs, "is_cuda") and seqs.is_cuda:
+            n, L = seqs.shape
+            ld = seqs.stride(0)
+            check(N.lib().rnj_aln_from_device(self.handle, ctypes.c_void_p(seqs.data_ptr()), n, L,
+                                              ld, t, flags, ctypes.byref(h)))
+        else:
+            a = np.ascontiguousarray(seqs, dtype=np.uint8)
+            n, L = a.shape
+            check(N.lib().rnj_aln_from_host_buffer(self.handle, a.ctypes.data, n, L, L, t, flags,
+                                                   ctypes.byref(h)))
+        return Alignment(self, h.value)
+
+    def alignment_from_rows(self, rows, type_=None, fastdist=True, compat_wrap=False,
+                            full_rows=False) -> Alignment:
+        """Packs from a list of equal-length bytes objects (row pointers)."""
+        n = len(rows)
+        L = len(rows[0]) if n else 0
+        arr = (ctypes.c_char_p * n)(*rows)
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_aln_from_host(self.handle, arr, n, L, TYPES[type_],
+                                        flags_of(fastdist, compat_wrap, full_rows), ctypes.byref(h)))
+        return Alignment(self, h.value)
+
+    def alignment_from_bitstrings(self, bit_strings, gap_filters, L: int, type_: int,
+                                  flags: int = RNJ_FASTDIST) -> Alignment:
+        """From the reference loader's packed arrays (lists of uint32 numpy arrays of
+        bitStringsCount * 4 words each)."""
+        n = len(bit_strings)
+        count = bit_strings[0].size // 4 if n else 0
+        bs = (ctypes.c_void_p * n)(*[b.ctypes.data for b in bit_strings])
+        gf = (ctypes.c_void_p * n)(*[g.ctypes.data for g in gap_filters]) if gap_filters else None
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_aln_from_bitstrings(self.handle, bs, gf, n, L, count, type_, flags,
+                                              ctypes.byref(h)))
+        return Alignment(self, h.value)
+
+    # --- distances
+    def distance(self, aln: Alignment, model="kim") -> Matrix:
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_distance(self.handle, aln.handle, MODELS[model], ctypes.byref(h)))
+        return Matrix(self, h.value)
+
+    def distance_into(self, aln: Alignment, model, out, want_max: bool = False):
+        """Into a CUDA float32 tensor of shape (n, >= n).  Returns the max when asked
+        (synchronising), else None."""
+        m = ctypes.c_float()
+        check(N.lib().rnj_distance_into(self.handle, aln.handle, MODELS[model],
+                                        ctypes.c_void_p(out.data_ptr()), out.stride(0),
+                                        ctypes.byref(m) if want_max else None))
+        return m.value if want_max else None
+
+    def counts_into(self, aln: Alignment, out) -> None:
+        """Raw counts into a CUDA int32/uint32 tensor of n*n*3 elements."""
+        check(N.lib().rnj_counts_into(self.handle, aln.handle, ctypes.c_void_p(out.data_ptr())))
+
+    def distance_matrix_host(self, seqs: np.ndarray, model="kim", type_=None, fastdist=True,
+                             compat_wrap=False, full_rows=False):
+        a = np.ascontiguousarray(seqs, dtype=np.uint8)
+        n, L = a.shape
+        out = np.empty((n, n), dtype=np.float32)
+        m = ctypes.c_float()
+        check(N.lib().rnj_distance_matrix_host(self.handle, a.ctypes.data, n, L, L, TYPES[type_],
+                                               MODELS[model],
+                                               flags_of(fastdist, compat_wrap, full_rows),
+                                               out.ctypes.data, ctypes.byref(m)))
+        return out, m.value
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().rnj_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# --- alignment files (host only) -------------------------------------------------
+
+def read_alignment(path: str, fmt: str | None = None):
+    """(names, chars (n, L) uint8, detected type) with the reference loaders' rules."""
+    h = ctypes.c_void_p()
+    check(N.lib().rnj_msa_read(path.encode(), fmt.encode() if fmt else None, ctypes.byref(h)))
+    try:
+        n, L, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(N.lib().rnj_msa_info(h, ctypes.byref(n), ctypes.byref(L), ctypes.byref(t)))
+        names = []
+        k = 0
+        while True:
+            nm = N.lib().rnj_msa_name(h, k)
+            if nm is None:
+                break
+            names.append(nm.decode("latin-1"))
+            k += 1
+        ptr = N.lib().rnj_msa_chars(h)
+        size = n.value * L.value
+        chars = np.frombuffer(ctypes.string_at(ptr, size), dtype=np.uint8).reshape(n.value, L.value).copy() \
+            if size else np.zeros((n.value, L.value), np.uint8)
+        return names, chars, t.value
+    finally:
+        N.lib().rnj_msa_destroy(h)
+
+
+def write_matrix_text(path: str | None, names, matrix: np.ndarray, threads: int = 0) -> None:
+    m = np.ascontiguousarray(matrix, dtype=np.float32)
+    n = m.shape[0]
+    nm = (ctypes.c_char_p * n)(*[x.encode("latin-1") for x in names[:n]])
+    rows = (ctypes.c_void_p * n)(*[m[i].ctypes.data for i in range(n)])
+    check(N.lib().rnj_write_matrix_text(path.encode() if path else None, nm, rows, n, threads))

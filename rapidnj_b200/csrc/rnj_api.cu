@@ -1,0 +1,763 @@
+// rnj_api.cu -- the C ABI of librnjgpu.so (declared in include/rnj.h): context,
+// alignment upload and packing, distance orchestration, copy-out into host rows.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "rnj.h"
+#include "rnj_internal.h"
+
+namespace rnj {
+
+static thread_local std::string g_error;
+
+int set_error(int code, const std::string &msg) {
+  g_error = msg;
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char *what) {
+  const int code = (e == cudaErrorMemoryAllocation) ? RNJ_ERR_NOMEM : RNJ_ERR_CUDA;
+  return set_error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RNJ_CUDA(call, what)                       \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_error(e_, what); \
+  } while (0)
+
+// cuTensorMapEncodeTiled, resolved through the runtime so the library loads on
+// hosts without a driver (the symbol is only needed once a device is in use).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+int encode_planes_map(Packed &p) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  cuuint64_t dims[3] = {(cuuint64_t)p.Np, (cuuint64_t)p.Wp, (cuuint64_t)p.NP};
+  cuuint64_t strides[2] = {(cuuint64_t)p.Np * 4, (cuuint64_t)p.Np * p.Wp * 4};
+  cuuint32_t box[3] = {(cuuint32_t)kTile, (cuuint32_t)kKW, (cuuint32_t)p.NP};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, p.planes, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return RNJ_OK;
+}
+
+// resolveChar of the loaders (dataloaderFasta.hpp:184-199).
+static char resolve_char(char c, int type) {
+  if (type == RNJ_DNA) {
+    if (!(c == 'a' || c == 'A' || c == 'c' || c == 'C' || c == 'g' || c == 'G' || c == 't' ||
+          c == 'T' || c == 'u' || c == 'U'))
+      return '-';
+    return c;
+  }
+  if (c == '-' || c == '.' || c == 'X' || c == 'x' || c == 'z' || c == 'Z' || c == 'b' ||
+      c == 'B' || c == 'J' || c == 'j' || c == '?')
+    return '-';
+  return c;
+}
+
+// Per-byte plane bits for DNA (bit0 code high, bit1 code low, bit2 valid, bit3
+// upper-case A/C/G/T).  Fast rule (dataloaderFasta.hpp:155-180): only A/C/G/T in
+// either case are valid.  Naive rule (simpleDistanceCalculator.cpp with
+// resolveChar): A/C/G/T/U in either case are valid.
+static void dna_lut(bool naive, uint8_t lut[256]) {
+  memset(lut, 0, 256);
+  struct { char c; int code; } letters[] = {{'A', 0}, {'G', 1}, {'T', 2}, {'C', 3}};
+  for (auto &l : letters) {
+    const uint8_t bits = (uint8_t)(((l.code >> 1) & 1) | ((l.code & 1) << 1) | 4);
+    lut[(uint8_t)l.c] = bits | 8;
+    lut[(uint8_t)(l.c - 'A' + 'a')] = bits;
+  }
+  if (naive) {
+    lut[(uint8_t)'U'] = 4;
+    lut[(uint8_t)'u'] = 4;
+  }
+}
+
+}  // namespace rnj
+
+using namespace rnj;
+
+struct rnj_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  Scratch scratch;
+  uint32_t *d_mask = nullptr;        // presence mask (8 words)
+  uint32_t *h_mask = nullptr;        // pinned
+  int *h_max = nullptr;              // pinned max bits / error word
+  void *h_stage[2] = {nullptr, nullptr};  // pinned staging for copy-out / upload
+  size_t stage_cap = 0;
+  bool profiling = false;
+  cudaEvent_t ev[6] = {};             // pack, count, fix-up: begin/end pairs
+  bool ev_used[3] = {false, false, false};
+};
+
+struct rnj_aln {
+  rnj_ctx *ctx = nullptr;
+  Packed p;
+};
+
+struct rnj_mat {
+  rnj_ctx *ctx = nullptr;
+  float *d = nullptr;
+  int n = 0;
+  size_t ld = 0;
+  int *d_max = nullptr;  // device copy of the max bits
+  bool owns = true;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+void mark(rnj_ctx *ctx, int stage, int end) {
+  if (!ctx->profiling) return;
+  cudaEventRecord(ctx->ev[2 * stage + end], ctx->stream);
+  if (end) ctx->ev_used[stage] = true;
+}
+
+int ensure_scratch_words(rnj_ctx *ctx, size_t words) {
+  Scratch &s = ctx->scratch;
+  if (s.words_cap >= words) return RNJ_OK;
+  if (s.words) cudaFreeAsync(s.words, ctx->stream);
+  s.words = nullptr;
+  s.words_cap = 0;
+  RNJ_CUDA(cudaMallocAsync((void **)&s.words, words * sizeof(int), ctx->stream), "scratch");
+  s.words_cap = words;
+  return RNJ_OK;
+}
+
+int ensure_stage(rnj_ctx *ctx, size_t bytes) {
+  if (ctx->stage_cap >= bytes) return RNJ_OK;
+  RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "staging sync");
+  for (int b = 0; b < 2; ++b) {
+    if (ctx->h_stage[b]) cudaFreeHost(ctx->h_stage[b]);
+    ctx->h_stage[b] = nullptr;
+  }
+  ctx->stage_cap = 0;
+  for (int b = 0; b < 2; ++b)
+    RNJ_CUDA(cudaMallocHost(&ctx->h_stage[b], bytes), "pinned staging");
+  ctx->stage_cap = bytes;
+  return RNJ_OK;
+}
+
+int host_threads(int threads) {
+  if (threads > 0) return threads;
+  long n = sysconf(_SC_NPROCESSORS_ONLN);
+  return n > 0 ? (int)std::min<long>(n, 64) : 1;
+}
+
+// Parallel row copy: dst[r] (n floats) <- src + r * n.
+void scatter_rows(const float *src, float **dst, int nrows, int n, int threads) {
+  const size_t bytes = (size_t)nrows * n * sizeof(float);
+  int t = std::max(1, std::min(threads, (int)(bytes / (1 << 20)) + 1));
+  t = std::min(t, nrows);
+  if (t <= 1) {
+    for (int r = 0; r < nrows; ++r) memcpy(dst[r], src + (size_t)r * n, (size_t)n * sizeof(float));
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int k = 0; k < t; ++k) {
+    pool.emplace_back([=] {
+      for (int r = k; r < nrows; r += t)
+        memcpy(dst[r], src + (size_t)r * n, (size_t)n * sizeof(float));
+    });
+  }
+  for (auto &th : pool) th.join();
+}
+
+// Upload raw bytes already on the device (n rows, stride ld) into planes.
+int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
+                           int type, int flags, rnj_aln **out) {
+  if (n < 0 || L < 0 || (n > 0 && ld < (size_t)L))
+    return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
+  if (type != RNJ_DNA && type != RNJ_PROTEIN)
+    return set_error(RNJ_ERR_INVALID, "sequence type must be resolved before packing");
+  const bool naive = (flags & RNJ_FASTDIST) == 0;
+  uint8_t lut[256];
+  int kind;
+  if (type == RNJ_DNA) {
+    kind = naive ? KIND_NAIVE : KIND_DNA;
+    dna_lut(naive, lut);
+  } else {
+    // Rank the residue alphabet present in the alignment.
+    RNJ_CUDA(cudaMemsetAsync(ctx->d_mask, 0, 8 * sizeof(uint32_t), ctx->stream), "mask clear");
+    if (n > 0 && L > 0)
+      RNJ_CUDA(launch_presence(d_chars, ld, n, L, ctx->d_mask, ctx->stream), "presence kernel");
+    RNJ_CUDA(cudaMemcpyAsync(ctx->h_mask, ctx->d_mask, 8 * sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost, ctx->stream),
+             "mask copy");
+    RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "mask sync");
+    int rank = 0;
+    for (int c = 0; c < 256; ++c) {
+      const bool present = (ctx->h_mask[c >> 5] >> (c & 31)) & 1u;
+      if (resolve_char((char)c, RNJ_PROTEIN) == '-') lut[c] = 0xFF;
+      else if (present) lut[c] = (uint8_t)(rank++);
+      else lut[c] = 0xFF;
+    }
+    kind = rank <= 4 ? KIND_MISM2 : (rank <= 32 ? KIND_MISM5 : KIND_MISM7);
+  }
+  rnj_aln *a = new rnj_aln();
+  a->ctx = ctx;
+  Packed &p = a->p;
+  p.n = n;
+  p.L = L;
+  p.type = type;
+  p.flags = flags;
+  p.kind = kind;
+  p.W = (L + 31) / 32;
+  p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
+  p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
+  p.NP = planes_of(kind);
+  const size_t bytes = (size_t)p.NP * p.Wp * p.Np * sizeof(uint32_t);
+  cudaError_t e = cudaMallocAsync((void **)&p.planes, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    delete a;
+    return cuda_error(e, "plane allocation");
+  }
+  mark(ctx, 0, 0);
+  e = launch_pack_chars(d_chars, ld, p, lut, ctx->stream);
+  mark(ctx, 0, 1);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(p.planes, ctx->stream);
+    delete a;
+    return cuda_error(e, "pack kernel");
+  }
+  int rc = encode_planes_map(p);
+  if (rc != RNJ_OK) {
+    cudaFreeAsync(p.planes, ctx->stream);
+    delete a;
+    return rc;
+  }
+  *out = a;
+  return RNJ_OK;
+}
+
+int count_kind_for(const Packed &p, int model) {
+  if (p.kind == KIND_DNA && model == RNJ_JC) return KIND_MISM2;
+  return p.kind;
+}
+
+EpiParams epi_for(rnj_ctx *ctx, const Packed &p, int model) {
+  EpiParams ep;
+  ep.n = p.n;
+  ep.L = p.L;
+  ep.model = model;
+  ep.type = p.type;
+  ep.compat_wrap = (p.type == RNJ_PROTEIN && (p.flags & RNJ_FASTDIST) &&
+                    (p.flags & RNJ_COMPAT_PROTEIN_WRAP)) ? 1 : 0;
+  ep.full = (p.kind == KIND_NAIVE && (p.flags & RNJ_FULL_ROWS)) ? 1 : 0;
+  ep.jc_b = (p.type == RNJ_PROTEIN) ? (20.0 - 1) / 20.0 : (4.0 - 1) / 4.0;
+  ep.max_bits = ctx->scratch.words;
+  ep.err = ctx->scratch.words + 1;
+  ep.tile_flags = ctx->scratch.words + 2;
+  return ep;
+}
+
+int check_device_error(rnj_ctx *ctx) {
+  RNJ_CUDA(cudaMemcpyAsync(ctx->h_max + 1, ctx->scratch.words + 1, sizeof(int),
+                           cudaMemcpyDeviceToHost, ctx->stream),
+           "error word copy");
+  RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "distance sync");
+  if (ctx->h_max[1] != 0)
+    return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out (pipeline stage lost)");
+  return RNJ_OK;
+}
+
+// The distance pipeline on the context's stream: counts + fused transform (or
+// split counts + transform for long alignments), then the saturation fix-up.
+int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t ld,
+                 int *d_max_copy) {
+  const int nt = tiles_of(p.n);
+  const long long ntiles = (p.kind == KIND_NAIVE && (p.flags & RNJ_FULL_ROWS))
+                               ? (long long)nt * nt
+                               : tri_tiles(nt);
+  int rc = ensure_scratch_words(ctx, (size_t)ntiles + 2);
+  if (rc != RNJ_OK) return rc;
+  RNJ_CUDA(cudaMemsetAsync(ctx->scratch.words, 0, ((size_t)ntiles + 2) * sizeof(int), ctx->stream),
+           "scratch clear");
+  EpiParams ep = epi_for(ctx, p, model);
+  ep.out = d_out;
+  ep.ld = ld;
+  if (p.n == 1) RNJ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float), ctx->stream), "diagonal");
+  const int ckind = count_kind_for(p, model);
+  const int nk = p.Wp / kKW;
+  mark(ctx, 1, 0);
+  if (nk <= kMaxFusedWords / kKW) {
+    RNJ_CUDA(launch_count_tiles(p, ckind, EPI_DIST, ep, ctx->stream), "count kernel");
+  } else {
+    const size_t cbytes = (size_t)p.n * p.n * 3 * sizeof(uint32_t);
+    uint32_t *counts = nullptr;
+    RNJ_CUDA(cudaMallocAsync((void **)&counts, cbytes, ctx->stream), "count buffer");
+    ep.counts = counts;
+    cudaError_t e = cudaMemsetAsync(counts, 0, cbytes, ctx->stream);
+    if (e == cudaSuccess) e = launch_count_tiles(p, ckind, EPI_ATOMIC, ep, ctx->stream);
+    if (e == cudaSuccess) e = launch_transform_counts(ep, nt, ctx->stream);
+    cudaFreeAsync(counts, ctx->stream);
+    if (e != cudaSuccess) return cuda_error(e, "split count pipeline");
+  }
+  mark(ctx, 1, 1);
+  mark(ctx, 2, 0);
+  RNJ_CUDA(launch_fixup(ep, nt, ctx->stream), "fix-up kernel");
+  mark(ctx, 2, 1);
+  if (d_max_copy)
+    RNJ_CUDA(cudaMemcpyAsync(d_max_copy, ctx->scratch.words, sizeof(int), cudaMemcpyDeviceToDevice,
+                             ctx->stream),
+             "max copy");
+  return RNJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *rnj_version(void) { return "rapidnj-b200 0.1.0 (sm_100a)"; }
+
+const char *rnj_last_error(void) { return g_error.c_str(); }
+
+int rnj_ctx_create(int device, rnj_ctx **out) {
+  if (!out) return set_error(RNJ_ERR_INVALID, "out is NULL");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= count) return set_error(RNJ_ERR_INVALID, "no such CUDA device");
+  DeviceGuard g(device);
+  rnj_ctx *c = new rnj_ctx();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  // A blocking stream: it orders with the legacy default stream, so buffers that
+  // callers fill on the default stream (as torch does) are complete before the
+  // library reads them, and the caller's later default-stream work sees our results.
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_mask, 8 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_mask, 8 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_max, 4 * sizeof(int));
+  if (e != cudaSuccess) {
+    rnj_ctx_destroy(c);
+    return cuda_error(e, "context setup");
+  }
+  if (!encode_fn()) {
+    rnj_ctx_destroy(c);
+    return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  }
+  *out = c;
+  return RNJ_OK;
+}
+
+int rnj_ctx_destroy(rnj_ctx *ctx) {
+  if (!ctx) return RNJ_OK;
+  DeviceGuard g(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->scratch.words) cudaFree(ctx->scratch.words);
+  if (ctx->d_mask) cudaFree(ctx->d_mask);
+  if (ctx->h_mask) cudaFreeHost(ctx->h_mask);
+  if (ctx->h_max) cudaFreeHost(ctx->h_max);
+  for (int b = 0; b < 2; ++b)
+    if (ctx->h_stage[b]) cudaFreeHost(ctx->h_stage[b]);
+  for (int k = 0; k < 6; ++k)
+    if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return RNJ_OK;
+}
+
+int rnj_ctx_stream(rnj_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return set_error(RNJ_ERR_INVALID, "null argument");
+  *stream = (void *)ctx->stream;
+  return RNJ_OK;
+}
+
+int rnj_ctx_set_profiling(rnj_ctx *ctx, int on) {
+  if (!ctx) return set_error(RNJ_ERR_INVALID, "null context");
+  DeviceGuard g(ctx->device);
+  if (on && !ctx->ev[0])
+    for (int k = 0; k < 6; ++k) RNJ_CUDA(cudaEventCreate(&ctx->ev[k]), "event");
+  ctx->profiling = on != 0;
+  for (int k = 0; k < 3; ++k) ctx->ev_used[k] = false;
+  return RNJ_OK;
+}
+
+int rnj_ctx_stage_times(rnj_ctx *ctx, float *ms) {
+  if (!ctx || !ms) return set_error(RNJ_ERR_INVALID, "null argument");
+  DeviceGuard g(ctx->device);
+  RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "stage sync");
+  for (int k = 0; k < 3; ++k) {
+    ms[k] = 0.0f;
+    if (ctx->profiling && ctx->ev_used[k])
+      RNJ_CUDA(cudaEventElapsedTime(&ms[k], ctx->ev[2 * k], ctx->ev[2 * k + 1]), "stage time");
+  }
+  return RNJ_OK;
+}
+
+int rnj_ctx_synchronize(rnj_ctx *ctx) {
+  if (!ctx) return set_error(RNJ_ERR_INVALID, "null context");
+  DeviceGuard g(ctx->device);
+  RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  return RNJ_OK;
+}
+
+int rnj_detect_type(const char *seq0, int L) {
+  for (int i = 0; i < L; ++i) {
+    const signed char c = (signed char)seq0[i];
+    if (!(c < 65 || c == 'A' || c == 'a' || c == 'C' || c == 'c' || c == 'G' || c == 'g' ||
+          c == 'T' || c == 't' || c == 'U' || c == 'u' || c == 'N' || c == 'n'))
+      return RNJ_PROTEIN;
+  }
+  return RNJ_DNA;
+}
+
+int rnj_aln_from_device(rnj_ctx *ctx, const void *d_chars, int n, int L, size_t ld, int type,
+                        int flags, rnj_aln **out) {
+  if (!ctx || !out || (n > 0 && L > 0 && !d_chars))
+    return set_error(RNJ_ERR_INVALID, "null argument");
+  DeviceGuard g(ctx->device);
+  if (type == RNJ_UNKNOWN) {
+    std::vector<char> row((size_t)std::max(L, 1));
+    if (n > 0 && L > 0) {
+      RNJ_CUDA(cudaMemcpyAsync(row.data(), d_chars, (size_t)L, cudaMemcpyDeviceToHost, ctx->stream),
+               "first row copy");
+      RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "first row sync");
+    }
+    type = rnj_detect_type(row.data(), n > 0 ? L : 0);
+  }
+  return pack_from_device_chars(ctx, (const uint8_t *)d_chars, n, L, ld, type, flags, out);
+}
+
+int rnj_aln_from_host_buffer(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int type,
+                             int flags, rnj_aln **out) {
+  if (!ctx || !out || (n > 0 && L > 0 && !chars))
+    return set_error(RNJ_ERR_INVALID, "null argument");
+  if (n < 0 || L < 0 || (n > 0 && ld < (size_t)L))
+    return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
+  DeviceGuard g(ctx->device);
+  if (type == RNJ_UNKNOWN) type = (n > 0) ? rnj_detect_type(chars, L) : RNJ_DNA;
+  uint8_t *d = nullptr;
+  const size_t bytes = std::max<size_t>((size_t)n * L, 1);
+  RNJ_CUDA(cudaMallocAsync((void **)&d, bytes, ctx->stream), "upload buffer");
+  cudaError_t e = cudaSuccess;
+  if (n > 0 && L > 0)
+    e = cudaMemcpy2DAsync(d, (size_t)L, chars, ld, (size_t)L, (size_t)n, cudaMemcpyHostToDevice,
+                          ctx->stream);
+  int rc = RNJ_OK;
+  if (e != cudaSuccess) rc = cuda_error(e, "alignment upload");
+  else rc = pack_from_device_chars(ctx, d, n, L, (size_t)std::max(L, 1), type, flags, out);
+  cudaFreeAsync(d, ctx->stream);
+  return rc;
+}
+
+int rnj_aln_from_host(rnj_ctx *ctx, const char *const *seqs, int n, int L, int type, int flags,
+                      rnj_aln **out) {
+  if (!ctx || !out || (n > 0 && !seqs)) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (n < 0 || L < 0) return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
+  DeviceGuard g(ctx->device);
+  const size_t bytes = std::max<size_t>((size_t)n * L, 1);
+  int rc = ensure_stage(ctx, bytes);
+  if (rc != RNJ_OK) return rc;
+  RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "staging reuse");
+  char *stage = (char *)ctx->h_stage[0];
+  for (int i = 0; i < n; ++i) memcpy(stage + (size_t)i * L, seqs[i], (size_t)L);
+  return rnj_aln_from_host_buffer(ctx, stage, n, L, (size_t)L, type, flags, out);
+}
+
+int rnj_aln_from_bitstrings(rnj_ctx *ctx, const unsigned int *const *bit_strings,
+                            const unsigned int *const *gap_filters, int n, int L,
+                            int bit_strings_count, int type, int flags, rnj_aln **out) {
+  if (!ctx || !out || (n > 0 && !bit_strings)) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (n < 0 || L < 0 || bit_strings_count < 0) return set_error(RNJ_ERR_INVALID, "invalid shape");
+  if (type != RNJ_DNA && type != RNJ_PROTEIN)
+    return set_error(RNJ_ERR_INVALID, "type must be RNJ_DNA or RNJ_PROTEIN");
+  DeviceGuard g(ctx->device);
+  const int bs_words = bit_strings_count * 4;  // 128-bit vectors -> uint32 words
+  if (type == RNJ_PROTEIN) {
+    // One resolved byte per site, bit_strings_count * 16 bytes per sequence.
+    const size_t row = (size_t)bit_strings_count * 16;
+    if (row < (size_t)L) return set_error(RNJ_ERR_INVALID, "bit strings shorter than L");
+    const size_t bytes = std::max<size_t>((size_t)n * row, 1);
+    int rc = ensure_stage(ctx, bytes);
+    if (rc != RNJ_OK) return rc;
+    RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "staging reuse");
+    char *stage = (char *)ctx->h_stage[0];
+    for (int i = 0; i < n; ++i) memcpy(stage + (size_t)i * row, bit_strings[i], row);
+    return rnj_aln_from_host_buffer(ctx, stage, n, L, row, RNJ_PROTEIN,
+                                    flags | RNJ_FASTDIST, out);
+  }
+  if (!gap_filters && n > 0) return set_error(RNJ_ERR_INVALID, "DNA needs gap filters");
+  if ((size_t)bs_words * 16 < (size_t)L) return set_error(RNJ_ERR_INVALID, "bit strings shorter than L");
+  const size_t words = (size_t)n * bs_words;
+  int rc = ensure_stage(ctx, std::max<size_t>(words * 4, 1));
+  if (rc != RNJ_OK) return rc;
+  RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "staging reuse");
+  uint32_t *sb = (uint32_t *)ctx->h_stage[0];
+  uint32_t *sg = (uint32_t *)ctx->h_stage[1];
+  for (int i = 0; i < n; ++i) {
+    memcpy(sb + (size_t)i * bs_words, bit_strings[i], (size_t)bs_words * 4);
+    memcpy(sg + (size_t)i * bs_words, gap_filters[i], (size_t)bs_words * 4);
+  }
+  rnj_aln *a = new rnj_aln();
+  a->ctx = ctx;
+  Packed &p = a->p;
+  p.n = n;
+  p.L = L;
+  p.type = RNJ_DNA;
+  p.flags = flags | RNJ_FASTDIST;
+  p.kind = KIND_DNA;
+  p.W = (L + 31) / 32;
+  p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
+  p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
+  p.NP = 3;
+  uint32_t *db = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&db, std::max<size_t>(words * 8, 8), ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMallocAsync((void **)&p.planes, (size_t)p.NP * p.Wp * p.Np * 4, ctx->stream);
+  if (e == cudaSuccess && words)
+    e = cudaMemcpyAsync(db, sb, words * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && words)
+    e = cudaMemcpyAsync(db + words, sg, words * 4, cudaMemcpyHostToDevice, ctx->stream);
+  mark(ctx, 0, 0);
+  if (e == cudaSuccess) e = launch_pack_bitstrings_dna(db, db + words, bs_words, p, ctx->stream);
+  mark(ctx, 0, 1);
+  if (db) cudaFreeAsync(db, ctx->stream);
+  if (e != cudaSuccess) {
+    if (p.planes) cudaFreeAsync(p.planes, ctx->stream);
+    delete a;
+    return cuda_error(e, "bit-string upload");
+  }
+  rc = encode_planes_map(p);
+  if (rc != RNJ_OK) {
+    cudaFreeAsync(p.planes, ctx->stream);
+    delete a;
+    return rc;
+  }
+  *out = a;
+  return RNJ_OK;
+}
+
+int rnj_aln_info(const rnj_aln *aln, int *n, int *L, int *type) {
+  if (!aln) return set_error(RNJ_ERR_INVALID, "null alignment");
+  if (n) *n = aln->p.n;
+  if (L) *L = aln->p.L;
+  if (type) *type = aln->p.type;
+  return RNJ_OK;
+}
+
+int rnj_aln_destroy(rnj_aln *aln) {
+  if (!aln) return RNJ_OK;
+  DeviceGuard g(aln->ctx->device);
+  if (aln->p.planes) cudaFreeAsync(aln->p.planes, aln->ctx->stream);
+  delete aln;
+  return RNJ_OK;
+}
+
+int rnj_distance_into(rnj_ctx *ctx, rnj_aln *aln, int model, float *d_out, size_t ld,
+                      float *max_out) {
+  if (!ctx || !aln || (!d_out && aln->p.n > 0)) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (model != RNJ_JC && model != RNJ_KIMURA) return set_error(RNJ_ERR_INVALID, "unknown model");
+  if (ld < (size_t)aln->p.n) return set_error(RNJ_ERR_INVALID, "ld < n");
+  DeviceGuard g(ctx->device);
+  if (aln->p.n == 0) {
+    if (max_out) *max_out = 0.0f;
+    return RNJ_OK;
+  }
+  int rc = run_distance(ctx, aln->p, model, d_out, ld, nullptr);
+  if (rc != RNJ_OK) return rc;
+  if (max_out) {
+    RNJ_CUDA(cudaMemcpyAsync(ctx->h_max, ctx->scratch.words, sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->stream),
+             "max copy");
+    rc = check_device_error(ctx);
+    if (rc != RNJ_OK) return rc;
+    float m;
+    memcpy(&m, ctx->h_max, sizeof(float));
+    *max_out = m;
+  }
+  return RNJ_OK;
+}
+
+int rnj_distance(rnj_ctx *ctx, rnj_aln *aln, int model, rnj_mat **out) {
+  if (!ctx || !aln || !out) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (model != RNJ_JC && model != RNJ_KIMURA) return set_error(RNJ_ERR_INVALID, "unknown model");
+  DeviceGuard g(ctx->device);
+  rnj_mat *m = new rnj_mat();
+  m->ctx = ctx;
+  m->n = aln->p.n;
+  m->ld = (size_t)std::max(4, (aln->p.n + 3) / 4 * 4);
+  cudaError_t e = cudaMallocAsync((void **)&m->d, std::max<size_t>(m->ld * m->n * 4, 4), ctx->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&m->d_max, sizeof(int), ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->d_max, 0, sizeof(int), ctx->stream);
+  if (e != cudaSuccess) {
+    rnj_mat_destroy(m);
+    return cuda_error(e, "matrix allocation");
+  }
+  if (m->n > 0) {
+    int rc = run_distance(ctx, aln->p, model, m->d, m->ld, m->d_max);
+    if (rc != RNJ_OK) {
+      rnj_mat_destroy(m);
+      return rc;
+    }
+  }
+  *out = m;
+  return RNJ_OK;
+}
+
+int rnj_counts_into(rnj_ctx *ctx, rnj_aln *aln, unsigned int *d_counts) {
+  if (!ctx || !aln || (!d_counts && aln->p.n > 0)) return set_error(RNJ_ERR_INVALID, "null argument");
+  DeviceGuard g(ctx->device);
+  const Packed &p = aln->p;
+  if (p.n == 0) return RNJ_OK;
+  const int nt = tiles_of(p.n);
+  const long long ntiles = (p.flags & RNJ_FULL_ROWS) ? (long long)nt * nt : tri_tiles(nt);
+  int rc = ensure_scratch_words(ctx, (size_t)ntiles + 2);
+  if (rc != RNJ_OK) return rc;
+  RNJ_CUDA(cudaMemsetAsync(ctx->scratch.words, 0, ((size_t)ntiles + 2) * sizeof(int), ctx->stream),
+           "scratch clear");
+  RNJ_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)p.n * p.n * 3 * sizeof(uint32_t), ctx->stream),
+           "count clear");
+  EpiParams ep = epi_for(ctx, p, RNJ_KIMURA);
+  ep.full = (p.flags & RNJ_FULL_ROWS) ? 1 : 0;
+  ep.counts = d_counts;
+  const int nk = p.Wp / kKW;
+  const int mode = (nk <= kMaxFusedWords / kKW) ? EPI_COUNTS : EPI_ATOMIC;
+  RNJ_CUDA(launch_count_tiles(p, p.kind, mode, ep, ctx->stream), "count kernel");
+  return check_device_error(ctx);
+}
+
+int rnj_mat_info(rnj_mat *mat, int *n, float *max_distance) {
+  if (!mat) return set_error(RNJ_ERR_INVALID, "null matrix");
+  if (n) *n = mat->n;
+  if (max_distance) {
+    DeviceGuard g(mat->ctx->device);
+    rnj_ctx *ctx = mat->ctx;
+    RNJ_CUDA(cudaMemcpyAsync(ctx->h_max, mat->d_max, sizeof(int), cudaMemcpyDeviceToHost,
+                             ctx->stream),
+             "max copy");
+    int rc = check_device_error(ctx);
+    if (rc != RNJ_OK) return rc;
+    memcpy(max_distance, ctx->h_max, sizeof(float));
+  }
+  return RNJ_OK;
+}
+
+int rnj_mat_device_ptr(rnj_mat *mat, float **d_ptr, size_t *ld) {
+  if (!mat) return set_error(RNJ_ERR_INVALID, "null matrix");
+  if (d_ptr) *d_ptr = mat->d;
+  if (ld) *ld = mat->ld;
+  return RNJ_OK;
+}
+
+int rnj_mat_copy_rows(rnj_ctx *ctx, rnj_mat *mat, int row0, int nrows, float **rows, int threads) {
+  if (!ctx || !mat || (nrows > 0 && !rows)) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (row0 < 0 || nrows < 0 || row0 + nrows > mat->n)
+    return set_error(RNJ_ERR_INVALID, "row range outside the matrix");
+  if (nrows == 0) return RNJ_OK;
+  DeviceGuard g(ctx->device);
+  const int n = mat->n;
+  const size_t row_bytes = (size_t)n * sizeof(float);
+  const size_t chunk_target = 32u << 20;  // 32 MB per staging buffer
+  int rows_per_chunk = (int)std::max<size_t>(1, chunk_target / row_bytes);
+  rows_per_chunk = std::min(rows_per_chunk, nrows);
+  int rc = ensure_stage(ctx, (size_t)rows_per_chunk * row_bytes);
+  if (rc != RNJ_OK) return rc;
+  const int T = host_threads(threads);
+  cudaEvent_t ev[2];
+  RNJ_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming), "event");
+  RNJ_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming), "event");
+  const int nchunks = (nrows + rows_per_chunk - 1) / rows_per_chunk;
+  cudaError_t e = cudaSuccess;
+  auto enqueue = [&](int c) {
+    const int r0 = row0 + c * rows_per_chunk;
+    const int rn = std::min(rows_per_chunk, row0 + nrows - r0);
+    const int b = c & 1;
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(ctx->h_stage[b], row_bytes, mat->d + (size_t)r0 * mat->ld,
+                            mat->ld * sizeof(float), row_bytes, (size_t)rn,
+                            cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[b], ctx->stream);
+  };
+  enqueue(0);
+  for (int c = 0; c < nchunks && e == cudaSuccess; ++c) {
+    if (c + 1 < nchunks) enqueue(c + 1);  // DMA of the next chunk overlaps this scatter
+    const int b = c & 1;
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[b]);
+    if (e != cudaSuccess) break;
+    const int r0 = c * rows_per_chunk;
+    const int rn = std::min(rows_per_chunk, nrows - r0);
+    scatter_rows((const float *)ctx->h_stage[b], rows + r0, rn, n, T);
+    // Buffer b is refilled by chunk c + 2, enqueued on the next iteration only
+    // after this scatter has finished.
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (e != cudaSuccess) return cuda_error(e, "row copy");
+  return RNJ_OK;
+}
+
+int rnj_mat_destroy(rnj_mat *mat) {
+  if (!mat) return RNJ_OK;
+  DeviceGuard g(mat->ctx->device);
+  if (mat->owns && mat->d) cudaFreeAsync(mat->d, mat->ctx->stream);
+  if (mat->d_max) cudaFreeAsync(mat->d_max, mat->ctx->stream);
+  delete mat;
+  return RNJ_OK;
+}
+
+int rnj_distance_matrix_host(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int type,
+                             int model, int flags, float *out, float *max_out) {
+  if (!ctx || (n > 0 && !out)) return set_error(RNJ_ERR_INVALID, "null argument");
+  rnj_aln *a = nullptr;
+  int rc = rnj_aln_from_host_buffer(ctx, chars, n, L, ld, type, flags, &a);
+  if (rc != RNJ_OK) return rc;
+  rnj_mat *m = nullptr;
+  rc = rnj_distance(ctx, a, model, &m);
+  rnj_aln_destroy(a);
+  if (rc != RNJ_OK) return rc;
+  std::vector<float *> rows((size_t)n);
+  for (int i = 0; i < n; ++i) rows[i] = out + (size_t)i * n;
+  rc = rnj_mat_copy_rows(ctx, m, 0, n, rows.data(), 0);
+  if (rc == RNJ_OK) rc = check_device_error(ctx);
+  if (rc == RNJ_OK && max_out) rc = rnj_mat_info(m, nullptr, max_out);
+  rnj_mat_destroy(m);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,150 @@
+// rnj_device.cuh -- device helpers shared by the sm_100a kernels: mbarrier and
+// TMA wrappers (inline PTX), bounded waits, and the exact distance transforms.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rnj {
+
+// ------------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// A wait on an mbarrier phase that gives up after kWaitLimitNs of wall time (or
+// an iteration cap), so that a lost transfer turns into an error status instead
+// of a hung GPU.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+constexpr uint32_t kWaitIterCap = 1u << 26;
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_timer_ns();
+  for (uint32_t it = 0; it < kWaitIterCap; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 255u && global_timer_ns() - t0 > kWaitLimitNs) break;
+  }
+  return false;
+}
+
+// 3-D tiled TMA load (no multicast): box lands in shared memory with dim0
+// fastest.  c0 (the sequence index, 4-byte elements) is always a multiple of
+// the 128-row tile, so c0 * 4 is a multiple of 16 bytes as TMA requires.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// ------------------------------------------------------------ exact transforms
+//
+// Each transform restates the reference's float/double arithmetic operation by
+// operation with explicitly rounded intrinsics, so that no multiply-add is
+// contracted (the reference is compiled for SSE2 without FMA).  The logarithm
+// is CUDA's double log().
+
+// Valid-site count as the fast protein estimator reports it for L % 128 == 0
+// (bitDistanceProtein.cpp:15-16,59): padded length minus the gaps counted over
+// one extra 128-byte block, stored in an unsigned long long.
+__device__ __forceinline__ unsigned long long protein_fast_valid(unsigned long long valid, int L) {
+  const long long padded = ((long long)L + 127) & ~127LL;
+  const long long span = 128LL * (((long long)L / 16 + 8) / 8);
+  const long long gaps_total = ((long long)L - (long long)valid) + (span - (long long)L);
+  return (unsigned long long)(padded - gaps_total);
+}
+
+// JCdistance.cpp:171-183.  b = (alpha - 1) / alpha in double, alpha 4 or 20.
+__device__ __forceinline__ float jc_distance(unsigned long long total,
+                                             unsigned long long valid, double b) {
+  float distance;
+  if (valid == 0) distance = 0.0f;
+  else distance = __fdiv_rn(__ll2float_rn((long long)total), __ull2float_rn(valid));
+  const double q = __ddiv_rn((double)distance, b);
+  if (q >= 1.0) return -1.0f;
+  return __double2float_rn(__dmul_rn(-b, log(__dsub_rn(1.0, q))));
+}
+
+// KimuraDistance.cpp:339-349.
+__device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
+                                              unsigned long long tv_count,
+                                              unsigned long long valid) {
+  if (valid == 0) return -1.0f;
+  const double dn = (double)valid;
+  const float ts = __double2float_rn(__ddiv_rn((double)ts_count, dn));
+  const float tv = __double2float_rn(__ddiv_rn((double)tv_count, dn));
+  const double a = __dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, (double)ts)), (double)tv);
+  const double b = __dsub_rn(1.0, __dmul_rn(2.0, (double)tv));
+  const float temp1 = __double2float_rn(a);
+  const float temp2 = __double2float_rn(b);
+  if (temp1 <= 0.0f || temp2 <= 0.0f) return -1.0f;
+  return __double2float_rn(__dsub_rn(__dmul_rn(-0.5, log(a)), __dmul_rn(0.25, log(b))));
+}
+
+// KimuraDistance.cpp:322-338 with the Dayhoff table of KimuraDistance.cpp:30-49.
+__device__ __forceinline__ float kimura_protein_distance(unsigned long long mism,
+                                                         unsigned long long valid,
+                                                         const int *pam) {
+  float distance = -1.0f;
+  if (valid != 0) distance = __fdiv_rn(__ll2float_rn((long long)mism), __ull2float_rn(valid));
+  const double dd = (double)distance;
+  if (dd < 0.75) {
+    if (dd > 0.0) {
+      const double sq = (double)__fmul_rn(distance, distance);
+      const double arg = __dsub_rn(__dsub_rn(1.0, dd), __dmul_rn(sq, 0.20));
+      distance = __double2float_rn(-log(arg));
+    }
+  } else {
+    if (dd > 0.930) {
+      distance = 10.0f;
+    } else {
+      const int idx = (int)__dsub_rn(__dmul_rn(dd, 1000.0), 750.0);
+      distance = __double2float_rn(__ddiv_rn((double)pam[idx], 100.0));
+    }
+  }
+  return distance;
+}
+
+}  // namespace rnj

@@ -1,0 +1,98 @@
+// rnj_internal.h -- host-side internals of librnjgpu.so shared by the C-ABI
+// implementation and the kernel launchers.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "rnj.h"
+
+namespace rnj {
+
+// Counting kernels, by bit-plane layout of the packed alignment.
+//   KIND_DNA    planes {hi, lo, valid}         -> {ts, tv, valid}
+//   KIND_NAIVE  planes {hi, lo, valid, upper}  -> {ts, tv, valid} (naive -f rules)
+//   KIND_MISM2  planes {c0, c1, valid}         -> {mismatch, valid}
+//   KIND_MISM5  planes {c0..c4, valid}         -> {mismatch, valid}
+//   KIND_MISM7  planes {c0..c6, valid}         -> {mismatch, valid}
+enum Kind { KIND_DNA = 0, KIND_NAIVE = 1, KIND_MISM2 = 2, KIND_MISM5 = 3, KIND_MISM7 = 4 };
+
+constexpr int kTile = 128;        // pairs per tile edge (rows and columns)
+constexpr int kWordBits = 32;     // sites per plane word
+constexpr int kKW = 8;            // words per pipeline stage
+constexpr int kMaxFusedWords = 2047;  // 16-bit packed accumulators: L <= 65504 per pass
+
+__host__ __device__ inline int planes_of(int kind) {
+  switch (kind) {
+    case KIND_DNA: return 3;
+    case KIND_NAIVE: return 4;
+    case KIND_MISM2: return 3;
+    case KIND_MISM5: return 6;
+    default: return 8;
+  }
+}
+
+// Packed alignment on the device.
+struct Packed {
+  int n = 0, L = 0;
+  int type = RNJ_DNA;
+  int flags = 0;
+  int kind = KIND_DNA;   // plane layout (for DNA JC the DNA layout is counted as MISM2)
+  int W = 0;             // words per sequence holding sites (ceil(L/32))
+  int Wp = 0;            // padded to a multiple of kKW
+  int Np = 0;            // sequences padded to a multiple of kTile
+  int NP = 0;            // planes
+  uint32_t *planes = nullptr;  // NP * Wp * Np words, word-major, sequence fastest
+  CUtensorMap tmap;      // 3-D map over (Np, Wp, NP), box (kTile, kKW, NP)
+};
+
+struct EpiParams {
+  int n = 0;
+  int L = 0;
+  int model = RNJ_KIMURA;
+  int type = RNJ_DNA;
+  int compat_wrap = 0;
+  int full = 0;
+  double jc_b = 0.75;
+  float *out = nullptr;
+  size_t ld = 0;
+  int *max_bits = nullptr;    // float bits, atomicMax target (init 0 = +0.0f)
+  int *tile_flags = nullptr;  // per tile: 1 if it holds a saturated (-1) entry
+  uint32_t *counts = nullptr; // n*n*3 counts (count-output and split modes)
+  int *err = nullptr;         // device error word (bit 0: a bounded wait ran out)
+};
+
+// Scratch of one distance call: the max slot, the error word and the per-tile
+// saturation flags (device), plus the split-K count buffer for long alignments.
+struct Scratch {
+  int *words = nullptr;       // [0] max bits, [1] error, [2..] tile flags
+  size_t words_cap = 0;
+  uint32_t *counts = nullptr; // split-K counts
+  size_t counts_cap = 0;
+};
+
+// Launchers (rnj_kernels.cu).
+cudaError_t launch_pack_chars(const uint8_t *d_chars, size_t ld, const Packed &p,
+                              const uint8_t lut[256], cudaStream_t s);
+cudaError_t launch_presence(const uint8_t *d_chars, size_t ld, int n, int L,
+                            uint32_t *d_mask /*8 words*/, cudaStream_t s);
+cudaError_t launch_pack_bitstrings_dna(const uint32_t *d_bits, const uint32_t *d_gaps,
+                                       int bs_words, const Packed &p, cudaStream_t s);
+cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode,
+                               const EpiParams &ep, cudaStream_t s);
+cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s);
+cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s);
+
+enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2 };
+
+inline int tiles_of(int n) { return (n + kTile - 1) / kTile; }
+inline long long tri_tiles(int nt) { return (long long)nt * (nt + 1) / 2; }
+
+// Error plumbing (rnj_api.cu).
+int set_error(int code, const std::string &msg);
+int cuda_error(cudaError_t e, const char *what);
+
+}  // namespace rnj

@@ -1,0 +1,242 @@
+// rnj_io.cpp -- host-side alignment reader and "-o m" matrix writer.
+//
+// The reader keeps the reference loaders' character rules so that the same file
+// gives the same n x L byte matrix:
+//   FASTA (dataloaderFasta.hpp:78-133,201-276): ';' lines are comments, '>'
+//   starts a name (bytes > 31), every other line contributes its bytes > 32;
+//   end of file reads as a newline.
+//   Stockholm (dataloaderStockholm.hpp:79-120,185-307): bytes < 32 between lines
+//   are skipped, '#' lines are markup, "//" ends the alignment (required), a
+//   sequence line is a name (bytes > 32) followed by its residues (bytes > 32).
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "rnj.h"
+#include "rnj_internal.h"
+
+struct rnj_msa {
+  std::vector<std::string> names;
+  std::vector<char> chars;  // n * L
+  int n = 0;
+  int L = 0;
+  int type = RNJ_DNA;
+};
+
+namespace {
+
+using rnj::set_error;
+
+bool read_file(const char *path, std::vector<char> &data) {
+  FILE *f = fopen(path, "rb");
+  if (!f) return false;
+  char buf[1 << 16];
+  size_t k;
+  while ((k = fread(buf, 1, sizeof(buf), f)) > 0) data.insert(data.end(), buf, buf + k);
+  fclose(f);
+  return true;
+}
+
+bool ends_with(const std::string &s, const char *suffix) {
+  const size_t k = strlen(suffix);
+  return s.size() >= k && s.compare(s.size() - k, k, suffix) == 0;
+}
+
+struct Builder {
+  rnj_msa *m;
+  bool first = true;
+  int store(std::vector<char> &buf) {
+    if (buf.empty()) return RNJ_OK;
+    if (first) {
+      m->L = (int)buf.size();
+      m->type = rnj_detect_type(buf.data(), m->L);
+      first = false;
+    } else if ((int)buf.size() != m->L) {
+      return set_error(RNJ_ERR_FORMAT, "ERROR: Sequence " + std::to_string(m->n) + " has length " +
+                                           std::to_string(buf.size()) +
+                                           " while the preceding sequences in the alignment which "
+                                           "have length " + std::to_string(m->L) + ".");
+    }
+    m->chars.insert(m->chars.end(), buf.begin(), buf.end());
+    m->n++;
+    buf.clear();
+    return RNJ_OK;
+  }
+};
+
+int parse_fasta(const std::vector<char> &data, rnj_msa *m) {
+  size_t pos = 0;
+  bool eof = false;
+  auto next = [&]() -> char {
+    if (pos < data.size()) return data[pos++];
+    eof = true;
+    return 10;
+  };
+  Builder b{m};
+  std::vector<char> buf;
+  while (!eof) {
+    char c = next();
+    if (eof) break;
+    if (c == ';') {
+      while (c != 10) c = next();
+    } else if (c == '>') {
+      int rc = b.store(buf);
+      if (rc != RNJ_OK) return rc;
+      c = next();
+      std::string name;
+      while (c > 31) {
+        name.push_back(c);
+        c = next();
+      }
+      m->names.push_back(name);
+    } else {
+      while (c != 10) {
+        if (c > 32) buf.push_back(c);
+        c = next();
+      }
+    }
+  }
+  return b.store(buf);
+}
+
+int parse_stockholm(const std::vector<char> &data, rnj_msa *m) {
+  size_t pos = 0;
+  bool eof = false;
+  auto next = [&]() -> char {
+    if (pos < data.size()) return data[pos++];
+    eof = true;
+    return 0;
+  };
+  const char *truncated = "Stream ended unexpectedly. Did not find '//' marking the end of the alignment";
+  Builder b{m};
+  std::vector<char> buf;
+  char c = next();
+  while (true) {
+    while (c < 32 && !eof) c = next();
+    if (eof) return set_error(RNJ_ERR_FORMAT, truncated);
+    std::string prefix;
+    if (c == '#') {
+      while (c != 10 && !eof) c = next();
+    } else {
+      if (c == '/') {
+        c = next();
+        if (c == '/') return RNJ_OK;
+        prefix = "/";
+      }
+      std::string name = prefix;
+      while (c > 32) {
+        name.push_back(c);
+        c = next();
+      }
+      m->names.push_back(name);
+      while (c < 32 && !eof) {
+        c = next();
+        if (c == 10) return set_error(RNJ_ERR_FORMAT, "ERROR: alignment with name \"" + name + "\" has zero length");
+      }
+      while (c != 10 && !eof) {
+        if (c > 32) buf.push_back(c);
+        c = next();
+      }
+      int rc = b.store(buf);
+      if (rc != RNJ_OK) return rc;
+    }
+    if (eof) return set_error(RNJ_ERR_FORMAT, truncated);
+    c = next();
+  }
+}
+
+// Six fixed decimals, as iostream's setprecision(6) << fixed prints a float
+// (main.cpp:218): the float is widened to double and rounded to nearest.
+inline int format_fixed6(char *out, float v) { return snprintf(out, 64, "%.6f ", (double)v); }
+
+}  // namespace
+
+extern "C" {
+
+int rnj_msa_read(const char *path, const char *format, rnj_msa **out) {
+  if (!path || !out) return set_error(RNJ_ERR_INVALID, "null argument");
+  std::string fmt = format ? format : "";
+  std::string p(path);
+  if (fmt.empty()) {
+    if (ends_with(p, ".sth") || ends_with(p, ".STH")) fmt = "sth";
+    else if (ends_with(p, ".fa") || ends_with(p, ".faa") || ends_with(p, ".fasta") ||
+             ends_with(p, ".FA") || ends_with(p, ".FAA") || ends_with(p, ".FASTA"))
+      fmt = "fa";
+    else
+      return set_error(RNJ_ERR_FORMAT, "ERROR: could not determine input file format. Please use "
+                                        "the '-i' option to indicate the format.");
+  }
+  if (fmt != "fa" && fmt != "sth") return set_error(RNJ_ERR_UNSUPPORTED, "Unkown input format " + fmt);
+  std::vector<char> data;
+  if (!read_file(path, data)) return set_error(RNJ_ERR_IO, std::string("ERROR: Could not read file: ") + path);
+  rnj_msa *m = new rnj_msa();
+  int rc = (fmt == "fa") ? parse_fasta(data, m) : parse_stockholm(data, m);
+  if (rc != RNJ_OK) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return RNJ_OK;
+}
+
+int rnj_msa_info(const rnj_msa *msa, int *n, int *L, int *detected_type) {
+  if (!msa) return set_error(RNJ_ERR_INVALID, "null alignment");
+  if (n) *n = msa->n;
+  if (L) *L = msa->L;
+  if (detected_type) *detected_type = msa->type;
+  return RNJ_OK;
+}
+
+const char *rnj_msa_name(const rnj_msa *msa, int i) {
+  if (!msa || i < 0 || i >= (int)msa->names.size()) return nullptr;
+  return msa->names[i].c_str();
+}
+
+const char *rnj_msa_chars(const rnj_msa *msa) { return msa && !msa->chars.empty() ? msa->chars.data() : ""; }
+
+int rnj_msa_destroy(rnj_msa *msa) {
+  delete msa;
+  return RNJ_OK;
+}
+
+int rnj_write_matrix_text(const char *path, const char *const *names, const float *const *rows,
+                          int n, int threads) {
+  if (n < 0 || (n > 0 && (!names || !rows))) return set_error(RNJ_ERR_INVALID, "null argument");
+  FILE *f = path ? fopen(path, "wb") : stdout;
+  if (!f) return set_error(RNJ_ERR_IO, std::string("Could not open the output file \"") + path + "\"");
+  fprintf(f, "\t%d\n", n);
+  // Rows are formatted in parallel blocks and written in order.
+  int T = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  T = std::max(1, std::min(T, 64));
+  const int block = 64;
+  std::vector<std::string> text(block);
+  for (int r0 = 0; r0 < n; r0 += block) {
+    const int rn = std::min(block, n - r0);
+    auto work = [&](int k) {
+      for (int r = k; r < rn; r += T) {
+        std::string &s = text[r];
+        s.clear();
+        s.append(names[r0 + r] ? names[r0 + r] : "");
+        s.push_back('\t');
+        char tmp[64];
+        for (int j = 0; j < n; ++j) s.append(tmp, format_fixed6(tmp, rows[r0 + r][j]));
+        s.push_back('\n');
+      }
+    };
+    std::vector<std::thread> pool;
+    const int t = std::min(T, rn);
+    for (int k = 1; k < t; ++k) pool.emplace_back(work, k);
+    work(0);
+    for (auto &th : pool) th.join();
+    for (int r = 0; r < rn; ++r) fwrite(text[r].data(), 1, text[r].size(), f);
+  }
+  if (path) fclose(f);
+  else fflush(f);
+  return RNJ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,631 @@
+// rnj_kernels.cu -- sm_100a kernels of the distance path.
+//
+//   pack_chars_kernel       alignment bytes -> bit planes (word-major, sequence fastest)
+//   pack_bitstrings_kernel  the reference loader's 2-bit DNA strings -> bit planes
+//   count_tiles_kernel      one 128 x 128 tile of sequence pairs per CTA: TMA-staged
+//                           plane tiles, LOP3 + POPC counting in registers, fused
+//                           exact transform + mirrored store + max + saturation flag
+//   transform_counts_kernel the same epilogue from a count buffer (long alignments)
+//   fixup_kernel            -1 -> 2 * max on the tiles that hold a saturated pair
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rnj_device.cuh"
+#include "rnj_internal.h"
+
+namespace rnj {
+
+// Dayhoff PAM distances (x100) for p = 0.750 .. 0.930, the table that defines the
+// protein Kimura distance above p = 0.75 (rapidNJ KimuraDistance.cpp:30-49).
+__constant__ int c_pam[181] = {
+    195, 196, 197, 198, 199, 200, 200, 201, 202, 203, 204, 205, 206, 207, 208,
+    209, 209, 210, 211, 212, 213, 214, 215, 216, 217, 218, 219, 220, 221, 222,
+    223, 224, 226, 227, 228, 229, 230, 231, 232, 233, 234, 236, 237, 238, 239,
+    240, 241, 243, 244, 245, 246, 248, 249, 250, 252, 253, 254, 255, 257, 258,
+    260, 261, 262, 264, 265, 267, 268, 270, 271, 273, 274, 276, 277, 279, 281,
+    282, 284, 285, 287, 289, 291, 292, 294, 296, 298, 299, 301, 303, 305, 307,
+    309, 311, 313, 315, 317, 319, 321, 323, 325, 328, 330, 332, 335, 337, 339,
+    342, 344, 347, 349, 352, 354, 357, 360, 362, 365, 368, 371, 374, 377, 380,
+    383, 386, 389, 393, 396, 399, 403, 407, 410, 414, 418, 422, 426, 430, 434,
+    438, 442, 447, 451, 456, 461, 466, 471, 476, 482, 487, 493, 498, 504, 511,
+    517, 524, 531, 538, 545, 553, 560, 569, 577, 586, 595, 605, 615, 626, 637,
+    649, 661, 675, 688, 703, 719, 736, 754, 775, 796, 819, 845, 874, 907, 945,
+    988};
+
+// ------------------------------------------------------------------- packing
+
+struct Lut256 {
+  uint8_t v[256];
+};
+
+// One thread per (sequence i, plane word w); i fastest so that the plane
+// stores of a warp are 32 consecutive words.  Covers the padded Np x Wp area, so
+// padding rows and words come out zero (invalid).
+//   DNA kinds: lut bit0 = code high bit, bit1 = code low bit, bit2 = valid,
+//              bit3 = upper-case A/C/G/T (naive rule).
+//   MISM kinds: lut = symbol rank, 0xFF = gap.
+__global__ void pack_chars_kernel(const uint8_t *__restrict__ chars, size_t ld, int n, int L,
+                                  int Np, int Wp, int kind, Lut256 lut,
+                                  uint32_t *__restrict__ planes) {
+  __shared__ uint8_t s_lut[256];
+  for (int k = threadIdx.x; k < 256; k += blockDim.x) s_lut[k] = lut.v[k];
+  __syncthreads();
+  const long long total = (long long)Np * Wp;
+  const size_t plane_stride = (size_t)Np * Wp;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % Np);
+    const int w = (int)(t / Np);
+    uint32_t p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int s0 = w * 32;
+    if (i < n && s0 < L) {
+      const int cnt = min(32, L - s0);
+      const uint8_t *src = chars + (size_t)i * ld + s0;
+      uint8_t buf[32];
+      if (cnt == 32 && (((uintptr_t)src) & 15) == 0) {
+        *reinterpret_cast<uint4 *>(buf) = reinterpret_cast<const uint4 *>(src)[0];
+        *reinterpret_cast<uint4 *>(buf + 16) = reinterpret_cast<const uint4 *>(src)[1];
+      } else {
+#pragma unroll 4
+        for (int b = 0; b < 32; ++b) buf[b] = (b < cnt) ? src[b] : (uint8_t)'-';
+      }
+      if (kind == KIND_DNA || kind == KIND_NAIVE) {
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+          const uint32_t x = (b < cnt) ? s_lut[buf[b]] : 0u;
+          p[0] |= (x & 1u) << b;
+          p[1] |= ((x >> 1) & 1u) << b;
+          p[2] |= ((x >> 2) & 1u) << b;
+          p[3] |= ((x >> 3) & 1u) << b;
+        }
+      } else {
+        const int ncode = (kind == KIND_MISM2) ? 2 : (kind == KIND_MISM5 ? 5 : 7);
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+          const uint32_t r = (b < cnt) ? s_lut[buf[b]] : 0xFFu;
+          if (r != 0xFFu) {
+            p[ncode] |= 1u << b;
+#pragma unroll
+            for (int q = 0; q < 7; ++q)
+              if (q < ncode) p[q] |= ((r >> q) & 1u) << b;
+          }
+        }
+      }
+    }
+    const int np = planes_of(kind);
+    uint32_t *dst = planes + (size_t)w * Np + i;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (q < np) dst[q * plane_stride] = p[q];
+  }
+}
+
+// Byte-presence mask of an alignment (bit c of the 256-bit mask set when byte
+// c occurs), used to rank the residue alphabet on the host.
+__global__ void presence_kernel(const uint8_t *__restrict__ chars, size_t ld, int n, int L,
+                                uint32_t *__restrict__ mask) {
+  __shared__ uint32_t s_mask[8];
+  if (threadIdx.x < 8) s_mask[threadIdx.x] = 0;
+  __syncthreads();
+  const long long total = (long long)n * L;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / L), k = (int)(t % L);
+    const uint8_t c = chars[(size_t)i * ld + k];
+    atomicOr(&s_mask[c >> 5], 1u << (c & 31));
+  }
+  __syncthreads();
+  if (threadIdx.x < 8 && s_mask[threadIdx.x]) atomicOr(&mask[threadIdx.x], s_mask[threadIdx.x]);
+}
+
+__device__ __forceinline__ uint32_t compress_even_bits(uint32_t x) {
+  x &= 0x55555555u;
+  x = (x | (x >> 1)) & 0x33333333u;
+  x = (x | (x >> 2)) & 0x0f0f0f0fu;
+  x = (x | (x >> 4)) & 0x00ff00ffu;
+  x = (x | (x >> 8)) & 0x0000ffffu;
+  return x;
+}
+
+// The reference loader's DNA layout (dataloaderFasta.hpp:147-182): 16 sites per
+// uint32, site k in bits 2k..2k+1 holding A=00 G=01 T=10 C=11, and a gap filter
+// with 01 in every valid slot.  Two source words make one 32-site plane word.
+__global__ void pack_bitstrings_kernel(const uint32_t *__restrict__ bits,
+                                       const uint32_t *__restrict__ gaps, int bs_words, int n,
+                                       int L, int Np, int Wp, uint32_t *__restrict__ planes) {
+  const long long total = (long long)Np * Wp;
+  const size_t plane_stride = (size_t)Np * Wp;
+  const int W = (L + 31) / 32;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % Np);
+    const int w = (int)(t / Np);
+    uint32_t hi = 0, lo = 0, v = 0;
+    if (i < n && w < W) {
+      const uint32_t *b = bits + (size_t)i * bs_words;
+      const uint32_t *g = gaps + (size_t)i * bs_words;
+      const int k0 = 2 * w, k1 = 2 * w + 1;
+      const uint32_t b0 = k0 < bs_words ? b[k0] : 0u, b1 = k1 < bs_words ? b[k1] : 0u;
+      const uint32_t g0 = k0 < bs_words ? g[k0] : 0u, g1 = k1 < bs_words ? g[k1] : 0u;
+      lo = compress_even_bits(b0) | (compress_even_bits(b1) << 16);
+      hi = compress_even_bits(b0 >> 1) | (compress_even_bits(b1 >> 1) << 16);
+      v = compress_even_bits(g0) | (compress_even_bits(g1) << 16);
+      const int rem = L - 32 * w;  // sites beyond L are padding: mask them out
+      if (rem < 32) {
+        const uint32_t m = (1u << rem) - 1u;
+        hi &= m; lo &= m; v &= m;
+      }
+    }
+    uint32_t *dst = planes + (size_t)w * Np + i;
+    dst[0] = hi;
+    dst[plane_stride] = lo;
+    dst[2 * plane_stride] = v;
+  }
+}
+
+// ------------------------------------------------------------- tile counting
+
+template <int KIND>
+struct KT;
+template <>
+struct KT<KIND_DNA> { static constexpr int NP = 3, NC = 3, ST = 4; };
+template <>
+struct KT<KIND_NAIVE> { static constexpr int NP = 4, NC = 3, ST = 4; };
+template <>
+struct KT<KIND_MISM2> { static constexpr int NP = 3, NC = 2, ST = 4; };
+template <>
+struct KT<KIND_MISM5> { static constexpr int NP = 6, NC = 2, ST = 3; };
+template <>
+struct KT<KIND_MISM7> { static constexpr int NP = 8, NC = 2, ST = 3; };
+
+template <int KIND>
+constexpr size_t count_smem_bytes() {
+  return (size_t)KT<KIND>::ST * 2 * KT<KIND>::NP * kKW * kTile * 4 + 1024 + 64;
+}
+
+// Upper-triangle tile t -> (ti, tj), ti <= tj, row-major over the triangle.
+__device__ __forceinline__ void tri_coords(int t, int nt, int &ti, int &tj) {
+  const double b = 2.0 * nt + 1.0;
+  int r = (int)floor((b - sqrt(b * b - 8.0 * (double)t)) * 0.5);
+  auto start = [nt](int x) { return (long long)x * nt - (long long)x * (x - 1) / 2; };
+  if (r < 0) r = 0;
+  if (r > nt - 1) r = nt - 1;
+  while (r > 0 && start(r) > t) --r;
+  while (r + 1 < nt && start(r + 1) <= t) ++r;
+  ti = r;
+  tj = r + (int)(t - start(r));
+}
+
+// Per-thread pair layout inside a 128 x 128 tile (256 threads = 4 x 2 warps, each
+// warp 32 rows x 64 columns, each lane 8 x 8 pairs): rows rbase + {0..3, 16..19},
+// columns cbase + {0..3, 32..35}.  The two 4-wide groups keep every 128-bit
+// shared load of a quarter warp on distinct banks.
+__device__ __forceinline__ int row_of(int rbase, int r) { return rbase + (r < 4 ? r : 12 + r); }
+__device__ __forceinline__ int col_of(int cbase, int c) { return cbase + (c < 4 ? c : 28 + c); }
+
+__device__ __forceinline__ float pair_distance(const EpiParams &ep, uint32_t c0, uint32_t c1,
+                                               uint32_t valid) {
+  unsigned long long v = valid;
+  if (ep.compat_wrap) v = protein_fast_valid(v, ep.L);
+  if (ep.model == RNJ_JC) return jc_distance((unsigned long long)c0 + c1, v, ep.jc_b);
+  if (ep.type == RNJ_PROTEIN) return kimura_protein_distance(c0, v, c_pam);
+  return k2p_distance(c0, c1, v);
+}
+
+// Row stride (floats) of the distance tile staged in shared memory: 129 keeps
+// both row-wise and column-wise reads on distinct banks.
+constexpr int kStageLd = kTile + 1;
+constexpr size_t kStageBytes = (size_t)kTile * kStageLd * 4;
+
+// Epilogue, part 1: this thread's distances into the shared tile S (row =
+// local i, column = local j), with the running max and saturation flag.  Counts
+// come from get(r, c, c0, c1, valid).
+template <class Get>
+__device__ __forceinline__ void stage_distances(const EpiParams &ep, int ti, int tj, int rbase,
+                                                int cbase, float *S, Get get, float &tmax,
+                                                bool &sat) {
+  const int i0 = ti * kTile, j0 = tj * kTile;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int rl = row_of(rbase, r);
+    const int i = i0 + rl;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int cl = col_of(cbase, c);
+      const int j = j0 + cl;
+      const bool ok = ep.full ? (i < ep.n && j < ep.n && i != j) : (i < j && j < ep.n);
+      float x = 0.0f;
+      if (ok) {
+        uint32_t c0, c1, cv;
+        get(r, c, c0, c1, cv);
+        x = pair_distance(ep, c0, c1, cv);
+        if (x > tmax) tmax = x;
+        if (x == -1.0f) sat = true;
+      }
+      S[rl * kStageLd + cl] = x;
+    }
+  }
+}
+
+// Epilogue, part 2 (after a block barrier): coalesced stores of the tile and of
+// its mirror image, zero diagonal, block max and saturation flag.
+__device__ __forceinline__ void store_distances(const EpiParams &ep, int ti, int tj, int tile_id,
+                                                const float *S, float tmax, bool sat) {
+  const int i0 = ti * kTile, j0 = tj * kTile, n = ep.n;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  // Tile region: row i0 + r, columns j0 + lane + 32 q.
+  for (int r = warp; r < kTile; r += nwarps) {
+    const int i = i0 + r;
+    if (i >= n) break;
+    float *row = ep.out + (size_t)i * ep.ld + j0;
+#pragma unroll
+    for (int q = 0; q < kTile / 32; ++q) {
+      const int cl = lane + 32 * q;
+      const int j = j0 + cl;
+      if (j >= n) continue;
+      if (ep.full) row[cl] = (i == j) ? 0.0f : S[r * kStageLd + cl];
+      else if (i < j) row[cl] = S[r * kStageLd + cl];
+      else if (i == j) row[cl] = 0.0f;
+    }
+  }
+  if (!ep.full) {
+    // Mirror region: row j0 + c holds column c of S.
+    for (int c = warp; c < kTile; c += nwarps) {
+      const int j = j0 + c;
+      if (j >= n) break;
+      float *row = ep.out + (size_t)j * ep.ld + i0;
+#pragma unroll
+      for (int q = 0; q < kTile / 32; ++q) {
+        const int rl = lane + 32 * q;
+        const int i = i0 + rl;
+        if (i < j) row[rl] = S[rl * kStageLd + c];
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, off));
+  const bool any_sat = __any_sync(0xffffffffu, sat);
+  if (lane == 0) {
+    if (tmax > 0.0f) atomicMax(ep.max_bits, __float_as_int(tmax));
+    if (any_sat) ep.tile_flags[tile_id] = 1;
+  }
+}
+
+template <int KIND>
+__device__ __forceinline__ void pair_op(const uint32_t (&a)[KT<KIND>::NP],
+                                        const uint32_t (&b)[KT<KIND>::NP], uint32_t &acc0,
+                                        uint32_t &acc1) {
+  if constexpr (KIND == KIND_DNA) {
+    // bitDistanceGap.cpp:146-161: tv = high bit of the code XOR, ts = low bit and
+    // not tv, both masked by the shared valid sites.
+    const uint32_t v = a[2] & b[2];
+    const uint32_t tv = (a[0] ^ b[0]) & v;
+    const uint32_t ts = (a[1] ^ b[1]) & (v & ~tv);
+    acc0 += __popc(ts) + (__popc(tv) << 16);
+    acc1 += __popc(v);
+  } else if constexpr (KIND == KIND_NAIVE) {
+    // simpleDistanceCalculator.cpp:58-98 over planes: only an upper-case A/C/G/T
+    // in the row sequence classifies a difference.
+    const uint32_t v = a[2] & b[2];
+    const uint32_t xh = a[0] ^ b[0], xl = a[1] ^ b[1];
+    const uint32_t ts = a[3] & b[3] & ~xh & xl;
+    const uint32_t tv = a[3] & b[2] & (~b[3] | xh);
+    acc0 += __popc(ts) + (__popc(tv) << 16);
+    acc1 += __popc(v);
+  } else {
+    // bitDistanceProtein.cpp:77-81: a site differs when any code bit differs;
+    // sites with a gap in either sequence are excluded.
+    constexpr int P = KT<KIND>::NP - 1;
+    uint32_t x = a[0] ^ b[0];
+#pragma unroll
+    for (int q = 1; q < P; ++q) x |= a[q] ^ b[q];
+    const uint32_t v = a[P] & b[P];
+    acc0 += __popc(x & v) + (__popc(v) << 16);
+  }
+}
+
+template <int KIND, int EPI>
+__global__ void __launch_bounds__(256, 1)
+    count_tiles_kernel(const __grid_constant__ CUtensorMap tmap, int nt, int nk, int kchunk,
+                       EpiParams ep) {
+  using T = KT<KIND>;
+  constexpr int NP = T::NP, NC = T::NC, ST = T::ST;
+  constexpr int TILE_WORDS = NP * kKW * kTile;
+  constexpr uint32_t STAGE_BYTES = 2u * TILE_WORDS * 4u;
+  static_assert((size_t)ST * STAGE_BYTES >= kStageBytes, "distance tile must fit the stage buffers");
+
+  extern __shared__ uint8_t smem_raw[];
+  uint32_t *smem =
+      reinterpret_cast<uint32_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + ST * 2 * TILE_WORDS);
+
+  int ti, tj;
+  const int tile_id = blockIdx.x;
+  if (ep.full) {
+    ti = tile_id / nt;
+    tj = tile_id % nt;
+  } else {
+    tri_coords(tile_id, nt, ti, tj);
+  }
+  const int kc0 = blockIdx.y * kchunk;
+  const int nks = min(nk, kc0 + kchunk) - kc0;
+
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+#pragma unroll
+    for (int s = 0; s < ST; ++s) mbar_init(&full_bar[s], 1);
+    fence_mbar_init();
+    prefetch_tmap(&tmap);
+  }
+  __syncthreads();
+
+  auto issue = [&](int k) {
+    const int s = k % ST;
+    uint32_t *a = smem + s * 2 * TILE_WORDS;
+    mbar_arrive_expect_tx(&full_bar[s], STAGE_BYTES);
+    tma_load_3d(a, &tmap, &full_bar[s], ti * kTile, (kc0 + k) * kKW, 0);
+    tma_load_3d(a + TILE_WORDS, &tmap, &full_bar[s], tj * kTile, (kc0 + k) * kKW, 0);
+  };
+  int issued = 0;
+  if (tid == 0) {
+    for (; issued < ST - 1 && issued < nks; ++issued) issue(issued);
+  }
+
+  const int warp = tid >> 5, lane = tid & 31;
+  const int rbase = (warp >> 1) * 32 + (lane >> 3) * 4;
+  const int cbase = (warp & 1) * 64 + (lane & 7) * 4;
+
+  uint32_t acc0[8][8], acc1[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      acc0[r][c] = 0;
+      acc1[r][c] = 0;
+    }
+
+  int kabort = -1;
+  for (int k = 0; k < nks; ++k) {
+    if (tid == 0 && issued < nks) issue(issued++);
+    const int s = k % ST;
+    const bool ok = mbar_wait_bounded(&full_bar[s], (uint32_t)((k / ST) & 1));
+    if (ok) {
+      const uint32_t *A = smem + s * 2 * TILE_WORDS;
+      const uint32_t *B = A + TILE_WORDS;
+#pragma unroll 2
+      for (int kw = 0; kw < kKW; ++kw) {
+        uint32_t bc[8][NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const uint4 x0 = *reinterpret_cast<const uint4 *>(B + (p * kKW + kw) * kTile + cbase);
+          const uint4 x1 = *reinterpret_cast<const uint4 *>(B + (p * kKW + kw) * kTile + cbase + 32);
+          bc[0][p] = x0.x; bc[1][p] = x0.y; bc[2][p] = x0.z; bc[3][p] = x0.w;
+          bc[4][p] = x1.x; bc[5][p] = x1.y; bc[6][p] = x1.z; bc[7][p] = x1.w;
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          uint32_t ar[NP];
+          const int row = row_of(rbase, r);
+#pragma unroll
+          for (int p = 0; p < NP; ++p) ar[p] = A[(p * kKW + kw) * kTile + row];
+#pragma unroll
+          for (int c = 0; c < 8; ++c) pair_op<KIND>(ar, bc[c], acc0[r][c], acc1[r][c]);
+        }
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      kabort = k;
+      break;
+    }
+  }
+  if (kabort >= 0) {
+    // Let the copies still in flight land before the CTA's shared memory is
+    // released, each wait again bounded, then report.
+    if (tid == 0) {
+      for (int k = kabort; k < issued; ++k)
+        mbar_wait_bounded(&full_bar[k % ST], (uint32_t)((k / ST) & 1));
+      atomicOr(ep.err, 1);
+    }
+    return;
+  }
+
+  // Per-pair counts from the 16-bit halves of the accumulators.
+  auto get = [&](int r, int c, uint32_t &c0, uint32_t &c1, uint32_t &cv) {
+    c0 = acc0[r][c] & 0xffffu;
+    if constexpr (NC == 3) {
+      c1 = acc0[r][c] >> 16;
+      cv = acc1[r][c];
+    } else {
+      c1 = 0;
+      cv = acc0[r][c] >> 16;
+    }
+  };
+
+  if constexpr (EPI == EPI_DIST) {
+    // The pipeline buffers are free once every thread is past the last stage
+    // (the loop ends on a block barrier); reuse them for the distance tile.
+    float *S = reinterpret_cast<float *>(smem);
+    float tmax = 0.0f;
+    bool sat = false;
+    stage_distances(ep, ti, tj, rbase, cbase, S, get, tmax, sat);
+    __syncthreads();
+    store_distances(ep, ti, tj, tile_id, S, tmax, sat);
+  } else {
+    const int i0 = ti * kTile, j0 = tj * kTile;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = i0 + row_of(rbase, r);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int j = j0 + col_of(cbase, c);
+        const bool ok = ep.full ? (i < ep.n && j < ep.n) : (i < j && j < ep.n);
+        if (!ok) continue;
+        uint32_t c0, c1, cv;
+        get(r, c, c0, c1, cv);
+        uint32_t *o = ep.counts + ((size_t)i * ep.n + j) * 3;
+        if constexpr (EPI == EPI_COUNTS) {
+          o[0] = c0;
+          o[1] = c1;
+          o[2] = cv;
+        } else {
+          atomicAdd(o + 0, c0);
+          if (NC == 3) atomicAdd(o + 1, c1);
+          atomicAdd(o + 2, cv);
+        }
+      }
+    }
+  }
+}
+
+// Epilogue over an already complete count buffer (split-K path).
+__global__ void __launch_bounds__(256) transform_counts_kernel(int nt, EpiParams ep) {
+  extern __shared__ uint8_t smem_raw[];
+  float *S = reinterpret_cast<float *>(smem_raw);
+  int ti, tj;
+  const int tile_id = blockIdx.x;
+  if (ep.full) {
+    ti = tile_id / nt;
+    tj = tile_id % nt;
+  } else {
+    tri_coords(tile_id, nt, ti, tj);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rbase = (warp >> 1) * 32 + (lane >> 3) * 4;
+  const int cbase = (warp & 1) * 64 + (lane & 7) * 4;
+  const int i0 = ti * kTile, j0 = tj * kTile;
+  auto get = [&](int r, int c, uint32_t &c0, uint32_t &c1, uint32_t &cv) {
+    const int i = i0 + row_of(rbase, r), j = j0 + col_of(cbase, c);
+    const uint32_t *o = ep.counts + ((size_t)i * ep.n + j) * 3;
+    c0 = o[0];
+    c1 = o[1];
+    cv = o[2];
+  };
+  float tmax = 0.0f;
+  bool sat = false;
+  stage_distances(ep, ti, tj, rbase, cbase, S, get, tmax, sat);
+  __syncthreads();
+  store_distances(ep, ti, tj, tile_id, S, tmax, sat);
+}
+
+// KimuraDistance.cpp:384-386 / JCdistance.cpp:219-221: every -1 becomes
+// maxDistance * 2, once the global maximum is known.  Only tiles flagged by the
+// epilogue are visited.
+__global__ void __launch_bounds__(256) fixup_kernel(int nt, EpiParams ep) {
+  const int tile_id = blockIdx.x;
+  if (ep.tile_flags[tile_id] == 0) return;
+  int ti, tj;
+  if (ep.full) {
+    ti = tile_id / nt;
+    tj = tile_id % nt;
+  } else {
+    tri_coords(tile_id, nt, ti, tj);
+  }
+  const float m2 = __fmul_rn(__int_as_float(*ep.max_bits), 2.0f);
+  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+    const int i = ti * kTile + e / kTile;
+    const int j = tj * kTile + e % kTile;
+    if (ep.full) {
+      if (i < ep.n && j < ep.n && i != j && ep.out[(size_t)i * ep.ld + j] == -1.0f)
+        ep.out[(size_t)i * ep.ld + j] = m2;
+    } else if (i < j && j < ep.n && ep.out[(size_t)i * ep.ld + j] == -1.0f) {
+      ep.out[(size_t)i * ep.ld + j] = m2;
+      ep.out[(size_t)j * ep.ld + i] = m2;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ launchers
+
+static int grid_for(long long work, int block) {
+  long long g = (work + block - 1) / block;
+  if (g > 148LL * 64) g = 148LL * 64;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+cudaError_t launch_pack_chars(const uint8_t *d_chars, size_t ld, const Packed &p,
+                              const uint8_t lut[256], cudaStream_t s) {
+  Lut256 l;
+  for (int k = 0; k < 256; ++k) l.v[k] = lut[k];
+  const long long work = (long long)p.Np * p.Wp;
+  pack_chars_kernel<<<grid_for(work, 256), 256, 0, s>>>(d_chars, ld, p.n, p.L, p.Np, p.Wp,
+                                                        p.kind, l, p.planes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_presence(const uint8_t *d_chars, size_t ld, int n, int L, uint32_t *d_mask,
+                            cudaStream_t s) {
+  const long long work = (long long)n * L;
+  presence_kernel<<<grid_for(work, 256), 256, 0, s>>>(d_chars, ld, n, L, d_mask);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_bitstrings_dna(const uint32_t *d_bits, const uint32_t *d_gaps,
+                                       int bs_words, const Packed &p, cudaStream_t s) {
+  const long long work = (long long)p.Np * p.Wp;
+  pack_bitstrings_kernel<<<grid_for(work, 256), 256, 0, s>>>(d_bits, d_gaps, bs_words, p.n, p.L,
+                                                             p.Np, p.Wp, p.planes);
+  return cudaGetLastError();
+}
+
+template <int KIND, int EPI>
+static cudaError_t launch_one(const Packed &p, const EpiParams &ep, dim3 grid, int nt, int nk,
+                              int kchunk, cudaStream_t s) {
+  constexpr size_t smem = count_smem_bytes<KIND>();
+  cudaError_t e = cudaFuncSetAttribute(count_tiles_kernel<KIND, EPI>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  count_tiles_kernel<KIND, EPI><<<grid, 256, smem, s>>>(p.tmap, nt, nk, kchunk, ep);
+  return cudaGetLastError();
+}
+
+template <int EPI>
+static cudaError_t launch_kind(int kind, const Packed &p, const EpiParams &ep, dim3 grid, int nt,
+                               int nk, int kchunk, cudaStream_t s) {
+  switch (kind) {
+    case KIND_DNA: return launch_one<KIND_DNA, EPI>(p, ep, grid, nt, nk, kchunk, s);
+    case KIND_NAIVE: return launch_one<KIND_NAIVE, EPI>(p, ep, grid, nt, nk, kchunk, s);
+    case KIND_MISM2: return launch_one<KIND_MISM2, EPI>(p, ep, grid, nt, nk, kchunk, s);
+    case KIND_MISM5: return launch_one<KIND_MISM5, EPI>(p, ep, grid, nt, nk, kchunk, s);
+    case KIND_MISM7: return launch_one<KIND_MISM7, EPI>(p, ep, grid, nt, nk, kchunk, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode, const EpiParams &ep,
+                               cudaStream_t s) {
+  const int nt = tiles_of(p.n);
+  const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
+  if (ntiles == 0) return cudaSuccess;
+  const int nk = p.Wp / kKW;
+  const int kmax = kMaxFusedWords / kKW;
+  const int kchunk = (epi_mode == EPI_ATOMIC) ? kmax : nk;
+  const int nsplit = (nk + kchunk - 1) / kchunk;
+  dim3 grid((unsigned)ntiles, (unsigned)nsplit);
+  switch (epi_mode) {
+    case EPI_DIST: return launch_kind<EPI_DIST>(count_kind, p, ep, grid, nt, nk, kchunk, s);
+    case EPI_COUNTS: return launch_kind<EPI_COUNTS>(count_kind, p, ep, grid, nt, nk, kchunk, s);
+    default: return launch_kind<EPI_ATOMIC>(count_kind, p, ep, grid, nt, nk, kchunk, s);
+  }
+}
+
+cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s) {
+  const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
+  if (ntiles == 0) return cudaSuccess;
+  fixup_kernel<<<(unsigned)ntiles, 256, 0, s>>>(nt, ep);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s) {
+  const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
+  if (ntiles == 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(transform_counts_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+  if (e != cudaSuccess) return e;
+  transform_counts_kernel<<<(unsigned)ntiles, 256, kStageBytes, s>>>(nt, ep);
+  return cudaGetLastError();
+}
+
+}  // namespace rnj

@@ -1,0 +1,94 @@
+// rnj_probe.cu -- microbenchmark of the integer pipes the counting kernels are
+// bound by: POPC (population count) and LOP3 (three-input logic) throughput of
+// the whole device, in operations per second.  The distance kernels report their
+// achieved rates against these measured peaks.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "rnj.h"
+#include "rnj_internal.h"
+
+namespace rnj {
+
+constexpr int kProbeIters = 4096;
+
+// 8 independent chains per thread; every op is a real popc.b32 whose result
+// feeds the next, and the final values are stored so nothing is dead code.
+__global__ void __launch_bounds__(256) probe_popc_kernel(uint32_t seed, uint32_t *out) {
+  uint32_t x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = seed ^ (threadIdx.x * 2654435761u + k * 40503u + blockIdx.x);
+  for (int it = 0; it < kProbeIters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      uint32_t p;
+      asm volatile("popc.b32 %0, %1;" : "=r"(p) : "r"(x[k]));
+      x[k] ^= p;
+    }
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(256) probe_lop3_kernel(uint32_t seed, uint32_t *out) {
+  uint32_t x[8], y = seed * 747796405u + threadIdx.x, z = seed ^ 0x9e3779b9u ^ blockIdx.x;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = seed ^ (threadIdx.x * 2654435761u + k * 40503u);
+  for (int it = 0; it < kProbeIters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(x[k]) : "r"(y), "r"(z));
+  }
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace rnj
+
+using namespace rnj;
+
+extern "C" int rnj_probe_int_peaks(rnj_ctx *ctx, double *popc_per_s, double *lop3_per_s) {
+  if (!ctx) return set_error(RNJ_ERR_INVALID, "null context");
+  void *sv = nullptr;
+  int rc = rnj_ctx_stream(ctx, &sv);
+  if (rc != RNJ_OK) return rc;
+  cudaStream_t s = (cudaStream_t)sv;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = sms * 8, threads = 256;
+  uint32_t *out = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&out, (size_t)blocks * threads * 4, s);
+  if (e != cudaSuccess) return cuda_error(e, "probe buffer");
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const double ops = (double)blocks * threads * 8.0 * kProbeIters;
+  double best[2] = {0, 0};
+  for (int which = 0; which < 2; ++which) {
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(a, s);
+      if (which == 0) probe_popc_kernel<<<blocks, threads, 0, s>>>(rep + 1, out);
+      else probe_lop3_kernel<<<blocks, threads, 0, s>>>(rep + 1, out);
+      cudaEventRecord(b, s);
+      e = cudaEventSynchronize(b);
+      if (e != cudaSuccess) break;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0 && ms > 0) best[which] = std::max(best[which], ops / (ms * 1e-3));
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFreeAsync(out, s);
+  if (e != cudaSuccess) return cuda_error(e, "probe kernels");
+  if (popc_per_s) *popc_per_s = best[0];
+  if (lop3_per_s) *lop3_per_s = best[1];
+  return RNJ_OK;
+}
