@@ -155,6 +155,26 @@ int rnj_mat_copy_rows(rnj_ctx *ctx, rnj_mat *mat, int row0, int nrows, float **r
                       int threads);
 int rnj_mat_destroy(rnj_mat *mat);
 
+/* Distances for callers that cannot allocate device memory: a process that owns
+ * the whole GPU through its own memory pool, or that forbids cudaMalloc because
+ * it synchronises the device.  No counterpart in the reference.  Same result as
+ * rnj_distance_into, computed on the caller's `stream` (a cudaStream_t; NULL =
+ * legacy default) from device bytes d_chars (n rows, stride ld) into d_out (n
+ * rows, stride ld_out floats).  type must be RNJ_DNA or RNJ_PROTEIN.  No context
+ * is needed and nothing is allocated: every intermediate buffer lives in one
+ * 16 MiB array built into the library, which each GPU that loads the library
+ * holds until the process exits.  Limits: the packed alignment must fit that
+ * array (about n * L * 0.375 bytes for DNA, 0.5 with -f rules, 1 for protein,
+ * n rounded up to 128 and L to 256) and L <= 65280; larger inputs return
+ * RNJ_ERR_INVALID with the size needed.  All calls share the array and keep the
+ * last call's contents (each call clears what must start at zero): calls whose
+ * work overlaps on the GPU race, so issue them one after another on one stream.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  max_out (host, may be NULL) receives the maximum
+ * distance and synchronises the stream. */
+int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld, int type, int model,
+                         int flags, float *d_out, size_t ld_out, void *stream, float *max_out);
+
 /* One call, host in / host out: pack, distances, copy into out (n*n floats,
  * row-major).  max_out may be NULL. */
 int rnj_distance_matrix_host(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,

@@ -66,6 +66,8 @@ SIGNATURES = {
     "rnj_mat_destroy": (c_int, [c_void_p]),
     "rnj_distance_matrix_host": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int, c_int,
                                          c_int, c_void_p, P(c_float)]),
+    "rnj_distance_noalloc": (c_int, [c_void_p, c_int, c_int, c_size_t, c_int, c_int, c_int,
+                                     c_void_p, c_size_t, c_void_p, P(c_float)]),
     "rnj_msa_read": (c_int, [c_char_p, c_char_p, P(c_void_p)]),
     "rnj_msa_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
     "rnj_msa_name": (c_char_p, [c_void_p, c_int]),

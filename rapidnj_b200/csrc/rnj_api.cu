@@ -72,7 +72,7 @@ int encode_planes_map(Packed &p) {
 }
 
 // resolveChar of the loaders (dataloaderFasta.hpp:184-199).
-static char resolve_char(char c, int type) {
+char resolve_char(char c, int type) {
   if (type == RNJ_DNA) {
     if (!(c == 'a' || c == 'A' || c == 'c' || c == 'C' || c == 'g' || c == 'G' || c == 't' ||
           c == 'T' || c == 'u' || c == 'U'))
@@ -89,7 +89,7 @@ static char resolve_char(char c, int type) {
 // upper-case A/C/G/T).  Fast rule (dataloaderFasta.hpp:155-180): only A/C/G/T in
 // either case are valid.  Naive rule (simpleDistanceCalculator.cpp with
 // resolveChar): A/C/G/T/U in either case are valid.
-static void dna_lut(bool naive, uint8_t lut[256]) {
+void dna_lut(bool naive, uint8_t lut[256]) {
   memset(lut, 0, 256);
   struct { char c; int code; } letters[] = {{'A', 0}, {'G', 1}, {'T', 2}, {'C', 3}};
   for (auto &l : letters) {

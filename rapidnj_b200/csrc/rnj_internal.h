@@ -95,4 +95,9 @@ inline long long tri_tiles(int nt) { return (long long)nt * (nt + 1) / 2; }
 int set_error(int code, const std::string &msg);
 int cuda_error(cudaError_t e, const char *what);
 
+// Packing helpers (rnj_api.cu).
+char resolve_char(char c, int type);
+void dna_lut(bool naive, uint8_t lut[256]);
+int encode_planes_map(Packed &p);
+
 }  // namespace rnj
