@@ -35,6 +35,9 @@ WORKLOADS = {
     "dna-jc-512x2000": ("iid_dna", 512, 2000, "dna", "jc"),
     "dna-k2p-50000x1000": ("tree_dna", 50000, 1000, "dna", "kim"),
     "protein-kimura-5000x1500": ("tree_protein", 5000, 1500, "protein", "kim"),
+    # the same kernel as the default workload at a size an ncu --set full capture
+    # finishes quickly (inputs + planes + output ~ 0.2 GB, larger than L2)
+    "dna-k2p-4096x10000": ("tree_dna", 4096, 10000, "dna", "kim"),
 }
 DEFAULT = "dna-k2p-10000x10000"
 # Algorithmic integer operations per pair per 32-column word:

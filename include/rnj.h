@@ -63,7 +63,11 @@ enum {
    * plus mirror, as the disk-matrix driver does (KimuraDistance.cpp:308-354 with
    * dm != NULL).  Only differs for the naive DNA estimator, whose counts are
    * asymmetric. */
-  RNJ_FULL_ROWS = 4
+  RNJ_FULL_ROWS = 4,
+  /* DNA on the fast path counted on the tensor cores (tcgen05, int8 features,
+   * exact int32 accumulation) instead of the bit-plane popcount kernel.  Same
+   * counts; only the kernel differs. */
+  RNJ_TENSOR_CORES = 8
 };
 
 typedef struct rnj_ctx rnj_ctx;

@@ -11,16 +11,17 @@ import numpy as np
 
 from . import _native as N
 from ._native import (RNJ_COMPAT_PROTEIN_WRAP, RNJ_DNA, RNJ_FASTDIST, RNJ_FULL_ROWS, RNJ_JC,
-                      RNJ_KIMURA, RNJ_PROTEIN, RNJ_UNKNOWN, check)
+                      RNJ_KIMURA, RNJ_PROTEIN, RNJ_TENSOR_CORES, RNJ_UNKNOWN, check)
 
 MODELS = {"jc": RNJ_JC, "kim": RNJ_KIMURA, RNJ_JC: RNJ_JC, RNJ_KIMURA: RNJ_KIMURA}
 TYPES = {None: RNJ_UNKNOWN, "d": RNJ_DNA, "p": RNJ_PROTEIN, "dna": RNJ_DNA, "protein": RNJ_PROTEIN,
          RNJ_DNA: RNJ_DNA, RNJ_PROTEIN: RNJ_PROTEIN, RNJ_UNKNOWN: RNJ_UNKNOWN}
 
 
-def flags_of(fastdist: bool = True, compat_wrap: bool = False, full_rows: bool = False) -> int:
+def flags_of(fastdist: bool = True, compat_wrap: bool = False, full_rows: bool = False,
+             tensor_cores: bool = False) -> int:
     return ((RNJ_FASTDIST if fastdist else 0) | (RNJ_COMPAT_PROTEIN_WRAP if compat_wrap else 0)
-            | (RNJ_FULL_ROWS if full_rows else 0))
+            | (RNJ_FULL_ROWS if full_rows else 0) | (RNJ_TENSOR_CORES if tensor_cores else 0))
 
 
 def detect_type(seq0: bytes) -> int:
@@ -131,9 +132,9 @@ class Context:
 
     # --- alignments
     def alignment(self, seqs, type_=None, fastdist: bool = True, compat_wrap: bool = False,
-                  full_rows: bool = False) -> Alignment:
+                  full_rows: bool = False, tensor_cores: bool = False) -> Alignment:
         """Packs an alignment from a host (n, L) uint8 array or a CUDA uint8 tensor."""
-        flags = flags_of(fastdist, compat_wrap, full_rows)
+        flags = flags_of(fastdist, compat_wrap, full_rows, tensor_cores)
         t = TYPES[type_]
         h = ctypes.c_void_p()
         if hasattr(seqs, "is_cuda") and seqs.is_cuda:

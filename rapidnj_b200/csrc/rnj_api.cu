@@ -71,6 +71,24 @@ int encode_planes_map(Packed &p) {
   return RNJ_OK;
 }
 
+// 2-D map over the int8 feature rows: (4 * Lk bytes, Np rows), 128 x 128 box,
+// 128-byte swizzle (the layout the tcgen05 shared-memory descriptors expect).
+int encode_features_map(Packed &p) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  cuuint64_t dims[2] = {(cuuint64_t)4 * p.Lk, (cuuint64_t)p.Np};
+  cuuint64_t strides[1] = {(cuuint64_t)4 * p.Lk};
+  cuuint32_t box[2] = {128, (cuuint32_t)kTile};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(&p.fmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, p.feat, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled (features) failed (" +
+                                       std::to_string((int)r) + ")");
+  return RNJ_OK;
+}
+
 // resolveChar of the loaders (dataloaderFasta.hpp:184-199).
 char resolve_char(char c, int type) {
   if (type == RNJ_DNA) {
@@ -249,6 +267,29 @@ int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, s
   p.W = (L + 31) / 32;
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
+  if (kind == KIND_DNA && (flags & RNJ_TENSOR_CORES)) {
+    // int8 feature rows for the tensor-core kernel instead of bit planes.
+    p.kind = KIND_DNA_TC;
+    p.NP = 0;
+    p.Lk = std::max(128, (L + 127) / 128 * 128);
+    const size_t fbytes = (size_t)p.Np * 4 * p.Lk;
+    cudaError_t e = cudaMallocAsync((void **)&p.feat, fbytes, ctx->stream);
+    if (e != cudaSuccess) {
+      delete a;
+      return cuda_error(e, "feature allocation");
+    }
+    mark(ctx, 0, 0);
+    e = launch_pack_features(d_chars, ld, n, L, p.Np, p.Lk, p.feat, ctx->stream);
+    mark(ctx, 0, 1);
+    int rc = (e == cudaSuccess) ? encode_features_map(p) : cuda_error(e, "feature pack kernel");
+    if (rc != RNJ_OK) {
+      cudaFreeAsync(p.feat, ctx->stream);
+      delete a;
+      return rc;
+    }
+    *out = a;
+    return RNJ_OK;
+  }
   p.NP = planes_of(kind);
   const size_t bytes = (size_t)p.NP * p.Wp * p.Np * sizeof(uint32_t);
   cudaError_t e = cudaMallocAsync((void **)&p.planes, bytes, ctx->stream);
@@ -324,7 +365,10 @@ int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t 
   const int ckind = count_kind_for(p, model);
   const int nk = p.Wp / kKW;
   mark(ctx, 1, 0);
-  if (nk <= kMaxFusedWords / kKW) {
+  if (p.kind == KIND_DNA_TC) {
+    // int32 tensor-memory accumulators: exact for any L, no split needed.
+    RNJ_CUDA(launch_tc_count(p.fmap, p.n, p.Lk, EPI_DIST, ep, ctx->stream), "tensor-core kernel");
+  } else if (nk <= kMaxFusedWords / kKW) {
     RNJ_CUDA(launch_count_tiles(p, ckind, EPI_DIST, ep, ctx->stream), "count kernel");
   } else {
     const size_t cbytes = (size_t)p.n * p.n * 3 * sizeof(uint32_t);
@@ -585,6 +629,7 @@ int rnj_aln_destroy(rnj_aln *aln) {
   if (!aln) return RNJ_OK;
   DeviceGuard g(aln->ctx->device);
   if (aln->p.planes) cudaFreeAsync(aln->p.planes, aln->ctx->stream);
+  if (aln->p.feat) cudaFreeAsync(aln->p.feat, aln->ctx->stream);
   delete aln;
   return RNJ_OK;
 }
@@ -656,6 +701,10 @@ int rnj_counts_into(rnj_ctx *ctx, rnj_aln *aln, unsigned int *d_counts) {
   EpiParams ep = epi_for(ctx, p, RNJ_KIMURA);
   ep.full = (p.flags & RNJ_FULL_ROWS) ? 1 : 0;
   ep.counts = d_counts;
+  if (p.kind == KIND_DNA_TC) {
+    RNJ_CUDA(launch_tc_count(p.fmap, p.n, p.Lk, EPI_COUNTS, ep, ctx->stream), "tensor-core kernel");
+    return check_device_error(ctx);
+  }
   const int nk = p.Wp / kKW;
   const int mode = (nk <= kMaxFusedWords / kKW) ? EPI_COUNTS : EPI_ATOMIC;
   RNJ_CUDA(launch_count_tiles(p, p.kind, mode, ep, ctx->stream), "count kernel");

@@ -18,7 +18,10 @@ namespace rnj {
 //   KIND_MISM2  planes {c0, c1, valid}         -> {mismatch, valid}
 //   KIND_MISM5  planes {c0..c4, valid}         -> {mismatch, valid}
 //   KIND_MISM7  planes {c0..c6, valid}         -> {mismatch, valid}
-enum Kind { KIND_DNA = 0, KIND_NAIVE = 1, KIND_MISM2 = 2, KIND_MISM5 = 3, KIND_MISM7 = 4 };
+//   KIND_DNA_TC int8 features {v | r | t | u}   -> {ts, tv, valid} on tensor cores
+enum Kind {
+  KIND_DNA = 0, KIND_NAIVE = 1, KIND_MISM2 = 2, KIND_MISM5 = 3, KIND_MISM7 = 4, KIND_DNA_TC = 5
+};
 
 constexpr int kTile = 128;        // pairs per tile edge (rows and columns)
 constexpr int kWordBits = 32;     // sites per plane word
@@ -47,6 +50,10 @@ struct Packed {
   int NP = 0;            // planes
   uint32_t *planes = nullptr;  // NP * Wp * Np words, word-major, sequence fastest
   CUtensorMap tmap;      // 3-D map over (Np, Wp, NP), box (kTile, kKW, NP)
+  // Tensor-core layout (KIND_DNA_TC): Np rows of 4 * Lk int8 features.
+  int8_t *feat = nullptr;
+  int Lk = 0;            // L rounded up to 128
+  CUtensorMap fmap;      // 2-D map over (4 * Lk bytes, Np), box (128, 128), 128-byte swizzle
 };
 
 struct EpiParams {
@@ -85,6 +92,11 @@ cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode,
                                const EpiParams &ep, cudaStream_t s);
 cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s);
 cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s);
+// Tensor-core DNA path (rnj_tc.cu).
+cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
+                                 int8_t *F, cudaStream_t s);
+cudaError_t launch_tc_count(const CUtensorMap &fmap, int n, int Lk, int epi_mode,
+                            const EpiParams &ep, cudaStream_t s);
 
 enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2 };
 

@@ -12,26 +12,10 @@
 #include <stdint.h>
 
 #include "rnj_device.cuh"
+#include "rnj_epilogue.cuh"
 #include "rnj_internal.h"
 
 namespace rnj {
-
-// Dayhoff PAM distances (x100) for p = 0.750 .. 0.930, the table that defines the
-// protein Kimura distance above p = 0.75 (rapidNJ KimuraDistance.cpp:30-49).
-__constant__ int c_pam[181] = {
-    195, 196, 197, 198, 199, 200, 200, 201, 202, 203, 204, 205, 206, 207, 208,
-    209, 209, 210, 211, 212, 213, 214, 215, 216, 217, 218, 219, 220, 221, 222,
-    223, 224, 226, 227, 228, 229, 230, 231, 232, 233, 234, 236, 237, 238, 239,
-    240, 241, 243, 244, 245, 246, 248, 249, 250, 252, 253, 254, 255, 257, 258,
-    260, 261, 262, 264, 265, 267, 268, 270, 271, 273, 274, 276, 277, 279, 281,
-    282, 284, 285, 287, 289, 291, 292, 294, 296, 298, 299, 301, 303, 305, 307,
-    309, 311, 313, 315, 317, 319, 321, 323, 325, 328, 330, 332, 335, 337, 339,
-    342, 344, 347, 349, 352, 354, 357, 360, 362, 365, 368, 371, 374, 377, 380,
-    383, 386, 389, 393, 396, 399, 403, 407, 410, 414, 418, 422, 426, 430, 434,
-    438, 442, 447, 451, 456, 461, 466, 471, 476, 482, 487, 493, 498, 504, 511,
-    517, 524, 531, 538, 545, 553, 560, 569, 577, 586, 595, 605, 615, 626, 637,
-    649, 661, 675, 688, 703, 719, 736, 754, 775, 796, 819, 845, 874, 907, 945,
-    988};
 
 // ------------------------------------------------------------------- packing
 
@@ -182,115 +166,6 @@ struct KT<KIND_MISM7> { static constexpr int NP = 8, NC = 2, ST = 3; };
 template <int KIND>
 constexpr size_t count_smem_bytes() {
   return (size_t)KT<KIND>::ST * 2 * KT<KIND>::NP * kKW * kTile * 4 + 1024 + 64;
-}
-
-// Upper-triangle tile t -> (ti, tj), ti <= tj, row-major over the triangle.
-__device__ __forceinline__ void tri_coords(int t, int nt, int &ti, int &tj) {
-  const double b = 2.0 * nt + 1.0;
-  int r = (int)floor((b - sqrt(b * b - 8.0 * (double)t)) * 0.5);
-  auto start = [nt](int x) { return (long long)x * nt - (long long)x * (x - 1) / 2; };
-  if (r < 0) r = 0;
-  if (r > nt - 1) r = nt - 1;
-  while (r > 0 && start(r) > t) --r;
-  while (r + 1 < nt && start(r + 1) <= t) ++r;
-  ti = r;
-  tj = r + (int)(t - start(r));
-}
-
-// Per-thread pair layout inside a 128 x 128 tile (256 threads = 4 x 2 warps, each
-// warp 32 rows x 64 columns, each lane 8 x 8 pairs): rows rbase + {0..3, 16..19},
-// columns cbase + {0..3, 32..35}.  The two 4-wide groups keep every 128-bit
-// shared load of a quarter warp on distinct banks.
-__device__ __forceinline__ int row_of(int rbase, int r) { return rbase + (r < 4 ? r : 12 + r); }
-__device__ __forceinline__ int col_of(int cbase, int c) { return cbase + (c < 4 ? c : 28 + c); }
-
-__device__ __forceinline__ float pair_distance(const EpiParams &ep, uint32_t c0, uint32_t c1,
-                                               uint32_t valid) {
-  unsigned long long v = valid;
-  if (ep.compat_wrap) v = protein_fast_valid(v, ep.L);
-  if (ep.model == RNJ_JC) return jc_distance((unsigned long long)c0 + c1, v, ep.jc_b);
-  if (ep.type == RNJ_PROTEIN) return kimura_protein_distance(c0, v, c_pam);
-  return k2p_distance(c0, c1, v);
-}
-
-// Row stride (floats) of the distance tile staged in shared memory: 129 keeps
-// both row-wise and column-wise reads on distinct banks.
-constexpr int kStageLd = kTile + 1;
-constexpr size_t kStageBytes = (size_t)kTile * kStageLd * 4;
-
-// Epilogue, part 1: this thread's distances into the shared tile S (row =
-// local i, column = local j), with the running max and saturation flag.  Counts
-// come from get(r, c, c0, c1, valid).
-template <class Get>
-__device__ __forceinline__ void stage_distances(const EpiParams &ep, int ti, int tj, int rbase,
-                                                int cbase, float *S, Get get, float &tmax,
-                                                bool &sat) {
-  const int i0 = ti * kTile, j0 = tj * kTile;
-#pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int rl = row_of(rbase, r);
-    const int i = i0 + rl;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const int cl = col_of(cbase, c);
-      const int j = j0 + cl;
-      const bool ok = ep.full ? (i < ep.n && j < ep.n && i != j) : (i < j && j < ep.n);
-      float x = 0.0f;
-      if (ok) {
-        uint32_t c0, c1, cv;
-        get(r, c, c0, c1, cv);
-        x = pair_distance(ep, c0, c1, cv);
-        if (x > tmax) tmax = x;
-        if (x == -1.0f) sat = true;
-      }
-      S[rl * kStageLd + cl] = x;
-    }
-  }
-}
-
-// Epilogue, part 2 (after a block barrier): coalesced stores of the tile and of
-// its mirror image, zero diagonal, block max and saturation flag.
-__device__ __forceinline__ void store_distances(const EpiParams &ep, int ti, int tj, int tile_id,
-                                                const float *S, float tmax, bool sat) {
-  const int i0 = ti * kTile, j0 = tj * kTile, n = ep.n;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
-  // Tile region: row i0 + r, columns j0 + lane + 32 q.
-  for (int r = warp; r < kTile; r += nwarps) {
-    const int i = i0 + r;
-    if (i >= n) break;
-    float *row = ep.out + (size_t)i * ep.ld + j0;
-#pragma unroll
-    for (int q = 0; q < kTile / 32; ++q) {
-      const int cl = lane + 32 * q;
-      const int j = j0 + cl;
-      if (j >= n) continue;
-      if (ep.full) row[cl] = (i == j) ? 0.0f : S[r * kStageLd + cl];
-      else if (i < j) row[cl] = S[r * kStageLd + cl];
-      else if (i == j) row[cl] = 0.0f;
-    }
-  }
-  if (!ep.full) {
-    // Mirror region: row j0 + c holds column c of S.
-    for (int c = warp; c < kTile; c += nwarps) {
-      const int j = j0 + c;
-      if (j >= n) break;
-      float *row = ep.out + (size_t)j * ep.ld + i0;
-#pragma unroll
-      for (int q = 0; q < kTile / 32; ++q) {
-        const int rl = lane + 32 * q;
-        const int i = i0 + rl;
-        if (i < j) row[rl] = S[rl * kStageLd + c];
-      }
-    }
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, off));
-  const bool any_sat = __any_sync(0xffffffffu, sat);
-  if (lane == 0) {
-    if (tmax > 0.0f) atomicMax(ep.max_bits, __float_as_int(tmax));
-    if (any_sat) ep.tile_flags[tile_id] = 1;
-  }
 }
 
 template <int KIND>
@@ -451,7 +326,7 @@ __global__ void __launch_bounds__(256, 1)
     bool sat = false;
     stage_distances(ep, ti, tj, rbase, cbase, S, get, tmax, sat);
     __syncthreads();
-    store_distances(ep, ti, tj, tile_id, S, tmax, sat);
+    store_distances(ep, ti, tj, tile_id, S, tmax, sat, threadIdx.x >> 5, blockDim.x >> 5);
   } else {
     const int i0 = ti * kTile, j0 = tj * kTile;
 #pragma unroll
@@ -506,7 +381,7 @@ __global__ void __launch_bounds__(256) transform_counts_kernel(int nt, EpiParams
   bool sat = false;
   stage_distances(ep, ti, tj, rbase, cbase, S, get, tmax, sat);
   __syncthreads();
-  store_distances(ep, ti, tj, tile_id, S, tmax, sat);
+  store_distances(ep, ti, tj, tile_id, S, tmax, sat, threadIdx.x >> 5, blockDim.x >> 5);
 }
 
 // KimuraDistance.cpp:384-386 / JCdistance.cpp:219-221: every -1 becomes

@@ -290,3 +290,38 @@ def test_full_size_k2p_properties(ctx):
         d = lib.orc_distance(c32, L, 0, 1, 0, 0)
         exp[k] = 2 * mx if d == -1 else d
     assert ulp_diff(got, exp).max() <= 1
+
+
+# ------------------------------------------------- tensor-core DNA kernel
+
+TC_SHAPES = [(2, 1), (3, 31), (17, 127), (128, 128), (129, 129), (200, 1000), (257, 4097),
+             (300, 300)]
+
+
+@pytest.mark.parametrize("n,L", TC_SHAPES)
+def test_tensor_core_counts_vs_oracle(ctx, n, L):
+    from rapidnj_b200 import synth
+    seqs = synth.tree_dna(n, L, seed=n + 7 * L, mean_branch=0.15)
+    aln = ctx.alignment(seqs, oracle.DNA, tensor_cores=True)
+    out = torch.zeros(n * n * 3, dtype=torch.int32, device="cuda")
+    ctx.counts_into(aln, out)
+    got = out.cpu().numpy().view(np.uint32).reshape(n, n, 3)
+    assert np.array_equal(got, oracle.counts(seqs, oracle.DNA))
+
+
+@pytest.mark.parametrize("path", [p for p in GOLDENS if "dna" in p or "LGT" in p],
+                         ids=lambda p: p.split("/")[-1])
+@pytest.mark.parametrize("model", ["jc", "kim"])
+def test_tensor_core_matrices_match_reference(ctx, path, model):
+    g = load_golden(path)
+    aln = ctx.alignment(g["chars"], oracle.DNA, tensor_cores=True)
+    m = ctx.distance(aln, model)
+    assert_matrix_parity(m.to_numpy(), g[f"{model}_fast"])
+
+
+def test_tensor_core_matches_popcount_kernel(ctx):
+    from rapidnj_b200 import synth
+    seqs = synth.tree_dna(1000, 3000, seed=21)
+    a = ctx.distance(ctx.alignment(seqs, oracle.DNA), "kim").to_numpy()
+    b = ctx.distance(ctx.alignment(seqs, oracle.DNA, tensor_cores=True), "kim").to_numpy()
+    assert np.array_equal(a, b)
