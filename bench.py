@@ -173,7 +173,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
 
     def step():
-        aln = ctx.alignment(d_chars, typ)
+        aln = ctx.alignment(d_chars, typ, popcount=args.popcount)
         ctx.distance_into(aln, model, out)
         aln.close()
 
@@ -209,22 +209,37 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
               "count_ms": count_ms}
 
     if rank == 0:
-        # Roofline of the dominant kernel (the tile count kernel) against the
-        # measured integer-pipe peak of this device.
-        popc_peak, lop3_peak = ctx.probe_int_peaks()
-        popc_w, lop3_w = OPS_PER_WORD[(type_, model)]
-        words = units(n, L) / 32.0
         cnt = sum(count_ms) / len(count_ms)
-        achieved = popc_w * words / (cnt * 1e-3)
-        result["roofline"] = {
-            "bound": "int", "pipe": "POPC", "achieved": achieved / 1e12, "peak": popc_peak / 1e12,
-            "unit": "Tops/s", "frac": achieved / popc_peak,
-            "traffic": traffic_from_profiles(name),
-            "kernel": "count_tiles_kernel", "kernel_ms": cnt,
-            "lop3_frac": (lop3_w * words / (cnt * 1e-3)) / lop3_peak,
-            "peak_source": "rnj_probe_int_peaks, measured on this device in this run",
-            "ops_per_pair_word": {"popc": popc_w, "lop3": lop3_w},
-        }
+        if type_ == "dna" and not args.popcount:
+            # tcgen05 kernel: 4 int8 MACs (8 ops) per pair-column, against the
+            # int8 dense tensor peak measured here with a cuBLAS GEMM.
+            peak = int8_tensor_peak(local_rank)
+            achieved = 8.0 * units(n, L) / (cnt * 1e-3)
+            result["roofline"] = {
+                "bound": "tensor", "achieved": achieved / 1e12, "peak": peak / 1e12,
+                "unit": "TOP/s (int8)", "frac": achieved / peak,
+                "traffic": traffic_from_profiles(name),
+                "kernel": "tc_count_kernel", "kernel_ms": cnt,
+                "peak_source": "cuBLAS int8 GEMM (torch._int_mm 8192^3, best of 10) measured on "
+                               "this device in this run",
+                "ops_per_pair_column": 8,
+            }
+        else:
+            # Bit-plane popcount kernel: bound by the POPC pipe, against the
+            # POPC peak measured on this device.
+            popc_peak, lop3_peak = ctx.probe_int_peaks()
+            popc_w, lop3_w = OPS_PER_WORD[(type_, model)]
+            words = units(n, L) / 32.0
+            achieved = popc_w * words / (cnt * 1e-3)
+            result["roofline"] = {
+                "bound": "int", "pipe": "POPC", "achieved": achieved / 1e12,
+                "peak": popc_peak / 1e12, "unit": "Tops/s", "frac": achieved / popc_peak,
+                "traffic": traffic_from_profiles(name),
+                "kernel": "count_tiles_kernel", "kernel_ms": cnt,
+                "lop3_frac": (lop3_w * words / (cnt * 1e-3)) / lop3_peak,
+                "peak_source": "rnj_probe_int_peaks, measured on this device in this run",
+                "ops_per_pair_word": {"popc": popc_w, "lop3": lop3_w},
+            }
         result["e2e"] = run_e2e(ctx, seqs, typ, model, args)
     ctx.close()
     return result
@@ -239,16 +254,35 @@ def run_e2e(ctx, seqs, typ, model, args):
     pinned = torch.from_numpy(seqs).pin_memory()
     host = pinned.numpy()
     steps = max(1, min(args.steps, 5))
-    ctx.distance_matrix_host(host, model, typ)  # warm-up
+    ctx.distance_matrix_host(host, model, typ, popcount=args.popcount)  # warm-up
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        ctx.distance_matrix_host(host, model, typ)
+        ctx.distance_matrix_host(host, model, typ, popcount=args.popcount)
         times.append(time.perf_counter() - t0)
     mean = sum(times) / len(times)
     return {"value": units(n, L) / mean, "unit": "pair-columns/s", "h2d_bytes_per_step": n * L,
             "d2h_bytes_per_step": n * n * 4, "ms_per_step": mean * 1e3, "steps": steps,
             "call": "rnj_distance_matrix_host"}
+
+
+def int8_tensor_peak(device: int) -> float:
+    """Dense int8 tensor throughput (ops/s) of a cuBLAS GEMM on this device."""
+    import torch
+    m = 8192
+    a = torch.randint(-64, 64, (m, m), dtype=torch.int8, device=f"cuda:{device}")
+    b = torch.randint(-64, 64, (m, m), dtype=torch.int8, device=f"cuda:{device}").t()
+    best = 0.0
+    for k in range(12):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        e.synchronize()
+        if k >= 2:
+            best = max(best, 2.0 * m ** 3 / (s.elapsed_time(e) * 1e-3))
+    return best
 
 
 def traffic_from_profiles(name: str):
@@ -269,6 +303,8 @@ def main():
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--popcount", action="store_true",
+                    help="count DNA with the bit-plane popcount kernel instead of tensor cores")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -276,6 +312,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     gen, n, L, type_, model = WORKLOADS[args.workload]
     config = {"workload": args.workload, "n": n, "L": L, "type": type_, "model": model,
+              "kernel": ("popcount" if (args.popcount or type_ != "dna") else "tcgen05"),
               "generator": gen, "seed": 0, "parallelism": f"tiles/{world}" if world > 1 else "single",
               "l2": "256 MiB buffer written between timed steps (L2 flushed)"}
 

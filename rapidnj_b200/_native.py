@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "librnjgpu.so")
 RNJ_OK = 0
 RNJ_DNA, RNJ_PROTEIN, RNJ_UNKNOWN = 0, 1, 2
 RNJ_JC, RNJ_KIMURA = 0, 1
-RNJ_FASTDIST, RNJ_COMPAT_PROTEIN_WRAP, RNJ_FULL_ROWS, RNJ_TENSOR_CORES = 1, 2, 4, 8
+RNJ_FASTDIST, RNJ_COMPAT_PROTEIN_WRAP, RNJ_FULL_ROWS, RNJ_POPCOUNT = 1, 2, 4, 8
 
 STATUS_NAMES = {
     0: "RNJ_OK", 1: "RNJ_ERR_INVALID", 2: "RNJ_ERR_CUDA", 3: "RNJ_ERR_NOMEM", 4: "RNJ_ERR_IO",

@@ -11,7 +11,7 @@ import numpy as np
 
 from . import _native as N
 from ._native import (RNJ_COMPAT_PROTEIN_WRAP, RNJ_DNA, RNJ_FASTDIST, RNJ_FULL_ROWS, RNJ_JC,
-                      RNJ_KIMURA, RNJ_PROTEIN, RNJ_TENSOR_CORES, RNJ_UNKNOWN, check)
+                      RNJ_KIMURA, RNJ_POPCOUNT, RNJ_PROTEIN, RNJ_UNKNOWN, check)
 
 MODELS = {"jc": RNJ_JC, "kim": RNJ_KIMURA, RNJ_JC: RNJ_JC, RNJ_KIMURA: RNJ_KIMURA}
 TYPES = {None: RNJ_UNKNOWN, "d": RNJ_DNA, "p": RNJ_PROTEIN, "dna": RNJ_DNA, "protein": RNJ_PROTEIN,
@@ -19,9 +19,9 @@ TYPES = {None: RNJ_UNKNOWN, "d": RNJ_DNA, "p": RNJ_PROTEIN, "dna": RNJ_DNA, "pro
 
 
 def flags_of(fastdist: bool = True, compat_wrap: bool = False, full_rows: bool = False,
-             tensor_cores: bool = False) -> int:
+             popcount: bool = False) -> int:
     return ((RNJ_FASTDIST if fastdist else 0) | (RNJ_COMPAT_PROTEIN_WRAP if compat_wrap else 0)
-            | (RNJ_FULL_ROWS if full_rows else 0) | (RNJ_TENSOR_CORES if tensor_cores else 0))
+            | (RNJ_FULL_ROWS if full_rows else 0) | (RNJ_POPCOUNT if popcount else 0))
 
 
 def detect_type(seq0: bytes) -> int:
@@ -132,9 +132,9 @@ class Context:
 
     # --- alignments
     def alignment(self, seqs, type_=None, fastdist: bool = True, compat_wrap: bool = False,
-                  full_rows: bool = False, tensor_cores: bool = False) -> Alignment:
+                  full_rows: bool = False, popcount: bool = False) -> Alignment:
         """Packs an alignment from a host (n, L) uint8 array or a CUDA uint8 tensor."""
-        flags = flags_of(fastdist, compat_wrap, full_rows, tensor_cores)
+        flags = flags_of(fastdist, compat_wrap, full_rows, popcount)
         t = TYPES[type_]
         h = ctypes.c_void_p()
         if hasattr(seqs, "is_cuda") and seqs.is_cuda:
@@ -193,14 +193,14 @@ class Context:
         check(N.lib().rnj_counts_into(self.handle, aln.handle, ctypes.c_void_p(out.data_ptr())))
 
     def distance_matrix_host(self, seqs: np.ndarray, model="kim", type_=None, fastdist=True,
-                             compat_wrap=False, full_rows=False):
+                             compat_wrap=False, full_rows=False, popcount=False):
         a = np.ascontiguousarray(seqs, dtype=np.uint8)
         n, L = a.shape
         out = np.empty((n, n), dtype=np.float32)
         m = ctypes.c_float()
         check(N.lib().rnj_distance_matrix_host(self.handle, a.ctypes.data, n, L, L, TYPES[type_],
                                                MODELS[model],
-                                               flags_of(fastdist, compat_wrap, full_rows),
+                                               flags_of(fastdist, compat_wrap, full_rows, popcount),
                                                out.ctypes.data, ctypes.byref(m)))
         return out, m.value
 

@@ -267,7 +267,7 @@ int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, s
   p.W = (L + 31) / 32;
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
-  if (kind == KIND_DNA && (flags & RNJ_TENSOR_CORES)) {
+  if (kind == KIND_DNA && !(flags & RNJ_POPCOUNT)) {
     // int8 feature rows for the tensor-core kernel instead of bit planes.
     p.kind = KIND_DNA_TC;
     p.NP = 0;
@@ -424,6 +424,14 @@ int rnj_ctx_create(int device, rnj_ctx **out) {
   if (!encode_fn()) {
     rnj_ctx_destroy(c);
     return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  }
+  // Packed alignments and matrices come from the device's stream-ordered pool;
+  // keep freed blocks in the pool instead of returning them at every
+  // synchronisation, so repeated calls of one shape do not remap memory.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   *out = c;
   return RNJ_OK;

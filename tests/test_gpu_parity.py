@@ -37,8 +37,8 @@ def assert_matrix_parity(got, ref):
     assert (d == 1).sum() <= max(2, int(1e-6 * d.size)), f"{(d == 1).sum()} one-ulp cells"
 
 
-def gpu_counts(ctx, seqs, typ, fastdist=True, full_rows=False):
-    aln = ctx.alignment(seqs, typ, fastdist=fastdist, full_rows=full_rows)
+def gpu_counts(ctx, seqs, typ, fastdist=True, full_rows=False, popcount=False):
+    aln = ctx.alignment(seqs, typ, fastdist=fastdist, full_rows=full_rows, popcount=popcount)
     n = seqs.shape[0]
     out = torch.zeros(n * n * 3, dtype=torch.int32, device="cuda")
     ctx.counts_into(aln, out)
@@ -46,8 +46,10 @@ def gpu_counts(ctx, seqs, typ, fastdist=True, full_rows=False):
     return out.cpu().numpy().view(np.uint32).reshape(n, n, 3)
 
 
-def gpu_matrix(ctx, seqs, typ, model, fastdist=True, compat_wrap=False, full_rows=False):
-    aln = ctx.alignment(seqs, typ, fastdist=fastdist, compat_wrap=compat_wrap, full_rows=full_rows)
+def gpu_matrix(ctx, seqs, typ, model, fastdist=True, compat_wrap=False, full_rows=False,
+               popcount=False):
+    aln = ctx.alignment(seqs, typ, fastdist=fastdist, compat_wrap=compat_wrap, full_rows=full_rows,
+                        popcount=popcount)
     mat = ctx.distance(aln, model)
     out, mx = mat.to_numpy(), mat.max
     mat.close()
@@ -58,11 +60,12 @@ def gpu_matrix(ctx, seqs, typ, model, fastdist=True, compat_wrap=False, full_row
 # ----------------------------------------------------------------- goldens
 
 @pytest.mark.parametrize("path", GOLDENS, ids=lambda p: p.split("/")[-1])
-def test_counts_match_reference(ctx, path):
+@pytest.mark.parametrize("popcount", [False, True], ids=["default", "popcount"])
+def test_counts_match_reference(ctx, path, popcount):
     g = load_golden(path)
     seqs, typ = g["chars"], golden_type(g)
     L = seqs.shape[1]
-    fast = gpu_counts(ctx, seqs, typ)
+    fast = gpu_counts(ctx, seqs, typ, popcount=popcount)
     if typ == oracle.PROTEIN and L % 128 == 0:
         # the reference fast estimator's valid count is wrong here; ours is the
         # naive estimator's, which is correct
@@ -76,11 +79,12 @@ def test_counts_match_reference(ctx, path):
 
 @pytest.mark.parametrize("path", GOLDENS, ids=lambda p: p.split("/")[-1])
 @pytest.mark.parametrize("model", ["jc", "kim"])
-def test_matrices_match_reference(ctx, path, model):
+@pytest.mark.parametrize("popcount", [False, True], ids=["default", "popcount"])
+def test_matrices_match_reference(ctx, path, model, popcount):
     g = load_golden(path)
     seqs, typ = g["chars"], golden_type(g)
     L = seqs.shape[1]
-    got, _ = gpu_matrix(ctx, seqs, typ, model)
+    got, _ = gpu_matrix(ctx, seqs, typ, model, popcount=popcount)
     if typ == oracle.PROTEIN and L % 128 == 0:
         assert_matrix_parity(got, g[f"{model}_naive"])
         wrapped, _ = gpu_matrix(ctx, seqs, typ, model, compat_wrap=True)
@@ -106,18 +110,19 @@ SHAPES = [(1, 10), (2, 1), (3, 31), (5, 32), (17, 33), (127, 255), (128, 256), (
 
 
 @pytest.mark.parametrize("n,L", SHAPES)
-@pytest.mark.parametrize("kind", ["dna", "protein"])
+@pytest.mark.parametrize("kind", ["dna", "dna-popcount", "protein"])
 def test_random_alignments_vs_oracle(ctx, n, L, kind):
     from rapidnj_b200 import synth
     seed = n * 1000 + L
-    seqs = synth.tree_dna(n, L, seed=seed, mean_branch=0.1) if kind == "dna" else \
+    seqs = synth.tree_dna(n, L, seed=seed, mean_branch=0.1) if kind != "protein" else \
         synth.tree_protein(n, L, seed=seed, mean_branch=0.3)
-    typ = oracle.DNA if kind == "dna" else oracle.PROTEIN
+    typ = oracle.DNA if kind != "protein" else oracle.PROTEIN
+    pc = kind == "dna-popcount"
     c = oracle.counts(seqs, typ)
-    assert np.array_equal(gpu_counts(ctx, seqs, typ), c)
+    assert np.array_equal(gpu_counts(ctx, seqs, typ, popcount=pc), c)
     for model, mo in (("jc", oracle.JC), ("kim", oracle.KIMURA)):
         ref, rmax = oracle.matrix(c, L, typ, mo)
-        got, gmax = gpu_matrix(ctx, seqs, typ, model)
+        got, gmax = gpu_matrix(ctx, seqs, typ, model, popcount=pc)
         assert_matrix_parity(got, ref)
         assert abs(gmax - rmax) <= 1e-6 * max(1.0, rmax)
 
@@ -295,33 +300,28 @@ def test_full_size_k2p_properties(ctx):
 # ------------------------------------------------- tensor-core DNA kernel
 
 TC_SHAPES = [(2, 1), (3, 31), (17, 127), (128, 128), (129, 129), (200, 1000), (257, 4097),
-             (300, 300)]
+             (300, 300), (1, 5)]
 
 
 @pytest.mark.parametrize("n,L", TC_SHAPES)
 def test_tensor_core_counts_vs_oracle(ctx, n, L):
+    """DNA on the fast path runs on the tensor cores by default."""
     from rapidnj_b200 import synth
     seqs = synth.tree_dna(n, L, seed=n + 7 * L, mean_branch=0.15)
-    aln = ctx.alignment(seqs, oracle.DNA, tensor_cores=True)
-    out = torch.zeros(n * n * 3, dtype=torch.int32, device="cuda")
-    ctx.counts_into(aln, out)
-    got = out.cpu().numpy().view(np.uint32).reshape(n, n, 3)
-    assert np.array_equal(got, oracle.counts(seqs, oracle.DNA))
+    assert np.array_equal(gpu_counts(ctx, seqs, oracle.DNA), oracle.counts(seqs, oracle.DNA))
 
 
-@pytest.mark.parametrize("path", [p for p in GOLDENS if "dna" in p or "LGT" in p],
-                         ids=lambda p: p.split("/")[-1])
-@pytest.mark.parametrize("model", ["jc", "kim"])
-def test_tensor_core_matrices_match_reference(ctx, path, model):
-    g = load_golden(path)
-    aln = ctx.alignment(g["chars"], oracle.DNA, tensor_cores=True)
-    m = ctx.distance(aln, model)
-    assert_matrix_parity(m.to_numpy(), g[f"{model}_fast"])
+def test_tensor_core_full_rows_counts(ctx):
+    from rapidnj_b200 import synth
+    seqs = synth.tree_dna(150, 500, seed=5, mean_branch=0.2)
+    got = gpu_counts(ctx, seqs, oracle.DNA, full_rows=True)
+    assert np.array_equal(got, oracle.counts(seqs, oracle.DNA, full=True))
 
 
 def test_tensor_core_matches_popcount_kernel(ctx):
     from rapidnj_b200 import synth
     seqs = synth.tree_dna(1000, 3000, seed=21)
-    a = ctx.distance(ctx.alignment(seqs, oracle.DNA), "kim").to_numpy()
-    b = ctx.distance(ctx.alignment(seqs, oracle.DNA, tensor_cores=True), "kim").to_numpy()
-    assert np.array_equal(a, b)
+    for model in ("jc", "kim"):
+        a, am = gpu_matrix(ctx, seqs, oracle.DNA, model, popcount=True)
+        b, bm = gpu_matrix(ctx, seqs, oracle.DNA, model)
+        assert np.array_equal(a, b) and am == bm
