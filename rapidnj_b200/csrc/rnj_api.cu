@@ -138,6 +138,7 @@ struct rnj_ctx {
   bool profiling = false;
   cudaEvent_t ev[6] = {};             // pack, count, fix-up: begin/end pairs
   bool ev_used[3] = {false, false, false};
+  AlnDesc *d_desc = nullptr;          // one-alignment work list of the persistent kernel
 };
 
 struct rnj_aln {
@@ -336,6 +337,47 @@ EpiParams epi_for(rnj_ctx *ctx, const Packed &p, int model) {
   return ep;
 }
 
+// Work-list descriptor of one packed alignment for the persistent kernels.
+AlnDesc desc_for(const Packed &p, const EpiParams &ep) {
+  AlnDesc d;
+  memset(&d, 0, sizeof(d));
+  d.map = (p.kind == KIND_DNA_TC) ? p.fmap : p.tmap;
+  d.out = ep.out;
+  d.counts = ep.counts;
+  d.ld = ep.ld;
+  d.max_bits = ep.max_bits;
+  d.tile_flags = ep.tile_flags;
+  d.err = ep.err;
+  d.n = p.n;
+  d.L = p.L;
+  d.nt = tiles_of(p.n);
+  d.kdim = (p.kind == KIND_DNA_TC) ? p.Lk : p.Wp;
+  d.model = ep.model;
+  d.type = ep.type;
+  d.compat = ep.compat_wrap;
+  d.full = ep.full;
+  d.kind = p.kind;
+  d.np = p.NP;
+  d.jc_b = ep.jc_b;
+  return d;
+}
+
+// One alignment through the persistent tensor-core kernel: its triangle (or
+// full) tiles are the work list, one CTA per SM.
+int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mode) {
+  const int nt = tiles_of(p.n);
+  const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
+  AlnDesc d = desc_for(p, ep);
+  // Pageable source: the copy is taken before the call returns, so the stack
+  // descriptor may go out of scope.
+  RNJ_CUDA(cudaMemcpyAsync(ctx->d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream),
+           "descriptor upload");
+  const int grid = (int)std::min<long long>(ntiles, ctx->num_sms);
+  RNJ_CUDA(launch_tc_batch(ctx->d_desc, nullptr, nullptr, (int)ntiles, grid, epi_mode, ctx->stream),
+           "tensor-core kernel");
+  return RNJ_OK;
+}
+
 int check_device_error(rnj_ctx *ctx) {
   RNJ_CUDA(cudaMemcpyAsync(ctx->h_max + 1, ctx->scratch.words + 1, sizeof(int),
                            cudaMemcpyDeviceToHost, ctx->stream),
@@ -366,8 +408,8 @@ int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t 
   const int nk = p.Wp / kKW;
   mark(ctx, 1, 0);
   if (p.kind == KIND_DNA_TC) {
-    // int32 tensor-memory accumulators: exact for any L, no split needed.
-    RNJ_CUDA(launch_tc_count(p.fmap, p.n, p.Lk, EPI_DIST, ep, ctx->stream), "tensor-core kernel");
+    rc = run_tc_single(ctx, p, ep, EPI_DIST);
+    if (rc != RNJ_OK) return rc;
   } else if (nk <= kMaxFusedWords / kKW) {
     RNJ_CUDA(launch_count_tiles(p, ckind, EPI_DIST, ep, ctx->stream), "count kernel");
   } else {
@@ -417,6 +459,7 @@ int rnj_ctx_create(int device, rnj_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_mask, 8 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_mask, 8 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_max, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_desc, sizeof(AlnDesc));
   if (e != cudaSuccess) {
     rnj_ctx_destroy(c);
     return cuda_error(e, "context setup");
@@ -443,6 +486,7 @@ int rnj_ctx_destroy(rnj_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->scratch.words) cudaFree(ctx->scratch.words);
   if (ctx->d_mask) cudaFree(ctx->d_mask);
+  if (ctx->d_desc) cudaFree(ctx->d_desc);
   if (ctx->h_mask) cudaFreeHost(ctx->h_mask);
   if (ctx->h_max) cudaFreeHost(ctx->h_max);
   for (int b = 0; b < 2; ++b)
@@ -710,7 +754,8 @@ int rnj_counts_into(rnj_ctx *ctx, rnj_aln *aln, unsigned int *d_counts) {
   ep.full = (p.flags & RNJ_FULL_ROWS) ? 1 : 0;
   ep.counts = d_counts;
   if (p.kind == KIND_DNA_TC) {
-    RNJ_CUDA(launch_tc_count(p.fmap, p.n, p.Lk, EPI_COUNTS, ep, ctx->stream), "tensor-core kernel");
+    rc = run_tc_single(ctx, p, ep, EPI_COUNTS);
+    if (rc != RNJ_OK) return rc;
     return check_device_error(ctx);
   }
   const int nk = p.Wp / kKW;

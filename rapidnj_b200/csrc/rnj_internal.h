@@ -72,6 +72,28 @@ struct EpiParams {
   int *err = nullptr;         // device error word (bit 0: a bounded wait ran out)
 };
 
+// One alignment of a work list, as the persistent kernels read it from device
+// memory: its TMA map, output, scratch slots and transform parameters.
+struct alignas(128) AlnDesc {
+  CUtensorMap map;            // features (tensor-core kind) or planes (popcount kinds)
+  float *out;                 // n rows of ld floats (distances), or null in count mode
+  uint32_t *counts;           // n*n*3 counts (count mode), or null
+  unsigned long long ld;
+  int *max_bits;              // per-alignment max slot (float bits)
+  int *tile_flags;            // per-alignment saturation flags, one per triangle tile
+  int *err;                   // shared error word
+  int n, L, nt, kdim;         // kdim: Lk (tensor-core) or Wp (popcount)
+  int model, type, compat, full;
+  int kind, np, pad0, pad1;
+  double jc_b;
+};
+
+// A work item: alignment index and linear triangle-tile index within it.
+struct WorkItem {
+  int aln;
+  int tile;
+};
+
 // Scratch of one distance call: the max slot, the error word and the per-tile
 // saturation flags (device), plus the split-K count buffer for long alignments.
 struct Scratch {
@@ -95,8 +117,10 @@ cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s)
 // Tensor-core DNA path (rnj_tc.cu).
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
                                  int8_t *F, cudaStream_t s);
-cudaError_t launch_tc_count(const CUtensorMap &fmap, int n, int Lk, int epi_mode,
-                            const EpiParams &ep, cudaStream_t s);
+// Persistent over work items; d_items == nullptr means items (0, 0..nitems-1) of
+// d_descs[0]; d_nitems == nullptr means nitems is the count.
+cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
+                            int nitems, int grid, int epi_mode, cudaStream_t s);
 
 enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2 };
 

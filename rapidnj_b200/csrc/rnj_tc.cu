@@ -14,14 +14,17 @@
 // v block (K = L), the r block (K = L) and the t|u block (K = 2L): 4 int8 MACs
 // per pair-column, accumulated in int32 in tensor memory.
 //
-// Kernel.  One CTA per 128 x 128 tile of the upper triangle, 320 threads:
+// Kernel.  Persistent, one CTA per SM, over a work list of 128 x 128 triangle
+// tiles (of one alignment, or of many in a batch), 320 threads:
 //   warp 0       TMA producer: 128-row x 128-byte K-blocks of both row tiles,
 //                128-byte swizzle, into a 6-stage mbarrier ring
 //   warp 1       TMEM owner and MMA issuer: tcgen05.mma.kind::i8, M = N = 128,
 //                K = 32 per instruction, three accumulators (V, R, T) of 128
 //                columns each; tcgen05.commit releases stages and signals the end
-//   warps 2..9   epilogue: tcgen05.ld of the accumulators, the exact transform,
-//                shared-memory staging and coalesced stores (tile and mirror)
+//   warps 2..9   epilogue: per 32-column chunk, tcgen05.ld of the accumulators,
+//                the exact transform and the stores (tile rows as float4, the
+//                mirror image with warp-coalesced column stores); then TMEM is
+//                handed back to the MMA warp
 // Every wait is bounded; on a timeout the CTA records an error, drains what it
 // issued, frees its tensor memory and ends.
 #include <cuda.h>
@@ -179,40 +182,70 @@ __global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t l
 }
 
 // ----------------------------------------------------------------- the kernel
+//
+// Persistent over a work list of (alignment, triangle tile) items: CTA b takes
+// items b, b + G, b + 2G, ... (the list is ordered by decreasing cost, so this
+// round robin balances).  Stage counters run on across items, so the producer
+// streams the next tile's operands while the epilogue of the current one runs
+// (the epilogue works from tensor memory and registers only, never from the
+// stage buffers); the MMA warp waits for the epilogue's hand-back of tensor
+// memory before it overwrites the accumulators.
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                   reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
+__device__ __forceinline__ void item_tile(const AlnDesc &d, int tile, int &ti, int &tj) {
+  if (d.full) {
+    ti = tile / d.nt;
+    tj = tile % d.nt;
+  } else {
+    tri_coords(tile, d.nt, ti, tj);
+  }
+}
+
+__device__ __forceinline__ WorkItem item_at(const WorkItem *items, int it) {
+  if (items) return items[it];
+  WorkItem w;
+  w.aln = 0;
+  w.tile = it;
+  return w;
+}
 
 template <int EPI>
 __global__ void __launch_bounds__(kTcThreads, 1)
-    tc_count_kernel(const __grid_constant__ CUtensorMap fmap, int nt, int Lk, EpiParams ep) {
+    tc_batch_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
+                    const int *__restrict__ nitems_ptr, int nitems_direct) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem =
       reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + kTcStages * kTcStageBytes);
   uint64_t *empty_bar = full_bar + kTcStages;
-  uint64_t *acc_bar = empty_bar + kTcStages;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_bar + 1);
+  uint64_t *acc_full = empty_bar + kTcStages;
+  uint64_t *tmem_empty = acc_full + 1;
+  uint64_t *drain_bar = tmem_empty + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain_bar + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int ti, tj;
-  const int tile_id = blockIdx.x;
-  if (ep.full) {
-    ti = tile_id / nt;
-    tj = tile_id % nt;
-  } else {
-    tri_coords(tile_id, nt, ti, tj);
-  }
-  const int nkb = 4 * Lk / kTcKBlock;   // k-blocks over the whole feature row
-  const int seg = Lk / kTcKBlock;       // k-blocks per feature block
+  const int nitems = nitems_ptr ? *nitems_ptr : nitems_direct;
 
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(acc_bar, 1);
+    mbar_init(acc_full, 1);
+    mbar_init(tmem_empty, 256);
+    mbar_init(drain_bar, 1);
     *abort_flag = 0;
     fence_mbar_init();
-    prefetch_tmap(&fmap);
   }
   if (warp == 1) {
     tmem_alloc(tmem_slot, kTmemCols);
@@ -222,120 +255,193 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  int issued = 0;  // k-blocks whose loads the producer issued (thread 0 only)
+  uint32_t issued = 0;  // producer: k-blocks issued in total (thread 0 only)
 
   if (warp == 0) {
     if (lane == 0) {
-      // Producer.
-      for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % kTcStages;
-        if (!tc_wait(&empty_bar[s], (uint32_t)(((kb / kTcStages) & 1) ^ 1), abort_flag)) {
-          *abort_flag = 1;
-          break;
+      // ----------------------------------------------------------- producer
+      uint32_t gkb = 0;
+      for (int it = blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x) {
+        const WorkItem w = item_at(items, it);
+        const AlnDesc &d = descs[w.aln];
+        tensormap_acquire(&d.map);
+        int ti, tj;
+        item_tile(d, w.tile, ti, tj);
+        const int nkb = 4 * d.kdim / kTcKBlock;
+        for (int kb = 0; kb < nkb; ++kb, ++gkb) {
+          const int s = gkb % kTcStages;
+          if (!tc_wait(&empty_bar[s], ((gkb / kTcStages) & 1) ^ 1, abort_flag)) {
+            *abort_flag = 1;
+            break;
+          }
+          uint8_t *a = smem + s * kTcStageBytes;
+          mbar_arrive_expect_tx(&full_bar[s], kTcStageBytes);
+          tma_load_2d(a, &d.map, &full_bar[s], kb * kTcKBlock, ti * kTile);
+          tma_load_2d(a + kTcTileBytes, &d.map, &full_bar[s], kb * kTcKBlock, tj * kTile);
+          issued = gkb + 1;
         }
-        uint8_t *a = smem + s * kTcStageBytes;
-        mbar_arrive_expect_tx(&full_bar[s], kTcStageBytes);
-        tma_load_2d(a, &fmap, &full_bar[s], kb * kTcKBlock, ti * kTile);
-        tma_load_2d(a + kTcTileBytes, &fmap, &full_bar[s], kb * kTcKBlock, tj * kTile);
-        issued = kb + 1;
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      // MMA issuer.
-      int issued_kb = 0;
-      for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % kTcStages;
-        if (!tc_wait(&full_bar[s], (uint32_t)((kb / kTcStages) & 1), abort_flag)) {
+      // -------------------------------------------------------- MMA issuer
+      uint32_t gkb = 0, titer = 0;
+      for (int it = blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x, ++titer) {
+        const WorkItem w = item_at(items, it);
+        const AlnDesc &d = descs[w.aln];
+        const int nkb = 4 * d.kdim / kTcKBlock;
+        const int seg = d.kdim / kTcKBlock;
+        // The epilogue of the previous item must have read the accumulators.
+        if (!tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag)) {
           *abort_flag = 1;
           break;
         }
         tc_fence_after();
-        const int acc = kb < seg ? 0 : (kb < 2 * seg ? 1 : 2);
-        const bool first = (kb == 0) || (kb == seg) || (kb == 2 * seg);
-        const uint32_t a_addr = smem_u32(smem + s * kTcStageBytes);
-        const uint64_t adesc = smem_desc_sw128(a_addr);
-        const uint64_t bdesc = smem_desc_sw128(a_addr + kTcTileBytes);
+        bool ok = true;
+        for (int kb = 0; kb < nkb; ++kb, ++gkb) {
+          const int s = gkb % kTcStages;
+          if (!tc_wait(&full_bar[s], (gkb / kTcStages) & 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int acc = kb < seg ? 0 : (kb < 2 * seg ? 1 : 2);
+          const bool first = (kb == 0) || (kb == seg) || (kb == 2 * seg);
+          const uint32_t a_addr = smem_u32(smem + s * kTcStageBytes);
+          const uint64_t adesc = smem_desc_sw128(a_addr);
+          const uint64_t bdesc = smem_desc_sw128(a_addr + kTcTileBytes);
 #pragma unroll
-        for (int kk = 0; kk < kTcKBlock / 32; ++kk)
-          tc_mma_i8(tmem + acc * kTile, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2),
-                    kIdescI8, (first && kk == 0) ? 0u : 1u);
-        tc_commit(&empty_bar[s]);
-        issued_kb = kb + 1;
+          for (int kk = 0; kk < kTcKBlock / 32; ++kk)
+            tc_mma_i8(tmem + acc * kTile, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2),
+                      kIdescI8, (first && kk == 0) ? 0u : 1u);
+          tc_commit(&empty_bar[s]);
+        }
+        if (!ok) {
+          *abort_flag = 1;
+          break;
+        }
+        tc_commit(acc_full);
       }
-      // Completion of every MMA issued (also on an abort, so that tensor memory
-      // is not freed under a running MMA).
-      tc_commit(acc_bar);
-      if (issued_kb < nkb) {
-        mbar_wait_bounded(acc_bar, 0);
-      }
+      // Every MMA issued has completed before tensor memory is released.
+      tc_commit(drain_bar);
+      mbar_wait_bounded(drain_bar, 0);
     }
   } else {
-    // Epilogue: warps 2..9.  TMEM lane quarter = warp % 4; column half by group.
+    // ----------------------------------------------------------- epilogue
+    // Warps 2..9: TMEM lane quarter = warp % 4 (row block), column half by group.
     const int q = warp & 3;
     const int half = (warp - 2) >> 2;
     const int row = 32 * q + lane;
-    float *S = reinterpret_cast<float *>(smem);
-    bool ok = tc_wait(acc_bar, 0, abort_flag);
-    if (!ok) *abort_flag = 1;
-    named_barrier(1, 256);
-    ok = (*abort_flag == 0);
-    tc_fence_after();
-    float tmax = 0.0f;
-    bool sat = false;
-    if (ok) {
+    uint32_t titer = 0;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++titer) {
+      const WorkItem w = item_at(items, it);
+      const AlnDesc &d = descs[w.aln];
+      int ti, tj;
+      item_tile(d, w.tile, ti, tj);
+      if (!tc_wait(acc_full, titer & 1, abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const int n = d.n;
       const int i = ti * kTile + row;
+      EpiParams ep;
+      ep.n = n;
+      ep.L = d.L;
+      ep.model = d.model;
+      ep.type = d.type;
+      ep.compat_wrap = d.compat;
+      ep.full = d.full;
+      ep.jc_b = d.jc_b;
+      float tmax = 0.0f;
+      bool sat = false;
+      // Per 32-column chunk: accumulators -> counts -> distances -> stores.
 #pragma unroll 1
       for (int cc = 0; cc < 2; ++cc) {
-        const int c0 = half * 64 + cc * 32;
         uint32_t V[32], R[32], T[32];
-        const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0;
+        const int cbase = half * 64 + cc * 32;
+        const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)cbase;
         tmem_ld32(base, V);
         tmem_ld32(base + kTile, R);
         tmem_ld32(base + 2 * kTile, T);
         tmem_ld_wait();
+        const int jb = tj * kTile + cbase;
+        if constexpr (EPI == EPI_DIST) {
+          float *orow = d.out + (size_t)i * d.ld;
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          const int j = tj * kTile + c0 + k;
-          const int vv = (int)V[k], rr = (int)R[k], tu = (int)T[k];
-          const uint32_t valid = (uint32_t)vv;
-          const uint32_t ts = (uint32_t)((vv + rr - tu) >> 2);
-          const uint32_t tv = (uint32_t)((vv - rr) >> 1);
-          const bool pair_ok = ep.full ? (i < ep.n && j < ep.n && i != j) : (i < j && j < ep.n);
-          if constexpr (EPI == EPI_DIST) {
-            float x = 0.0f;
-            if (pair_ok) {
-              x = pair_distance(ep, ep.model == RNJ_JC ? ts + tv : ts, ep.model == RNJ_JC ? 0u : tv,
-                                valid);
-              if (x > tmax) tmax = x;
-              if (x == -1.0f) sat = true;
+          for (int c4 = 0; c4 < 32; c4 += 4) {
+            float x[4];
+            bool okc[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int k = c4 + u;
+              const int j = jb + k;
+              const int vv = (int)V[k], rr = (int)R[k], tu = (int)T[k];
+              const uint32_t ts = (uint32_t)((vv + rr - tu) >> 2);
+              const uint32_t tv = (uint32_t)((vv - rr) >> 1);
+              okc[u] = d.full ? (i < n && j < n && i != j) : (i < j && j < n);
+              x[u] = 0.0f;
+              if (okc[u]) {
+                x[u] = pair_distance(ep, d.model == RNJ_JC ? ts + tv : ts,
+                                     d.model == RNJ_JC ? 0u : tv, (uint32_t)vv);
+                if (x[u] > tmax) tmax = x[u];
+                if (x[u] == -1.0f) sat = true;
+              }
+              // Mirror (column j of the tile is row j of the matrix): the lanes of
+              // a warp hold 32 consecutive rows i, so these stores coalesce.
+              if (okc[u] && !d.full) d.out[(size_t)j * d.ld + i] = x[u];
             }
-            S[row * kStageLd + c0 + k] = x;
-          } else {
-            if (pair_ok || (ep.full && i < ep.n && j < ep.n)) {
-              uint32_t *o = ep.counts + ((size_t)i * ep.n + j) * 3;
-              o[0] = ts;
-              o[1] = tv;
-              o[2] = valid;
+            const int j0 = jb + c4;
+            if (okc[0] && okc[1] && okc[2] && okc[3] && ((d.ld & 3) == 0)) {
+              *reinterpret_cast<float4 *>(orow + j0) = make_float4(x[0], x[1], x[2], x[3]);
+            } else {
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const int j = j0 + u;
+                if (okc[u]) orow[j] = x[u];
+                else if (i == j && i < n) orow[j] = 0.0f;
+              }
+            }
+          }
+        } else {
+          if (i < n) {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+              const int j = jb + k;
+              const bool ok = d.full ? (j < n) : (i < j && j < n);
+              if (!ok) continue;
+              const int vv = (int)V[k], rr = (int)R[k], tu = (int)T[k];
+              uint32_t *o = d.counts + ((size_t)i * n + j) * 3;
+              o[0] = (uint32_t)((vv + rr - tu) >> 2);
+              o[1] = (uint32_t)((vv - rr) >> 1);
+              o[2] = (uint32_t)vv;
             }
           }
         }
       }
+      // Accumulators read: the MMA warp may start the next item.
+      tc_fence_before();
+      mbar_arrive(tmem_empty);
+      if constexpr (EPI == EPI_DIST) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+          tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, off));
+        const bool any_sat = __any_sync(0xffffffffu, sat);
+        if (lane == 0) {
+          if (tmax > 0.0f) atomicMax(d.max_bits, __float_as_int(tmax));
+          if (any_sat) d.tile_flags[w.tile] = 1;
+        }
+      }
     }
-    tc_fence_before();
-    named_barrier(1, 256);
-    if constexpr (EPI == EPI_DIST) {
-      if (ok) store_distances(ep, ti, tj, tile_id, S, tmax, sat, warp - 2, 8);
-    }
-    if (!ok && tid == 64) atomicOr(ep.err, 1);
   }
+
   __syncthreads();
   if (tid == 0 && *abort_flag) {
-    // After an abort, loads may still be in flight into stages the MMA never
-    // consumed: let the last ring's worth land (bounded) before the shared
-    // memory is released.
-    for (int kb = issued > kTcStages ? issued - kTcStages : 0; kb < issued; ++kb)
-      mbar_wait_bounded(&full_bar[kb % kTcStages], (uint32_t)((kb / kTcStages) & 1));
+    // Loads may still be in flight into stages the MMA never consumed: let the
+    // last ring's worth land (bounded) before shared memory is released.
+    for (uint32_t k = issued > (uint32_t)kTcStages ? issued - kTcStages : 0; k < issued; ++k)
+      mbar_wait_bounded(&full_bar[k % kTcStages], (k / kTcStages) & 1);
+    atomicOr(descs[0].err, 1);
   }
   __syncthreads();
   if (warp == 1) {
@@ -356,22 +462,22 @@ cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L
   return cudaGetLastError();
 }
 
-cudaError_t launch_tc_count(const CUtensorMap &fmap, int n, int Lk, int epi_mode, const EpiParams &ep,
-                            cudaStream_t s) {
-  const int nt = tiles_of(n);
-  const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
-  if (ntiles == 0) return cudaSuccess;
+cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
+                            int nitems, int grid, int epi_mode, cudaStream_t s) {
+  if (grid <= 0) return cudaSuccess;
   cudaError_t e;
   if (epi_mode == EPI_DIST) {
-    e = cudaFuncSetAttribute(tc_count_kernel<EPI_DIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(tc_batch_kernel<EPI_DIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTcSmemBytes);
     if (e != cudaSuccess) return e;
-    tc_count_kernel<EPI_DIST><<<(unsigned)ntiles, kTcThreads, kTcSmemBytes, s>>>(fmap, nt, Lk, ep);
+    tc_batch_kernel<EPI_DIST><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(d_descs, d_items,
+                                                                               d_nitems, nitems);
   } else {
-    e = cudaFuncSetAttribute(tc_count_kernel<EPI_COUNTS>,
+    e = cudaFuncSetAttribute(tc_batch_kernel<EPI_COUNTS>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes);
     if (e != cudaSuccess) return e;
-    tc_count_kernel<EPI_COUNTS><<<(unsigned)ntiles, kTcThreads, kTcSmemBytes, s>>>(fmap, nt, Lk, ep);
+    tc_batch_kernel<EPI_COUNTS><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(d_descs, d_items,
+                                                                                 d_nitems, nitems);
   }
   return cudaGetLastError();
 }
