@@ -189,6 +189,39 @@ int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld, int type,
 int rnj_distance_matrix_host(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
                              int type, int model, int flags, float *out, float *max_out);
 
+/* ------------------------------------------------------------------ batches */
+
+/* Many alignments computed together.  The triangle tiles of every alignment
+ * added form one device work list, ordered by decreasing cost, that one
+ * persistent launch per kernel family consumes (the tensor-core kernel for DNA,
+ * the bit-plane kernel for protein and -f alignments), followed by the
+ * saturation fix-up; the launch sequence is captured once, at creation, in a
+ * CUDA graph, and a run only uploads the descriptors and work lists the graph
+ * reads.  For a stream of alignments this replaces one driver call per
+ * alignment (JCdistance / KimuraDistance per input, or per bootstrap replicate
+ * of main.cpp:519-532).  Capacities bound the alignments and the total tiles
+ * (128 x 128 pairs each, (ceil(n/128)+1)*ceil(n/128)/2 per alignment).  The
+ * alignments added must stay alive until the run has completed.  Bit-plane
+ * alignments longer than 65280 columns are not batched (use rnj_distance). */
+typedef struct rnj_batch rnj_batch;
+int rnj_batch_create(rnj_ctx *ctx, int max_alignments, long long max_tiles, rnj_batch **out);
+/* Adds an alignment; d_out NULL lets the batch allocate the n x n output.  The
+ * slot index identifies the alignment in this batch. */
+int rnj_batch_add(rnj_batch *batch, rnj_aln *aln, int model, float *d_out, size_t ld, int *slot);
+/* Runs the batch asynchronously after the work already queued on the context
+ * stream; later work on that stream sees the results. */
+int rnj_batch_run(rnj_batch *batch);
+int rnj_batch_synchronize(rnj_batch *batch);
+/* The output of a slot (device pointer and stride); max_out (may be NULL)
+ * waits for the run and reads the slot's maximum distance. */
+int rnj_batch_output(rnj_batch *batch, int slot, float **d_out, size_t *ld, float *max_out);
+/* Moves a batch-allocated output into a matrix handle (for rnj_mat_copy_rows). */
+int rnj_batch_take(rnj_batch *batch, int slot, rnj_mat **out);
+int rnj_batch_size(rnj_batch *batch, int *alignments, long long *tiles);
+/* Forgets the alignments (frees outputs still owned by the batch); the graph stays. */
+int rnj_batch_clear(rnj_batch *batch);
+int rnj_batch_destroy(rnj_batch *batch);
+
 /* ------------------------------------------------------- alignment files */
 
 /* A parsed multiple alignment on the host: names and n*L bytes (row-major). */

@@ -68,6 +68,15 @@ SIGNATURES = {
                                          c_int, c_void_p, P(c_float)]),
     "rnj_distance_noalloc": (c_int, [c_void_p, c_int, c_int, c_size_t, c_int, c_int, c_int,
                                      c_void_p, c_size_t, c_void_p, P(c_float)]),
+    "rnj_batch_create": (c_int, [c_void_p, c_int, ctypes.c_longlong, P(c_void_p)]),
+    "rnj_batch_add": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_size_t, P(c_int)]),
+    "rnj_batch_run": (c_int, [c_void_p]),
+    "rnj_batch_synchronize": (c_int, [c_void_p]),
+    "rnj_batch_output": (c_int, [c_void_p, c_int, P(c_void_p), P(c_size_t), P(c_float)]),
+    "rnj_batch_take": (c_int, [c_void_p, c_int, P(c_void_p)]),
+    "rnj_batch_size": (c_int, [c_void_p, P(c_int), P(ctypes.c_longlong)]),
+    "rnj_batch_clear": (c_int, [c_void_p]),
+    "rnj_batch_destroy": (c_int, [c_void_p]),
     "rnj_msa_read": (c_int, [c_char_p, c_char_p, P(c_void_p)]),
     "rnj_msa_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
     "rnj_msa_name": (c_char_p, [c_void_p, c_int]),

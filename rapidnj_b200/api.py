@@ -222,6 +222,64 @@ class Context:
             pass
 
 
+class Batch:
+    """Many alignments in one persistent pass (rnj_batch): a device work list of
+    all their tiles, consumed by graph-captured persistent kernels."""
+
+    def __init__(self, ctx: Context, max_alignments: int = 1024, max_tiles: int = 1 << 20):
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_batch_create(ctx.handle, max_alignments, max_tiles, ctypes.byref(h)))
+        self.ctx = ctx
+        self.handle = h
+        self._keep = []
+
+    def add(self, aln: Alignment, model="kim", out=None) -> int:
+        """Adds a packed alignment; out (CUDA float32 tensor n x >= n) or None."""
+        slot = ctypes.c_int()
+        ptr = ctypes.c_void_p(out.data_ptr()) if out is not None else None
+        ld = out.stride(0) if out is not None else 0
+        check(N.lib().rnj_batch_add(self.handle, aln.handle, MODELS[model], ptr, ld,
+                                    ctypes.byref(slot)))
+        self._keep.append(aln)
+        return slot.value
+
+    def run(self) -> None:
+        check(N.lib().rnj_batch_run(self.handle))
+
+    def synchronize(self) -> None:
+        check(N.lib().rnj_batch_synchronize(self.handle))
+
+    def max(self, slot: int) -> float:
+        m = ctypes.c_float()
+        check(N.lib().rnj_batch_output(self.handle, slot, None, None, ctypes.byref(m)))
+        return m.value
+
+    def take(self, slot: int) -> Matrix:
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_batch_take(self.handle, slot, ctypes.byref(h)))
+        return Matrix(self.ctx, h.value)
+
+    def size(self):
+        a, t = ctypes.c_int(), ctypes.c_longlong()
+        check(N.lib().rnj_batch_size(self.handle, ctypes.byref(a), ctypes.byref(t)))
+        return a.value, t.value
+
+    def clear(self) -> None:
+        check(N.lib().rnj_batch_clear(self.handle))
+        self._keep = []
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().rnj_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # --- alignment files (host only) -------------------------------------------------
 
 def read_alignment(path: str, fmt: str | None = None):

@@ -14,6 +14,7 @@
 
 #include "rnj.h"
 #include "rnj_internal.h"
+#include "rnj_objects.h"
 
 namespace rnj {
 
@@ -121,54 +122,50 @@ void dna_lut(bool naive, uint8_t lut[256]) {
   }
 }
 
+// Transform parameters of a packed alignment (scratch pointers left null).
+EpiParams epi_params_for(const Packed &p, int model) {
+  EpiParams ep;
+  ep.n = p.n;
+  ep.L = p.L;
+  ep.model = model;
+  ep.type = p.type;
+  ep.compat_wrap = (p.type == RNJ_PROTEIN && (p.flags & RNJ_FASTDIST) &&
+                    (p.flags & RNJ_COMPAT_PROTEIN_WRAP)) ? 1 : 0;
+  ep.full = (p.kind == KIND_NAIVE && (p.flags & RNJ_FULL_ROWS)) ? 1 : 0;
+  ep.jc_b = (p.type == RNJ_PROTEIN) ? (20.0 - 1) / 20.0 : (4.0 - 1) / 4.0;
+  return ep;
+}
+
+// Work-list descriptor of one packed alignment for the persistent kernels.
+AlnDesc desc_for(const Packed &p, const EpiParams &ep) {
+  AlnDesc d;
+  memset(&d, 0, sizeof(d));
+  d.map = (p.kind == KIND_DNA_TC) ? p.fmap : p.tmap;
+  d.out = ep.out;
+  d.counts = ep.counts;
+  d.ld = ep.ld;
+  d.max_bits = ep.max_bits;
+  d.tile_flags = ep.tile_flags;
+  d.err = ep.err;
+  d.n = p.n;
+  d.L = p.L;
+  d.nt = tiles_of(p.n);
+  d.kdim = (p.kind == KIND_DNA_TC) ? p.Lk : p.Wp;
+  d.model = ep.model;
+  d.type = ep.type;
+  d.compat = ep.compat_wrap;
+  d.full = ep.full;
+  d.kind = p.kind;
+  d.np = p.NP;
+  d.jc_b = ep.jc_b;
+  return d;
+}
+
 }  // namespace rnj
 
 using namespace rnj;
 
-struct rnj_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int num_sms = 148;
-  Scratch scratch;
-  uint32_t *d_mask = nullptr;        // presence mask (8 words)
-  uint32_t *h_mask = nullptr;        // pinned
-  int *h_max = nullptr;              // pinned max bits / error word
-  void *h_stage[2] = {nullptr, nullptr};  // pinned staging for copy-out / upload
-  size_t stage_cap = 0;
-  bool profiling = false;
-  cudaEvent_t ev[6] = {};             // pack, count, fix-up: begin/end pairs
-  bool ev_used[3] = {false, false, false};
-  AlnDesc *d_desc = nullptr;          // one-alignment work list of the persistent kernel
-};
-
-struct rnj_aln {
-  rnj_ctx *ctx = nullptr;
-  Packed p;
-};
-
-struct rnj_mat {
-  rnj_ctx *ctx = nullptr;
-  float *d = nullptr;
-  int n = 0;
-  size_t ld = 0;
-  int *d_max = nullptr;  // device copy of the max bits
-  bool owns = true;
-};
-
 namespace {
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 void mark(rnj_ctx *ctx, int stage, int end) {
   if (!ctx->profiling) return;
@@ -322,44 +319,11 @@ int count_kind_for(const Packed &p, int model) {
 }
 
 EpiParams epi_for(rnj_ctx *ctx, const Packed &p, int model) {
-  EpiParams ep;
-  ep.n = p.n;
-  ep.L = p.L;
-  ep.model = model;
-  ep.type = p.type;
-  ep.compat_wrap = (p.type == RNJ_PROTEIN && (p.flags & RNJ_FASTDIST) &&
-                    (p.flags & RNJ_COMPAT_PROTEIN_WRAP)) ? 1 : 0;
-  ep.full = (p.kind == KIND_NAIVE && (p.flags & RNJ_FULL_ROWS)) ? 1 : 0;
-  ep.jc_b = (p.type == RNJ_PROTEIN) ? (20.0 - 1) / 20.0 : (4.0 - 1) / 4.0;
+  EpiParams ep = epi_params_for(p, model);
   ep.max_bits = ctx->scratch.words;
   ep.err = ctx->scratch.words + 1;
   ep.tile_flags = ctx->scratch.words + 2;
   return ep;
-}
-
-// Work-list descriptor of one packed alignment for the persistent kernels.
-AlnDesc desc_for(const Packed &p, const EpiParams &ep) {
-  AlnDesc d;
-  memset(&d, 0, sizeof(d));
-  d.map = (p.kind == KIND_DNA_TC) ? p.fmap : p.tmap;
-  d.out = ep.out;
-  d.counts = ep.counts;
-  d.ld = ep.ld;
-  d.max_bits = ep.max_bits;
-  d.tile_flags = ep.tile_flags;
-  d.err = ep.err;
-  d.n = p.n;
-  d.L = p.L;
-  d.nt = tiles_of(p.n);
-  d.kdim = (p.kind == KIND_DNA_TC) ? p.Lk : p.Wp;
-  d.model = ep.model;
-  d.type = ep.type;
-  d.compat = ep.compat_wrap;
-  d.full = ep.full;
-  d.kind = p.kind;
-  d.np = p.NP;
-  d.jc_b = ep.jc_b;
-  return d;
 }
 
 // One alignment through the persistent tensor-core kernel: its triangle (or

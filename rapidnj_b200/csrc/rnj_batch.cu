@@ -1,0 +1,337 @@
+// rnj_batch.cu -- many alignments in one pass: a device work list of the
+// triangle tiles of every alignment in the batch, ordered by decreasing cost,
+// consumed by one persistent launch per kernel family (the tcgen05 kernel for
+// DNA, the bit-plane kernel for protein and -f alignments) and a fix-up over the
+// flagged tiles.  The launch sequence is captured once in a CUDA graph; a run
+// only uploads the descriptors and work lists the graph's kernels read.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "rnj.h"
+#include "rnj_internal.h"
+#include "rnj_objects.h"
+
+using namespace rnj;
+
+namespace {
+
+#define RNJ_CUDA(call, what)                                \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_error(e_, what);     \
+  } while (0)
+
+struct Entry {
+  rnj_aln *aln;
+  int model;
+  float *out;
+  size_t ld;
+  bool owned;
+  long long flag_off;  // offset of this alignment's tile flags
+  long long ntiles;
+};
+
+}  // namespace
+
+struct rnj_batch {
+  rnj_ctx *ctx = nullptr;
+  int cap_aln = 0;
+  long long cap_tiles = 0;
+  cudaStream_t stream = nullptr;  // capture / launch stream (non-blocking)
+  cudaEvent_t ev_ready = nullptr, ev_uploaded = nullptr, ev_done = nullptr;
+  bool uploaded_pending = false;
+  // device
+  AlnDesc *d_descs = nullptr;
+  WorkItem *d_items_tc = nullptr, *d_items_pc = nullptr;
+  int *d_ints = nullptr;  // [0] tensor-core items, [1] popcount items, [2] item counter, [3] error
+  int *d_max = nullptr;   // per-alignment max bits
+  int *d_flags = nullptr; // per-tile saturation flags of all alignments
+  // pinned host staging of the uploads
+  AlnDesc *h_descs = nullptr;
+  WorkItem *h_items_tc = nullptr, *h_items_pc = nullptr;
+  int *h_ints = nullptr;
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<Entry> entries;
+  long long tiles_used = 0;
+};
+
+namespace {
+
+void free_batch(rnj_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto &e : b->entries)
+    if (e.owned && e.out) cudaFreeAsync(e.out, b->ctx->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  cudaFree(b->d_descs);
+  cudaFree(b->d_items_tc);
+  cudaFree(b->d_items_pc);
+  cudaFree(b->d_ints);
+  cudaFree(b->d_max);
+  cudaFree(b->d_flags);
+  cudaFreeHost(b->h_descs);
+  cudaFreeHost(b->h_items_tc);
+  cudaFreeHost(b->h_items_pc);
+  cudaFreeHost(b->h_ints);
+  if (b->ev_ready) cudaEventDestroy(b->ev_ready);
+  if (b->ev_uploaded) cudaEventDestroy(b->ev_uploaded);
+  if (b->ev_done) cudaEventDestroy(b->ev_done);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+// Captures: clear scratch -> tensor-core kernel -> popcount kernel -> fix-up.
+int capture_graph(rnj_batch *b) {
+  const int sms = b->ctx->num_sms;
+  RNJ_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaError_t e = cudaMemsetAsync(b->d_max, 0, sizeof(int) * b->cap_aln, b->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_flags, 0, sizeof(int) * b->cap_tiles, b->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ints + 2, 0, 2 * sizeof(int), b->stream);
+  if (e == cudaSuccess)
+    e = launch_tc_batch(b->d_descs, b->d_items_tc, b->d_ints + 0, 0, sms, EPI_DIST, b->stream);
+  if (e == cudaSuccess)
+    e = launch_count_batch(b->d_descs, b->d_items_pc, b->d_ints + 1, b->d_ints + 2, sms, EPI_DIST,
+                           b->stream);
+  if (e == cudaSuccess)
+    e = launch_fixup_batch(b->d_descs, b->d_items_tc, b->d_ints + 0, b->d_items_pc, b->d_ints + 1,
+                           sms * 4, b->stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cuda_error(e, "batch graph capture");
+  }
+  if (e2 != cudaSuccess) return cuda_error(e2, "end capture");
+  b->graph = g;
+  RNJ_CUDA(cudaGraphInstantiate(&b->exec, g, 0), "graph instantiate");
+  return RNJ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rnj_batch_create(rnj_ctx *ctx, int max_alignments, long long max_tiles, rnj_batch **out) {
+  if (!ctx || !out || max_alignments <= 0 || max_tiles <= 0)
+    return set_error(RNJ_ERR_INVALID, "invalid batch capacity");
+  DeviceGuard g(ctx->device);
+  rnj_batch *b = new rnj_batch();
+  b->ctx = ctx;
+  b->cap_aln = max_alignments;
+  b->cap_tiles = max_tiles;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_uploaded, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_descs, sizeof(AlnDesc) * max_alignments);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_items_tc, sizeof(WorkItem) * max_tiles);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_items_pc, sizeof(WorkItem) * max_tiles);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_ints, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_max, sizeof(int) * max_alignments);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_flags, sizeof(int) * max_tiles);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_descs, sizeof(AlnDesc) * max_alignments);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_items_tc, sizeof(WorkItem) * max_tiles);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_items_pc, sizeof(WorkItem) * max_tiles);
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_ints, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(b->d_ints, 0, 4 * sizeof(int));
+  if (e != cudaSuccess) {
+    free_batch(b);
+    return cuda_error(e, "batch allocation");
+  }
+  int rc = capture_graph(b);
+  if (rc != RNJ_OK) {
+    free_batch(b);
+    return rc;
+  }
+  *out = b;
+  return RNJ_OK;
+}
+
+int rnj_batch_add(rnj_batch *b, rnj_aln *aln, int model, float *d_out, size_t ld, int *slot) {
+  if (!b || !aln) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (model != RNJ_JC && model != RNJ_KIMURA) return set_error(RNJ_ERR_INVALID, "unknown model");
+  if (aln->ctx != b->ctx) return set_error(RNJ_ERR_INVALID, "alignment from another context");
+  const Packed &p = aln->p;
+  if (p.n < 1) return set_error(RNJ_ERR_INVALID, "empty alignment");
+  if (p.kind != KIND_DNA_TC && p.Wp / kKW > kMaxFusedWords / kKW)
+    return set_error(RNJ_ERR_INVALID, "alignments longer than 65280 columns on the bit-plane "
+                                      "kernels are not batched; use rnj_distance");
+  if ((int)b->entries.size() >= b->cap_aln)
+    return set_error(RNJ_ERR_BUSY, "batch is full (alignments)");
+  const int nt = tiles_of(p.n);
+  const long long ntiles = (p.kind == KIND_NAIVE && (p.flags & RNJ_FULL_ROWS))
+                               ? (long long)nt * nt
+                               : tri_tiles(nt);
+  if (b->tiles_used + ntiles > b->cap_tiles) return set_error(RNJ_ERR_BUSY, "batch is full (tiles)");
+  DeviceGuard g(b->ctx->device);
+  Entry en;
+  en.aln = aln;
+  en.model = model;
+  en.owned = (d_out == nullptr);
+  en.ld = d_out ? ld : (size_t)std::max(4, (p.n + 3) / 4 * 4);
+  en.out = d_out;
+  if (d_out && ld < (size_t)p.n) return set_error(RNJ_ERR_INVALID, "ld < n");
+  if (!d_out) {
+    cudaError_t e = cudaMallocAsync((void **)&en.out, en.ld * p.n * sizeof(float), b->ctx->stream);
+    if (e != cudaSuccess) return cuda_error(e, "batch output allocation");
+  }
+  en.flag_off = b->tiles_used;
+  en.ntiles = ntiles;
+  b->tiles_used += ntiles;
+  b->entries.push_back(en);
+  if (slot) *slot = (int)b->entries.size() - 1;
+  return RNJ_OK;
+}
+
+int rnj_batch_run(rnj_batch *b) {
+  if (!b) return set_error(RNJ_ERR_INVALID, "null batch");
+  rnj_ctx *ctx = b->ctx;
+  DeviceGuard g(ctx->device);
+  // The pinned upload buffers of the previous run must have been read.
+  if (b->uploaded_pending) RNJ_CUDA(cudaEventSynchronize(b->ev_uploaded), "previous upload");
+  const int na = (int)b->entries.size();
+  long long ntc = 0, npc = 0;
+  std::vector<int> order(na);
+  for (int a = 0; a < na; ++a) order[a] = a;
+  // Cost per tile grows with the columns; longest first.
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return b->entries[x].aln->p.L > b->entries[y].aln->p.L;
+  });
+  for (int a = 0; a < na; ++a) {
+    const Entry &en = b->entries[a];
+    const Packed &p = en.aln->p;
+    EpiParams ep = epi_params_for(p, en.model);
+    ep.out = en.out;
+    ep.ld = en.ld;
+    ep.max_bits = b->d_max + a;
+    ep.tile_flags = b->d_flags + en.flag_off;
+    ep.err = b->d_ints + 3;
+    b->h_descs[a] = desc_for(p, ep);
+  }
+  for (int oi = 0; oi < na; ++oi) {
+    const int a = order[oi];
+    const Entry &en = b->entries[a];
+    const bool tc = en.aln->p.kind == KIND_DNA_TC;
+    for (long long t = 0; t < en.ntiles; ++t) {
+      WorkItem w;
+      w.aln = a;
+      w.tile = (int)t;
+      if (tc) b->h_items_tc[ntc++] = w;
+      else b->h_items_pc[npc++] = w;
+    }
+  }
+  b->h_ints[0] = (int)ntc;
+  b->h_ints[1] = (int)npc;
+  // Order after the packing work queued on the context stream.
+  RNJ_CUDA(cudaEventRecord(b->ev_ready, ctx->stream), "ready event");
+  RNJ_CUDA(cudaStreamWaitEvent(b->stream, b->ev_ready, 0), "wait ready");
+  if (na > 0)
+    RNJ_CUDA(cudaMemcpyAsync(b->d_descs, b->h_descs, sizeof(AlnDesc) * na, cudaMemcpyHostToDevice,
+                             b->stream),
+             "descriptor upload");
+  if (ntc > 0)
+    RNJ_CUDA(cudaMemcpyAsync(b->d_items_tc, b->h_items_tc, sizeof(WorkItem) * ntc,
+                             cudaMemcpyHostToDevice, b->stream),
+             "work list upload");
+  if (npc > 0)
+    RNJ_CUDA(cudaMemcpyAsync(b->d_items_pc, b->h_items_pc, sizeof(WorkItem) * npc,
+                             cudaMemcpyHostToDevice, b->stream),
+             "work list upload");
+  RNJ_CUDA(cudaMemcpyAsync(b->d_ints, b->h_ints, 2 * sizeof(int), cudaMemcpyHostToDevice, b->stream),
+           "count upload");
+  RNJ_CUDA(cudaMemsetAsync(b->d_ints + 3, 0, sizeof(int), b->stream), "error clear");
+  RNJ_CUDA(cudaEventRecord(b->ev_uploaded, b->stream), "upload event");
+  b->uploaded_pending = true;
+  RNJ_CUDA(cudaGraphLaunch(b->exec, b->stream), "graph launch");
+  RNJ_CUDA(cudaEventRecord(b->ev_done, b->stream), "done event");
+  // Later work on the context stream (copies, new packs) sees the results.
+  RNJ_CUDA(cudaStreamWaitEvent(ctx->stream, b->ev_done, 0), "join");
+  return RNJ_OK;
+}
+
+int rnj_batch_synchronize(rnj_batch *b) {
+  if (!b) return set_error(RNJ_ERR_INVALID, "null batch");
+  DeviceGuard g(b->ctx->device);
+  RNJ_CUDA(cudaEventSynchronize(b->ev_done), "batch sync");
+  int err = 0;
+  RNJ_CUDA(cudaMemcpy(&err, b->d_ints + 3, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+  if (err) return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out in the batch");
+  return RNJ_OK;
+}
+
+int rnj_batch_output(rnj_batch *b, int slot, float **d_out, size_t *ld, float *max_out) {
+  if (!b || slot < 0 || slot >= (int)b->entries.size())
+    return set_error(RNJ_ERR_INVALID, "no such batch slot");
+  const Entry &en = b->entries[slot];
+  if (d_out) *d_out = en.out;
+  if (ld) *ld = en.ld;
+  if (max_out) {
+    DeviceGuard g(b->ctx->device);
+    RNJ_CUDA(cudaEventSynchronize(b->ev_done), "batch sync");
+    int bits = 0;
+    RNJ_CUDA(cudaMemcpy(&bits, b->d_max + slot, sizeof(int), cudaMemcpyDeviceToHost), "max copy");
+    memcpy(max_out, &bits, sizeof(float));
+  }
+  return RNJ_OK;
+}
+
+int rnj_batch_take(rnj_batch *b, int slot, rnj_mat **out) {
+  if (!b || !out || slot < 0 || slot >= (int)b->entries.size())
+    return set_error(RNJ_ERR_INVALID, "no such batch slot");
+  Entry &en = b->entries[slot];
+  if (!en.owned || !en.out) return set_error(RNJ_ERR_INVALID, "slot output is not owned by the batch");
+  DeviceGuard g(b->ctx->device);
+  RNJ_CUDA(cudaEventSynchronize(b->ev_done), "batch sync");
+  rnj_mat *m = new rnj_mat();
+  m->ctx = b->ctx;
+  m->d = en.out;
+  m->n = en.aln->p.n;
+  m->ld = en.ld;
+  m->owns = true;  // the matrix now owns the output buffer
+  cudaError_t e = cudaMallocAsync((void **)&m->d_max, sizeof(int), b->ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->d_max, b->d_max + slot, sizeof(int), cudaMemcpyDeviceToDevice,
+                        b->ctx->stream);
+  if (e != cudaSuccess) {
+    delete m;
+    return cuda_error(e, "batch output hand-over");
+  }
+  en.owned = false;
+  en.out = nullptr;
+  *out = m;
+  return RNJ_OK;
+}
+
+int rnj_batch_size(rnj_batch *b, int *alignments, long long *tiles) {
+  if (!b) return set_error(RNJ_ERR_INVALID, "null batch");
+  if (alignments) *alignments = (int)b->entries.size();
+  if (tiles) *tiles = b->tiles_used;
+  return RNJ_OK;
+}
+
+int rnj_batch_clear(rnj_batch *b) {
+  if (!b) return set_error(RNJ_ERR_INVALID, "null batch");
+  DeviceGuard g(b->ctx->device);
+  RNJ_CUDA(cudaStreamSynchronize(b->stream), "batch sync");
+  for (auto &e : b->entries)
+    if (e.owned && e.out) cudaFreeAsync(e.out, b->ctx->stream);
+  b->entries.clear();
+  b->tiles_used = 0;
+  return RNJ_OK;
+}
+
+int rnj_batch_destroy(rnj_batch *b) {
+  if (!b) return RNJ_OK;
+  DeviceGuard g(b->ctx->device);
+  free_batch(b);
+  return RNJ_OK;
+}
+
+}  // extern "C"

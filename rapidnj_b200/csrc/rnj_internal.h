@@ -117,6 +117,14 @@ cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s)
 // Tensor-core DNA path (rnj_tc.cu).
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
                                  int8_t *F, cudaStream_t s);
+// Batched popcount path (rnj_kernels.cu): persistent, atomic item counter.
+cudaError_t launch_count_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
+                               int *d_counter, int grid, int epi_mode, cudaStream_t s);
+cudaError_t launch_fixup_batch(const AlnDesc *d_descs, const WorkItem *items_a, const int *n_a,
+                               const WorkItem *items_b, const int *n_b, int grid, cudaStream_t s);
+// Host helpers shared by the single and batched paths (rnj_api.cu).
+EpiParams epi_params_for(const Packed &p, int model);
+AlnDesc desc_for(const Packed &p, const EpiParams &ep);
 // Persistent over work items; d_items == nullptr means items (0, 0..nitems-1) of
 // d_descs[0]; d_nitems == nullptr means nitems is the count.
 cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,

@@ -411,6 +411,267 @@ __global__ void __launch_bounds__(256) fixup_kernel(int nt, EpiParams ep) {
   }
 }
 
+// ------------------------------------------------------- batched popcount path
+//
+// Persistent over a work list of (alignment, tile) items of any plane layout:
+// thread 0 takes the next item with an atomic counter (the list is ordered by
+// decreasing cost), the CTA dispatches on the item's kind and runs the same
+// TMA-staged counting and epilogue as count_tiles_kernel.  The stage ring is
+// sized for the widest layout (8 planes) and its phase counter runs on across
+// items.
+
+constexpr int kBatchST = 3;
+constexpr uint32_t kBatchStageBytes = 2u * 8 * kKW * kTile * 4;  // 64 KB
+constexpr size_t kBatchSmem = (size_t)kBatchST * kBatchStageBytes + 1024 + 64;
+
+__device__ __forceinline__ void tensormap_acquire_pc(const CUtensorMap *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                   reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
+// One tile of one alignment; returns false (uniformly across the CTA) when a
+// bounded wait ran out.  gk: stages consumed so far by this CTA.
+template <int KIND, int EPI>
+__device__ __forceinline__ bool batch_tile(const AlnDesc &d, int tile, uint32_t *smem,
+                                           uint64_t *full_bar, uint32_t &gk) {
+  using T = KT<KIND>;
+  constexpr int NP = T::NP, NC = T::NC;
+  constexpr int TILE_WORDS = NP * kKW * kTile;
+  constexpr uint32_t STAGE_BYTES = 2u * TILE_WORDS * 4u;
+  constexpr int RING_WORDS = kBatchStageBytes / 4;
+  const int tid = threadIdx.x;
+  int ti, tj;
+  if (d.full) {
+    ti = tile / d.nt;
+    tj = tile % d.nt;
+  } else {
+    tri_coords(tile, d.nt, ti, tj);
+  }
+  const int nks = d.kdim / kKW;
+  auto issue = [&](int k) {
+    const uint32_t g = gk + (uint32_t)k;
+    const int s = g % kBatchST;
+    uint32_t *a = smem + s * RING_WORDS;
+    mbar_arrive_expect_tx(&full_bar[s], STAGE_BYTES);
+    tma_load_3d(a, &d.map, &full_bar[s], ti * kTile, k * kKW, 0);
+    tma_load_3d(a + TILE_WORDS, &d.map, &full_bar[s], tj * kTile, k * kKW, 0);
+  };
+  int issued = 0;
+  if (tid == 0) {
+    tensormap_acquire_pc(&d.map);
+    for (; issued < kBatchST - 1 && issued < nks; ++issued) issue(issued);
+  }
+  const int warp = tid >> 5, lane = tid & 31;
+  const int rbase = (warp >> 1) * 32 + (lane >> 3) * 4;
+  const int cbase = (warp & 1) * 64 + (lane & 7) * 4;
+  uint32_t acc0[8][8], acc1[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      acc0[r][c] = 0;
+      acc1[r][c] = 0;
+    }
+  int kabort = -1;
+  for (int k = 0; k < nks; ++k) {
+    if (tid == 0 && issued < nks) issue(issued++);
+    const uint32_t g = gk + (uint32_t)k;
+    const int s = g % kBatchST;
+    const bool ok = mbar_wait_bounded(&full_bar[s], (g / kBatchST) & 1);
+    if (ok) {
+      const uint32_t *A = smem + s * RING_WORDS;
+      const uint32_t *B = A + TILE_WORDS;
+#pragma unroll 2
+      for (int kw = 0; kw < kKW; ++kw) {
+        uint32_t bc[8][NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const uint4 x0 = *reinterpret_cast<const uint4 *>(B + (p * kKW + kw) * kTile + cbase);
+          const uint4 x1 = *reinterpret_cast<const uint4 *>(B + (p * kKW + kw) * kTile + cbase + 32);
+          bc[0][p] = x0.x; bc[1][p] = x0.y; bc[2][p] = x0.z; bc[3][p] = x0.w;
+          bc[4][p] = x1.x; bc[5][p] = x1.y; bc[6][p] = x1.z; bc[7][p] = x1.w;
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          uint32_t ar[NP];
+          const int row = row_of(rbase, r);
+#pragma unroll
+          for (int p = 0; p < NP; ++p) ar[p] = A[(p * kKW + kw) * kTile + row];
+#pragma unroll
+          for (int c = 0; c < 8; ++c) pair_op<KIND>(ar, bc[c], acc0[r][c], acc1[r][c]);
+        }
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      kabort = k;
+      break;
+    }
+  }
+  if (kabort >= 0) {
+    if (tid == 0)
+      for (int k = kabort; k < issued; ++k) {
+        const uint32_t g = gk + (uint32_t)k;
+        mbar_wait_bounded(&full_bar[g % kBatchST], (g / kBatchST) & 1);
+      }
+    return false;
+  }
+  gk += (uint32_t)nks;
+
+  auto get = [&](int r, int c, uint32_t &c0, uint32_t &c1, uint32_t &cv) {
+    c0 = acc0[r][c] & 0xffffu;
+    if constexpr (NC == 3) {
+      c1 = acc0[r][c] >> 16;
+      cv = acc1[r][c];
+    } else {
+      c1 = 0;
+      cv = acc0[r][c] >> 16;
+    }
+  };
+  EpiParams ep;
+  ep.n = d.n;
+  ep.L = d.L;
+  ep.model = d.model;
+  ep.type = d.type;
+  ep.compat_wrap = d.compat;
+  ep.full = d.full;
+  ep.jc_b = d.jc_b;
+  ep.out = d.out;
+  ep.ld = (size_t)d.ld;
+  ep.max_bits = d.max_bits;
+  ep.tile_flags = d.tile_flags;
+  ep.counts = d.counts;
+  ep.err = d.err;
+  if constexpr (EPI == EPI_DIST) {
+    float *S = reinterpret_cast<float *>(smem);
+    float tmax = 0.0f;
+    bool sat = false;
+    stage_distances(ep, ti, tj, rbase, cbase, S, get, tmax, sat);
+    __syncthreads();
+    store_distances(ep, ti, tj, tile, S, tmax, sat, threadIdx.x >> 5, blockDim.x >> 5);
+  } else {
+    const int i0 = ti * kTile, j0 = tj * kTile;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int i = i0 + row_of(rbase, r);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int j = j0 + col_of(cbase, c);
+        const bool ok = ep.full ? (i < ep.n && j < ep.n) : (i < j && j < ep.n);
+        if (!ok) continue;
+        uint32_t c0, c1, cv;
+        get(r, c, c0, c1, cv);
+        uint32_t *o = ep.counts + ((size_t)i * ep.n + j) * 3;
+        o[0] = c0;
+        o[1] = c1;
+        o[2] = cv;
+      }
+    }
+  }
+  // The next item's loads reuse the shared memory the epilogue just read.
+  __syncthreads();
+  return true;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(256, 1)
+    count_batch_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
+                       const int *__restrict__ nitems_ptr, int *__restrict__ counter) {
+  extern __shared__ uint8_t smem_raw[];
+  uint32_t *smem =
+      reinterpret_cast<uint32_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + kBatchST * (kBatchStageBytes / 4));
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < kBatchST; ++s) mbar_init(&full_bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const int nitems = *nitems_ptr;
+  uint32_t gk = 0;
+  while (true) {
+    if (tid == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= nitems) break;
+    const WorkItem w = items[it];
+    const AlnDesc &d = descs[w.aln];
+    bool ok = true;
+    switch (d.kind) {
+      case KIND_DNA: ok = batch_tile<KIND_DNA, EPI>(d, w.tile, smem, full_bar, gk); break;
+      case KIND_NAIVE: ok = batch_tile<KIND_NAIVE, EPI>(d, w.tile, smem, full_bar, gk); break;
+      case KIND_MISM2: ok = batch_tile<KIND_MISM2, EPI>(d, w.tile, smem, full_bar, gk); break;
+      case KIND_MISM5: ok = batch_tile<KIND_MISM5, EPI>(d, w.tile, smem, full_bar, gk); break;
+      case KIND_MISM7: ok = batch_tile<KIND_MISM7, EPI>(d, w.tile, smem, full_bar, gk); break;
+      default: break;
+    }
+    if (!ok) {
+      if (tid == 0) atomicOr(d.err, 1);
+      break;
+    }
+  }
+}
+
+// Saturation fix-up over every item of a batch whose tile holds a -1.
+__global__ void __launch_bounds__(256) fixup_batch_kernel(const AlnDesc *__restrict__ descs,
+                                                          const WorkItem *__restrict__ items_a,
+                                                          const int *__restrict__ n_a,
+                                                          const WorkItem *__restrict__ items_b,
+                                                          const int *__restrict__ n_b) {
+  const int na = *n_a, nb = *n_b;
+  for (int it = blockIdx.x; it < na + nb; it += gridDim.x) {
+    const WorkItem w = it < na ? items_a[it] : items_b[it - na];
+    const AlnDesc &d = descs[w.aln];
+    if (d.out == nullptr || d.tile_flags[w.tile] == 0) continue;
+    int ti, tj;
+    if (d.full) {
+      ti = w.tile / d.nt;
+      tj = w.tile % d.nt;
+    } else {
+      tri_coords(w.tile, d.nt, ti, tj);
+    }
+    const float m2 = __fmul_rn(__int_as_float(*d.max_bits), 2.0f);
+    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
+      const int i = ti * kTile + e / kTile;
+      const int j = tj * kTile + e % kTile;
+      if (d.full) {
+        if (i < d.n && j < d.n && i != j && d.out[(size_t)i * d.ld + j] == -1.0f)
+          d.out[(size_t)i * d.ld + j] = m2;
+      } else if (i < j && j < d.n && d.out[(size_t)i * d.ld + j] == -1.0f) {
+        d.out[(size_t)i * d.ld + j] = m2;
+        d.out[(size_t)j * d.ld + i] = m2;
+      }
+    }
+  }
+}
+
+cudaError_t launch_count_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
+                               int *d_counter, int grid, int epi_mode, cudaStream_t s) {
+  if (grid <= 0) return cudaSuccess;
+  cudaError_t e;
+  if (epi_mode == EPI_DIST) {
+    e = cudaFuncSetAttribute(count_batch_kernel<EPI_DIST>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem);
+    if (e != cudaSuccess) return e;
+    count_batch_kernel<EPI_DIST><<<grid, 256, kBatchSmem, s>>>(d_descs, d_items, d_nitems, d_counter);
+  } else {
+    e = cudaFuncSetAttribute(count_batch_kernel<EPI_COUNTS>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem);
+    if (e != cudaSuccess) return e;
+    count_batch_kernel<EPI_COUNTS><<<grid, 256, kBatchSmem, s>>>(d_descs, d_items, d_nitems,
+                                                                 d_counter);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fixup_batch(const AlnDesc *d_descs, const WorkItem *items_a, const int *n_a,
+                               const WorkItem *items_b, const int *n_b, int grid, cudaStream_t s) {
+  fixup_batch_kernel<<<grid, 256, 0, s>>>(d_descs, items_a, n_a, items_b, n_b);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ launchers
 
 static int grid_for(long long work, int block) {

@@ -1,0 +1,54 @@
+// rnj_objects.h -- the opaque C-ABI objects (context, packed alignment, device
+// matrix), shared by the translation units that implement the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rnj.h"
+#include "rnj_internal.h"
+
+struct rnj_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  rnj::Scratch scratch;
+  uint32_t *d_mask = nullptr;             // presence mask (8 words)
+  uint32_t *h_mask = nullptr;             // pinned
+  int *h_max = nullptr;                   // pinned max bits / error word
+  void *h_stage[2] = {nullptr, nullptr};  // pinned staging for copy-out / upload
+  size_t stage_cap = 0;
+  bool profiling = false;
+  cudaEvent_t ev[6] = {};                 // pack, count, fix-up: begin/end pairs
+  bool ev_used[3] = {false, false, false};
+  rnj::AlnDesc *d_desc = nullptr;         // one-alignment work list of the persistent kernel
+};
+
+struct rnj_aln {
+  rnj_ctx *ctx = nullptr;
+  rnj::Packed p;
+};
+
+struct rnj_mat {
+  rnj_ctx *ctx = nullptr;
+  float *d = nullptr;
+  int n = 0;
+  size_t ld = 0;
+  int *d_max = nullptr;  // device copy of the max bits
+  bool owns = true;
+};
+
+namespace rnj {
+// Sets the calling thread's current device for a scope.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+}  // namespace rnj
