@@ -292,12 +292,8 @@ def run_batched(args, local_rank: int = 0, count: int = 256):
             a.close()
 
     def batched():
-        alns = [ctx.alignment(d, t) for d, t in zip(dev, typ)]
-        for a, o in zip(alns, outs_b):
-            batch.add(a, "kim", out=o)
+        batch.add_many(dev, typ, ["kim"] * count, outs=outs_b)
         batch.run()
-        for a in alns:
-            a.close()
         batch.clear()
 
     def timed(fn, steps):

@@ -208,6 +208,15 @@ int rnj_batch_create(rnj_ctx *ctx, int max_alignments, long long max_tiles, rnj_
 /* Adds an alignment; d_out NULL lets the batch allocate the n x n output.  The
  * slot index identifies the alignment in this batch. */
 int rnj_batch_add(rnj_batch *batch, rnj_aln *aln, int model, float *d_out, size_t ld, int *slot);
+/* Packs and adds `count` alignments already on the device (d_chars[k]: n[k] rows
+ * of stride ld[k], L[k] columns, type[k] RNJ_DNA or RNJ_PROTEIN, model[k]) in one
+ * call: the residue alphabets of all protein alignments are scanned with a
+ * single synchronisation.  The batch owns these packed alignments (freed by
+ * rnj_batch_clear / _destroy).  d_out / ld_out may be NULL (batch-allocated
+ * outputs); slots (may be NULL) receives the slot of each alignment. */
+int rnj_batch_add_many(rnj_batch *batch, int count, const void *const *d_chars, const int *n,
+                       const int *L, const size_t *ld, const int *type, const int *model,
+                       int flags, float *const *d_out, const size_t *ld_out, int *slots);
 /* Runs the batch asynchronously after the work already queued on the context
  * stream; later work on that stream sees the results. */
 int rnj_batch_run(rnj_batch *batch);

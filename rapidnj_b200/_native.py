@@ -70,6 +70,8 @@ SIGNATURES = {
                                      c_void_p, c_size_t, c_void_p, P(c_float)]),
     "rnj_batch_create": (c_int, [c_void_p, c_int, ctypes.c_longlong, P(c_void_p)]),
     "rnj_batch_add": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_size_t, P(c_int)]),
+    "rnj_batch_add_many": (c_int, [c_void_p, c_int, P(c_void_p), P(c_int), P(c_int), P(c_size_t),
+                                   P(c_int), P(c_int), c_int, P(c_void_p), P(c_size_t), P(c_int)]),
     "rnj_batch_run": (c_int, [c_void_p]),
     "rnj_batch_synchronize": (c_int, [c_void_p]),
     "rnj_batch_output": (c_int, [c_void_p, c_int, P(c_void_p), P(c_size_t), P(c_float)]),

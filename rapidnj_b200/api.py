@@ -243,6 +243,23 @@ class Batch:
         self._keep.append(aln)
         return slot.value
 
+    def add_many(self, seqs_dev, types, models, outs=None, fastdist=True, popcount=False):
+        """Packs and adds CUDA uint8 tensors (n x L views) in one call; returns slots."""
+        k = len(seqs_dev)
+        ptrs = (ctypes.c_void_p * k)(*[s.data_ptr() for s in seqs_dev])
+        ns = (ctypes.c_int * k)(*[s.shape[0] for s in seqs_dev])
+        Ls = (ctypes.c_int * k)(*[s.shape[1] for s in seqs_dev])
+        lds = (ctypes.c_size_t * k)(*[s.stride(0) for s in seqs_dev])
+        ts = (ctypes.c_int * k)(*[TYPES[t] for t in types])
+        ms = (ctypes.c_int * k)(*[MODELS[m] for m in models])
+        outp = (ctypes.c_void_p * k)(*[o.data_ptr() for o in outs]) if outs is not None else None
+        ldo = (ctypes.c_size_t * k)(*[o.stride(0) for o in outs]) if outs is not None else None
+        slots = (ctypes.c_int * k)()
+        check(N.lib().rnj_batch_add_many(self.handle, k, ptrs, ns, Ls, lds, ts, ms,
+                                         flags_of(fastdist, False, False, popcount), outp, ldo,
+                                         slots))
+        return list(slots)
+
     def run(self) -> None:
         check(N.lib().rnj_batch_run(self.handle))
 

@@ -224,18 +224,44 @@ void scatter_rows(const float *src, float **dst, int nrows, int n, int threads) 
 }
 
 // Upload raw bytes already on the device (n rows, stride ld) into planes.
+}  // namespace
+
+// Packing LUT and plane layout.  DNA needs nothing from the data; protein ranks
+// the residue bytes present (mask: 256-bit byte-presence mask).
+void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *kind) {
+  const bool naive = (flags & RNJ_FASTDIST) == 0;
+  if (type == RNJ_DNA) {
+    *kind = naive ? KIND_NAIVE : KIND_DNA;
+    dna_lut(naive, lut);
+    return;
+  }
+  int rank = 0;
+  for (int c = 0; c < 256; ++c) {
+    const bool present = (mask[c >> 5] >> (c & 31)) & 1u;
+    if (resolve_char((char)c, RNJ_PROTEIN) == '-') lut[c] = 0xFF;
+    else if (present) lut[c] = (uint8_t)(rank++);
+    else lut[c] = 0xFF;
+  }
+  *kind = rank <= 4 ? KIND_MISM2 : (rank <= 32 ? KIND_MISM5 : KIND_MISM7);
+}
+
+// Allocation, pack kernel and TMA map of an alignment whose LUT is known; no
+// synchronisation.
+int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
+                  int flags, int kind, const uint8_t lut[256], rnj_aln **out);
+
+namespace {
+
 int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
                            int type, int flags, rnj_aln **out) {
   if (n < 0 || L < 0 || (n > 0 && ld < (size_t)L))
     return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
   if (type != RNJ_DNA && type != RNJ_PROTEIN)
     return set_error(RNJ_ERR_INVALID, "sequence type must be resolved before packing");
-  const bool naive = (flags & RNJ_FASTDIST) == 0;
   uint8_t lut[256];
   int kind;
   if (type == RNJ_DNA) {
-    kind = naive ? KIND_NAIVE : KIND_DNA;
-    dna_lut(naive, lut);
+    lut_for(type, flags, nullptr, lut, &kind);
   } else {
     // Rank the residue alphabet present in the alignment.
     RNJ_CUDA(cudaMemsetAsync(ctx->d_mask, 0, 8 * sizeof(uint32_t), ctx->stream), "mask clear");
@@ -245,15 +271,15 @@ int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, s
                              cudaMemcpyDeviceToHost, ctx->stream),
              "mask copy");
     RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "mask sync");
-    int rank = 0;
-    for (int c = 0; c < 256; ++c) {
-      const bool present = (ctx->h_mask[c >> 5] >> (c & 31)) & 1u;
-      if (resolve_char((char)c, RNJ_PROTEIN) == '-') lut[c] = 0xFF;
-      else if (present) lut[c] = (uint8_t)(rank++);
-      else lut[c] = 0xFF;
-    }
-    kind = rank <= 4 ? KIND_MISM2 : (rank <= 32 ? KIND_MISM5 : KIND_MISM7);
+    lut_for(type, flags, ctx->h_mask, lut, &kind);
   }
+  return pack_prepared(ctx, d_chars, n, L, ld, type, flags, kind, lut, out);
+}
+
+}  // namespace
+
+int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
+                  int flags, int kind, const uint8_t lut[256], rnj_aln **out) {
   rnj_aln *a = new rnj_aln();
   a->ctx = ctx;
   Packed &p = a->p;
@@ -312,6 +338,8 @@ int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, s
   *out = a;
   return RNJ_OK;
 }
+
+namespace {
 
 int count_kind_for(const Packed &p, int model) {
   if (p.kind == KIND_DNA && model == RNJ_JC) return KIND_MISM2;

@@ -33,6 +33,7 @@ struct Entry {
   bool owned;
   long long flag_off;  // offset of this alignment's tile flags
   long long ntiles;
+  bool owns_aln;       // packed by rnj_batch_add_many: freed with the entry
 };
 
 }  // namespace
@@ -67,7 +68,10 @@ void free_batch(rnj_batch *b) {
   if (!b) return;
   if (b->stream) cudaStreamSynchronize(b->stream);
   for (auto &e : b->entries)
+  {
     if (e.owned && e.out) cudaFreeAsync(e.out, b->ctx->stream);
+    if (e.owns_aln) rnj_aln_destroy(e.aln);
+  }
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   cudaFree(b->d_descs);
@@ -182,11 +186,68 @@ int rnj_batch_add(rnj_batch *b, rnj_aln *aln, int model, float *d_out, size_t ld
     cudaError_t e = cudaMallocAsync((void **)&en.out, en.ld * p.n * sizeof(float), b->ctx->stream);
     if (e != cudaSuccess) return cuda_error(e, "batch output allocation");
   }
+  en.owns_aln = false;
   en.flag_off = b->tiles_used;
   en.ntiles = ntiles;
   b->tiles_used += ntiles;
   b->entries.push_back(en);
   if (slot) *slot = (int)b->entries.size() - 1;
+  return RNJ_OK;
+}
+
+int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, const int *n,
+                       const int *L, const size_t *ld, const int *type, const int *model, int flags,
+                       float *const *d_out, const size_t *ld_out, int *slots) {
+  if (!b || count < 0 || (count > 0 && (!d_chars || !n || !L || !ld || !type || !model)))
+    return set_error(RNJ_ERR_INVALID, "null argument");
+  rnj_ctx *ctx = b->ctx;
+  DeviceGuard g(ctx->device);
+  for (int k = 0; k < count; ++k) {
+    if (type[k] != RNJ_DNA && type[k] != RNJ_PROTEIN)
+      return set_error(RNJ_ERR_INVALID, "types must be resolved (RNJ_DNA or RNJ_PROTEIN)");
+    if (n[k] < 1 || L[k] < 0 || ld[k] < (size_t)L[k])
+      return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
+  }
+  // Residue alphabets of every protein alignment: one presence scan each, one
+  // copy and one synchronisation for all.
+  std::vector<int> pidx(count, -1);
+  int np = 0;
+  for (int k = 0; k < count; ++k)
+    if (type[k] == RNJ_PROTEIN) pidx[k] = np++;
+  std::vector<uint32_t> masks((size_t)np * 8, 0);
+  if (np > 0) {
+    uint32_t *d_masks = nullptr;
+    RNJ_CUDA(cudaMallocAsync((void **)&d_masks, (size_t)np * 8 * sizeof(uint32_t), ctx->stream),
+             "mask buffer");
+    cudaError_t e = cudaMemsetAsync(d_masks, 0, (size_t)np * 8 * sizeof(uint32_t), ctx->stream);
+    for (int k = 0; k < count && e == cudaSuccess; ++k)
+      if (pidx[k] >= 0 && L[k] > 0)
+        e = launch_presence((const uint8_t *)d_chars[k], ld[k], n[k], L[k], d_masks + 8 * pidx[k],
+                            ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(masks.data(), d_masks, masks.size() * sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, ctx->stream);
+    cudaFreeAsync(d_masks, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_error(e, "residue presence");
+  }
+  for (int k = 0; k < count; ++k) {
+    uint8_t lut[256];
+    int kind;
+    lut_for(type[k], flags, pidx[k] >= 0 ? masks.data() + 8 * pidx[k] : nullptr, lut, &kind);
+    rnj_aln *a = nullptr;
+    int rc = pack_prepared(ctx, (const uint8_t *)d_chars[k], n[k], L[k], ld[k], type[k], flags, kind,
+                           lut, &a);
+    if (rc != RNJ_OK) return rc;
+    int slot = -1;
+    rc = rnj_batch_add(b, a, model[k], d_out ? d_out[k] : nullptr, ld_out ? ld_out[k] : 0, &slot);
+    if (rc != RNJ_OK) {
+      rnj_aln_destroy(a);
+      return rc;
+    }
+    b->entries[slot].owns_aln = true;
+    if (slots) slots[k] = slot;
+  }
   return RNJ_OK;
 }
 
@@ -321,7 +382,10 @@ int rnj_batch_clear(rnj_batch *b) {
   DeviceGuard g(b->ctx->device);
   RNJ_CUDA(cudaStreamSynchronize(b->stream), "batch sync");
   for (auto &e : b->entries)
+  {
     if (e.owned && e.out) cudaFreeAsync(e.out, b->ctx->stream);
+    if (e.owns_aln) rnj_aln_destroy(e.aln);
+  }
   b->entries.clear();
   b->tiles_used = 0;
   return RNJ_OK;

@@ -23,84 +23,121 @@ struct Lut256 {
   uint8_t v[256];
 };
 
-// One thread per (sequence i, plane word w); i fastest so that the plane
-// stores of a warp are 32 consecutive words.  Covers the padded Np x Wp area, so
-// padding rows and words come out zero (invalid).
+// Plane words of one 32-site word of one sequence from its bytes.
 //   DNA kinds: lut bit0 = code high bit, bit1 = code low bit, bit2 = valid,
 //              bit3 = upper-case A/C/G/T (naive rule).
 //   MISM kinds: lut = symbol rank, 0xFF = gap.
-__global__ void pack_chars_kernel(const uint8_t *__restrict__ chars, size_t ld, int n, int L,
-                                  int Np, int Wp, int kind, Lut256 lut,
-                                  uint32_t *__restrict__ planes) {
-  __shared__ uint8_t s_lut[256];
-  for (int k = threadIdx.x; k < 256; k += blockDim.x) s_lut[k] = lut.v[k];
-  __syncthreads();
-  const long long total = (long long)Np * Wp;
-  const size_t plane_stride = (size_t)Np * Wp;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t % Np);
-    const int w = (int)(t / Np);
-    uint32_t p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const int s0 = w * 32;
-    if (i < n && s0 < L) {
-      const int cnt = min(32, L - s0);
-      const uint8_t *src = chars + (size_t)i * ld + s0;
-      uint8_t buf[32];
-      if (cnt == 32 && (((uintptr_t)src) & 15) == 0) {
-        *reinterpret_cast<uint4 *>(buf) = reinterpret_cast<const uint4 *>(src)[0];
-        *reinterpret_cast<uint4 *>(buf + 16) = reinterpret_cast<const uint4 *>(src)[1];
-      } else {
-#pragma unroll 4
-        for (int b = 0; b < 32; ++b) buf[b] = (b < cnt) ? src[b] : (uint8_t)'-';
-      }
-      if (kind == KIND_DNA || kind == KIND_NAIVE) {
+__device__ __forceinline__ void pack_word(const uint8_t *src, int cnt, int kind,
+                                          const uint8_t *s_lut, uint32_t (&p)[8]) {
 #pragma unroll
-        for (int b = 0; b < 32; ++b) {
-          const uint32_t x = (b < cnt) ? s_lut[buf[b]] : 0u;
-          p[0] |= (x & 1u) << b;
-          p[1] |= ((x >> 1) & 1u) << b;
-          p[2] |= ((x >> 2) & 1u) << b;
-          p[3] |= ((x >> 3) & 1u) << b;
-        }
-      } else {
-        const int ncode = (kind == KIND_MISM2) ? 2 : (kind == KIND_MISM5 ? 5 : 7);
+  for (int q = 0; q < 8; ++q) p[q] = 0;
+  if (cnt <= 0) return;
+  if (kind == KIND_DNA || kind == KIND_NAIVE) {
+#pragma unroll 8
+    for (int b = 0; b < 32; ++b) {
+      const uint32_t x = (b < cnt) ? s_lut[src[b]] : 0u;
+      p[0] |= (x & 1u) << b;
+      p[1] |= ((x >> 1) & 1u) << b;
+      p[2] |= ((x >> 2) & 1u) << b;
+      p[3] |= ((x >> 3) & 1u) << b;
+    }
+  } else {
+    const int ncode = (kind == KIND_MISM2) ? 2 : (kind == KIND_MISM5 ? 5 : 7);
+#pragma unroll 8
+    for (int b = 0; b < 32; ++b) {
+      const uint32_t r = (b < cnt) ? s_lut[src[b]] : 0xFFu;
+      if (r != 0xFFu) {
+        p[ncode] |= 1u << b;
 #pragma unroll
-        for (int b = 0; b < 32; ++b) {
-          const uint32_t r = (b < cnt) ? s_lut[buf[b]] : 0xFFu;
-          if (r != 0xFFu) {
-            p[ncode] |= 1u << b;
-#pragma unroll
-            for (int q = 0; q < 7; ++q)
-              if (q < ncode) p[q] |= ((r >> q) & 1u) << b;
-          }
-        }
+        for (int q = 0; q < 7; ++q)
+          if (q < ncode) p[q] |= ((r >> q) & 1u) << b;
       }
     }
-    const int np = planes_of(kind);
-    uint32_t *dst = planes + (size_t)w * Np + i;
+  }
+}
+
+// Bytes -> bit planes, one 32-sequence x 8-word tile per block (256 threads, one
+// (sequence, word) each).  Reads: the 8 threads of a sequence cover 256
+// contiguous bytes of its row.  The plane words go through shared memory so
+// the stores run along the sequence axis (32 consecutive words per warp).  The
+// grid covers the padded Np x Wp area, so padding rows and words come out zero.
+constexpr int kPackRows = 32, kPackWords = 8;
+
+__global__ void __launch_bounds__(256) pack_chars_kernel(const uint8_t *__restrict__ chars,
+                                                         size_t ld, int n, int L, int Np, int Wp,
+                                                         int kind, Lut256 lut,
+                                                         uint32_t *__restrict__ planes) {
+  __shared__ uint8_t s_lut[256];
+  __shared__ uint32_t s_words[8][kPackWords][kPackRows + 1];
+  for (int k = threadIdx.x; k < 256; k += blockDim.x) s_lut[k] = lut.v[k];
+  __syncthreads();
+  const int np = planes_of(kind);
+  const size_t plane_stride = (size_t)Np * Wp;
+  const int row_tiles = Np / kPackRows, word_tiles = Wp / kPackWords;
+  const long long tiles = (long long)row_tiles * word_tiles;
+  for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const int i0 = (int)(t % row_tiles) * kPackRows;
+    const int w0 = (int)(t / row_tiles) * kPackWords;
+    {
+      const int r = threadIdx.x >> 3, ww = threadIdx.x & 7;
+      const int i = i0 + r, w = w0 + ww;
+      uint32_t p[8];
+      const int cnt = (i < n) ? min(32, L - w * 32) : 0;
+      pack_word(chars + (size_t)i * ld + (size_t)w * 32, cnt, kind, s_lut, p);
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      if (q < np) dst[q * plane_stride] = p[q];
+      for (int q = 0; q < 8; ++q)
+        if (q < np) s_words[q][ww][r] = p[q];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int pw = warp; pw < np * kPackWords; pw += 8) {
+      const int q = pw / kPackWords, ww = pw % kPackWords;
+      planes[q * plane_stride + (size_t)(w0 + ww) * Np + i0 + lane] = s_words[q][ww][lane];
+    }
+    __syncthreads();
   }
 }
 
 // Byte-presence mask of an alignment (bit c of the 256-bit mask set when byte
-// c occurs), used to rank the residue alphabet on the host.
-__global__ void presence_kernel(const uint8_t *__restrict__ chars, size_t ld, int n, int L,
-                                uint32_t *__restrict__ mask) {
-  __shared__ uint32_t s_mask[8];
-  if (threadIdx.x < 8) s_mask[threadIdx.x] = 0;
-  __syncthreads();
-  const long long total = (long long)n * L;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / L), k = (int)(t % L);
-    const uint8_t c = chars[(size_t)i * ld + k];
-    atomicOr(&s_mask[c >> 5], 1u << (c & 31));
+// c occurs), used to rank the residue alphabet on the host.  A warp walks a
+// row, 32 consecutive bytes per step; each lane keeps its own 256-bit mask in
+// registers and the warp merges them before one atomic per word.
+__device__ __forceinline__ void mask_set(uint32_t (&m)[8], uint32_t c) {
+  const uint32_t bit = 1u << (c & 31);
+  switch (c >> 5) {
+    case 0: m[0] |= bit; break;
+    case 1: m[1] |= bit; break;
+    case 2: m[2] |= bit; break;
+    case 3: m[3] |= bit; break;
+    case 4: m[4] |= bit; break;
+    case 5: m[5] |= bit; break;
+    case 6: m[6] |= bit; break;
+    default: m[7] |= bit; break;
   }
-  __syncthreads();
-  if (threadIdx.x < 8 && s_mask[threadIdx.x]) atomicOr(&mask[threadIdx.x], s_mask[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) presence_kernel(const uint8_t *__restrict__ chars,
+                                                       size_t ld, int n, int L,
+                                                       uint32_t *__restrict__ mask) {
+  uint32_t m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int segs = (L + 1023) / 1024;  // 1 KB row segments
+  const long long units = (long long)n * segs;
+  for (long long u = gwarp; u < units; u += nwarps) {
+    const int i = (int)(u / segs), s = (int)(u % segs);
+    const uint8_t *row = chars + (size_t)i * ld;
+    const int k1 = min(L, (s + 1) * 1024);
+    for (int k = s * 1024 + lane; k < k1; k += 32) mask_set(m, row[k]);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    uint32_t v = m[q];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0 && v) atomicOr(&mask[q], v);
+  }
 }
 
 __device__ __forceinline__ uint32_t compress_even_bits(uint32_t x) {

@@ -37,6 +37,12 @@ struct rnj_mat {
   bool owns = true;
 };
 
+// Packing in two steps (rnj_api.cu): the LUT and plane layout of an alignment
+// (protein needs its byte-presence mask), then allocation + pack kernel + map.
+void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *kind);
+int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
+                  int flags, int kind, const uint8_t lut[256], rnj_aln **out);
+
 namespace rnj {
 // Sets the calling thread's current device for a scope.
 struct DeviceGuard {

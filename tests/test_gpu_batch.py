@@ -80,6 +80,23 @@ def test_batch_graph_reused_across_runs(ctx):
     batch.close()
 
 
+def test_batch_add_many_matches_plain(ctx):
+    """Packing and adding many device alignments in one call (one alphabet
+    synchronisation for all protein alignments) gives the plain matrices."""
+    from rapidnj_b200 import api
+    items = [it for it in mixed_set(5, count=18) if not it[3]]  # default flags only
+    batch = api.Batch(ctx, max_alignments=32, max_tiles=2048)
+    dev = [torch.from_numpy(s).cuda() for s, _, _, _ in items]
+    slots = batch.add_many(dev, [t for _, t, _, _ in items], [m for _, _, m, _ in items])
+    batch.run()
+    for (seqs, typ, model, _), slot in zip(items, slots):
+        ref = ctx.distance(ctx.alignment(seqs, typ), model).to_numpy()
+        assert np.array_equal(batch.take(slot).to_numpy(), ref)
+    batch.clear()
+    assert batch.size() == (0, 0)
+    batch.close()
+
+
 def test_batch_against_oracle(ctx):
     from rapidnj_b200 import api, synth
     batch = api.Batch(ctx, max_alignments=8, max_tiles=256)
