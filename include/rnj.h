@@ -221,6 +221,8 @@ int rnj_batch_add_many(rnj_batch *batch, int count, const void *const *d_chars, 
  * stream; later work on that stream sees the results. */
 int rnj_batch_run(rnj_batch *batch);
 int rnj_batch_synchronize(rnj_batch *batch);
+/* Non-blocking: *done = 1 once the last run has completed on the device. */
+int rnj_batch_poll(rnj_batch *batch, int *done);
 /* The output of a slot (device pointer and stride); max_out (may be NULL)
  * waits for the run and reads the slot's maximum distance. */
 int rnj_batch_output(rnj_batch *batch, int slot, float **d_out, size_t *ld, float *max_out);
@@ -230,6 +232,39 @@ int rnj_batch_size(rnj_batch *batch, int *alignments, long long *tiles);
 /* Forgets the alignments (frees outputs still owned by the batch); the graph stays. */
 int rnj_batch_clear(rnj_batch *batch);
 int rnj_batch_destroy(rnj_batch *batch);
+
+/* ------------------------------------------------------------------ serving */
+
+/* Continuous batching of distance requests.  Clients submit host alignments
+ * from any thread; a scheduler thread of the server (with its own context on
+ * `device`) admits requests first come, first served while the device memory
+ * they need (bytes, packed operands, output) fits `memory_budget` (0: 60 % of
+ * the free memory at creation), uploads and packs them, and launches them as a
+ * batch; up to two batches are in flight, so requests that arrive while one
+ * batch computes form the next, which starts as soon as it has work and
+ * overlaps the first on the device.  Packed inputs are freed when a request
+ * completes; its output matrix stays on the device until the client takes it.
+ * No counterpart in the reference (which computes one matrix per process run). */
+typedef struct rnj_server rnj_server;
+enum { RNJ_REQ_QUEUED = 0, RNJ_REQ_RUNNING = 1, RNJ_REQ_DONE = 2, RNJ_REQ_FAILED = 3 };
+int rnj_server_create(int device, size_t memory_budget, int max_batch, rnj_server **out);
+/* chars: n rows of stride ld; the bytes are copied before the call returns. */
+int rnj_server_submit(rnj_server *server, const char *chars, int n, int L, size_t ld, int type,
+                      int model, int flags, uint64_t *id);
+int rnj_server_poll(rnj_server *server, uint64_t id, int *state);
+int rnj_server_wait(rnj_server *server, uint64_t id, int timeout_ms);
+/* Hands the finished matrix to the caller.  `owner` (a context of the caller on
+ * the same device) becomes the matrix's context: it is read and freed on that
+ * context's stream and outlives the server; pass it to rnj_mat_copy_rows too.
+ * latency_ms (may be NULL) is the time from submit to the matrix complete on
+ * the device. */
+int rnj_server_result(rnj_server *server, uint64_t id, rnj_ctx *owner, rnj_mat **out,
+                      double *latency_ms);
+/* Completed requests, their pair-columns, the seconds from the first submit to
+ * the last completion, and the device bytes the server currently holds. */
+int rnj_server_stats(rnj_server *server, uint64_t *completed, double *pair_columns,
+                     double *seconds, size_t *bytes_in_use);
+int rnj_server_destroy(rnj_server *server);
 
 /* ------------------------------------------------------- alignment files */
 

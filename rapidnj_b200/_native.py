@@ -79,6 +79,17 @@ SIGNATURES = {
     "rnj_batch_size": (c_int, [c_void_p, P(c_int), P(ctypes.c_longlong)]),
     "rnj_batch_clear": (c_int, [c_void_p]),
     "rnj_batch_destroy": (c_int, [c_void_p]),
+    "rnj_batch_poll": (c_int, [c_void_p, P(c_int)]),
+    "rnj_server_create": (c_int, [c_int, c_size_t, c_int, P(c_void_p)]),
+    "rnj_server_submit": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int, c_int, c_int,
+                                  P(ctypes.c_uint64)]),
+    "rnj_server_poll": (c_int, [c_void_p, ctypes.c_uint64, P(c_int)]),
+    "rnj_server_wait": (c_int, [c_void_p, ctypes.c_uint64, c_int]),
+    "rnj_server_result": (c_int, [c_void_p, ctypes.c_uint64, c_void_p, P(c_void_p),
+                                  P(ctypes.c_double)]),
+    "rnj_server_stats": (c_int, [c_void_p, P(ctypes.c_uint64), P(ctypes.c_double),
+                                 P(ctypes.c_double), P(c_size_t)]),
+    "rnj_server_destroy": (c_int, [c_void_p]),
     "rnj_msa_read": (c_int, [c_char_p, c_char_p, P(c_void_p)]),
     "rnj_msa_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
     "rnj_msa_name": (c_char_p, [c_void_p, c_int]),

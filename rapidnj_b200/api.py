@@ -43,9 +43,10 @@ class Alignment:
         self.n, self.L, self.type = n.value, L.value, t.value
 
     def close(self) -> None:
-        if self.handle:
+        # After its context is closed the native object is gone with it.
+        if self.handle and self.ctx.handle:
             N.lib().rnj_aln_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -86,9 +87,9 @@ class Matrix:
         return out
 
     def close(self) -> None:
-        if self.handle:
+        if self.handle and self.ctx.handle:
             N.lib().rnj_mat_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -286,8 +287,62 @@ class Batch:
         self._keep = []
 
     def close(self) -> None:
-        if self.handle:
+        if self.handle and self.ctx.handle:
             N.lib().rnj_batch_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching distance server (rnj_server) with its own device context."""
+
+    def __init__(self, device: int = 0, memory_budget: int = 0, max_batch: int = 256):
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_server_create(device, memory_budget, max_batch, ctypes.byref(h)))
+        self.handle = h
+
+    def submit(self, seqs: np.ndarray, model="kim", type_=None, fastdist=True,
+               popcount=False) -> int:
+        a = np.ascontiguousarray(seqs, dtype=np.uint8)
+        n, L = a.shape
+        rid = ctypes.c_uint64()
+        check(N.lib().rnj_server_submit(self.handle, a.ctypes.data, n, L, L, TYPES[type_],
+                                        MODELS[model], flags_of(fastdist, False, False, popcount),
+                                        ctypes.byref(rid)))
+        return rid.value
+
+    def state(self, rid: int) -> int:
+        s = ctypes.c_int()
+        check(N.lib().rnj_server_poll(self.handle, rid, ctypes.byref(s)))
+        return s.value
+
+    def wait(self, rid: int, timeout_ms: int = 60000) -> None:
+        check(N.lib().rnj_server_wait(self.handle, rid, timeout_ms))
+
+    def result(self, ctx: Context, rid: int):
+        """(Matrix on the device, latency in ms); the matrix belongs to the caller."""
+        h = ctypes.c_void_p()
+        lat = ctypes.c_double()
+        check(N.lib().rnj_server_result(self.handle, rid, ctx.handle, ctypes.byref(h),
+                                        ctypes.byref(lat)))
+        m = Matrix(ctx, h.value)
+        return m, lat.value
+
+    def stats(self):
+        c, w, s, b = ctypes.c_uint64(), ctypes.c_double(), ctypes.c_double(), ctypes.c_size_t()
+        check(N.lib().rnj_server_stats(self.handle, ctypes.byref(c), ctypes.byref(w),
+                                       ctypes.byref(s), ctypes.byref(b)))
+        return {"completed": c.value, "pair_columns": w.value, "seconds": s.value,
+                "bytes_in_use": b.value}
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().rnj_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

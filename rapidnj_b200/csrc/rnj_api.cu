@@ -371,6 +371,10 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
 }
 
 int check_device_error(rnj_ctx *ctx) {
+  if (!ctx->scratch.words) {  // no single-call distance ran on this context yet
+    RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "distance sync");
+    return RNJ_OK;
+  }
   RNJ_CUDA(cudaMemcpyAsync(ctx->h_max + 1, ctx->scratch.words + 1, sizeof(int),
                            cudaMemcpyDeviceToHost, ctx->stream),
            "error word copy");
@@ -759,9 +763,12 @@ int rnj_counts_into(rnj_ctx *ctx, rnj_aln *aln, unsigned int *d_counts) {
 int rnj_mat_info(rnj_mat *mat, int *n, float *max_distance) {
   if (!mat) return set_error(RNJ_ERR_INVALID, "null matrix");
   if (n) *n = mat->n;
-  if (max_distance) {
+  if (max_distance && mat->has_host_max) {
+    *max_distance = mat->host_max;
+  } else if (max_distance) {
     DeviceGuard g(mat->ctx->device);
     rnj_ctx *ctx = mat->ctx;
+    if (!mat->d_max) return set_error(RNJ_ERR_INVALID, "matrix carries no maximum");
     RNJ_CUDA(cudaMemcpyAsync(ctx->h_max, mat->d_max, sizeof(int), cudaMemcpyDeviceToHost,
                              ctx->stream),
              "max copy");

@@ -60,7 +60,12 @@ struct rnj_batch {
   cudaGraphExec_t exec = nullptr;
   std::vector<Entry> entries;
   long long tiles_used = 0;
+  bool join = true;  // make the context stream wait for each run's completion
+  std::vector<int> host_max;  // maxima of the last run, read once per run
+  bool host_max_valid = false;
 };
+
+void batch_set_join(rnj_batch *b, bool join) { b->join = join; }
 
 namespace {
 
@@ -310,10 +315,24 @@ int rnj_batch_run(rnj_batch *b) {
   RNJ_CUDA(cudaMemsetAsync(b->d_ints + 3, 0, sizeof(int), b->stream), "error clear");
   RNJ_CUDA(cudaEventRecord(b->ev_uploaded, b->stream), "upload event");
   b->uploaded_pending = true;
+  b->host_max_valid = false;
   RNJ_CUDA(cudaGraphLaunch(b->exec, b->stream), "graph launch");
   RNJ_CUDA(cudaEventRecord(b->ev_done, b->stream), "done event");
   // Later work on the context stream (copies, new packs) sees the results.
-  RNJ_CUDA(cudaStreamWaitEvent(ctx->stream, b->ev_done, 0), "join");
+  if (b->join) RNJ_CUDA(cudaStreamWaitEvent(ctx->stream, b->ev_done, 0), "join");
+  return RNJ_OK;
+}
+
+int rnj_batch_poll(rnj_batch *b, int *done) {
+  if (!b || !done) return set_error(RNJ_ERR_INVALID, "null argument");
+  DeviceGuard g(b->ctx->device);
+  const cudaError_t e = cudaEventQuery(b->ev_done);
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return RNJ_OK;
+  }
+  if (e != cudaSuccess) return cuda_error(e, "batch poll");
+  *done = 1;
   return RNJ_OK;
 }
 
@@ -322,7 +341,9 @@ int rnj_batch_synchronize(rnj_batch *b) {
   DeviceGuard g(b->ctx->device);
   RNJ_CUDA(cudaEventSynchronize(b->ev_done), "batch sync");
   int err = 0;
-  RNJ_CUDA(cudaMemcpy(&err, b->d_ints + 3, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+  RNJ_CUDA(cudaMemcpyAsync(&err, b->d_ints + 3, sizeof(int), cudaMemcpyDeviceToHost, b->stream),
+           "error word");
+  RNJ_CUDA(cudaStreamSynchronize(b->stream), "error word");
   if (err) return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out in the batch");
   return RNJ_OK;
 }
@@ -337,7 +358,10 @@ int rnj_batch_output(rnj_batch *b, int slot, float **d_out, size_t *ld, float *m
     DeviceGuard g(b->ctx->device);
     RNJ_CUDA(cudaEventSynchronize(b->ev_done), "batch sync");
     int bits = 0;
-    RNJ_CUDA(cudaMemcpy(&bits, b->d_max + slot, sizeof(int), cudaMemcpyDeviceToHost), "max copy");
+    RNJ_CUDA(cudaMemcpyAsync(&bits, b->d_max + slot, sizeof(int), cudaMemcpyDeviceToHost,
+                             b->stream),
+             "max copy");
+    RNJ_CUDA(cudaStreamSynchronize(b->stream), "max copy");
     memcpy(max_out, &bits, sizeof(float));
   }
   return RNJ_OK;
@@ -350,20 +374,23 @@ int rnj_batch_take(rnj_batch *b, int slot, rnj_mat **out) {
   if (!en.owned || !en.out) return set_error(RNJ_ERR_INVALID, "slot output is not owned by the batch");
   DeviceGuard g(b->ctx->device);
   RNJ_CUDA(cudaEventSynchronize(b->ev_done), "batch sync");
+  if (!b->host_max_valid) {
+    b->host_max.assign(b->entries.size(), 0);
+    RNJ_CUDA(cudaMemcpyAsync(b->host_max.data(), b->d_max, sizeof(int) * b->entries.size(),
+                             cudaMemcpyDeviceToHost, b->stream),
+             "max copy");
+    RNJ_CUDA(cudaStreamSynchronize(b->stream), "max copy");
+    b->host_max_valid = true;
+  }
+  const int bits = b->host_max[slot];
   rnj_mat *m = new rnj_mat();
   m->ctx = b->ctx;
   m->d = en.out;
   m->n = en.aln->p.n;
   m->ld = en.ld;
   m->owns = true;  // the matrix now owns the output buffer
-  cudaError_t e = cudaMallocAsync((void **)&m->d_max, sizeof(int), b->ctx->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(m->d_max, b->d_max + slot, sizeof(int), cudaMemcpyDeviceToDevice,
-                        b->ctx->stream);
-  if (e != cudaSuccess) {
-    delete m;
-    return cuda_error(e, "batch output hand-over");
-  }
+  m->has_host_max = true;
+  memcpy(&m->host_max, &bits, sizeof(float));
   en.owned = false;
   en.out = nullptr;
   *out = m;

@@ -29,11 +29,13 @@ struct rnj_aln {
 };
 
 struct rnj_mat {
-  rnj_ctx *ctx = nullptr;
+  rnj_ctx *ctx = nullptr;  // stream the matrix is freed and read on
   float *d = nullptr;
   int n = 0;
   size_t ld = 0;
-  int *d_max = nullptr;  // device copy of the max bits
+  int *d_max = nullptr;    // device copy of the max bits (single calls)
+  bool has_host_max = false;  // batch and served results carry the max on the host
+  float host_max = 0.0f;
   bool owns = true;
 };
 
@@ -42,6 +44,10 @@ struct rnj_mat {
 void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *kind);
 int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
                   int flags, int kind, const uint8_t lut[256], rnj_aln **out);
+
+// A batch whose runs do not make the context stream wait (the server follows
+// completion through the batch's event and keeps packing the next batch).
+void batch_set_join(rnj_batch *b, bool join);
 
 namespace rnj {
 // Sets the calling thread's current device for a scope.

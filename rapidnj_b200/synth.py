@@ -42,6 +42,15 @@ def iid_dna(n: int, L: int, gap: float = 0.05, seed: int = 0) -> np.ndarray:
     return seqs
 
 
+def iid_protein(n: int, L: int, gap: float = 0.05, seed: int = 0) -> np.ndarray:
+    """Uniform i.i.d. amino acids, each cell '-' with probability ``gap``."""
+    rng = np.random.default_rng(seed)
+    seqs = AMINO[rng.integers(0, AMINO.size, size=(n, L), dtype=np.uint8)]
+    if gap > 0:
+        seqs[rng.random((n, L), dtype=np.float32) < gap] = GAP
+    return seqs
+
+
 def _k2p_probs(t: float, kappa: float) -> tuple[float, float]:
     """Per-site transition and (total) transversion probabilities after a
     branch of t substitutions per site (rate normalised to alpha + 2 beta = 1)."""

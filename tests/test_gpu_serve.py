@@ -1,0 +1,80 @@
+"""The served form: requests submitted concurrently, admitted by device memory,
+batched while others run, give exactly the matrix each gives alone."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def request_mix(seed=0, count=24):
+    from rapidnj_b200 import synth
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(np.exp(rng.uniform(np.log(16), np.log(700))))
+        L = int(np.exp(rng.uniform(np.log(200), np.log(3000))))
+        if k % 3 == 0:
+            out.append((synth.iid_dna(n, L, seed=k), 0, "jc"))
+        elif k % 3 == 1:
+            out.append((synth.tree_protein(n, L, seed=k), 1, "kim"))
+        else:
+            out.append((synth.tree_dna(n, L, seed=k, mean_branch=0.1), 0, "kim"))
+    return out
+
+
+def test_served_results_equal_alone(ctx):
+    from rapidnj_b200 import api
+    reqs = request_mix(0)
+    server = api.Server(0, max_batch=8)
+    ids = [None] * len(reqs)
+
+    def submit(part):
+        for k in part:
+            seqs, typ, model = reqs[k]
+            ids[k] = server.submit(seqs, model, typ)
+
+    threads = [threading.Thread(target=submit, args=(range(p, len(reqs), 2),)) for p in (0, 1)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for k, (seqs, typ, model) in enumerate(reqs):
+        server.wait(ids[k])
+        mat, lat = server.result(ctx, ids[k])
+        alone = ctx.distance(ctx.alignment(seqs, typ), model)
+        assert np.array_equal(mat.to_numpy(), alone.to_numpy())
+        assert mat.max == alone.max
+        assert lat > 0
+        mat.close()
+    st = server.stats()
+    assert st["completed"] == len(reqs)
+    assert st["bytes_in_use"] == 0
+    server.close()
+
+
+def test_served_admission_by_memory(ctx):
+    """A budget that holds about two requests at a time still serves all, in order."""
+    from rapidnj_b200 import api, synth
+    seqs = [synth.tree_dna(256, 1000, seed=s) for s in range(6)]
+    budget = 2 * (256 * 1000 + 256 * 4 * 1024 + 256 * 256 * 4 + 4096) + 1000
+    server = api.Server(0, memory_budget=budget, max_batch=4)
+    ids = [server.submit(s, "kim", 0) for s in seqs]
+    for rid, s in zip(ids, seqs):
+        server.wait(rid)
+        m, _ = server.result(ctx, rid)
+        ref = ctx.distance(ctx.alignment(s, 0), "kim").to_numpy()
+        assert np.array_equal(m.to_numpy(), ref)
+        m.close()
+    server.close()
+
+
+def test_served_rejects_requests_beyond_budget():
+    from rapidnj_b200 import api, synth, RnjError
+    server = api.Server(0, memory_budget=1 << 20)
+    with pytest.raises(RnjError, match="budget"):
+        server.submit(synth.tree_dna(512, 4000, seed=1), "kim", 0)
+    server.close()
