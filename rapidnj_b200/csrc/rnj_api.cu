@@ -638,26 +638,39 @@ int rnj_aln_from_bitstrings(rnj_ctx *ctx, const unsigned int *const *bit_strings
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
   p.NP = 3;
+  const bool tc = !(flags & RNJ_POPCOUNT);
   uint32_t *db = nullptr;
   cudaError_t e = cudaMallocAsync((void **)&db, std::max<size_t>(words * 8, 8), ctx->stream);
-  if (e == cudaSuccess)
+  if (tc) {
+    p.kind = KIND_DNA_TC;
+    p.NP = 0;
+    p.Lk = std::max(128, (L + 127) / 128 * 128);
+    if (e == cudaSuccess)
+      e = cudaMallocAsync((void **)&p.feat, (size_t)p.Np * 4 * p.Lk, ctx->stream);
+  } else if (e == cudaSuccess) {
     e = cudaMallocAsync((void **)&p.planes, (size_t)p.NP * p.Wp * p.Np * 4, ctx->stream);
+  }
   if (e == cudaSuccess && words)
     e = cudaMemcpyAsync(db, sb, words * 4, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess && words)
     e = cudaMemcpyAsync(db + words, sg, words * 4, cudaMemcpyHostToDevice, ctx->stream);
   mark(ctx, 0, 0);
-  if (e == cudaSuccess) e = launch_pack_bitstrings_dna(db, db + words, bs_words, p, ctx->stream);
+  if (e == cudaSuccess)
+    e = tc ? launch_pack_features_bits(db, db + words, bs_words, n, L, p.Np, p.Lk, p.feat,
+                                       ctx->stream)
+           : launch_pack_bitstrings_dna(db, db + words, bs_words, p, ctx->stream);
   mark(ctx, 0, 1);
   if (db) cudaFreeAsync(db, ctx->stream);
   if (e != cudaSuccess) {
     if (p.planes) cudaFreeAsync(p.planes, ctx->stream);
+    if (p.feat) cudaFreeAsync(p.feat, ctx->stream);
     delete a;
     return cuda_error(e, "bit-string upload");
   }
-  rc = encode_planes_map(p);
+  rc = tc ? encode_features_map(p) : encode_planes_map(p);
   if (rc != RNJ_OK) {
-    cudaFreeAsync(p.planes, ctx->stream);
+    if (p.planes) cudaFreeAsync(p.planes, ctx->stream);
+    if (p.feat) cudaFreeAsync(p.feat, ctx->stream);
     delete a;
     return rc;
   }

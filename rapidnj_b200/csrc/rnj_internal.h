@@ -117,6 +117,9 @@ cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s)
 // Tensor-core DNA path (rnj_tc.cu).
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
                                  int8_t *F, cudaStream_t s);
+cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_gaps, int bs_words,
+                                      int n, int L, int Np, int Lk, int8_t *F, cudaStream_t s);
+int encode_features_map(Packed &p);
 // Batched popcount path (rnj_kernels.cu): persistent, atomic item counter.
 cudaError_t launch_count_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
                                int *d_counter, int grid, int epi_mode, cudaStream_t s);

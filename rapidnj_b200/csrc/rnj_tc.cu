@@ -181,6 +181,53 @@ __global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t l
   }
 }
 
+// The reference loader's DNA layout (16 sites per uint32, 2-bit codes A=00 G=01
+// T=10 C=11, gap filter 01 per valid site, dataloaderFasta.hpp:147-182) ->
+// features.  One thread per (sequence, source word) = 16 sites.
+__global__ void pack_features_bits_kernel(const uint32_t *__restrict__ bits,
+                                          const uint32_t *__restrict__ gaps, int bs_words, int n,
+                                          int L, int Np, int Lk, int8_t *__restrict__ F) {
+  const int chunks = Lk / 16;
+  const long long total = (long long)Np * chunks;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / chunks);
+    const int c = (int)(t % chunks);
+    uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
+    if (i < n && c < bs_words) {
+      const uint32_t b = bits[(size_t)i * bs_words + c];
+      const uint32_t g = gaps[(size_t)i * bs_words + c];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        if (c * 16 + k >= L || !((g >> (2 * k)) & 1u)) continue;
+        const uint32_t code = (b >> (2 * k)) & 3u;  // A=0 G=1 T=2 C=3
+        const int rr = (code < 2) ? 1 : -1;
+        const int ts = (code == 0 || code == 3) ? 1 : -1;
+        const int sh = (k & 3) * 8;
+        v[k >> 2] |= 1u << sh;
+        r[k >> 2] |= (uint32_t)(uint8_t)(int8_t)rr << sh;
+        tt[k >> 2] |= (uint32_t)(uint8_t)(int8_t)ts << sh;
+        u[k >> 2] |= (uint32_t)(uint8_t)(int8_t)(rr * ts) << sh;
+      }
+    }
+    int8_t *row = F + (size_t)i * 4 * Lk + c * 16;
+    *reinterpret_cast<uint4 *>(row) = make_uint4(v[0], v[1], v[2], v[3]);
+    *reinterpret_cast<uint4 *>(row + Lk) = make_uint4(r[0], r[1], r[2], r[3]);
+    *reinterpret_cast<uint4 *>(row + 2 * (size_t)Lk) = make_uint4(tt[0], tt[1], tt[2], tt[3]);
+    *reinterpret_cast<uint4 *>(row + 3 * (size_t)Lk) = make_uint4(u[0], u[1], u[2], u[3]);
+  }
+}
+
+cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_gaps, int bs_words,
+                                      int n, int L, int Np, int Lk, int8_t *F, cudaStream_t s) {
+  const long long work = (long long)Np * (Lk / 16);
+  long long g = (work + 255) / 256;
+  if (g > 148LL * 64) g = 148LL * 64;
+  if (g < 1) g = 1;
+  pack_features_bits_kernel<<<(unsigned)g, 256, 0, s>>>(d_bits, d_gaps, bs_words, n, L, Np, Lk, F);
+  return cudaGetLastError();
+}
+
 // ----------------------------------------------------------------- the kernel
 //
 // Persistent over a work list of (alignment, triangle tile) items: CTA b takes

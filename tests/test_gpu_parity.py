@@ -213,6 +213,13 @@ def test_input_paths_agree(ctx):
     bs, gf = reference_bitstrings(seqs)
     aln = ctx.alignment_from_bitstrings(bs, gf, 777, oracle.DNA)
     assert np.array_equal(ctx.distance(aln, "kim").to_numpy(), ref)
+    # ... on the popcount kernel, and the JC model on both kernels
+    from rapidnj_b200.api import RNJ_FASTDIST, RNJ_POPCOUNT
+    aln_p = ctx.alignment_from_bitstrings(bs, gf, 777, oracle.DNA, RNJ_FASTDIST | RNJ_POPCOUNT)
+    assert np.array_equal(ctx.distance(aln_p, "kim").to_numpy(), ref)
+    ref_jc, _ = gpu_matrix(ctx, seqs, oracle.DNA, "jc")
+    assert np.array_equal(ctx.distance(aln, "jc").to_numpy(), ref_jc)
+    assert np.array_equal(ctx.distance(aln_p, "jc").to_numpy(), ref_jc)
     # one-call host path
     out, mx = ctx.distance_matrix_host(seqs, "kim")
     assert np.array_equal(out, ref)
