@@ -157,7 +157,7 @@ def cpu_reference(seqs: np.ndarray, model: str, type_: str, warmup: int, steps: 
 def run_gpu(args, rank: int, world: int, local_rank: int):
     import torch
     import torch.distributed as dist
-    from rapidnj_b200 import api
+    from rapidnj_b200 import api, sharded
 
     name = args.workload
     gen, n, L, type_, model = WORKLOADS[name]
@@ -174,7 +174,13 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
 
     def step():
         aln = ctx.alignment(d_chars, typ, popcount=args.popcount)
-        ctx.distance_into(aln, model, out)
+        if world > 1:
+            # this rank's contiguous range of tiles; one float MAX all-reduce
+            sh = api.Shard(ctx, aln, model, rank, world, out)
+            sharded.run_sharded(sh, None, local_rank)
+            sh.close()
+        else:
+            ctx.distance_into(aln, model, out)
         aln.close()
 
     for _ in range(args.warmup):
@@ -204,7 +210,10 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         total_ms = float(t.item())
         dist.barrier()
     ms_per_step = total_ms / args.steps
-    W = units(n, L) * world
+    W = units(n, L)  # the whole matrix, whatever the number of ranks
+    # this rank's share of the tiles (all of them on one GPU)
+    t0, t1, ntiles = api.shard_tiles(n, rank, world)
+    share = (t1 - t0) / ntiles
     result = {"ms_per_step": ms_per_step, "value": W / (ms_per_step * 1e-3), "clocks": clk,
               "count_ms": count_ms}
 
@@ -214,12 +223,12 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             # tcgen05 kernel: 4 int8 MACs (8 ops) per pair-column, against the
             # int8 dense tensor peak measured here with a cuBLAS GEMM.
             peak = int8_tensor_peak(local_rank)
-            achieved = 8.0 * units(n, L) / (cnt * 1e-3)
+            achieved = 8.0 * units(n, L) * share / (cnt * 1e-3)
             result["roofline"] = {
                 "bound": "tensor", "achieved": achieved / 1e12, "peak": peak / 1e12,
                 "unit": "TOP/s (int8)", "frac": achieved / peak,
                 "traffic": traffic_from_profiles(name),
-                "kernel": "tc_count_kernel", "kernel_ms": cnt,
+                "kernel": "tc_batch_kernel", "kernel_ms": cnt,
                 "peak_source": "cuBLAS int8 GEMM (torch._int_mm 8192^3, best of 10) measured on "
                                "this device in this run",
                 "ops_per_pair_column": 8,
@@ -229,17 +238,21 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             # POPC peak measured on this device.
             popc_peak, lop3_peak = ctx.probe_int_peaks()
             popc_w, lop3_w = OPS_PER_WORD[(type_, model)]
-            words = units(n, L) / 32.0
+            words = units(n, L) * share / 32.0
             achieved = popc_w * words / (cnt * 1e-3)
             result["roofline"] = {
                 "bound": "int", "pipe": "POPC", "achieved": achieved / 1e12,
                 "peak": popc_peak / 1e12, "unit": "Tops/s", "frac": achieved / popc_peak,
                 "traffic": traffic_from_profiles(name),
-                "kernel": "count_tiles_kernel", "kernel_ms": cnt,
+                "kernel": "count_batch_kernel" if world > 1 else "count_tiles_kernel",
+                "kernel_ms": cnt,
                 "lop3_frac": (lop3_w * words / (cnt * 1e-3)) / lop3_peak,
                 "peak_source": "rnj_probe_int_peaks, measured on this device in this run",
                 "ops_per_pair_word": {"popc": popc_w, "lop3": lop3_w},
             }
+    if world > 1:
+        result["e2e"] = run_e2e_sharded(ctx, seqs, typ, model, args, rank, world, local_rank)
+    elif rank == 0:
         result["e2e"] = run_e2e(ctx, seqs, typ, model, args)
     ctx.close()
     return result
@@ -264,6 +277,49 @@ def run_e2e(ctx, seqs, typ, model, args):
     return {"value": units(n, L) / mean, "unit": "pair-columns/s", "h2d_bytes_per_step": n * L,
             "d2h_bytes_per_step": n * n * 4, "ms_per_step": mean * 1e3, "steps": steps,
             "call": "rnj_distance_matrix_host"}
+
+
+def run_e2e_sharded(ctx, seqs, typ, model, args, rank, world, local_rank):
+    """The multi-GPU end to end: every rank uploads the host alignment (pinned),
+    packs it, computes its tiles, joins the one MAX all-reduce, applies the cap
+    and copies its own tiles into pinned host memory.  Time = max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from rapidnj_b200 import api, sharded
+    n, L = seqs.shape
+    pinned = torch.from_numpy(seqs).pin_memory()
+    host = torch.empty((n, n), dtype=torch.float32).pin_memory().numpy()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    steps = max(1, min(args.steps, 5))
+
+    def once():
+        with torch.cuda.stream(stream):
+            d = pinned.to(f"cuda:{local_rank}", non_blocking=True)
+        aln = ctx.alignment(d, typ, popcount=args.popcount)
+        sh = api.Shard(ctx, aln, model, rank, world)
+        sharded.run_sharded(sh, None, local_rank)
+        nbytes = sh.copy_tiles(host)
+        sh.close()
+        aln.close()
+        return nbytes
+
+    once()  # warm-up
+    dist.barrier()
+    times, d2h = [], 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        d2h = once()
+        times.append(time.perf_counter() - t0)
+    t = torch.tensor([sum(times) / len(times), float(d2h)], dtype=torch.float64,
+                     device=f"cuda:{local_rank}")
+    tot = t.clone()
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    mean = float(t[0].item())
+    return {"value": units(n, L) / mean, "unit": "pair-columns/s",
+            "h2d_bytes_per_step": n * L * world, "d2h_bytes_per_step": int(tot[1].item()),
+            "ms_per_step": mean * 1e3, "steps": steps,
+            "call": "rnj_aln_from_device + rnj_shard_run/finish + rnj_shard_copy_tiles per rank"}
 
 
 def run_batched(args, local_rank: int = 0, count: int = 256):
@@ -492,18 +548,19 @@ def main():
         line = {"metric": "pair-column comparisons/s", "value": res["value"],
                 "unit": "pair-columns/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
-                "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
-                "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": config,
-                "roofline": res["roofline"], "e2e": res["e2e"], "clocks": res["clocks"],
-                "gpu_launches": 3 * args.steps}
-        if not args.no_cpu_baseline:
+                "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "int8" if config["kernel"] == "tcgen05" else "u32",
+                "data": "synthetic", "config": config, "roofline": res["roofline"], "e2e": res["e2e"], "clocks": res["clocks"],
+                "gpu_launches": (4 if type_ == "protein" else 3) * args.steps}
+        if not args.no_cpu_baseline and world == 1:
             seqs = make_alignment(args.workload)
             cpu = cpu_reference(seqs, model, type_, 0, 1)
             line["cpu_baseline"] = ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
                                     if cpu else None)
-        if args.mode in ("all", "batched"):
+        # the batched and served forms are single-GPU (replicas at N > 1)
+        if args.mode in ("all", "batched") and world == 1:
             line["batched"] = run_batched(args, local_rank)
-        if args.mode in ("all", "served"):
+        if args.mode in ("all", "served") and world == 1:
             line["served"] = run_served(args, local_rank)
         print(json.dumps(line))
     if world > 1:

@@ -266,6 +266,47 @@ int rnj_server_stats(rnj_server *server, uint64_t *completed, double *pair_colum
                      double *seconds, size_t *bytes_in_use);
 int rnj_server_destroy(rnj_server *server);
 
+/* ------------------------------------------------------------ shards */
+
+/* One alignment over several GPUs, one process (and context) per GPU.  The
+ * triangle tiles (128 x 128 pairs; every tile with RNJ_FULL_ROWS -f alignments)
+ * are split into `nshards` contiguous ranges of equal tile count, in row-major
+ * order of the upper triangle; shard s computes range s into its own n x n
+ * device buffer (each tile and its mirror).  The post-process needs the maximum
+ * over the whole matrix before any saturated pair is replaced
+ * (KimuraDistance.cpp:366-395, JCdistance.cpp:201-230), so a shard runs in two
+ * steps around one exchange, which the caller makes with its own collective:
+ *   rnj_shard_run(shard, &local)         counts + transform, local maximum
+ *   global = max over shards of local    (one float, e.g. an NCCL all-reduce)
+ *   rnj_shard_finish(shard, global)      saturated pairs -> 2 * global
+ * Every shard holds the whole packed alignment (it is small next to the
+ * matrix).  No counterpart in the reference, which runs on one host. */
+typedef struct rnj_shard rnj_shard;
+/* Number of tiles of an n-sequence alignment and the range [tile0, tile1) of
+ * shard `shard` of `nshards`.  Host arithmetic only. */
+int rnj_shard_tiles(int n, int full_rows, int shard, int nshards, long long *tile0,
+                    long long *tile1, long long *ntiles);
+/* Row and column tile of linear tile index `tile` (row-major upper triangle, or
+ * row-major full square with full_rows).  Host arithmetic only. */
+int rnj_tile_coords(int n, int full_rows, long long tile, int *tile_row, int *tile_col);
+/* d_out: n rows of stride ld floats on the context's device (NULL: allocated by
+ * the shard and freed with it).  The alignment must outlive the shard. */
+int rnj_shard_create(rnj_ctx *ctx, rnj_aln *aln, int model, int shard, int nshards,
+                     float *d_out, size_t ld, rnj_shard **out);
+/* Computes this shard's tiles (saturated pairs hold -1) and returns their
+ * maximum distance (synchronises the context's stream). */
+int rnj_shard_run(rnj_shard *shard, float *local_max);
+/* Replaces the shard's saturated pairs with 2 * global_max and synchronises. */
+int rnj_shard_finish(rnj_shard *shard, float global_max);
+/* The shard's output (device pointer and stride). */
+int rnj_shard_output(rnj_shard *shard, float **d_out, size_t *ld);
+/* Copies the shard's own tiles (upper-triangle blocks; every block with
+ * RNJ_FULL_ROWS) into the host matrix `host` (n rows of stride host_ld floats),
+ * one 2-D copy per tile row; entries of other shards are not touched.  Returns
+ * the bytes copied in *bytes (may be NULL). */
+int rnj_shard_copy_tiles(rnj_shard *shard, float *host, size_t host_ld, size_t *bytes);
+int rnj_shard_destroy(rnj_shard *shard);
+
 /* ------------------------------------------------------- alignment files */
 
 /* A parsed multiple alignment on the host: names and n*L bytes (row-major). */

@@ -57,6 +57,10 @@ def lib():
         L.orc_matrix.restype = ctypes.c_float
         L.orc_matrix_full.argtypes = L.orc_matrix.argtypes
         L.orc_matrix_full.restype = ctypes.c_float
+        L.orc_raw_distances.argtypes = [u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        f32p]
+        L.orc_raw_distances.restype = None
         L.orc_detect_type.argtypes = [ctypes.c_char_p, ctypes.c_int]
         L.orc_detect_type.restype = ctypes.c_int
         L.orc_jc.argtypes = [ctypes.c_uint64] * 3 + [ctypes.c_int]
@@ -97,6 +101,17 @@ def matrix(cnt: np.ndarray, L: int, type_: int, model: int, naive: bool = False,
     mx = fn(np.ascontiguousarray(cnt, dtype=np.uint32).reshape(-1), n, L, type_, model,
             int(naive), int(compat_wrap), out.reshape(-1))
     return out, float(mx)
+
+
+def raw_distances(cnt: np.ndarray, L: int, type_: int, model: int, naive: bool = False,
+                  compat_wrap: bool = False, full: bool = False) -> np.ndarray:
+    """Distances before the post-process (saturated pairs are -1) for j > i (every
+    pair when ``full``); other entries zero."""
+    n = cnt.shape[0]
+    out = np.zeros((n, n), dtype=np.float32)
+    lib().orc_raw_distances(np.ascontiguousarray(cnt, dtype=np.uint32).reshape(-1), n, L, type_,
+                            model, int(naive), int(compat_wrap), int(full), out.reshape(-1))
+    return out
 
 
 def distance_matrix(seqs: np.ndarray, model: int, type_: int | None = None, naive: bool = False,

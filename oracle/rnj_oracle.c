@@ -273,3 +273,15 @@ float orc_matrix_full(const uint32_t *counts, int n, int L, int type, int model,
   }
   return maxd;
 }
+
+/* Distances before the post-process (saturated pairs stay -1, no mirror, no
+ * diagonal rule): every j > i, or every (i, j) when full.  Other entries are
+ * left as they are.  Checker for split computations that post-process later
+ * (the multi-GPU shards). */
+void orc_raw_distances(const uint32_t *counts, int n, int L, int type, int model, int naive,
+                       int compat_wrap, int full, float *out) {
+  for (int i = 0; i < n; i++)
+    for (int j = full ? 0 : i + 1; j < n; j++)
+      out[(size_t)i * n + j] = orc_distance(counts + ((size_t)i * n + j) * 3, L, type, model,
+                                            naive, compat_wrap);
+}

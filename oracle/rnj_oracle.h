@@ -31,6 +31,10 @@ float orc_matrix(const uint32_t *counts, int n, int L, int type, int model, int 
 float orc_matrix_full(const uint32_t *counts, int n, int L, int type, int model, int naive,
                       int compat_wrap, float *out);
 
+/* Pre-post-process distances (saturated = -1) for j > i, or every pair when full. */
+void orc_raw_distances(const uint32_t *counts, int n, int L, int type, int model, int naive,
+                       int compat_wrap, int full, float *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -90,6 +90,16 @@ SIGNATURES = {
     "rnj_server_stats": (c_int, [c_void_p, P(ctypes.c_uint64), P(ctypes.c_double),
                                  P(ctypes.c_double), P(c_size_t)]),
     "rnj_server_destroy": (c_int, [c_void_p]),
+    "rnj_shard_tiles": (c_int, [c_int, c_int, c_int, c_int, P(ctypes.c_longlong),
+                                P(ctypes.c_longlong), P(ctypes.c_longlong)]),
+    "rnj_tile_coords": (c_int, [c_int, c_int, ctypes.c_longlong, P(c_int), P(c_int)]),
+    "rnj_shard_create": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_size_t,
+                                 P(c_void_p)]),
+    "rnj_shard_run": (c_int, [c_void_p, P(c_float)]),
+    "rnj_shard_finish": (c_int, [c_void_p, c_float]),
+    "rnj_shard_output": (c_int, [c_void_p, P(c_void_p), P(c_size_t)]),
+    "rnj_shard_copy_tiles": (c_int, [c_void_p, c_void_p, c_size_t, P(c_size_t)]),
+    "rnj_shard_destroy": (c_int, [c_void_p]),
     "rnj_msa_read": (c_int, [c_char_p, c_char_p, P(c_void_p)]),
     "rnj_msa_info": (c_int, [c_void_p, P(c_int), P(c_int), P(c_int)]),
     "rnj_msa_name": (c_char_p, [c_void_p, c_int]),

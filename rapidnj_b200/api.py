@@ -298,6 +298,67 @@ class Batch:
             pass
 
 
+def shard_tiles(n: int, shard: int, nshards: int, full_rows: bool = False):
+    """(tile0, tile1, ntiles): the contiguous tile range of one shard (host only)."""
+    t0, t1, nt = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    check(N.lib().rnj_shard_tiles(n, int(full_rows), shard, nshards, ctypes.byref(t0),
+                                  ctypes.byref(t1), ctypes.byref(nt)))
+    return t0.value, t1.value, nt.value
+
+
+def tile_coords(n: int, tile: int, full_rows: bool = False):
+    """(tile_row, tile_col) of a linear tile index (host only)."""
+    r, c = ctypes.c_int(), ctypes.c_int()
+    check(N.lib().rnj_tile_coords(n, int(full_rows), tile, ctypes.byref(r), ctypes.byref(c)))
+    return r.value, c.value
+
+
+class Shard:
+    """One GPU's share of one alignment's tiles (rnj_shard): run() gives the
+    local maximum, finish(global_max) applies the saturation cap."""
+
+    def __init__(self, ctx: Context, aln: Alignment, model, shard: int, nshards: int, out=None):
+        h = ctypes.c_void_p()
+        ptr = ctypes.c_void_p(out.data_ptr()) if out is not None else None
+        ld = out.stride(0) if out is not None else 0
+        check(N.lib().rnj_shard_create(ctx.handle, aln.handle, MODELS[model], shard, nshards, ptr,
+                                       ld, ctypes.byref(h)))
+        self.ctx, self.aln, self.handle = ctx, aln, h
+        self.n = aln.n
+
+    def run(self) -> float:
+        m = ctypes.c_float()
+        check(N.lib().rnj_shard_run(self.handle, ctypes.byref(m)))
+        return m.value
+
+    def finish(self, global_max: float) -> None:
+        check(N.lib().rnj_shard_finish(self.handle, ctypes.c_float(global_max)))
+
+    def output(self):
+        p, ld = ctypes.c_void_p(), ctypes.c_size_t()
+        check(N.lib().rnj_shard_output(self.handle, ctypes.byref(p), ctypes.byref(ld)))
+        return p.value, ld.value
+
+    def copy_tiles(self, host: np.ndarray) -> int:
+        """Copies this shard's tiles into a float32 (n, >= n) C-contiguous host array."""
+        assert host.dtype == np.float32 and host.flags.c_contiguous and host.shape[0] == self.n
+        nbytes = ctypes.c_size_t()
+        check(N.lib().rnj_shard_copy_tiles(self.handle, host.ctypes.data, host.shape[1],
+                                           ctypes.byref(nbytes)))
+        return nbytes.value
+
+    def close(self) -> None:
+        if self.handle and self.ctx.handle:
+            N.lib().rnj_shard_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Server:
     """Continuous-batching distance server (rnj_server) with its own device context."""
 

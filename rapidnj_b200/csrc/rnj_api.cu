@@ -432,6 +432,8 @@ int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t 
 
 }  // namespace
 
+void ctx_mark(rnj_ctx *ctx, int stage, int end) { mark(ctx, stage, end); }
+
 extern "C" {
 
 const char *rnj_version(void) { return "rapidnj-b200 0.1.0 (sm_100a)"; }

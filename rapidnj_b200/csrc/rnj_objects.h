@@ -45,6 +45,10 @@ void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *k
 int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
                   int flags, int kind, const uint8_t lut[256], rnj_aln **out);
 
+// Profiling marks on the context stream (stage 0 pack, 1 count, 2 fix-up;
+// end 0 = begin), read back by rnj_ctx_stage_times.
+void ctx_mark(rnj_ctx *ctx, int stage, int end);
+
 // A batch whose runs do not make the context stream wait (the server follows
 // completion through the batch's event and keeps packing the next batch).
 void batch_set_join(rnj_batch *b, bool join);
