@@ -39,6 +39,10 @@ def build() -> None:
     if os.path.isdir(os.environ.get("RNJ_REFERENCE", "/root/reference")):
         subprocess.run(["make", "-s", "-C", HERE, "ref",
                         "REF=" + os.environ.get("RNJ_REFERENCE", "/root/reference")], check=True)
+        if os.path.exists(os.path.join(HERE, "..", "rapidnj_b200", "librnjgpu.so")):
+            subprocess.run(["make", "-s", "-C", HERE, "dropin",
+                            "REF=" + os.environ.get("RNJ_REFERENCE", "/root/reference")],
+                           check=True)
 
 
 def lib():
