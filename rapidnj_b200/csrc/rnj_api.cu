@@ -72,16 +72,17 @@ int encode_planes_map(Packed &p) {
   return RNJ_OK;
 }
 
-// 2-D map over the int8 feature rows: (4 * Lk bytes, Np rows), 128 x 128 box,
-// 128-byte swizzle (the layout the tcgen05 shared-memory descriptors expect).
+// 3-D map over the K-blocked FP4 features: (128 bytes, Np rows, 4 * Lk / 256
+// blocks), box 128 x 128 x 1 = one contiguous 16 KB run, 128-byte swizzle (the
+// layout the tcgen05 shared-memory descriptors expect).
 int encode_features_map(Packed &p) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-  cuuint64_t dims[2] = {(cuuint64_t)4 * p.Lk, (cuuint64_t)p.Np};
-  cuuint64_t strides[1] = {(cuuint64_t)4 * p.Lk};
-  cuuint32_t box[2] = {128, (cuuint32_t)kTile};
-  cuuint32_t estr[2] = {1, 1};
-  CUresult r = fn(&p.fmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, p.feat, dims, strides, box, estr,
+  cuuint64_t dims[3] = {128, (cuuint64_t)p.Np, (cuuint64_t)(4 * p.Lk / 256)};
+  cuuint64_t strides[2] = {128, (cuuint64_t)p.Np * 128};
+  cuuint32_t box[3] = {128, (cuuint32_t)kTile, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(&p.fmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, p.feat, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS)
@@ -291,12 +292,12 @@ int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
   p.W = (L + 31) / 32;
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
-  if (kind == KIND_DNA && !(flags & RNJ_POPCOUNT)) {
-    // int8 feature rows for the tensor-core kernel instead of bit planes.
+  if (kind == KIND_DNA && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns) {
+    // FP4 feature rows for the tensor-core kernel instead of bit planes.
     p.kind = KIND_DNA_TC;
     p.NP = 0;
-    p.Lk = std::max(128, (L + 127) / 128 * 128);
-    const size_t fbytes = (size_t)p.Np * 4 * p.Lk;
+    p.Lk = std::max(256, (L + 255) / 256 * 256);
+    const size_t fbytes = (size_t)p.Np * 4 * p.Lk / 2;
     cudaError_t e = cudaMallocAsync((void **)&p.feat, fbytes, ctx->stream);
     if (e != cudaSuccess) {
       delete a;
@@ -640,15 +641,15 @@ int rnj_aln_from_bitstrings(rnj_ctx *ctx, const unsigned int *const *bit_strings
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
   p.NP = 3;
-  const bool tc = !(flags & RNJ_POPCOUNT);
+  const bool tc = !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns;
   uint32_t *db = nullptr;
   cudaError_t e = cudaMallocAsync((void **)&db, std::max<size_t>(words * 8, 8), ctx->stream);
   if (tc) {
     p.kind = KIND_DNA_TC;
     p.NP = 0;
-    p.Lk = std::max(128, (L + 127) / 128 * 128);
+    p.Lk = std::max(256, (L + 255) / 256 * 256);
     if (e == cudaSuccess)
-      e = cudaMallocAsync((void **)&p.feat, (size_t)p.Np * 4 * p.Lk, ctx->stream);
+      e = cudaMallocAsync((void **)&p.feat, (size_t)p.Np * 4 * p.Lk / 2, ctx->stream);
   } else if (e == cudaSuccess) {
     e = cudaMallocAsync((void **)&p.planes, (size_t)p.NP * p.Wp * p.Np * 4, ctx->stream);
   }

@@ -64,8 +64,9 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 }
 
 // 3-D tiled TMA load (no multicast): box lands in shared memory with dim0
-// fastest.  c0 (the sequence index, 4-byte elements) is always a multiple of
-// the 128-row tile, so c0 * 4 is a multiple of 16 bytes as TMA requires.
+// fastest.  c0 is always 16-byte aligned as TMA requires: for bit planes it is
+// a sequence index (4-byte elements) that is a multiple of the 128-row tile, for
+// the K-blocked tensor-core features it is 0.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
                                             int c0, int c1, int c2) {
   asm volatile(

@@ -18,7 +18,7 @@ namespace rnj {
 //   KIND_MISM2  planes {c0, c1, valid}         -> {mismatch, valid}
 //   KIND_MISM5  planes {c0..c4, valid}         -> {mismatch, valid}
 //   KIND_MISM7  planes {c0..c6, valid}         -> {mismatch, valid}
-//   KIND_DNA_TC int8 features {v | r | t | u}   -> {ts, tv, valid} on tensor cores
+//   KIND_DNA_TC FP4 features {v | r | t | u}    -> {ts, tv, valid} on tensor cores
 enum Kind {
   KIND_DNA = 0, KIND_NAIVE = 1, KIND_MISM2 = 2, KIND_MISM5 = 3, KIND_MISM7 = 4, KIND_DNA_TC = 5
 };
@@ -27,6 +27,9 @@ constexpr int kTile = 128;        // pairs per tile edge (rows and columns)
 constexpr int kWordBits = 32;     // sites per plane word
 constexpr int kKW = 8;            // words per pipeline stage
 constexpr int kMaxFusedWords = 2047;  // 16-bit packed accumulators: L <= 65504 per pass
+// The tensor-core sums reach 2L in magnitude and stay exact in f32 while below
+// 2^24; longer DNA alignments are counted on the bit-plane kernels.
+constexpr int kMaxTcColumns = 1 << 22;
 
 __host__ __device__ inline int planes_of(int kind) {
   switch (kind) {
@@ -50,10 +53,14 @@ struct Packed {
   int NP = 0;            // planes
   uint32_t *planes = nullptr;  // NP * Wp * Np words, word-major, sequence fastest
   CUtensorMap tmap;      // 3-D map over (Np, Wp, NP), box (kTile, kKW, NP)
-  // Tensor-core layout (KIND_DNA_TC): Np rows of 4 * Lk int8 features.
-  int8_t *feat = nullptr;
-  int Lk = 0;            // L rounded up to 128
-  CUtensorMap fmap;      // 2-D map over (4 * Lk bytes, Np), box (128, 128), 128-byte swizzle
+  // Tensor-core layout (KIND_DNA_TC): the Np x (4 * Lk) FP4 feature matrix
+  // [v | r | t | u], two columns per byte, cut into K blocks of 256 columns
+  // (128 bytes), block-major: column k of row i in byte
+  // ((k / 256) * Np + i) * 128 + (k % 256) / 2, so the 128-row slab of one K
+  // block is a contiguous 16 KB run.
+  uint8_t *feat = nullptr;
+  int Lk = 0;            // L rounded up to 256
+  CUtensorMap fmap;      // 3-D map over (128, Np, 4 * Lk / 256), box (128, 128, 1), 128-byte swizzle
 };
 
 struct EpiParams {
@@ -82,7 +89,7 @@ struct alignas(128) AlnDesc {
   int *max_bits;              // per-alignment max slot (float bits)
   int *tile_flags;            // per-alignment saturation flags, one per triangle tile
   int *err;                   // shared error word
-  int n, L, nt, kdim;         // kdim: Lk (tensor-core) or Wp (popcount)
+  int n, L, nt, kdim;         // kdim: Lk columns (tensor-core) or Wp words (popcount)
   int model, type, compat, full;
   int kind, np, pad0, pad1;
   double jc_b;
@@ -116,9 +123,9 @@ cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s);
 cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s);
 // Tensor-core DNA path (rnj_tc.cu).
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
-                                 int8_t *F, cudaStream_t s);
+                                 uint8_t *F, cudaStream_t s);
 cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_gaps, int bs_words,
-                                      int n, int L, int Np, int Lk, int8_t *F, cudaStream_t s);
+                                      int n, int L, int Np, int Lk, uint8_t *F, cudaStream_t s);
 int encode_features_map(Packed &p);
 // Batched popcount path (rnj_kernels.cu): persistent, atomic item counter.
 cudaError_t launch_count_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,

@@ -64,7 +64,7 @@ size_t bytes_needed(int n, int L, int type, int flags) {
   const size_t raw = (size_t)n * L;
   size_t packed;
   if (type == RNJ_DNA && (flags & RNJ_FASTDIST) && !(flags & RNJ_POPCOUNT))
-    packed = np * 4 * round_up((size_t)std::max(L, 1), 128);
+    packed = np * 2 * round_up((size_t)std::max(L, 1), 256);  // 4 FP4 features per site
   else
     packed = (size_t)8 * np * round_up((size_t)(L + 31) / 32, 8) * 4;
   const size_t out = (size_t)n * round_up((size_t)std::max(n, 4), 4) * 4;

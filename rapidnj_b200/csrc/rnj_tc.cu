@@ -1,7 +1,7 @@
 // rnj_tc.cu -- DNA pair counting on the 5th-generation tensor cores (tcgen05).
 //
-// Encoding.  Every valid site of a sequence becomes four signed 8-bit features
-// (v, r, t, u): v = 1; r = +1 for a purine (A, G), -1 for a pyrimidine (C, T);
+// Encoding.  Every valid site of a sequence becomes four features (v, r, t, u)
+// in {-1, 0, +1}: v = 1; r = +1 for a purine (A, G), -1 for a pyrimidine (C, T);
 // t = +1 for A and C, -1 for G and T; u = r * t.  A gap is (0, 0, 0, 0).  For
 // two sites of a pair the products satisfy
 //   identical:     vv' = 1, rr' = 1, tt' + uu' =  2
@@ -11,16 +11,26 @@
 //   valid = V,   transitions = (V + R - T) / 4,   transversions = (V - R) / 2,
 // exactly (integers), which are the counts bitDistanceGap.cpp:146-161 produces.
 // The three sums are three Gram matrices of the feature matrix F (n x 4L): the
-// v block (K = L), the r block (K = L) and the t|u block (K = 2L): 4 int8 MACs
-// per pair-column, accumulated in int32 in tensor memory.
+// v block (K = L), the r block (K = L) and the t|u block (K = 2L): 4 MACs per
+// pair-column.
+//
+// Number format.  The features are stored as FP4 (e2m1: +1 = 0x2, -1 = 0xA,
+// 0 = 0x0), two per byte, and multiplied by tcgen05.mma.kind::mxf4 with every
+// block scale factor 1.0 (UE8M0 127) into f32 accumulators.  Every product is
+// -1, 0 or +1 and every partial sum an integer of magnitude <= 2L < 2^24, so
+// the f32 sums are exact and convert to the integer counts without rounding.
+// FP4 halves the operand bytes per MAC of an 8-bit encoding, and the FP4
+// tensor rate is twice the 8-bit one.
 //
 // Kernel.  Persistent, one CTA per SM, over a work list of 128 x 128 triangle
 // tiles (of one alignment, or of many in a batch), 320 threads:
-//   warp 0       TMA producer: 128-row x 128-byte K-blocks of both row tiles,
-//                128-byte swizzle, into a 6-stage mbarrier ring
-//   warp 1       TMEM owner and MMA issuer: tcgen05.mma.kind::i8, M = N = 128,
-//                K = 32 per instruction, three accumulators (V, R, T) of 128
-//                columns each; tcgen05.commit releases stages and signals the end
+//   warp 0       TMA producer: 128-row x 128-byte (256-column) K-blocks of both
+//                row tiles (one contiguous 16 KB run each in the K-blocked
+//                layout), 128-byte swizzle, into a 7-stage mbarrier ring
+//   warp 1       TMEM owner and MMA issuer: M = N = 128, K = 64 per instruction,
+//                three accumulators (V, R, T) of 128 columns each, the scale
+//                factors in the last 128 columns; tcgen05.commit releases
+//                stages and signals the end of a tile
 //   warps 2..9   epilogue: per 32-column chunk, tcgen05.ld of the accumulators,
 //                the exact transform and the stores (tile rows as float4, the
 //                mirror image with warp-coalesced column stores); then TMEM is
@@ -37,12 +47,14 @@
 
 namespace rnj {
 
-constexpr int kTcStages = 6;
-constexpr int kTcKBlock = 128;                            // bytes of K per stage
+constexpr int kTcStages = 7;
+constexpr int kTcKBlock = 128;                            // bytes of K per stage (256 FP4 columns)
+constexpr int kTcKCols = 256;                             // feature columns per stage
 constexpr uint32_t kTcTileBytes = kTile * kTcKBlock;      // 16 KB per operand tile
 constexpr uint32_t kTcStageBytes = 2 * kTcTileBytes;      // A + B
 constexpr int kTcThreads = 320;
-constexpr uint32_t kTmemCols = 512;                       // 3 x 128 used
+constexpr uint32_t kTmemCols = 512;                       // 3 x 128 accumulators + scale factors
+constexpr uint32_t kTmemSfa = 384, kTmemSfb = 448;        // scale-factor columns (all 1.0)
 constexpr size_t kTcSmemBytes = (size_t)kTcStages * kTcStageBytes + 1024 + 256;
 
 // ---------------------------------------------------------------- tcgen05 PTX
@@ -70,14 +82,29 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
                    smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void tc_mma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                          uint32_t idesc, uint32_t accumulate) {
+// D (f32, tensor memory) (+)= A x B^T with FP4 operands from shared memory and
+// block scale factors from tensor memory (block of 32 columns).
+__device__ __forceinline__ void tc_mma_fp4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t sfa_tmem, uint32_t sfb_tmem,
+                                           uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}"
+      ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa_tmem),
+      "r"(sfb_tmem)
       : "memory");
+}
+// 32 lanes x 32 columns of 32-bit words from registers into tensor memory.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, uint32_t x) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+      "%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1};"
+      ::"r"(taddr), "r"(x)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_st_wait() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
@@ -98,14 +125,6 @@ __device__ __forceinline__ void tmem_ld_wait() {
 __device__ __forceinline__ void named_barrier(int id, int threads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0,
-                                            int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
-      : "memory");
-}
 
 // Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, 8-row
 // groups 1024 bytes apart (stride byte offset), descriptor version 1.
@@ -119,10 +138,11 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
   return d;
 }
 
-// Instruction descriptor, kind::i8: D s32 (bits 4-5 = 2), A and B signed 8-bit
-// (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28.
-constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) |
-                              ((uint32_t)(kTile >> 4) << 24);
+// Instruction descriptor, kind::mxf4 (block-scaled layout): A and B E2M1
+// (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bits 17-22, scale factors
+// UE8M0 (bit 23), M >> 4 at bits 24-28, scale-factor ids 0, dense K = 64.
+constexpr uint32_t kIdescFp4 = (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) | (1u << 23) |
+                               ((uint32_t)(kTile >> 4) << 24);
 
 // A bounded wait that also gives up early once another role has aborted.
 __device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
@@ -140,12 +160,47 @@ __device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile
 
 // --------------------------------------------------------------- feature pack
 
-// chars (n rows, stride ld) -> F (Np rows, 4 * Lk bytes): [v | r | t | u] blocks
-// of Lk bytes each; padding rows and columns are zero.  One thread per
-// (sequence, 16-column chunk); writes 4 x 16 bytes.
+// FP4 (e2m1) codes of the feature values: +1 = 0x2, -1 = 0xA (sign bit 3), 0 = 0.
+__device__ __forceinline__ uint32_t fp4_of(int x) { return x > 0 ? 0x2u : (x < 0 ? 0xAu : 0u); }
+
+// The 32 features of feature block f (0 v, 1 r, 2 t, 3 u) of sequence i,
+// columns 32c .. 32c+31 (16 bytes, two per byte, column 32c + k in nibble k of
+// the 128-bit word), in the K-blocked layout (see Packed::feat).
+__device__ __forceinline__ uint4 *feat_chunk(uint8_t *F, int Np, int Lk, int f, int i, int c) {
+  const size_t kb = (size_t)f * (Lk / 256) + (c >> 3);
+  return reinterpret_cast<uint4 *>(F + (kb * Np + i) * 128 + (c & 7) * 16);
+}
+
+// Accumulates one site's features (k = 0..31 within the chunk).  code: A=0 G=1
+// T=2 C=3 (stdinclude.h:25), or -1 for a gap.
+__device__ __forceinline__ void add_site(int k, int code, uint32_t (&v)[4], uint32_t (&r)[4],
+                                         uint32_t (&t)[4], uint32_t (&u)[4]) {
+  if (code < 0) return;
+  const int rr = (code < 2) ? 1 : -1;                 // purine A, G
+  const int ts = (code == 0 || code == 3) ? 1 : -1;  // A, C
+  const int w = k >> 3, sh = (k & 7) * 4;
+  v[w] |= fp4_of(1) << sh;
+  r[w] |= fp4_of(rr) << sh;
+  t[w] |= fp4_of(ts) << sh;
+  u[w] |= fp4_of(rr * ts) << sh;
+}
+
+__device__ __forceinline__ void store_chunk(uint8_t *F, int Np, int Lk, int i, int c,
+                                            const uint32_t (&v)[4], const uint32_t (&r)[4],
+                                            const uint32_t (&t)[4], const uint32_t (&u)[4]) {
+  *feat_chunk(F, Np, Lk, 0, i, c) = make_uint4(v[0], v[1], v[2], v[3]);
+  *feat_chunk(F, Np, Lk, 1, i, c) = make_uint4(r[0], r[1], r[2], r[3]);
+  *feat_chunk(F, Np, Lk, 2, i, c) = make_uint4(t[0], t[1], t[2], t[3]);
+  *feat_chunk(F, Np, Lk, 3, i, c) = make_uint4(u[0], u[1], u[2], u[3]);
+}
+
+// chars (n rows, stride ld) -> F (Np rows of 4 * Lk FP4 features [v | r | t | u],
+// K-blocked); padding rows and columns are zero.  One thread per (sequence,
+// 32-column chunk); writes 4 x 16 bytes.  Valid sites are A/C/G/T in either
+// case (dataloaderFasta.hpp:155-180).
 __global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t ld, int n, int L,
-                                     int Np, int Lk, int8_t *__restrict__ F) {
-  const int chunks = Lk / 16;
+                                     int Np, int Lk, uint8_t *__restrict__ F) {
+  const int chunks = Lk / 32;
   const long long total = (long long)Np * chunks;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
@@ -153,74 +208,57 @@ __global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t l
     const int c = (int)(t % chunks);
     uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
     if (i < n) {
-      const uint8_t *src = chars + (size_t)i * ld + c * 16;
+      const uint8_t *src = chars + (size_t)i * ld + c * 32;
 #pragma unroll
-      for (int b = 0; b < 16; ++b) {
-        const int k = c * 16 + b;
-        if (k >= L) break;
-        int vv = 1, rr, ts;
+      for (int b = 0; b < 32; ++b) {
+        if (c * 32 + b >= L) break;
+        int code;
         switch (src[b]) {
-          case 'A': case 'a': rr = 1; ts = 1; break;
-          case 'G': case 'g': rr = 1; ts = -1; break;
-          case 'C': case 'c': rr = -1; ts = 1; break;
-          case 'T': case 't': rr = -1; ts = -1; break;
-          default: vv = 0; rr = 0; ts = 0; break;
+          case 'A': case 'a': code = 0; break;
+          case 'G': case 'g': code = 1; break;
+          case 'T': case 't': code = 2; break;
+          case 'C': case 'c': code = 3; break;
+          default: code = -1; break;
         }
-        const int sh = (b & 3) * 8;
-        v[b >> 2] |= (uint32_t)(uint8_t)vv << sh;
-        r[b >> 2] |= (uint32_t)(uint8_t)(int8_t)rr << sh;
-        tt[b >> 2] |= (uint32_t)(uint8_t)(int8_t)ts << sh;
-        u[b >> 2] |= (uint32_t)(uint8_t)(int8_t)(rr * ts) << sh;
+        add_site(b, code, v, r, tt, u);
       }
     }
-    int8_t *row = F + (size_t)i * 4 * Lk + c * 16;
-    *reinterpret_cast<uint4 *>(row) = make_uint4(v[0], v[1], v[2], v[3]);
-    *reinterpret_cast<uint4 *>(row + Lk) = make_uint4(r[0], r[1], r[2], r[3]);
-    *reinterpret_cast<uint4 *>(row + 2 * (size_t)Lk) = make_uint4(tt[0], tt[1], tt[2], tt[3]);
-    *reinterpret_cast<uint4 *>(row + 3 * (size_t)Lk) = make_uint4(u[0], u[1], u[2], u[3]);
+    store_chunk(F, Np, Lk, i, c, v, r, tt, u);
   }
 }
 
 // The reference loader's DNA layout (16 sites per uint32, 2-bit codes A=00 G=01
 // T=10 C=11, gap filter 01 per valid site, dataloaderFasta.hpp:147-182) ->
-// features.  One thread per (sequence, source word) = 16 sites.
+// features.  One thread per (sequence, 32 sites) = two source words.
 __global__ void pack_features_bits_kernel(const uint32_t *__restrict__ bits,
                                           const uint32_t *__restrict__ gaps, int bs_words, int n,
-                                          int L, int Np, int Lk, int8_t *__restrict__ F) {
-  const int chunks = Lk / 16;
+                                          int L, int Np, int Lk, uint8_t *__restrict__ F) {
+  const int chunks = Lk / 32;
   const long long total = (long long)Np * chunks;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / chunks);
     const int c = (int)(t % chunks);
     uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
-    if (i < n && c < bs_words) {
-      const uint32_t b = bits[(size_t)i * bs_words + c];
-      const uint32_t g = gaps[(size_t)i * bs_words + c];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int wd = 2 * c + h;
+      if (i >= n || wd >= bs_words) continue;
+      const uint32_t b = bits[(size_t)i * bs_words + wd];
+      const uint32_t g = gaps[(size_t)i * bs_words + wd];
 #pragma unroll
       for (int k = 0; k < 16; ++k) {
-        if (c * 16 + k >= L || !((g >> (2 * k)) & 1u)) continue;
-        const uint32_t code = (b >> (2 * k)) & 3u;  // A=0 G=1 T=2 C=3
-        const int rr = (code < 2) ? 1 : -1;
-        const int ts = (code == 0 || code == 3) ? 1 : -1;
-        const int sh = (k & 3) * 8;
-        v[k >> 2] |= 1u << sh;
-        r[k >> 2] |= (uint32_t)(uint8_t)(int8_t)rr << sh;
-        tt[k >> 2] |= (uint32_t)(uint8_t)(int8_t)ts << sh;
-        u[k >> 2] |= (uint32_t)(uint8_t)(int8_t)(rr * ts) << sh;
+        const bool ok = wd * 16 + k < L && ((g >> (2 * k)) & 1u);
+        add_site(16 * h + k, ok ? (int)((b >> (2 * k)) & 3u) : -1, v, r, tt, u);
       }
     }
-    int8_t *row = F + (size_t)i * 4 * Lk + c * 16;
-    *reinterpret_cast<uint4 *>(row) = make_uint4(v[0], v[1], v[2], v[3]);
-    *reinterpret_cast<uint4 *>(row + Lk) = make_uint4(r[0], r[1], r[2], r[3]);
-    *reinterpret_cast<uint4 *>(row + 2 * (size_t)Lk) = make_uint4(tt[0], tt[1], tt[2], tt[3]);
-    *reinterpret_cast<uint4 *>(row + 3 * (size_t)Lk) = make_uint4(u[0], u[1], u[2], u[3]);
+    store_chunk(F, Np, Lk, i, c, v, r, tt, u);
   }
 }
 
 cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_gaps, int bs_words,
-                                      int n, int L, int Np, int Lk, int8_t *F, cudaStream_t s) {
-  const long long work = (long long)Np * (Lk / 16);
+                                      int n, int L, int Np, int Lk, uint8_t *F, cudaStream_t s) {
+  const long long work = (long long)Np * (Lk / 32);
   long long g = (work + 255) / 256;
   if (g > 148LL * 64) g = 148LL * 64;
   if (g < 1) g = 1;
@@ -257,11 +295,45 @@ __device__ __forceinline__ void item_tile(const AlnDesc &d, int tile, int &ti, i
   }
 }
 
-__device__ __forceinline__ WorkItem item_at(const WorkItem *items, int it) {
+// Work order of a single alignment's triangle (no explicit work list): bands of
+// kBand tile rows, each walked column by column (within a column, its rows of
+// the band).  The kernels resident at one time then share about kBand row tiles
+// and 148 / kBand column tiles of operands instead of two rows and every
+// column, which keeps the operand working set of the running tiles in L2.
+// Returns the tile's row-major triangle index (the index of its saturation flag).
+constexpr int kBand = 12;
+
+__device__ __forceinline__ int banded_tile(int it, int nt) {
+  int r0 = 0;
+  while (true) {
+    const int g = min(kBand, nt - r0);
+    const int tri = g * (g + 1) / 2;
+    const int count = tri + (nt - r0 - g) * g;
+    if (it < count || r0 + g >= nt) {
+      int ti, tj;
+      if (it < tri) {
+        int c = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
+        while (c * (c + 1) / 2 > it) --c;
+        while ((c + 1) * (c + 2) / 2 <= it) ++c;
+        tj = r0 + c;
+        ti = r0 + (it - c * (c + 1) / 2);
+      } else {
+        const int k = it - tri;
+        tj = r0 + g + k / g;
+        ti = r0 + k % g;
+      }
+      return ti * nt - ti * (ti - 1) / 2 + (tj - ti);
+    }
+    it -= count;
+    r0 += g;
+  }
+}
+
+__device__ __forceinline__ WorkItem item_at(const AlnDesc *descs, const WorkItem *items, int it) {
   if (items) return items[it];
   WorkItem w;
   w.aln = 0;
-  w.tile = it;
+  w.tile = descs[0].full ? it : banded_tile(it, descs[0].nt);
   return w;
 }
 
@@ -302,6 +374,18 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // Block scale factors: every byte of columns kTmemSfa..511 of all 128 lanes is
+  // UE8M0 127 (2^0); the MMAs read theirs from kTmemSfa and kTmemSfb.
+  if (warp >= 2) {
+    const uint32_t base = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kTmemSfa +
+                          64u * (uint32_t)((warp - 2) >> 2);
+    tmem_st32(base, 0x7F7F7F7Fu);
+    tmem_st32(base + 32, 0x7F7F7F7Fu);
+    tmem_st_wait();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
   uint32_t issued = 0;  // producer: k-blocks issued in total (thread 0 only)
 
   if (warp == 0) {
@@ -309,12 +393,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // ----------------------------------------------------------- producer
       uint32_t gkb = 0;
       for (int it = blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x) {
-        const WorkItem w = item_at(items, it);
+        const WorkItem w = item_at(descs, items, it);
         const AlnDesc &d = descs[w.aln];
         tensormap_acquire(&d.map);
         int ti, tj;
         item_tile(d, w.tile, ti, tj);
-        const int nkb = 4 * d.kdim / kTcKBlock;
+        const int nkb = 4 * d.kdim / kTcKCols;
         for (int kb = 0; kb < nkb; ++kb, ++gkb) {
           const int s = gkb % kTcStages;
           if (!tc_wait(&empty_bar[s], ((gkb / kTcStages) & 1) ^ 1, abort_flag)) {
@@ -323,8 +407,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           }
           uint8_t *a = smem + s * kTcStageBytes;
           mbar_arrive_expect_tx(&full_bar[s], kTcStageBytes);
-          tma_load_2d(a, &d.map, &full_bar[s], kb * kTcKBlock, ti * kTile);
-          tma_load_2d(a + kTcTileBytes, &d.map, &full_bar[s], kb * kTcKBlock, tj * kTile);
+          tma_load_3d(a, &d.map, &full_bar[s], 0, ti * kTile, kb);
+          tma_load_3d(a + kTcTileBytes, &d.map, &full_bar[s], 0, tj * kTile, kb);
           issued = gkb + 1;
         }
       }
@@ -334,10 +418,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       // -------------------------------------------------------- MMA issuer
       uint32_t gkb = 0, titer = 0;
       for (int it = blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x, ++titer) {
-        const WorkItem w = item_at(items, it);
+        const WorkItem w = item_at(descs, items, it);
         const AlnDesc &d = descs[w.aln];
-        const int nkb = 4 * d.kdim / kTcKBlock;
-        const int seg = d.kdim / kTcKBlock;
+        const int nkb = 4 * d.kdim / kTcKCols;
+        const int seg = d.kdim / kTcKCols;
         // The epilogue of the previous item must have read the accumulators.
         if (!tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag)) {
           *abort_flag = 1;
@@ -358,9 +442,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const uint64_t adesc = smem_desc_sw128(a_addr);
           const uint64_t bdesc = smem_desc_sw128(a_addr + kTcTileBytes);
 #pragma unroll
-          for (int kk = 0; kk < kTcKBlock / 32; ++kk)
-            tc_mma_i8(tmem + acc * kTile, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2),
-                      kIdescI8, (first && kk == 0) ? 0u : 1u);
+          for (int kk = 0; kk < kTcKBlock / 32; ++kk)  // 32 bytes = 64 columns per MMA
+            tc_mma_fp4(tmem + acc * kTile, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2),
+                       kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, (first && kk == 0) ? 0u : 1u);
           tc_commit(&empty_bar[s]);
         }
         if (!ok) {
@@ -381,7 +465,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int row = 32 * q + lane;
     uint32_t titer = 0;
     for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++titer) {
-      const WorkItem w = item_at(items, it);
+      const WorkItem w = item_at(descs, items, it);
       const AlnDesc &d = descs[w.aln];
       int ti, tj;
       item_tile(d, w.tile, ti, tj);
@@ -423,7 +507,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             for (int u = 0; u < 4; ++u) {
               const int k = c4 + u;
               const int j = jb + k;
-              const int vv = (int)V[k], rr = (int)R[k], tu = (int)T[k];
+              const int vv = __float2int_rn(__uint_as_float(V[k]));
+              const int rr = __float2int_rn(__uint_as_float(R[k]));
+              const int tu = __float2int_rn(__uint_as_float(T[k]));
               const uint32_t ts = (uint32_t)((vv + rr - tu) >> 2);
               const uint32_t tv = (uint32_t)((vv - rr) >> 1);
               okc[u] = d.full ? (i < n && j < n && i != j) : (i < j && j < n);
@@ -457,7 +543,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
               const int j = jb + k;
               const bool ok = d.full ? (j < n) : (i < j && j < n);
               if (!ok) continue;
-              const int vv = (int)V[k], rr = (int)R[k], tu = (int)T[k];
+              const int vv = __float2int_rn(__uint_as_float(V[k]));
+              const int rr = __float2int_rn(__uint_as_float(R[k]));
+              const int tu = __float2int_rn(__uint_as_float(T[k]));
               uint32_t *o = d.counts + ((size_t)i * n + j) * 3;
               o[0] = (uint32_t)((vv + rr - tu) >> 2);
               o[1] = (uint32_t)((vv - rr) >> 1);
@@ -500,8 +588,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ------------------------------------------------------------------ launchers
 
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
-                                 int8_t *F, cudaStream_t s) {
-  const long long work = (long long)Np * (Lk / 16);
+                                 uint8_t *F, cudaStream_t s) {
+  const long long work = (long long)Np * (Lk / 32);
   long long g = (work + 255) / 256;
   if (g > 148LL * 64) g = 148LL * 64;
   if (g < 1) g = 1;
