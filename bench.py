@@ -74,10 +74,15 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi needs a moment to start: begin timing once it samples.
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()
         except Exception:
             self.proc = None
         return self
@@ -220,18 +225,16 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     if rank == 0:
         cnt = sum(count_ms) / len(count_ms)
         if type_ == "dna" and not args.popcount:
-            # tcgen05 kernel: 4 int8 MACs (8 ops) per pair-column, against the
-            # int8 dense tensor peak measured here with a cuBLAS GEMM.
-            peak = int8_tensor_peak(local_rank)
+            # tcgen05 kernel: 4 FP4 MACs (8 flops) per pair-column, against the
+            # dense FP4 tensor peak.
+            peak, peak_source = fp4_tensor_peak(local_rank)
             achieved = 8.0 * units(n, L) * share / (cnt * 1e-3)
             result["roofline"] = {
                 "bound": "tensor", "achieved": achieved / 1e12, "peak": peak / 1e12,
-                "unit": "TOP/s (int8)", "frac": achieved / peak,
-                "traffic": traffic_from_profiles(name),
-                "kernel": "tc_batch_kernel", "kernel_ms": cnt,
-                "peak_source": "cuBLAS int8 GEMM (torch._int_mm 8192^3, best of 10) measured on "
-                               "this device in this run",
-                "ops_per_pair_column": 8,
+                "unit": "TFLOP/s", "format": "fp4 e2m1 operands (tcgen05 kind::mxf4), f32 sums",
+                "frac": achieved / peak, "traffic": traffic_from_profiles(name),
+                "kernel": "tc_batch_kernel", "kernel_ms": cnt, "peak_source": peak_source,
+                "flops_per_pair_column": 8,
             }
         else:
             # Bit-plane popcount kernel: bound by the POPC pipe, against the
@@ -468,23 +471,41 @@ def run_served(args, local_rank: int = 0, rate: float = 1000.0, seconds: float =
                         "alignments, host input (H2D inside)"}
 
 
-def int8_tensor_peak(device: int) -> float:
-    """Dense int8 tensor throughput (ops/s) of a cuBLAS GEMM on this device."""
+def fp4_tensor_peak(device: int):
+    """Dense FP4 tensor throughput (flop/s) of a library GEMM on this device, and
+    how it was obtained: an MXFP4 GEMM (torch._scaled_mm, unit block scales,
+    8192^3) when this torch build offers one, else four times the measured dense
+    bf16 peak of MEASURED_PEAKS.json (the dense FP4 : BF16 rate ratio of B200)."""
     import torch
     m = 8192
-    a = torch.randint(-64, 64, (m, m), dtype=torch.int8, device=f"cuda:{device}")
-    b = torch.randint(-64, 64, (m, m), dtype=torch.int8, device=f"cuda:{device}").t()
-    best = 0.0
-    for k in range(12):
-        s = torch.cuda.Event(enable_timing=True)
-        e = torch.cuda.Event(enable_timing=True)
-        s.record()
-        torch._int_mm(a, b)
-        e.record()
-        e.synchronize()
-        if k >= 2:
-            best = max(best, 2.0 * m ** 3 / (s.elapsed_time(e) * 1e-3))
-    return best
+    dev = f"cuda:{device}"
+    try:
+        a = torch.randint(0, 256, (m, m // 2), dtype=torch.uint8, device=dev)
+        b = torch.randint(0, 256, (m, m // 2), dtype=torch.uint8, device=dev)
+        a = a.view(torch.float4_e2m1fn_x2)
+        b = b.view(torch.float4_e2m1fn_x2).t()
+        sa = torch.full((m, m // 32), 127, dtype=torch.uint8, device=dev).view(torch.float8_e8m0fnu)
+        sb = torch.full((m, m // 32), 127, dtype=torch.uint8, device=dev).view(torch.float8_e8m0fnu)
+        best = 0.0
+        for k in range(12):
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record()
+            torch._scaled_mm(a, b, sa, sb, out_dtype=torch.bfloat16)
+            s1.record()
+            s1.synchronize()
+            if k >= 2:
+                best = max(best, 2.0 * m ** 3 / (s0.elapsed_time(s1) * 1e-3))
+        return best, "MXFP4 GEMM (torch._scaled_mm, 8192^3, unit scales, best of 10) measured on " \
+                     "this device in this run"
+    except Exception as e:  # no FP4 GEMM in this torch build
+        why = str(e).splitlines()[0][:120] if str(e) else type(e).__name__
+        try:
+            bf16 = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"] * 1e12
+            src = "MEASURED_PEAKS.json bf16_tflops"
+        except Exception:
+            bf16, src = 1.59e15, "fallback bf16 1.59 PFLOP/s"
+        return 4.0 * bf16, f"4 x measured dense bf16 ({src}); FP4 GEMM unavailable: {why}"
 
 
 def traffic_from_profiles(name: str):
@@ -500,7 +521,7 @@ def traffic_from_profiles(name: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -524,7 +545,9 @@ def main():
         if rank != 0:
             return
         seqs = make_alignment(args.workload)
-        cpu = cpu_reference(seqs, model, type_, args.warmup, args.steps, budget_s=8.0)
+        # each step a bounded sample, the whole run a few minutes at most
+        budget = max(0.5, min(8.0, 150.0 / max(1, args.warmup + args.steps)))
+        cpu = cpu_reference(seqs, model, type_, args.warmup, args.steps, budget_s=budget)
         if cpu is None:
             print(json.dumps({"impl": "reference", "unavailable":
                               "oracle/_ref/ref_harness not built (needs the reference sources)"}))
@@ -549,7 +572,7 @@ def main():
                 "unit": "pair-columns/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "strong",
-                "vs_baseline": None, "dtype": "int8" if config["kernel"] == "tcgen05" else "u32",
+                "vs_baseline": None, "dtype": "fp4" if config["kernel"] == "tcgen05" else "u32",
                 "data": "synthetic", "config": config, "roofline": res["roofline"], "e2e": res["e2e"], "clocks": res["clocks"],
                 "gpu_launches": (4 if type_ == "protein" else 3) * args.steps}
         if not args.no_cpu_baseline and world == 1:

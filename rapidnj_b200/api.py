@@ -227,7 +227,7 @@ class Batch:
     """Many alignments in one persistent pass (rnj_batch): a device work list of
     all their tiles, consumed by graph-captured persistent kernels."""
 
-    def __init__(self, ctx: Context, max_alignments: int = 1024, max_tiles: int = 1 << 20):
+    def __init__(self, ctx: Context, max_alignments: int = 1024, max_tiles: int = 1 << 16):
         h = ctypes.c_void_p()
         check(N.lib().rnj_batch_create(ctx.handle, max_alignments, max_tiles, ctypes.byref(h)))
         self.ctx = ctx

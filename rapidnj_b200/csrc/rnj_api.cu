@@ -355,8 +355,9 @@ EpiParams epi_for(rnj_ctx *ctx, const Packed &p, int model) {
   return ep;
 }
 
-// One alignment through the persistent tensor-core kernel: its triangle (or
-// full) tiles are the work list, one CTA per SM.
+// One alignment through the persistent tensor-core kernel: its triangle tiles
+// are the work list, one CTA per SM.  Distances go through the packed counts
+// and the transform kernel; EPI_COUNTS writes the raw counts directly.
 int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mode) {
   const int nt = tiles_of(p.n);
   const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
@@ -365,10 +366,16 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
   // descriptor may go out of scope.
   RNJ_CUDA(cudaMemcpyAsync(ctx->d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream),
            "descriptor upload");
-  const int grid = (int)std::min<long long>(ntiles, ctx->num_sms);
-  RNJ_CUDA(launch_tc_batch(ctx->d_desc, nullptr, nullptr, (int)ntiles, grid, epi_mode, ctx->stream),
-           "tensor-core kernel");
-  return RNJ_OK;
+  if (epi_mode == EPI_COUNTS) {
+    const int grid = (int)std::min<long long>(ntiles, ctx->num_sms);
+    RNJ_CUDA(launch_tc_batch(ctx->d_desc, nullptr, nullptr, (int)ntiles, 0, (int)ntiles, nullptr,
+                             grid, EPI_COUNTS, ctx->stream),
+             "tensor-core kernel");
+    return RNJ_OK;
+  }
+  int rc = ensure_packed(ctx, std::min<long long>(ntiles, kTcChunkTiles));
+  if (rc != RNJ_OK) return rc;
+  return run_tc_chunks(ctx, ctx->d_desc, nullptr, ntiles, ctx->d_packed, ctx->stream);
 }
 
 int check_device_error(rnj_ctx *ctx) {
@@ -385,8 +392,11 @@ int check_device_error(rnj_ctx *ctx) {
   return RNJ_OK;
 }
 
-// The distance pipeline on the context's stream: counts + fused transform (or
-// split counts + transform for long alignments), then the saturation fix-up.
+int run_popcount(rnj_ctx *ctx, const Packed &p, int ckind, int nk, int nt, EpiParams &ep);
+
+// The distance pipeline on the context's stream: counts and transform (the
+// tensor-core path through packed counts, the bit-plane path fused or split),
+// then the saturation fix-up.
 int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t ld,
                  int *d_max_copy) {
   const int nt = tiles_of(p.n);
@@ -403,11 +413,30 @@ int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t 
   if (p.n == 1) RNJ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float), ctx->stream), "diagonal");
   const int ckind = count_kind_for(p, model);
   const int nk = p.Wp / kKW;
-  mark(ctx, 1, 0);
   if (p.kind == KIND_DNA_TC) {
-    rc = run_tc_single(ctx, p, ep, EPI_DIST);
+    // Marks stage 1 (the counting kernels) and opens stage 2 (the transforms).
+    rc = run_tc_single(ctx, p, ep, EPI_PACKED);
     if (rc != RNJ_OK) return rc;
-  } else if (nk <= kMaxFusedWords / kKW) {
+  } else {
+    mark(ctx, 1, 0);
+    rc = run_popcount(ctx, p, ckind, nk, nt, ep);
+    if (rc != RNJ_OK) return rc;
+    mark(ctx, 1, 1);
+    mark(ctx, 2, 0);
+  }
+  RNJ_CUDA(launch_fixup(ep, nt, ctx->stream), "fix-up kernel");
+  mark(ctx, 2, 1);
+  if (d_max_copy)
+    RNJ_CUDA(cudaMemcpyAsync(d_max_copy, ctx->scratch.words, sizeof(int), cudaMemcpyDeviceToDevice,
+                             ctx->stream),
+             "max copy");
+  return RNJ_OK;
+}
+
+// The bit-plane counting kernels: fused counts + transform, or split counts +
+// transform for alignments longer than one 16-bit accumulator pass.
+int run_popcount(rnj_ctx *ctx, const Packed &p, int ckind, int nk, int nt, EpiParams &ep) {
+  if (nk <= kMaxFusedWords / kKW) {
     RNJ_CUDA(launch_count_tiles(p, ckind, EPI_DIST, ep, ctx->stream), "count kernel");
   } else {
     const size_t cbytes = (size_t)p.n * p.n * 3 * sizeof(uint32_t);
@@ -420,20 +449,42 @@ int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t 
     cudaFreeAsync(counts, ctx->stream);
     if (e != cudaSuccess) return cuda_error(e, "split count pipeline");
   }
-  mark(ctx, 1, 1);
-  mark(ctx, 2, 0);
-  RNJ_CUDA(launch_fixup(ep, nt, ctx->stream), "fix-up kernel");
-  mark(ctx, 2, 1);
-  if (d_max_copy)
-    RNJ_CUDA(cudaMemcpyAsync(d_max_copy, ctx->scratch.words, sizeof(int), cudaMemcpyDeviceToDevice,
-                             ctx->stream),
-             "max copy");
   return RNJ_OK;
 }
 
 }  // namespace
 
 void ctx_mark(rnj_ctx *ctx, int stage, int end) { mark(ctx, stage, end); }
+
+int ensure_packed(rnj_ctx *ctx, long long tiles) {
+  if (ctx->packed_tiles >= tiles) return RNJ_OK;
+  if (ctx->d_packed) cudaFreeAsync(ctx->d_packed, ctx->stream);
+  ctx->d_packed = nullptr;
+  ctx->packed_tiles = 0;
+  RNJ_CUDA(cudaMallocAsync((void **)&ctx->d_packed, (size_t)tiles * kPackedTileWords * 8,
+                           ctx->stream),
+           "packed-count buffer");
+  ctx->packed_tiles = tiles;
+  return RNJ_OK;
+}
+
+int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, long long nitems,
+                  uint64_t *packed, cudaStream_t s) {
+  const int chunk = (int)std::min<long long>(nitems, kTcChunkTiles);
+  for (long long i0 = 0; i0 < nitems; i0 += chunk) {
+    const int cnt = (int)std::min<long long>(chunk, nitems - i0);
+    if (i0 == 0) mark(ctx, 1, 0);
+    RNJ_CUDA(launch_tc_batch(d_desc, d_items, nullptr, (int)nitems, (int)i0, cnt, packed,
+                             std::min(cnt, ctx->num_sms), EPI_PACKED, s),
+             "tensor-core kernel");
+    if (i0 + chunk >= nitems) mark(ctx, 1, 1);
+    if (i0 + chunk >= nitems) mark(ctx, 2, 0);
+    RNJ_CUDA(launch_tc_transform(d_desc, d_items, nullptr, (int)nitems, (int)i0, cnt, packed,
+                                 std::min(cnt, kTransformCtasPerSm * ctx->num_sms), s),
+             "transform kernel");
+  }
+  return RNJ_OK;
+}
 
 extern "C" {
 
@@ -486,6 +537,7 @@ int rnj_ctx_destroy(rnj_ctx *ctx) {
   if (ctx->scratch.words) cudaFree(ctx->scratch.words);
   if (ctx->d_mask) cudaFree(ctx->d_mask);
   if (ctx->d_desc) cudaFree(ctx->d_desc);
+  if (ctx->d_packed) cudaFree(ctx->d_packed);
   if (ctx->h_mask) cudaFreeHost(ctx->h_mask);
   if (ctx->h_max) cudaFreeHost(ctx->h_max);
   for (int b = 0; b < 2; ++b)

@@ -113,9 +113,21 @@ __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
                                               unsigned long long tv_count,
                                               unsigned long long valid) {
   if (valid == 0) return -1.0f;
-  const double dn = (double)valid;
-  const float ts = __double2float_rn(__ddiv_rn((double)ts_count, dn));
-  const float tv = __double2float_rn(__ddiv_rn((double)tv_count, dn));
+  // ts = (float)((double)P / (double)n): for integers P <= n < 2^24 this equals
+  // the float quotient rounded once.  A float midpoint m has at most 25
+  // significant bits, so a quotient P / n that is not m lies at least
+  // 1 / (n * 2^25) > 2^-49 (relative) away from it, while the double rounding
+  // moves it by at most 2^-53: both roundings land on the same float.
+  float ts, tv;
+  if (valid < (1u << 24)) {
+    const float fn = (float)valid;
+    ts = __fdiv_rn((float)ts_count, fn);
+    tv = __fdiv_rn((float)tv_count, fn);
+  } else {
+    const double dn = (double)valid;
+    ts = __double2float_rn(__ddiv_rn((double)ts_count, dn));
+    tv = __double2float_rn(__ddiv_rn((double)tv_count, dn));
+  }
   const double a = __dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, (double)ts)), (double)tv);
   const double b = __dsub_rn(1.0, __dmul_rn(2.0, (double)tv));
   const float temp1 = __double2float_rn(a);

@@ -28,8 +28,9 @@ constexpr int kWordBits = 32;     // sites per plane word
 constexpr int kKW = 8;            // words per pipeline stage
 constexpr int kMaxFusedWords = 2047;  // 16-bit packed accumulators: L <= 65504 per pass
 // The tensor-core sums reach 2L in magnitude and stay exact in f32 while below
-// 2^24; longer DNA alignments are counted on the bit-plane kernels.
-constexpr int kMaxTcColumns = 1 << 22;
+// 2^24, and the packed counts hold 21 bits; longer DNA alignments are counted on
+// the bit-plane kernels.
+constexpr int kMaxTcColumns = (1 << 21) - 1;
 
 __host__ __device__ inline int planes_of(int kind) {
   switch (kind) {
@@ -135,12 +136,37 @@ cudaError_t launch_fixup_batch(const AlnDesc *d_descs, const WorkItem *items_a, 
 // Host helpers shared by the single and batched paths (rnj_api.cu).
 EpiParams epi_params_for(const Packed &p, int model);
 AlnDesc desc_for(const Packed &p, const EpiParams &ep);
-// Persistent over work items; d_items == nullptr means items (0, 0..nitems-1) of
-// d_descs[0]; d_nitems == nullptr means nitems is the count.
+// Persistent over work items [item0, min(n, item0 + count)); d_items == nullptr
+// means the tiles of d_descs[0] in banded order; d_nitems == nullptr means
+// nitems is n.  EPI_PACKED writes packed counts (kPackedTileWords per item) for
+// launch_tc_transform; EPI_COUNTS writes each alignment's n x n x 3 counts.
 cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
-                            int nitems, int grid, int epi_mode, cudaStream_t s);
+                            int nitems, int item0, int count, uint64_t *packed, int grid,
+                            int epi_mode, cudaStream_t s);
+cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
+                                const int *d_nitems, int nitems, int item0, int count,
+                                const uint64_t *packed, int grid, cudaStream_t s);
 
-enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2 };
+enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2, EPI_PACKED = 3 };
+
+// Packed counts of one pair for the tensor-core path: ts, tv and valid in 21
+// bits each (the tensor-core path takes L < 2^21).
+__host__ __device__ inline uint64_t pack_counts(uint32_t ts, uint32_t tv, uint32_t valid) {
+  return (uint64_t)ts | ((uint64_t)tv << 21) | ((uint64_t)valid << 42);
+}
+__host__ __device__ inline void unpack_counts(uint64_t x, uint32_t &ts, uint32_t &tv,
+                                              uint32_t &valid) {
+  ts = (uint32_t)(x & 0x1FFFFFu);
+  tv = (uint32_t)((x >> 21) & 0x1FFFFFu);
+  valid = (uint32_t)(x >> 42);
+}
+// Tiles per pass of the tensor-core path: the packed-count buffer holds this
+// many 128 x 128 tiles (8 bytes per pair, 512 MiB).
+constexpr int kTcChunkTiles = 4096;
+// Resident CTAs per SM of the transform kernel (its 66 KB staging tile): the
+// persistent grid is exactly this many per SM, so the tiles spread evenly.
+constexpr int kTransformCtasPerSm = 3;
+constexpr size_t kPackedTileWords = (size_t)kTile * kTile;
 
 inline int tiles_of(int n) { return (n + kTile - 1) / kTile; }
 inline long long tri_tiles(int nt) { return (long long)nt * (nt + 1) / 2; }

@@ -21,7 +21,18 @@ struct rnj_ctx {
   cudaEvent_t ev[6] = {};                 // pack, count, fix-up: begin/end pairs
   bool ev_used[3] = {false, false, false};
   rnj::AlnDesc *d_desc = nullptr;         // one-alignment work list of the persistent kernel
+  uint64_t *d_packed = nullptr;           // packed counts of the tensor-core path
+  long long packed_tiles = 0;             // its capacity in tiles
 };
+
+// Grows the context's packed-count buffer to `tiles` tiles (rnj_api.cu).
+int ensure_packed(rnj_ctx *ctx, long long tiles);
+// Counts + transform of work items [0, nitems) of the tensor-core path in
+// passes of at most kTcChunkTiles tiles through `packed` (capacity
+// min(nitems, kTcChunkTiles) tiles), on stream s.  Profiling marks: stage 1
+// spans the counting kernels, stage 2 the transforms (rnj_api.cu).
+int run_tc_chunks(rnj_ctx *ctx, const rnj::AlnDesc *d_desc, const rnj::WorkItem *d_items,
+                  long long nitems, uint64_t *packed, cudaStream_t s);
 
 struct rnj_aln {
   rnj_ctx *ctx = nullptr;

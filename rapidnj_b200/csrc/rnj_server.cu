@@ -261,7 +261,7 @@ int rnj_server_create(int device, size_t memory_budget, int max_batch, rnj_serve
   cudaMemGetInfo(&free_b, &total_b);
   s->budget = memory_budget ? memory_budget : (size_t)(0.6 * (double)free_b);
   s->max_batch = max_batch > 0 ? max_batch : 256;
-  s->max_tiles = 1 << 20;
+  s->max_tiles = 255 * 256 / 2;  // n <= 32640; eight tensor-core passes per batch graph
   for (int b = 0; b < 2; ++b) {
     rc = rnj_batch_create(s->ctx, s->max_batch, s->max_tiles, &s->batch[b]);
     if (rc != RNJ_OK) {
@@ -283,6 +283,9 @@ int rnj_server_submit(rnj_server *s, const char *chars, int n, int L, size_t ld,
     return set_error(RNJ_ERR_INVALID, "invalid request");
   if (model != RNJ_JC && model != RNJ_KIMURA) return set_error(RNJ_ERR_INVALID, "unknown model");
   if (type == RNJ_UNKNOWN) type = rnj_detect_type(chars, L);
+  if (tri_tiles(tiles_of(n)) > s->max_tiles)
+    return set_error(RNJ_ERR_INVALID, "alignment has more tiles than a server batch holds (n > " +
+                                          std::to_string(kTile * 255) + "); use rnj_distance");
   Request *r = new Request();
   r->id = s->next_id.fetch_add(1);
   r->n = n;

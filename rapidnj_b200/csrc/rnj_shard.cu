@@ -188,18 +188,22 @@ int rnj_shard_run(rnj_shard *s, float *local_max) {
   RNJ_CUDA(cudaMemsetAsync(s->d_ints + 1, 0, sizeof(int), st), "shard counter clear");
   if (p.n == 1 && nitems > 0)
     RNJ_CUDA(cudaMemsetAsync(s->out, 0, sizeof(float), st), "diagonal");
-  ctx_mark(ctx, 1, 0);
   if (nitems > 0) {
     const int grid = (int)std::min<long long>(nitems, ctx->num_sms);
-    if (p.kind == KIND_DNA_TC)
-      RNJ_CUDA(launch_tc_batch(s->d_desc, s->d_items, s->d_ints, 0, grid, EPI_DIST, st),
-               "tensor-core kernel");
-    else
+    if (p.kind == KIND_DNA_TC) {
+      // Marks stage 1 around the counting kernels.
+      int rc = ensure_packed(ctx, std::min<long long>(nitems, kTcChunkTiles));
+      if (rc != RNJ_OK) return rc;
+      rc = run_tc_chunks(ctx, s->d_desc, s->d_items, nitems, ctx->d_packed, st);
+      if (rc != RNJ_OK) return rc;
+    } else {
+      ctx_mark(ctx, 1, 0);
       RNJ_CUDA(launch_count_batch(s->d_desc, s->d_items, s->d_ints, s->d_ints + 1, grid, EPI_DIST,
                                   st),
                "count kernel");
+      ctx_mark(ctx, 1, 1);
+    }
   }
-  ctx_mark(ctx, 1, 1);
   return read_words(s, local_max);
 }
 

@@ -209,11 +209,20 @@ __global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t l
     uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
     if (i < n) {
       const uint8_t *src = chars + (size_t)i * ld + c * 32;
+      // 32 bytes per thread: two 16-byte loads when the rows are 16-byte aligned
+      // and the chunk is whole (a warp then reads 1 KB of a row contiguously).
+      uint4 q[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+      const bool vec = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0 && c * 32 + 32 <= L;
+      if (vec) {
+        q[0] = __ldg(reinterpret_cast<const uint4 *>(src));
+        q[1] = __ldg(reinterpret_cast<const uint4 *>(src) + 1);
+      }
+      const uint8_t *qb = reinterpret_cast<const uint8_t *>(q);
 #pragma unroll
       for (int b = 0; b < 32; ++b) {
         if (c * 32 + b >= L) break;
         int code;
-        switch (src[b]) {
+        switch (vec ? qb[b] : src[b]) {
           case 'A': case 'a': code = 0; break;
           case 'G': case 'g': code = 1; break;
           case 'T': case 't': code = 2; break;
@@ -337,10 +346,14 @@ __device__ __forceinline__ WorkItem item_at(const AlnDesc *descs, const WorkItem
   return w;
 }
 
+// Items [item0, min(nitems, item0 + count)) of the work list.  EPI_PACKED: the
+// counts of item it go to packed[(it - item0) * 128 * 128 ...] (see
+// pack_counts); EPI_COUNTS: n x n x 3 counts into each alignment's counts.
 template <int EPI>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_batch_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
-                    const int *__restrict__ nitems_ptr, int nitems_direct) {
+                    const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
+                    uint64_t *__restrict__ packed) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem =
       reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -353,7 +366,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nitems = nitems_ptr ? *nitems_ptr : nitems_direct;
+  const int nitems = (int)min((long long)(nitems_ptr ? *nitems_ptr : nitems_direct),
+                              (long long)item0 + count);
+  if (item0 + (int)blockIdx.x >= nitems) return;  // no item for this CTA (before any setup)
 
   if (tid == 0) {
     for (int s = 0; s < kTcStages; ++s) {
@@ -392,7 +407,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       // ----------------------------------------------------------- producer
       uint32_t gkb = 0;
-      for (int it = blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x) {
+      for (int it = item0 + blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x) {
         const WorkItem w = item_at(descs, items, it);
         const AlnDesc &d = descs[w.aln];
         tensormap_acquire(&d.map);
@@ -417,7 +432,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       // -------------------------------------------------------- MMA issuer
       uint32_t gkb = 0, titer = 0;
-      for (int it = blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x, ++titer) {
+      for (int it = item0 + blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x, ++titer) {
         const WorkItem w = item_at(descs, items, it);
         const AlnDesc &d = descs[w.aln];
         const int nkb = 4 * d.kdim / kTcKCols;
@@ -464,7 +479,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const int half = (warp - 2) >> 2;
     const int row = 32 * q + lane;
     uint32_t titer = 0;
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++titer) {
+    for (int it = item0 + blockIdx.x; it < nitems; it += gridDim.x, ++titer) {
       const WorkItem w = item_at(descs, items, it);
       const AlnDesc &d = descs[w.aln];
       int ti, tj;
@@ -476,17 +491,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tc_fence_after();
       const int n = d.n;
       const int i = ti * kTile + row;
-      EpiParams ep;
-      ep.n = n;
-      ep.L = d.L;
-      ep.model = d.model;
-      ep.type = d.type;
-      ep.compat_wrap = d.compat;
-      ep.full = d.full;
-      ep.jc_b = d.jc_b;
-      float tmax = 0.0f;
-      bool sat = false;
-      // Per 32-column chunk: accumulators -> counts -> distances -> stores.
+      uint64_t *dst = packed + (size_t)(it - item0) * (kTile * kTile);
+      // Per 32-column chunk: accumulators -> integer counts -> stores.  Tensor
+      // memory is handed back as soon as the last chunk is in registers.
 #pragma unroll 1
       for (int cc = 0; cc < 2; ++cc) {
         uint32_t V[32], R[32], T[32];
@@ -496,75 +503,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tmem_ld32(base + kTile, R);
         tmem_ld32(base + 2 * kTile, T);
         tmem_ld_wait();
+        if (cc == 1) {
+          tc_fence_before();
+          mbar_arrive(tmem_empty);
+        }
         const int jb = tj * kTile + cbase;
-        if constexpr (EPI == EPI_DIST) {
-          float *orow = d.out + (size_t)i * d.ld;
 #pragma unroll
-          for (int c4 = 0; c4 < 32; c4 += 4) {
-            float x[4];
-            bool okc[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int k = c4 + u;
-              const int j = jb + k;
-              const int vv = __float2int_rn(__uint_as_float(V[k]));
-              const int rr = __float2int_rn(__uint_as_float(R[k]));
-              const int tu = __float2int_rn(__uint_as_float(T[k]));
-              const uint32_t ts = (uint32_t)((vv + rr - tu) >> 2);
-              const uint32_t tv = (uint32_t)((vv - rr) >> 1);
-              okc[u] = d.full ? (i < n && j < n && i != j) : (i < j && j < n);
-              x[u] = 0.0f;
-              if (okc[u]) {
-                x[u] = pair_distance(ep, d.model == RNJ_JC ? ts + tv : ts,
-                                     d.model == RNJ_JC ? 0u : tv, (uint32_t)vv);
-                if (x[u] > tmax) tmax = x[u];
-                if (x[u] == -1.0f) sat = true;
-              }
-              // Mirror (column j of the tile is row j of the matrix): the lanes of
-              // a warp hold 32 consecutive rows i, so these stores coalesce.
-              if (okc[u] && !d.full) d.out[(size_t)j * d.ld + i] = x[u];
-            }
-            const int j0 = jb + c4;
-            if (okc[0] && okc[1] && okc[2] && okc[3] && ((d.ld & 3) == 0)) {
-              *reinterpret_cast<float4 *>(orow + j0) = make_float4(x[0], x[1], x[2], x[3]);
-            } else {
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                const int j = j0 + u;
-                if (okc[u]) orow[j] = x[u];
-                else if (i == j && i < n) orow[j] = 0.0f;
-              }
-            }
-          }
-        } else {
-          if (i < n) {
-#pragma unroll
-            for (int k = 0; k < 32; ++k) {
-              const int j = jb + k;
-              const bool ok = d.full ? (j < n) : (i < j && j < n);
-              if (!ok) continue;
-              const int vv = __float2int_rn(__uint_as_float(V[k]));
-              const int rr = __float2int_rn(__uint_as_float(R[k]));
-              const int tu = __float2int_rn(__uint_as_float(T[k]));
+        for (int k = 0; k < 32; ++k) {
+          const int vv = __float2int_rn(__uint_as_float(V[k]));
+          const int rr = __float2int_rn(__uint_as_float(R[k]));
+          const int tu = __float2int_rn(__uint_as_float(T[k]));
+          const uint32_t ts = (uint32_t)((vv + rr - tu) >> 2);
+          const uint32_t tv = (uint32_t)((vv - rr) >> 1);
+          if constexpr (EPI == EPI_PACKED) {
+            // Column-major within the tile: the 32 lanes (consecutive rows)
+            // store 256 contiguous bytes.
+            dst[(cbase + k) * kTile + row] = pack_counts(ts, tv, (uint32_t)vv);
+          } else {
+            const int j = jb + k;
+            if (i < n && (d.full ? (j < n) : (i < j && j < n))) {
               uint32_t *o = d.counts + ((size_t)i * n + j) * 3;
-              o[0] = (uint32_t)((vv + rr - tu) >> 2);
-              o[1] = (uint32_t)((vv - rr) >> 1);
+              o[0] = ts;
+              o[1] = tv;
               o[2] = (uint32_t)vv;
             }
           }
-        }
-      }
-      // Accumulators read: the MMA warp may start the next item.
-      tc_fence_before();
-      mbar_arrive(tmem_empty);
-      if constexpr (EPI == EPI_DIST) {
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
-          tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, off));
-        const bool any_sat = __any_sync(0xffffffffu, sat);
-        if (lane == 0) {
-          if (tmax > 0.0f) atomicMax(d.max_bits, __float_as_int(tmax));
-          if (any_sat) d.tile_flags[w.tile] = 1;
         }
       }
     }
@@ -585,6 +548,77 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   }
 }
 
+// ------------------------------------------------------------ the transform
+//
+// Items [item0, min(nitems, item0 + count)): the packed counts of each tile ->
+// the exact transform (pair_distance) -> the tile and its mirror image through
+// the shared-memory stage (coalesced stores), the running maximum and the
+// saturation flag of the tile.  Separate from the tensor-core kernel so that the
+// double-precision logarithms run at full occupancy instead of on the eight
+// epilogue warps of a tensor-core CTA, between its tiles.
+__global__ void __launch_bounds__(256) tc_transform_kernel(const AlnDesc *__restrict__ descs,
+                                                           const WorkItem *__restrict__ items,
+                                                           const int *__restrict__ nitems_ptr,
+                                                           int nitems_direct, int item0, int count,
+                                                           const uint64_t *__restrict__ packed) {
+  extern __shared__ uint8_t smem_raw[];
+  float *S = reinterpret_cast<float *>(smem_raw);
+  const int nitems = (int)min((long long)(nitems_ptr ? *nitems_ptr : nitems_direct),
+                              (long long)item0 + count);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int rbase = (warp >> 1) * 32 + (lane >> 3) * 4;
+  const int cbase = (warp & 1) * 64 + (lane & 7) * 4;
+  for (int it = item0 + blockIdx.x; it < nitems; it += gridDim.x) {
+    const WorkItem w = item_at(descs, items, it);
+    const AlnDesc &d = descs[w.aln];
+    int ti, tj;
+    item_tile(d, w.tile, ti, tj);
+    EpiParams ep;
+    ep.n = d.n;
+    ep.L = d.L;
+    ep.model = d.model;
+    ep.type = d.type;
+    ep.compat_wrap = d.compat;
+    ep.full = d.full;
+    ep.jc_b = d.jc_b;
+    ep.out = d.out;
+    ep.ld = d.ld;
+    ep.max_bits = d.max_bits;
+    ep.tile_flags = d.tile_flags;
+    const uint64_t *src = packed + (size_t)(it - item0) * (kTile * kTile);
+    float tmax = 0.0f;
+    bool sat = false;
+    // This thread's 64 pairs (8 rows x 8 columns of the tile, the layout of
+    // row_of / col_of) in 16 steps of 4: a short loop body keeps the inlined
+    // logarithms in the instruction cache while 4 pairs give the scheduler
+    // independent work.
+    const int i0 = ti * kTile, j0 = tj * kTile;
+#pragma unroll 1
+    for (int g = 0; g < 16; ++g) {
+      const int rl = row_of(rbase, g >> 1);
+      const int i = i0 + rl;
+      const int cb = (g & 1) * 4;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int cl = col_of(cbase, cb + u);
+        const int j = j0 + cl;
+        uint32_t ts, tv, vv;
+        unpack_counts(src[cl * kTile + rl], ts, tv, vv);
+        float x = 0.0f;
+        if (i < j && j < ep.n) {
+          x = pair_distance(ep, ts, tv, vv);
+          tmax = fmaxf(tmax, x);
+          sat |= (x == -1.0f);
+        }
+        S[rl * kStageLd + cl] = x;
+      }
+    }
+    __syncthreads();
+    store_distances(ep, ti, tj, w.tile, S, tmax, sat, warp, 8);
+    __syncthreads();  // S is rewritten by the next item
+  }
+}
+
 // ------------------------------------------------------------------ launchers
 
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
@@ -598,22 +632,35 @@ cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L
 }
 
 cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
-                            int nitems, int grid, int epi_mode, cudaStream_t s) {
+                            int nitems, int item0, int count, uint64_t *packed, int grid,
+                            int epi_mode, cudaStream_t s) {
   if (grid <= 0) return cudaSuccess;
   cudaError_t e;
-  if (epi_mode == EPI_DIST) {
-    e = cudaFuncSetAttribute(tc_batch_kernel<EPI_DIST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kTcSmemBytes);
+  if (epi_mode == EPI_PACKED) {
+    e = cudaFuncSetAttribute(tc_batch_kernel<EPI_PACKED>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes);
     if (e != cudaSuccess) return e;
-    tc_batch_kernel<EPI_DIST><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(d_descs, d_items,
-                                                                               d_nitems, nitems);
+    tc_batch_kernel<EPI_PACKED><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(
+        d_descs, d_items, d_nitems, nitems, item0, count, packed);
   } else {
     e = cudaFuncSetAttribute(tc_batch_kernel<EPI_COUNTS>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes);
     if (e != cudaSuccess) return e;
-    tc_batch_kernel<EPI_COUNTS><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(d_descs, d_items,
-                                                                                 d_nitems, nitems);
+    tc_batch_kernel<EPI_COUNTS><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(
+        d_descs, d_items, d_nitems, nitems, item0, count, packed);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
+                                const int *d_nitems, int nitems, int item0, int count,
+                                const uint64_t *packed, int grid, cudaStream_t s) {
+  if (grid <= 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(tc_transform_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
+  if (e != cudaSuccess) return e;
+  tc_transform_kernel<<<(unsigned)grid, 256, kStageBytes, s>>>(d_descs, d_items, d_nitems, nitems,
+                                                               item0, count, packed);
   return cudaGetLastError();
 }
 
