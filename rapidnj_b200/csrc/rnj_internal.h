@@ -163,9 +163,10 @@ __host__ __device__ inline void unpack_counts(uint64_t x, uint32_t &ts, uint32_t
 // Tiles per pass of the tensor-core path: the packed-count buffer holds this
 // many 128 x 128 tiles (8 bytes per pair, 512 MiB).
 constexpr int kTcChunkTiles = 4096;
-// Resident CTAs per SM of the transform kernel (its 66 KB staging tile): the
-// persistent grid is exactly this many per SM, so the tiles spread evenly.
-constexpr int kTransformCtasPerSm = 3;
+// Resident CTAs per SM of the transform kernel (256 threads of at most 51
+// registers, 34 KB of transpose buffers each): the persistent grid is exactly
+// this many per SM, so the tiles spread evenly.
+constexpr int kTransformCtasPerSm = 5;
 constexpr size_t kPackedTileWords = (size_t)kTile * kTile;
 
 inline int tiles_of(int n) { return (n + kTile - 1) / kTile; }

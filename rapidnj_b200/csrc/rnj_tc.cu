@@ -197,11 +197,30 @@ __device__ __forceinline__ void store_chunk(uint8_t *F, int Np, int Lk, int i, i
 // chars (n rows, stride ld) -> F (Np rows of 4 * Lk FP4 features [v | r | t | u],
 // K-blocked); padding rows and columns are zero.  One thread per (sequence,
 // 32-column chunk); writes 4 x 16 bytes.  Valid sites are A/C/G/T in either
-// case (dataloaderFasta.hpp:155-180).
-__global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t ld, int n, int L,
-                                     int Np, int Lk, uint8_t *__restrict__ F) {
+// case (dataloaderFasta.hpp:155-180).  A 256-entry table in shared memory maps
+// each byte to its four FP4 codes (v | r << 4 | t << 8 | u << 12).
+__global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__restrict__ chars,
+                                                            size_t ld, int n, int L, int Np, int Lk,
+                                                            uint8_t *__restrict__ F) {
+  __shared__ uint16_t lut[256];
+  {
+    const int ch = threadIdx.x;
+    int code = -1;
+    switch (ch) {
+      case 'A': case 'a': code = 0; break;
+      case 'G': case 'g': code = 1; break;
+      case 'T': case 't': code = 2; break;
+      case 'C': case 'c': code = 3; break;
+      default: break;
+    }
+    uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, t[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
+    add_site(0, code, v, r, t, u);
+    lut[ch] = (uint16_t)(v[0] | (r[0] << 4) | (t[0] << 8) | (u[0] << 12));
+  }
+  __syncthreads();
   const int chunks = Lk / 32;
   const long long total = (long long)Np * chunks;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(t / chunks);
@@ -209,10 +228,10 @@ __global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t l
     uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
     if (i < n) {
       const uint8_t *src = chars + (size_t)i * ld + c * 32;
-      // 32 bytes per thread: two 16-byte loads when the rows are 16-byte aligned
-      // and the chunk is whole (a warp then reads 1 KB of a row contiguously).
+      // Two 16-byte loads when the rows are 16-byte aligned and the chunk is
+      // whole (a warp then reads 1 KB of a row contiguously).
       uint4 q[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-      const bool vec = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0 && c * 32 + 32 <= L;
+      const bool vec = aligned && c * 32 + 32 <= L;
       if (vec) {
         q[0] = __ldg(reinterpret_cast<const uint4 *>(src));
         q[1] = __ldg(reinterpret_cast<const uint4 *>(src) + 1);
@@ -221,15 +240,12 @@ __global__ void pack_features_kernel(const uint8_t *__restrict__ chars, size_t l
 #pragma unroll
       for (int b = 0; b < 32; ++b) {
         if (c * 32 + b >= L) break;
-        int code;
-        switch (vec ? qb[b] : src[b]) {
-          case 'A': case 'a': code = 0; break;
-          case 'G': case 'g': code = 1; break;
-          case 'T': case 't': code = 2; break;
-          case 'C': case 'c': code = 3; break;
-          default: code = -1; break;
-        }
-        add_site(b, code, v, r, tt, u);
+        const uint32_t e = lut[vec ? qb[b] : src[b]];
+        const int w = b >> 3, sh = (b & 7) * 4;
+        v[w] |= (e & 0xFu) << sh;
+        r[w] |= ((e >> 4) & 0xFu) << sh;
+        tt[w] |= ((e >> 8) & 0xFu) << sh;
+        u[w] |= (e >> 12) << sh;
       }
     }
     store_chunk(F, Np, Lk, i, c, v, r, tt, u);
@@ -551,23 +567,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ------------------------------------------------------------ the transform
 //
 // Items [item0, min(nitems, item0 + count)): the packed counts of each tile ->
-// the exact transform (pair_distance) -> the tile and its mirror image through
-// the shared-memory stage (coalesced stores), the running maximum and the
-// saturation flag of the tile.  Separate from the tensor-core kernel so that the
-// double-precision logarithms run at full occupancy instead of on the eight
-// epilogue warps of a tensor-core CTA, between its tiles.
-__global__ void __launch_bounds__(256) tc_transform_kernel(const AlnDesc *__restrict__ descs,
-                                                           const WorkItem *__restrict__ items,
-                                                           const int *__restrict__ nitems_ptr,
-                                                           int nitems_direct, int item0, int count,
-                                                           const uint64_t *__restrict__ packed) {
+// the exact transform (pair_distance) -> the tile and its mirror image, the
+// running maximum and the saturation flag of the tile.  Separate from the
+// tensor-core kernel so that the double-precision logarithms run at high
+// occupancy instead of on the eight epilogue warps of a tensor-core CTA.
+//
+// Warp w takes rows 32 (w % 4) .. +31 of the tile (lane = row) and columns
+// 64 (w / 4) .. +63 in two 32 x 32 blocks.  For column c the lanes read 32
+// consecutive packed counts (the tile's column-major layout) and store the
+// mirror entries out[j0 + c][i0 + lane] as one coalesced 128-byte row segment;
+// the tile entries out[i0 + row][j0 + c] go through a 32 x 33 per-warp
+// transpose buffer and leave as coalesced row segments too.
+constexpr int kTransformThreads = 256;
+constexpr size_t kTransformSmem = (size_t)(kTransformThreads / 32) * 32 * 33 * sizeof(float);
+
+__global__ void __launch_bounds__(kTransformThreads, kTransformCtasPerSm)
+    tc_transform_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
+                        const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
+                        const uint64_t *__restrict__ packed) {
   extern __shared__ uint8_t smem_raw[];
-  float *S = reinterpret_cast<float *>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float *T = reinterpret_cast<float *>(smem_raw) + warp * (32 * 33);
   const int nitems = (int)min((long long)(nitems_ptr ? *nitems_ptr : nitems_direct),
                               (long long)item0 + count);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int rbase = (warp >> 1) * 32 + (lane >> 3) * 4;
-  const int cbase = (warp & 1) * 64 + (lane & 7) * 4;
+  const int rblk = 32 * (warp & 3), chalf = 64 * (warp >> 2);
   for (int it = item0 + blockIdx.x; it < nitems; it += gridDim.x) {
     const WorkItem w = item_at(descs, items, it);
     const AlnDesc &d = descs[w.aln];
@@ -579,43 +602,54 @@ __global__ void __launch_bounds__(256) tc_transform_kernel(const AlnDesc *__rest
     ep.model = d.model;
     ep.type = d.type;
     ep.compat_wrap = d.compat;
-    ep.full = d.full;
+    ep.full = 0;
     ep.jc_b = d.jc_b;
-    ep.out = d.out;
-    ep.ld = d.ld;
-    ep.max_bits = d.max_bits;
-    ep.tile_flags = d.tile_flags;
-    const uint64_t *src = packed + (size_t)(it - item0) * (kTile * kTile);
+    const int n = d.n;
+    const int i0 = ti * kTile, j0 = tj * kTile;
+    const int i = i0 + rblk + lane;  // this lane's row
+    const uint64_t *src = packed + (size_t)(it - item0) * (kTile * kTile) + rblk + lane;
     float tmax = 0.0f;
     bool sat = false;
-    // This thread's 64 pairs (8 rows x 8 columns of the tile, the layout of
-    // row_of / col_of) in 16 steps of 4: a short loop body keeps the inlined
-    // logarithms in the instruction cache while 4 pairs give the scheduler
-    // independent work.
-    const int i0 = ti * kTile, j0 = tj * kTile;
 #pragma unroll 1
-    for (int g = 0; g < 16; ++g) {
-      const int rl = row_of(rbase, g >> 1);
-      const int i = i0 + rl;
-      const int cb = (g & 1) * 4;
+    for (int cb = chalf; cb < chalf + 64; cb += 32) {
+#pragma unroll 1
+      for (int k0 = 0; k0 < 32; k0 += 4) {
+        float x[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int cl = col_of(cbase, cb + u);
-        const int j = j0 + cl;
-        uint32_t ts, tv, vv;
-        unpack_counts(src[cl * kTile + rl], ts, tv, vv);
-        float x = 0.0f;
-        if (i < j && j < ep.n) {
-          x = pair_distance(ep, ts, tv, vv);
-          tmax = fmaxf(tmax, x);
-          sat |= (x == -1.0f);
+        for (int u = 0; u < 4; ++u) {
+          const int c = cb + k0 + u;
+          const int j = j0 + c;
+          uint32_t ts, tv, vv;
+          unpack_counts(src[(size_t)c * kTile], ts, tv, vv);
+          x[u] = 0.0f;
+          if (i < j && j < n) {
+            x[u] = pair_distance(ep, ts, tv, vv);
+            tmax = fmaxf(tmax, x[u]);
+            sat |= (x[u] == -1.0f);
+            d.out[(size_t)j * d.ld + i] = x[u];  // mirror: consecutive i across lanes
+          }
         }
-        S[rl * kStageLd + cl] = x;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) T[lane * 33 + k0 + u] = x[u];
       }
+      __syncwarp();
+      // Tile entries: row i0 + rblk + r, columns j0 + cb + lane.
+      const int j = j0 + cb + lane;
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        const int ir = i0 + rblk + r;
+        if (ir >= n || j >= n || ir > j) continue;
+        d.out[(size_t)ir * d.ld + j] = (ir == j) ? 0.0f : T[r * 33 + lane];
+      }
+      __syncwarp();
     }
-    __syncthreads();
-    store_distances(ep, ti, tj, w.tile, S, tmax, sat, warp, 8);
-    __syncthreads();  // S is rewritten by the next item
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, off));
+    const bool any_sat = __any_sync(0xffffffffu, sat);
+    if (lane == 0) {
+      if (tmax > 0.0f) atomicMax(d.max_bits, __float_as_int(tmax));
+      if (any_sat) d.tile_flags[w.tile] = 1;
+    }
   }
 }
 
@@ -656,11 +690,8 @@ cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
                                 const int *d_nitems, int nitems, int item0, int count,
                                 const uint64_t *packed, int grid, cudaStream_t s) {
   if (grid <= 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(tc_transform_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kStageBytes);
-  if (e != cudaSuccess) return e;
-  tc_transform_kernel<<<(unsigned)grid, 256, kStageBytes, s>>>(d_descs, d_items, d_nitems, nitems,
-                                                               item0, count, packed);
+  tc_transform_kernel<<<(unsigned)grid, kTransformThreads, kTransformSmem, s>>>(
+      d_descs, d_items, d_nitems, nitems, item0, count, packed);
   return cudaGetLastError();
 }
 
