@@ -194,10 +194,14 @@ class Context:
         check(N.lib().rnj_counts_into(self.handle, aln.handle, ctypes.c_void_p(out.data_ptr())))
 
     def distance_matrix_host(self, seqs: np.ndarray, model="kim", type_=None, fastdist=True,
-                             compat_wrap=False, full_rows=False, popcount=False):
+                             compat_wrap=False, full_rows=False, popcount=False, out=None):
+        """Host bytes in, host n x n float32 matrix out (``out``, C-contiguous, may be
+        page-locked memory, which the library then fills by direct DMA)."""
         a = np.ascontiguousarray(seqs, dtype=np.uint8)
         n, L = a.shape
-        out = np.empty((n, n), dtype=np.float32)
+        if out is None:
+            out = np.empty((n, n), dtype=np.float32)
+        assert out.dtype == np.float32 and out.shape == (n, n) and out.flags.c_contiguous
         m = ctypes.c_float()
         check(N.lib().rnj_distance_matrix_host(self.handle, a.ctypes.data, n, L, L, TYPES[type_],
                                                MODELS[model],

@@ -205,6 +205,21 @@ int host_threads(int threads) {
   return n > 0 ? (int)std::min<long>(n, 64) : 1;
 }
 
+// True when rows[0..nrows) are one contiguous block of n-float rows in
+// page-locked (pinned or registered) host memory: the device can write it
+// directly, without the staging buffers.
+bool rows_pinned_block(float *const *rows, int nrows, int n) {
+  for (int r = 1; r < nrows; ++r)
+    if (rows[r] != rows[0] + (size_t)r * n) return false;
+  cudaPointerAttributes a0, a1;
+  if (cudaPointerGetAttributes(&a0, rows[0]) != cudaSuccess ||
+      cudaPointerGetAttributes(&a1, rows[0] + (size_t)nrows * n - 1) != cudaSuccess) {
+    cudaGetLastError();  // clear the sticky-free error of a failed query
+    return false;
+  }
+  return a0.type == cudaMemoryTypeHost && a1.type == cudaMemoryTypeHost;
+}
+
 // Parallel row copy: dst[r] (n floats) <- src + r * n.
 void scatter_rows(const float *src, float **dst, int nrows, int n, int threads) {
   const size_t bytes = (size_t)nrows * n * sizeof(float);
@@ -862,6 +877,15 @@ int rnj_mat_copy_rows(rnj_ctx *ctx, rnj_mat *mat, int row0, int nrows, float **r
   DeviceGuard g(ctx->device);
   const int n = mat->n;
   const size_t row_bytes = (size_t)n * sizeof(float);
+  if (rows_pinned_block(rows, nrows, n)) {
+    // One 2-D DMA straight into the caller's page-locked rows.
+    RNJ_CUDA(cudaMemcpy2DAsync(rows[0], row_bytes, mat->d + (size_t)row0 * mat->ld,
+                               mat->ld * sizeof(float), row_bytes, (size_t)nrows,
+                               cudaMemcpyDeviceToHost, ctx->stream),
+             "row copy");
+    RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "row copy sync");
+    return RNJ_OK;
+  }
   const size_t chunk_target = 32u << 20;  // 32 MB per staging buffer
   int rows_per_chunk = (int)std::max<size_t>(1, chunk_target / row_bytes);
   rows_per_chunk = std::min(rows_per_chunk, nrows);

@@ -220,9 +220,12 @@ def test_input_paths_agree(ctx):
     ref_jc, _ = gpu_matrix(ctx, seqs, oracle.DNA, "jc")
     assert np.array_equal(ctx.distance(aln, "jc").to_numpy(), ref_jc)
     assert np.array_equal(ctx.distance(aln_p, "jc").to_numpy(), ref_jc)
-    # one-call host path
+    # one-call host path, into pageable and into page-locked host memory
     out, mx = ctx.distance_matrix_host(seqs, "kim")
     assert np.array_equal(out, ref)
+    locked = torch.full((150, 150), 3.0, dtype=torch.float32).pin_memory().numpy()
+    _, mx_locked = ctx.distance_matrix_host(seqs, "kim", out=locked)
+    assert np.array_equal(locked, ref) and mx_locked == mx
     # caller-owned device buffer with a stride
     buf = torch.full((150, 160), 7.0, dtype=torch.float32, device="cuda")
     mx2 = ctx.distance_into(ctx.alignment(seqs, oracle.DNA), "kim", buf, want_max=True)
