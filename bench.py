@@ -520,9 +520,12 @@ def fp4_tensor_peak(device: int):
 
 
 def traffic_from_profiles(name: str):
+    """DRAM bytes per launch of the counting kernel for this workload, from the
+    ncu summaries committed under profiles/ (None when there is none)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
-        return json.load(open(p)).get(name)
+        v = json.load(open(p)).get(name)
+        return float(v) if isinstance(v, (int, float)) else None
     except Exception:
         return None
 
