@@ -185,9 +185,21 @@ int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld, int type,
                          int flags, float *d_out, size_t ld_out, void *stream, float *max_out);
 
 /* One call, host in / host out: pack, distances, copy into out (n*n floats,
- * row-major).  max_out may be NULL. */
+ * row-major).  max_out may be NULL.  This is what JCdistance::computeDistanceMatrix
+ * (JCdistance.cpp:24-44) and KimuraDistance::computeDistances
+ * (KimuraDistance.cpp:75-99) produce, from the loader's sequences to the filled
+ * matrix.  For DNA on the tensor-core kernel with a page-locked `out`, the call
+ * is streamed: bands of rows are computed last band first, and each band's
+ * finished rows and columns are copied to `out` while the next band is uploaded
+ * and computed (the n*n*4-byte download then bounds the call). */
 int rnj_distance_matrix_host(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
                              int type, int model, int flags, float *out, float *max_out);
+/* The same with the band height of the streamed form in 128-row tiles:
+ * 0 = the library's choice, > 0 = that many tile rows per band, < 0 = not
+ * streamed (upload, compute, then one download). */
+int rnj_distance_matrix_host_ex(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
+                                int type, int model, int flags, int band_tiles, float *out,
+                                float *max_out);
 
 /* ------------------------------------------------------------------ batches */
 

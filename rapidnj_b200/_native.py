@@ -66,6 +66,8 @@ SIGNATURES = {
     "rnj_mat_destroy": (c_int, [c_void_p]),
     "rnj_distance_matrix_host": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int, c_int,
                                          c_int, c_void_p, P(c_float)]),
+    "rnj_distance_matrix_host_ex": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int,
+                                            c_int, c_int, c_int, c_void_p, P(c_float)]),
     "rnj_distance_noalloc": (c_int, [c_void_p, c_int, c_int, c_size_t, c_int, c_int, c_int,
                                      c_void_p, c_size_t, c_void_p, P(c_float)]),
     "rnj_batch_create": (c_int, [c_void_p, c_int, ctypes.c_longlong, P(c_void_p)]),

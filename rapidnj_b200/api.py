@@ -194,19 +194,30 @@ class Context:
         check(N.lib().rnj_counts_into(self.handle, aln.handle, ctypes.c_void_p(out.data_ptr())))
 
     def distance_matrix_host(self, seqs: np.ndarray, model="kim", type_=None, fastdist=True,
-                             compat_wrap=False, full_rows=False, popcount=False, out=None):
+                             compat_wrap=False, full_rows=False, popcount=False, out=None,
+                             band_tiles=None):
         """Host bytes in, host n x n float32 matrix out (``out``, C-contiguous, may be
-        page-locked memory, which the library then fills by direct DMA)."""
+        page-locked memory, which the library then fills by direct DMA).
+
+        ``band_tiles`` (rnj_distance_matrix_host_ex): None or 0 = the library's
+        choice, > 0 = band height in 128-row tiles of the streamed form, < 0 =
+        not streamed."""
         a = np.ascontiguousarray(seqs, dtype=np.uint8)
         n, L = a.shape
         if out is None:
             out = np.empty((n, n), dtype=np.float32)
         assert out.dtype == np.float32 and out.shape == (n, n) and out.flags.c_contiguous
         m = ctypes.c_float()
-        check(N.lib().rnj_distance_matrix_host(self.handle, a.ctypes.data, n, L, L, TYPES[type_],
-                                               MODELS[model],
-                                               flags_of(fastdist, compat_wrap, full_rows, popcount),
-                                               out.ctypes.data, ctypes.byref(m)))
+        flags = flags_of(fastdist, compat_wrap, full_rows, popcount)
+        if band_tiles is None:
+            check(N.lib().rnj_distance_matrix_host(self.handle, a.ctypes.data, n, L, L,
+                                                   TYPES[type_], MODELS[model], flags,
+                                                   out.ctypes.data, ctypes.byref(m)))
+        else:
+            check(N.lib().rnj_distance_matrix_host_ex(self.handle, a.ctypes.data, n, L, L,
+                                                      TYPES[type_], MODELS[model], flags,
+                                                      int(band_tiles), out.ctypes.data,
+                                                      ctypes.byref(m)))
         return out, m.value
 
     def close(self) -> None:

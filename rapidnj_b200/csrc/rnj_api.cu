@@ -471,6 +471,23 @@ int run_popcount(rnj_ctx *ctx, const Packed &p, int ckind, int nk, int nt, EpiPa
 
 void ctx_mark(rnj_ctx *ctx, int stage, int end) { mark(ctx, stage, end); }
 
+int ctx_scratch(rnj_ctx *ctx, size_t words) { return ensure_scratch_words(ctx, words); }
+
+EpiParams ctx_epi(rnj_ctx *ctx, const Packed &p, int model) { return epi_for(ctx, p, model); }
+
+int ctx_check_error(rnj_ctx *ctx) { return check_device_error(ctx); }
+
+bool ctx_block_pinned(const void *p, size_t bytes) {
+  if (!p || bytes == 0) return false;
+  cudaPointerAttributes a0, a1;
+  if (cudaPointerGetAttributes(&a0, p) != cudaSuccess ||
+      cudaPointerGetAttributes(&a1, (const char *)p + bytes - 1) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a0.type == cudaMemoryTypeHost && a1.type == cudaMemoryTypeHost;
+}
+
 int ensure_packed(rnj_ctx *ctx, long long tiles) {
   if (ctx->packed_tiles >= tiles) return RNJ_OK;
   if (ctx->d_packed) cudaFreeAsync(ctx->d_packed, ctx->stream);
@@ -559,6 +576,15 @@ int rnj_ctx_destroy(rnj_ctx *ctx) {
     if (ctx->h_stage[b]) cudaFreeHost(ctx->h_stage[b]);
   for (int k = 0; k < 6; ++k)
     if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+  if (ctx->h_words) cudaFreeHost(ctx->h_words);
+  if (ctx->s_up) {
+    cudaStreamSynchronize(ctx->s_up);
+    cudaStreamDestroy(ctx->s_up);
+  }
+  if (ctx->s_down) {
+    cudaStreamSynchronize(ctx->s_down);
+    cudaStreamDestroy(ctx->s_down);
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return RNJ_OK;
@@ -936,7 +962,23 @@ int rnj_mat_destroy(rnj_mat *mat) {
 
 int rnj_distance_matrix_host(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int type,
                              int model, int flags, float *out, float *max_out) {
+  return rnj_distance_matrix_host_ex(ctx, chars, n, L, ld, type, model, flags, 0, out, max_out);
+}
+
+int rnj_distance_matrix_host_ex(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
+                                int type, int model, int flags, int band_tiles, float *out,
+                                float *max_out) {
   if (!ctx || (n > 0 && !out)) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (n > 0 && L > 0 && !chars) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (n < 0 || L < 0 || (n > 0 && ld < (size_t)L))
+    return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
+  if (model != RNJ_JC && model != RNJ_KIMURA) return set_error(RNJ_ERR_INVALID, "unknown model");
+  if (type == RNJ_UNKNOWN && n > 0) type = rnj_detect_type(chars, L);
+  if (type == RNJ_DNA && band_tiles >= 0) {
+    const int rc = distance_host_streamed(ctx, chars, n, L, ld, model, flags, band_tiles, out,
+                                          max_out);
+    if (rc != RNJ_ERR_UNSUPPORTED) return rc;
+  }
   rnj_aln *a = nullptr;
   int rc = rnj_aln_from_host_buffer(ctx, chars, n, L, ld, type, flags, &a);
   if (rc != RNJ_OK) return rc;

@@ -123,8 +123,9 @@ cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode,
 cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s);
 cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s);
 // Tensor-core DNA path (rnj_tc.cu).
+// Rows [row0, row0 + rows) of the feature matrix (rows < 0: through Np).
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
-                                 uint8_t *F, cudaStream_t s);
+                                 uint8_t *F, cudaStream_t s, int row0 = 0, int rows = -1);
 cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_gaps, int bs_words,
                                       int n, int L, int Np, int Lk, uint8_t *F, cudaStream_t s);
 int encode_features_map(Packed &p);

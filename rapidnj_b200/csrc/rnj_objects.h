@@ -20,6 +20,10 @@ struct rnj_ctx {
   bool profiling = false;
   cudaEvent_t ev[6] = {};                 // pack, count, fix-up: begin/end pairs
   bool ev_used[3] = {false, false, false};
+  cudaStream_t s_up = nullptr;            // host-to-host calls: uploads (created on first use)
+  cudaStream_t s_down = nullptr;          // host-to-host calls: downloads
+  int *h_words = nullptr;                 // pinned copy of the scratch words (flags, max, error)
+  size_t h_words_cap = 0;
   rnj::AlnDesc *d_desc = nullptr;         // one-alignment work list of the persistent kernel
   uint64_t *d_packed = nullptr;           // packed counts of the tensor-core path
   long long packed_tiles = 0;             // its capacity in tiles
@@ -55,6 +59,20 @@ struct rnj_mat {
 void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *kind);
 int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
                   int flags, int kind, const uint8_t lut[256], rnj_aln **out);
+
+// Helpers of rnj_api.cu shared with the streamed host-to-host path
+// (rnj_stream.cu): grow the scratch words, transform parameters wired to the
+// scratch, the error-word check (synchronises the context stream), and whether
+// [p, p + bytes) is page-locked host memory.
+int ctx_scratch(rnj_ctx *ctx, size_t words);
+rnj::EpiParams ctx_epi(rnj_ctx *ctx, const rnj::Packed &p, int model);
+int ctx_check_error(rnj_ctx *ctx);
+bool ctx_block_pinned(const void *p, size_t bytes);
+// The streamed host-to-host distance call of the tensor-core DNA path
+// (rnj_stream.cu).  Returns RNJ_ERR_UNSUPPORTED, having done nothing, when the
+// input does not take that path.
+int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int model,
+                           int flags, int band_tiles, float *out, float *max_out);
 
 // Profiling marks on the context stream (stage 0 pack, 1 count, 2 fix-up;
 // end 0 = begin), read back by rnj_ctx_stage_times.

@@ -195,12 +195,14 @@ __device__ __forceinline__ void store_chunk(uint8_t *F, int Np, int Lk, int i, i
 }
 
 // chars (n rows, stride ld) -> F (Np rows of 4 * Lk FP4 features [v | r | t | u],
-// K-blocked); padding rows and columns are zero.  One thread per (sequence,
-// 32-column chunk); writes 4 x 16 bytes.  Valid sites are A/C/G/T in either
-// case (dataloaderFasta.hpp:155-180).  A 256-entry table in shared memory maps
-// each byte to its four FP4 codes (v | r << 4 | t << 8 | u << 12).
+// K-blocked), rows row0 .. row0 + rows - 1 of F; padding rows and columns are
+// zero.  One thread per (sequence, 32-column chunk); writes 4 x 16 bytes.
+// Valid sites are A/C/G/T in either case (dataloaderFasta.hpp:155-180).  A
+// 256-entry table in shared memory maps each byte to its four FP4 codes
+// (v | r << 4 | t << 8 | u << 12).
 __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__restrict__ chars,
                                                             size_t ld, int n, int L, int Np, int Lk,
+                                                            int row0, int rows,
                                                             uint8_t *__restrict__ F) {
   __shared__ uint16_t lut[256];
   {
@@ -219,11 +221,11 @@ __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__res
   }
   __syncthreads();
   const int chunks = Lk / 32;
-  const long long total = (long long)Np * chunks;
+  const long long total = (long long)rows * chunks;
   const bool aligned = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(t / chunks);
+    const int i = row0 + (int)(t / chunks);
     const int c = (int)(t % chunks);
     uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
     if (i < n) {
@@ -656,12 +658,15 @@ __global__ void __launch_bounds__(kTransformThreads, kTransformCtasPerSm)
 // ------------------------------------------------------------------ launchers
 
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
-                                 uint8_t *F, cudaStream_t s) {
-  const long long work = (long long)Np * (Lk / 32);
+                                 uint8_t *F, cudaStream_t s, int row0, int rows) {
+  if (rows < 0) rows = Np - row0;
+  if (row0 < 0 || rows < 0 || row0 + rows > Np) return cudaErrorInvalidValue;
+  if (rows == 0) return cudaSuccess;
+  const long long work = (long long)rows * (Lk / 32);
   long long g = (work + 255) / 256;
   if (g > 148LL * 64) g = 148LL * 64;
   if (g < 1) g = 1;
-  pack_features_kernel<<<(unsigned)g, 256, 0, s>>>(d_chars, ld, n, L, Np, Lk, F);
+  pack_features_kernel<<<(unsigned)g, 256, 0, s>>>(d_chars, ld, n, L, Np, Lk, row0, rows, F);
   return cudaGetLastError();
 }
 
