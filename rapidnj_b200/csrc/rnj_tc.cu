@@ -77,22 +77,31 @@ __device__ __forceinline__ void tc_fence_before() {
 __device__ __forceinline__ void tc_fence_after() {
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
-__device__ __forceinline__ void tc_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
 // D (f32, tensor memory) (+)= A x B^T with FP4 operands from shared memory and
-// block scale factors from tensor memory (block of 32 columns).
-__device__ __forceinline__ void tc_mma_fp4(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                           uint32_t idesc, uint32_t sfa_tmem, uint32_t sfb_tmem,
-                                           uint32_t accumulate) {
+// block scale factors from tensor memory (block of 32 columns), issued by one
+// elected lane of a converged warp.  The whole warp runs the issue loop, so the
+// descriptor and tensor-memory operands are warp-uniform values; issued from a
+// single divergent lane with per-instruction operand arithmetic, the MMA issue
+// rate, not the tensor pipe, bounded the kernel (about 150 instead of 64
+// cycles per 128 x 128 x 64 instruction).
+__device__ __forceinline__ void tc_mma_fp4_elect(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                                 uint32_t idesc, uint32_t sfa_tmem,
+                                                 uint32_t sfb_tmem, uint32_t accumulate) {
   asm volatile(
-      "{\n\t.reg .pred p;\n\t"
+      "{\n\t.reg .pred p, e;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "@e tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}"
       ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa_tmem),
       "r"(sfb_tmem)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit_elect(uint64_t *bar) {
+  asm volatile(
+      "{\n\t.reg .pred e;\n\t"
+      "elect.sync _|e, 0xffffffff;\n\t"
+      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}"
+      ::"r"(smem_u32(bar))
       : "memory");
 }
 // 32 lanes x 32 columns of 32-bit words from registers into tensor memory.
@@ -447,49 +456,59 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
     }
   } else if (warp == 1) {
-    if (lane == 0) {
-      // -------------------------------------------------------- MMA issuer
-      uint32_t gkb = 0, titer = 0;
-      for (int it = item0 + blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x, ++titer) {
-        const WorkItem w = item_at(descs, items, it);
-        const AlnDesc &d = descs[w.aln];
-        const int nkb = 4 * d.kdim / kTcKCols;
-        const int seg = d.kdim / kTcKCols;
-        // The epilogue of the previous item must have read the accumulators.
-        if (!tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag)) {
-          *abort_flag = 1;
-          break;
-        }
-        tc_fence_after();
-        bool ok = true;
-        for (int kb = 0; kb < nkb; ++kb, ++gkb) {
-          const int s = gkb % kTcStages;
-          if (!tc_wait(&full_bar[s], (gkb / kTcStages) & 1, abort_flag)) {
-            ok = false;
-            break;
-          }
-          tc_fence_after();
-          const int acc = kb < seg ? 0 : (kb < 2 * seg ? 1 : 2);
-          const bool first = (kb == 0) || (kb == seg) || (kb == 2 * seg);
-          const uint32_t a_addr = smem_u32(smem + s * kTcStageBytes);
-          const uint64_t adesc = smem_desc_sw128(a_addr);
-          const uint64_t bdesc = smem_desc_sw128(a_addr + kTcTileBytes);
-#pragma unroll
-          for (int kk = 0; kk < kTcKBlock / 32; ++kk)  // 32 bytes = 64 columns per MMA
-            tc_mma_fp4(tmem + acc * kTile, adesc + (uint64_t)(kk * 2), bdesc + (uint64_t)(kk * 2),
-                       kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, (first && kk == 0) ? 0u : 1u);
-          tc_commit(&empty_bar[s]);
-        }
-        if (!ok) {
-          *abort_flag = 1;
-          break;
-        }
-        tc_commit(acc_full);
+    // ---------------------------------------------------------- MMA issuer
+    // The whole warp runs this loop (lane 0 waits, the result is broadcast);
+    // one elected lane issues each MMA and commit.  Descriptors are the stage
+    // base descriptors plus constant offsets: the 14-bit start-address field
+    // (16-byte units) of a shared address below 228 KB cannot carry out.
+    const uint64_t desc0 = smem_desc_sw128(smem_u32(smem));
+    constexpr uint64_t kStageStep = kTcStageBytes >> 4, kBStep = kTcTileBytes >> 4;
+    uint32_t gkb = 0, titer = 0;
+    for (int it = item0 + blockIdx.x;; it += gridDim.x, ++titer) {
+      int go = it < nitems && !*abort_flag;
+      go = __shfl_sync(0xffffffffu, go, 0);
+      if (!go) break;
+      const WorkItem w = item_at(descs, items, it);
+      const AlnDesc &d = descs[w.aln];
+      const int nkb = 4 * d.kdim / kTcKCols;
+      const int seg = d.kdim / kTcKCols;
+      // The epilogue of the previous item must have read the accumulators.
+      int ok = 1;
+      if (lane == 0) ok = tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) *abort_flag = 1;
+        break;
       }
-      // Every MMA issued has completed before tensor memory is released.
-      tc_commit(drain_bar);
-      mbar_wait_bounded(drain_bar, 0);
+      tc_fence_after();
+      for (int kb = 0; kb < nkb; ++kb, ++gkb) {
+        const int s = gkb % kTcStages;
+        if (lane == 0) ok = tc_wait(&full_bar[s], (gkb / kTcStages) & 1, abort_flag);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        tc_fence_after();
+        const int acc = kb < seg ? 0 : (kb < 2 * seg ? 1 : 2);
+        const uint32_t first = (kb == 0) || (kb == seg) || (kb == 2 * seg);
+        const uint64_t adesc = desc0 + (uint64_t)s * kStageStep;
+        const uint64_t bdesc = adesc + kBStep;
+        const uint32_t dt = tmem + (uint32_t)(acc * kTile);
+        // 32 bytes = 64 columns per MMA, four per 128-byte stage.
+        tc_mma_fp4_elect(dt, adesc, bdesc, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, first ^ 1u);
+        tc_mma_fp4_elect(dt, adesc + 2, bdesc + 2, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+        tc_mma_fp4_elect(dt, adesc + 4, bdesc + 4, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+        tc_mma_fp4_elect(dt, adesc + 6, bdesc + 6, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+        tc_commit_elect(&empty_bar[s]);
+      }
+      if (!ok) {
+        if (lane == 0) *abort_flag = 1;
+        break;
+      }
+      tc_commit_elect(acc_full);
     }
+    // Every MMA issued has completed before tensor memory is released.
+    tc_commit_elect(drain_bar);
+    if (lane == 0) mbar_wait_bounded(drain_bar, 0);
+    __syncwarp();
   } else {
     // ----------------------------------------------------------- epilogue
     // Warps 2..9: TMEM lane quarter = warp % 4 (row block), column half by group.
