@@ -133,6 +133,27 @@ __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
   const float temp1 = __double2float_rn(a);
   const float temp2 = __double2float_rn(b);
   if (temp1 <= 0.0f || temp2 <= 0.0f) return -1.0f;
+  // Identical pairs: -0.5 log(1) - 0.25 log(1) = -0.0 - 0.0 = -0.0.
+  if ((ts_count | tv_count) == 0) return -0.0f;
+  // Fast path, one logarithm: D = -0.5 log a - 0.25 log b = -0.25 log(a^2 b),
+  // a, b in (0, 1], so D >= 0 and 0.5|log a| + 0.25|log b| = D.
+  //   reference  d_ref = (-0.5 log a) - (0.25 log b), each log within 1 ulp,
+  //              one rounded subtraction:   |d_ref - D| <= 1.5 * 2^-52 * D
+  //   this path  dd = -0.25 log(fl(fl(a a) b)): the product is within 2^-52
+  //              (relative) of a^2 b, so its log within 2^-52 + 1 ulp:
+  //                                          |dd - D| <= 2^-54 + 2^-52 * D
+  // so |dd - d_ref| <= 2^-52 (0.25 + 2.5 D) < eps = 2^-50 (1 + 4 dd).  (a^2 b
+  // stays far from the double underflow range: a, b >= 2^-46 when positive.)
+  // If dd - eps and dd + eps round to the same float, so does every value
+  // between them (rounding is monotone), d_ref included: the float result is
+  // the reference's.  Otherwise -- about one pair in 10^7 -- the reference's
+  // own two-logarithm formula decides.
+  const double x = __dmul_rn(__dmul_rn(a, a), b);
+  const double dd = __dmul_rn(-0.25, log(x));
+  const double eps = __dmul_rn(0x1p-50, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
+  const float lo = __double2float_rn(__dsub_rn(dd, eps));
+  const float hi = __double2float_rn(__dadd_rn(dd, eps));
+  if (__float_as_int(lo) == __float_as_int(hi)) return lo;
   return __double2float_rn(__dsub_rn(__dmul_rn(-0.5, log(a)), __dmul_rn(0.25, log(b))));
 }
 

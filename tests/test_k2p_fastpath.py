@@ -1,0 +1,74 @@
+"""The one-logarithm fast path of the device K2P transform (rnj_device.cuh,
+k2p_distance), restated in numpy with the host's log, checked against the
+reference's two-logarithm arithmetic (KimuraDistance.cpp:339-349, as the oracle
+computes it): whenever the fast path's rounding check accepts, its float must
+be the reference's float.  This pins the error bound the check relies on; the
+device path itself is compared with the oracle by the GPU parity tests.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+
+def reference_k2p(P, Q, n):
+    """KimuraDistance.cpp:339-349 in numpy (float ratios, double logs)."""
+    ts = (P.astype(np.float64) / n).astype(np.float32)
+    tv = (Q.astype(np.float64) / n).astype(np.float32)
+    a = 1.0 - 2.0 * ts.astype(np.float64) - tv.astype(np.float64)
+    b = 1.0 - 2.0 * tv.astype(np.float64)
+    ok = (a.astype(np.float32) > 0) & (b.astype(np.float32) > 0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d = (-0.5 * np.log(a) - 0.25 * np.log(b)).astype(np.float32)
+    return np.where(ok, d, np.float32(-1.0)), a, b, ok
+
+
+def fast_k2p(a, b):
+    """The device fast path: (accepted, float)."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        x = (a * a) * b
+        dd = -0.25 * np.log(x)
+        eps = 2.0 ** -50 * (1.0 + 4.0 * dd)
+        lo = (dd - eps).astype(np.float32)
+        hi = (dd + eps).astype(np.float32)
+    return lo.view(np.int32) == hi.view(np.int32), lo
+
+
+@pytest.mark.parametrize("n", [7, 100, 997, 1000, 2048])
+def test_fast_path_agrees_with_reference_exhaustive(n):
+    P, Q = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    keep = (P + Q <= n) & ((P + Q) > 0)
+    P, Q = P[keep], Q[keep]
+    ref, a, b, ok = reference_k2p(P, Q, float(n))
+    acc, got = fast_k2p(a[ok], b[ok])
+    r = ref[ok]
+    assert np.array_equal(got[acc].view(np.int32), r[acc].view(np.int32))
+    # the check rejects only a tiny fraction (then the two-log formula runs)
+    assert (~acc).mean() < 1e-4
+
+
+def test_fast_path_agrees_with_reference_random_large_n():
+    rng = np.random.default_rng(0)
+    n = rng.integers(1000, 2_000_000, size=2_000_000)
+    P = (rng.random(n.size) * 0.4 * n).astype(np.int64)
+    Q = (rng.random(n.size) * 0.45 * n).astype(np.int64)
+    ref, a, b, ok = reference_k2p(P, Q, n.astype(np.float64))
+    acc, got = fast_k2p(a[ok], b[ok])
+    r = ref[ok]
+    assert np.array_equal(got[acc].view(np.int32), r[acc].view(np.int32))
+    assert (~acc).mean() < 1e-5
+
+
+def test_fast_path_matches_oracle_transform():
+    # The oracle's C transform (the reference's arithmetic, glibc log) on count
+    # triples near the saturation boundary 1 - 2P/n - Q/n -> 0.
+    rng = np.random.default_rng(1)
+    n = rng.integers(50, 50_000, size=50_000).astype(np.uint32)
+    Q = (rng.random(n.size) * 0.5 * n).astype(np.uint32)
+    P = ((n - Q).astype(np.float64) / 2 * (0.9 + 0.1 * rng.random(n.size))).astype(np.uint32)
+    k2p = oracle.lib().orc_k2p
+    want = np.array([k2p(int(p), int(q), int(v)) for p, q, v in zip(P, Q, n)], dtype=np.float32)
+    ref, a, b, ok = reference_k2p(P, Q, n.astype(np.float64))
+    assert np.array_equal(want.view(np.int32), ref.view(np.int32))
+    acc, got = fast_k2p(a[ok], b[ok])
+    assert np.array_equal(got[acc].view(np.int32), ref[ok][acc].view(np.int32))
