@@ -242,6 +242,11 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                 "kernel": "tc_batch_kernel", "kernel_ms": cnt, "peak_source": peak_source,
                 "flops_per_pair_column": 8,
             }
+            # The raw tensor pipe: back-to-back kind::mxf4 MMAs on every SM with
+            # the operands already in shared memory (rnj_probe_tc_peak, this run).
+            pipe = ctx.probe_tc_peak()
+            result["roofline"]["tensor_pipe_peak"] = pipe / 1e12
+            result["roofline"]["frac_of_tensor_pipe"] = achieved / pipe
         else:
             # Bit-plane popcount kernel: bound by the POPC pipe, against the
             # POPC peak measured on this device.

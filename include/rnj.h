@@ -64,11 +64,11 @@ enum {
    * dm != NULL).  Only differs for the naive DNA estimator, whose counts are
    * asymmetric. */
   RNJ_FULL_ROWS = 4,
-  /* DNA on the fast path is counted on the tensor cores by default (tcgen05,
-   * int8 features, exact int32 accumulation).  This flag selects the bit-plane
-   * popcount kernel instead: same counts, a quarter of the speed, 0.375 instead
-   * of 4 bytes of packed input per site.  Protein and -f alignments always use
-   * the popcount kernels. */
+  /* DNA on the fast path is counted on the tensor cores by default (tcgen05
+   * kind::mxf4: FP4 features in {-1, 0, +1} with unit block scales, exact f32
+   * sums).  This flag selects the bit-plane popcount kernel instead: same
+   * counts, 0.375 instead of 2 bytes of packed input per site.  Protein and -f
+   * alignments always use the popcount kernels. */
   RNJ_POPCOUNT = 8
 };
 
@@ -102,6 +102,11 @@ int rnj_ctx_stage_times(rnj_ctx *ctx, float *ms);
 /* Measured device-wide throughput of the two integer pipes the counting kernels
  * run on: POPC and LOP3 operations per second (a short microbenchmark). */
 int rnj_probe_int_peaks(rnj_ctx *ctx, double *popc_per_s, double *lop3_per_s);
+/* FP4 tensor-pipe throughput of the context's device in flop/s: every SM issues
+ * back-to-back 128 x 128 x 64 tcgen05 kind::mxf4 MMAs (the instruction the DNA
+ * counting kernel uses) with operands already in shared memory.  No counterpart
+ * in the reference; the roofline of the tensor-core kernel is quoted against it. */
+int rnj_probe_tc_peak(rnj_ctx *ctx, double *fp4_flops_per_s);
 
 /* Sequence type of an alignment from its first sequence: any byte >= 65 outside
  * ACGTUN/acgtun makes it protein (dataloaderFasta.hpp:54-76). */
@@ -340,6 +345,43 @@ int rnj_msa_destroy(rnj_msa *msa);
  * space).  rows[i] are n floats; path NULL writes to stdout. */
 int rnj_write_matrix_text(const char *path, const char *const *names, const float *const *rows,
                           int n, int threads);
+
+/* ---------------------------------------------------------------- autotuner */
+
+/* Launch parameters of one bucket of inputs: the alphabet (DNA or protein),
+ * the counting rules (RNJ_FASTDIST or not), floor(log2 n) and floor(log2 L).
+ * No counterpart in the reference (its CPU code has nothing to tune).  The
+ * tile edge itself is fixed at 128 pairs: the tensor-core MMA is 128 rows
+ * (M = 128) and three 128-column f32 accumulators fill the 512 columns of
+ * tensor memory with the scale factors; what varies is how the tiles are
+ * scheduled and how the columns are split.  Zero fields mean the default. */
+typedef struct rnj_tune_params {
+  int dna_kernel;      /* DNA, fast rules: 0 tensor cores, 1 bit-plane popcount */
+  int ksplit;          /* bit-plane kernel: columns split over this many CTAs per tile */
+  int tile_band;       /* tensor-core kernel: tile-order band height in tile rows (0 = 12) */
+  int transform_ctas;  /* tensor-core transform: resident CTAs per SM, 1..5 (0 = 5) */
+  int stream_band;     /* rnj_distance_matrix_host: band height in tile rows (0 = automatic) */
+  float ms;            /* the tuned configuration's time for the measured shape (output) */
+} rnj_tune_params;
+
+/* Times the candidate configurations of the bucket of (n, L, type, flags) on a
+ * seeded synthetic alignment of exactly n x L (related sequences with gaps) on
+ * the context's device, through the same calls as rnj_distance_into and
+ * rnj_distance_matrix_host, and stores the fastest in the process-wide table
+ * that every later call of that bucket uses.  Every candidate computes the same
+ * distances; only the time differs.  If the environment variable
+ * RNJ_TUNE_CACHE names a file, the table is read from it on first use and
+ * written back after each rnj_tune.  out (may be NULL) receives the choice. */
+int rnj_tune(rnj_ctx *ctx, int n, int L, int type, int flags, rnj_tune_params *out);
+/* The stored entry of the bucket (RNJ_ERR_NOTREADY if there is none). */
+int rnj_tune_get(int n, int L, int type, int flags, rnj_tune_params *out);
+/* Stores an entry for the bucket (fields validated; RNJ_ERR_INVALID if out of range). */
+int rnj_tune_set(int n, int L, int type, int flags, const rnj_tune_params *params);
+/* Empties the table. */
+int rnj_tune_clear(void);
+/* Writes / reads the table as text, one bucket per line (reading merges). */
+int rnj_tune_save(const char *path);
+int rnj_tune_load(const char *path);
 
 #ifdef __cplusplus
 }

@@ -48,6 +48,7 @@ SIGNATURES = {
     "rnj_ctx_set_profiling": (c_int, [c_void_p, c_int]),
     "rnj_ctx_stage_times": (c_int, [c_void_p, P(c_float)]),
     "rnj_probe_int_peaks": (c_int, [c_void_p, P(ctypes.c_double), P(ctypes.c_double)]),
+    "rnj_probe_tc_peak": (c_int, [c_void_p, P(ctypes.c_double)]),
     "rnj_aln_from_host": (c_int, [c_void_p, P(c_char_p), c_int, c_int, c_int, c_int, P(c_void_p)]),
     "rnj_aln_from_host_buffer": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int, c_int,
                                          P(c_void_p)]),
@@ -68,6 +69,12 @@ SIGNATURES = {
                                          c_int, c_void_p, P(c_float)]),
     "rnj_distance_matrix_host_ex": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int,
                                             c_int, c_int, c_int, c_void_p, P(c_float)]),
+    "rnj_tune": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+    "rnj_tune_get": (c_int, [c_int, c_int, c_int, c_int, c_void_p]),
+    "rnj_tune_set": (c_int, [c_int, c_int, c_int, c_int, c_void_p]),
+    "rnj_tune_clear": (c_int, []),
+    "rnj_tune_save": (c_int, [c_char_p]),
+    "rnj_tune_load": (c_int, [c_char_p]),
     "rnj_distance_noalloc": (c_int, [c_void_p, c_int, c_int, c_size_t, c_int, c_int, c_int,
                                      c_void_p, c_size_t, c_void_p, P(c_float)]),
     "rnj_batch_create": (c_int, [c_void_p, c_int, ctypes.c_longlong, P(c_void_p)]),

@@ -131,6 +131,13 @@ class Context:
         check(N.lib().rnj_probe_int_peaks(self.handle, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def probe_tc_peak(self) -> float:
+        """FP4 tensor-pipe flop/s measured on this device (back-to-back 128 x 128 x 64
+        kind::mxf4 MMAs on every SM)."""
+        x = ctypes.c_double()
+        check(N.lib().rnj_probe_tc_peak(self.handle, ctypes.byref(x)))
+        return x.value
+
     # --- alignments
     def alignment(self, seqs, type_=None, fastdist: bool = True, compat_wrap: bool = False,
                   full_rows: bool = False, popcount: bool = False) -> Alignment:
@@ -219,6 +226,14 @@ class Context:
                                                       int(band_tiles), out.ctypes.data,
                                                       ctypes.byref(m)))
         return out, m.value
+
+    def tune(self, n: int, L: int, type_="dna", fastdist: bool = True) -> "TuneParams":
+        """rnj_tune: time the candidate launch choices of the bucket of (n, L) on a
+        seeded synthetic n x L alignment and keep the fastest for later calls."""
+        p = TuneParams()
+        check(N.lib().rnj_tune(self.handle, n, L, TYPES[type_], flags_of(fastdist),
+                               ctypes.byref(p)))
+        return p
 
     def close(self) -> None:
         if self.handle:
@@ -311,6 +326,44 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class TuneParams(ctypes.Structure):
+    """rnj_tune_params: the launch choices of one bucket (alphabet, rules,
+    floor(log2 n), floor(log2 L)); zero fields mean the library default."""
+    _fields_ = [("dna_kernel", ctypes.c_int), ("ksplit", ctypes.c_int),
+                ("tile_band", ctypes.c_int), ("transform_ctas", ctypes.c_int),
+                ("stream_band", ctypes.c_int), ("ms", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def tune_get(n: int, L: int, type_="dna", fastdist: bool = True):
+    """The stored entry of the bucket of (n, L), or None."""
+    p = TuneParams()
+    rc = N.lib().rnj_tune_get(n, L, TYPES[type_], flags_of(fastdist), ctypes.byref(p))
+    if rc == 9:  # RNJ_ERR_NOTREADY: no entry for this bucket
+        return None
+    check(rc)
+    return p
+
+
+def tune_set(n: int, L: int, type_="dna", fastdist: bool = True, **fields) -> None:
+    p = TuneParams(**fields)
+    check(N.lib().rnj_tune_set(n, L, TYPES[type_], flags_of(fastdist), ctypes.byref(p)))
+
+
+def tune_clear() -> None:
+    check(N.lib().rnj_tune_clear())
+
+
+def tune_save(path: str) -> None:
+    check(N.lib().rnj_tune_save(path.encode()))
+
+
+def tune_load(path: str) -> None:
+    check(N.lib().rnj_tune_load(path.encode()))
 
 
 def shard_tiles(n: int, shard: int, nshards: int, full_rows: bool = False):

@@ -307,7 +307,8 @@ int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
   p.W = (L + 31) / 32;
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
-  if (kind == KIND_DNA && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns) {
+  if (kind == KIND_DNA && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns &&
+      tune_lookup(n, L, type, flags).dna_kernel == 0) {
     // FP4 feature rows for the tensor-core kernel instead of bit planes.
     p.kind = KIND_DNA_TC;
     p.NP = 0;
@@ -376,7 +377,9 @@ EpiParams epi_for(rnj_ctx *ctx, const Packed &p, int model) {
 int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mode) {
   const int nt = tiles_of(p.n);
   const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
+  const TuneParams tp = tune_lookup(p.n, p.L, p.type, p.flags);
   AlnDesc d = desc_for(p, ep);
+  d.band = tp.tile_band;
   // Pageable source: the copy is taken before the call returns, so the stack
   // descriptor may go out of scope.
   RNJ_CUDA(cudaMemcpyAsync(ctx->d_desc, &d, sizeof(d), cudaMemcpyHostToDevice, ctx->stream),
@@ -390,7 +393,8 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
   }
   int rc = ensure_packed(ctx, std::min<long long>(ntiles, kTcChunkTiles));
   if (rc != RNJ_OK) return rc;
-  return run_tc_chunks(ctx, ctx->d_desc, nullptr, ntiles, ctx->d_packed, ctx->stream);
+  return run_tc_chunks(ctx, ctx->d_desc, nullptr, ntiles, ctx->d_packed, ctx->stream,
+                       tp.transform_ctas);
 }
 
 int check_device_error(rnj_ctx *ctx) {
@@ -451,7 +455,13 @@ int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t 
 // The bit-plane counting kernels: fused counts + transform, or split counts +
 // transform for alignments longer than one 16-bit accumulator pass.
 int run_popcount(rnj_ctx *ctx, const Packed &p, int ckind, int nk, int nt, EpiParams &ep) {
-  if (nk <= kMaxFusedWords / kKW) {
+  // K split (tuned per bucket): short triangles of long alignments leave most
+  // SMs idle with one CTA per tile; splitting the columns over several CTAs
+  // per tile (atomic count accumulation, then the transform) fills them.
+  const TuneParams tp = tune_lookup(p.n, p.L, p.type, p.flags);
+  const bool split = tp.ksplit > 1 && nk >= 2 && !ep.full &&
+                     (size_t)p.n * p.n * 3 * sizeof(uint32_t) <= (size_t)1 << 30;
+  if (nk <= kMaxFusedWords / kKW && !split) {
     RNJ_CUDA(launch_count_tiles(p, ckind, EPI_DIST, ep, ctx->stream), "count kernel");
   } else {
     const size_t cbytes = (size_t)p.n * p.n * 3 * sizeof(uint32_t);
@@ -459,7 +469,8 @@ int run_popcount(rnj_ctx *ctx, const Packed &p, int ckind, int nk, int nt, EpiPa
     RNJ_CUDA(cudaMallocAsync((void **)&counts, cbytes, ctx->stream), "count buffer");
     ep.counts = counts;
     cudaError_t e = cudaMemsetAsync(counts, 0, cbytes, ctx->stream);
-    if (e == cudaSuccess) e = launch_count_tiles(p, ckind, EPI_ATOMIC, ep, ctx->stream);
+    const int kchunk = split ? (nk + tp.ksplit - 1) / tp.ksplit * kKW : 0;
+    if (e == cudaSuccess) e = launch_count_tiles(p, ckind, EPI_ATOMIC, ep, ctx->stream, kchunk);
     if (e == cudaSuccess) e = launch_transform_counts(ep, nt, ctx->stream);
     cudaFreeAsync(counts, ctx->stream);
     if (e != cudaSuccess) return cuda_error(e, "split count pipeline");
@@ -501,7 +512,9 @@ int ensure_packed(rnj_ctx *ctx, long long tiles) {
 }
 
 int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, long long nitems,
-                  uint64_t *packed, cudaStream_t s) {
+                  uint64_t *packed, cudaStream_t s, int transform_ctas) {
+  const int ctas = transform_ctas > 0 ? std::min(transform_ctas, kTransformCtasPerSm)
+                                      : kTransformCtasPerSm;
   const int chunk = (int)std::min<long long>(nitems, kTcChunkTiles);
   for (long long i0 = 0; i0 < nitems; i0 += chunk) {
     const int cnt = (int)std::min<long long>(chunk, nitems - i0);
@@ -512,7 +525,7 @@ int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, 
     if (i0 + chunk >= nitems) mark(ctx, 1, 1);
     if (i0 + chunk >= nitems) mark(ctx, 2, 0);
     RNJ_CUDA(launch_tc_transform(d_desc, d_items, nullptr, (int)nitems, (int)i0, cnt, packed,
-                                 std::min(cnt, kTransformCtasPerSm * ctx->num_sms), s),
+                                 std::min(cnt, ctas * ctx->num_sms), s),
              "transform kernel");
   }
   return RNJ_OK;

@@ -92,7 +92,7 @@ struct alignas(128) AlnDesc {
   int *err;                   // shared error word
   int n, L, nt, kdim;         // kdim: Lk columns (tensor-core) or Wp words (popcount)
   int model, type, compat, full;
-  int kind, np, pad0, pad1;
+  int kind, np, band, pad1;    // band: tile-order band height (single alignment), 0 = 12
   double jc_b;
 };
 
@@ -111,6 +111,20 @@ struct Scratch {
   size_t counts_cap = 0;
 };
 
+// Tuned launch parameters of one (alphabet, rules, n, L) bucket (rnj_tune.cu).
+// Zero means the built-in default.
+struct TuneParams {
+  int dna_kernel = 0;      // DNA fast rules: 0 tensor cores, 1 bit-plane popcount
+  int ksplit = 1;          // bit-plane kernel: K (columns) split over this many CTAs per tile
+  int tile_band = 0;       // tensor-core kernel: tile-order band height in tile rows (0 = 12)
+  int transform_ctas = 0;  // tensor-core transform: resident CTAs per SM (0 = 5)
+  int stream_band = 0;     // streamed host call: band height in tile rows (0 = automatic)
+};
+// The parameters of the bucket of (n, L, type, flags): the tuned entry if the
+// table (filled by rnj_tune / rnj_tune_load / RNJ_TUNE_CACHE) holds one, else
+// the defaults.
+TuneParams tune_lookup(int n, int L, int type, int flags);
+
 // Launchers (rnj_kernels.cu).
 cudaError_t launch_pack_chars(const uint8_t *d_chars, size_t ld, const Packed &p,
                               const uint8_t lut[256], cudaStream_t s);
@@ -118,8 +132,9 @@ cudaError_t launch_presence(const uint8_t *d_chars, size_t ld, int n, int L,
                             uint32_t *d_mask /*8 words*/, cudaStream_t s);
 cudaError_t launch_pack_bitstrings_dna(const uint32_t *d_bits, const uint32_t *d_gaps,
                                        int bs_words, const Packed &p, cudaStream_t s);
+// kchunk > 0: words of K per CTA (EPI_ATOMIC splits K over grid.y).
 cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode,
-                               const EpiParams &ep, cudaStream_t s);
+                               const EpiParams &ep, cudaStream_t s, int kchunk = 0);
 cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s);
 cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s);
 // Tensor-core DNA path (rnj_tc.cu).
@@ -144,6 +159,8 @@ AlnDesc desc_for(const Packed &p, const EpiParams &ep);
 cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
                             int nitems, int item0, int count, uint64_t *packed, int grid,
                             int epi_mode, cudaStream_t s);
+// Tensor-pipe probe (rnj_probe_tc_peak): one CTA per SM, `iters` FP4 MMAs each.
+cudaError_t launch_tc_peak_probe(int grid, int iters, int *err, cudaStream_t s);
 cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
                                 const int *d_nitems, int nitems, int item0, int count,
                                 const uint64_t *packed, int grid, cudaStream_t s);

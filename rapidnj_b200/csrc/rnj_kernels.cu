@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "rnj_device.cuh"
 #include "rnj_epilogue.cuh"
 #include "rnj_internal.h"
@@ -768,13 +770,15 @@ static cudaError_t launch_kind(int kind, const Packed &p, const EpiParams &ep, d
 }
 
 cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode, const EpiParams &ep,
-                               cudaStream_t s) {
+                               cudaStream_t s, int kchunk_words) {
   const int nt = tiles_of(p.n);
   const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
   if (ntiles == 0) return cudaSuccess;
   const int nk = p.Wp / kKW;
   const int kmax = kMaxFusedWords / kKW;
-  const int kchunk = (epi_mode == EPI_ATOMIC) ? kmax : nk;
+  int kchunk = (epi_mode == EPI_ATOMIC) ? kmax : nk;
+  if (epi_mode == EPI_ATOMIC && kchunk_words > 0)
+    kchunk = std::max(1, std::min(kmax, kchunk_words / kKW));
   const int nsplit = (nk + kchunk - 1) / kchunk;
   dim3 grid((unsigned)ntiles, (unsigned)nsplit);
   switch (epi_mode) {

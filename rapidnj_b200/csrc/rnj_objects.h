@@ -35,8 +35,9 @@ int ensure_packed(rnj_ctx *ctx, long long tiles);
 // passes of at most kTcChunkTiles tiles through `packed` (capacity
 // min(nitems, kTcChunkTiles) tiles), on stream s.  Profiling marks: stage 1
 // spans the counting kernels, stage 2 the transforms (rnj_api.cu).
+// transform_ctas > 0: resident CTAs per SM of the transform grid (else 5).
 int run_tc_chunks(rnj_ctx *ctx, const rnj::AlnDesc *d_desc, const rnj::WorkItem *d_items,
-                  long long nitems, uint64_t *packed, cudaStream_t s);
+                  long long nitems, uint64_t *packed, cudaStream_t s, int transform_ctas = 0);
 
 struct rnj_aln {
   rnj_ctx *ctx = nullptr;

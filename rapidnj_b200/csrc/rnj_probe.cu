@@ -92,3 +92,44 @@ extern "C" int rnj_probe_int_peaks(rnj_ctx *ctx, double *popc_per_s, double *lop
   if (lop3_per_s) *lop3_per_s = best[1];
   return RNJ_OK;
 }
+
+// FP4 tensor-pipe peak: every SM issues back-to-back 128 x 128 x 64 kind::mxf4
+// MMAs (2 * 128 * 128 * 64 flops each); best of three launches.
+extern "C" int rnj_probe_tc_peak(rnj_ctx *ctx, double *fp4_flops_per_s) {
+  if (!ctx || !fp4_flops_per_s) return set_error(RNJ_ERR_INVALID, "null argument");
+  void *sv = nullptr;
+  int rc = rnj_ctx_stream(ctx, &sv);
+  if (rc != RNJ_OK) return rc;
+  cudaStream_t s = (cudaStream_t)sv;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int iters = 16384;
+  int *err = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&err, sizeof(int), s);
+  if (e != cudaSuccess) return cuda_error(e, "probe flag");
+  e = cudaMemsetAsync(err, 0, sizeof(int), s);
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  double best = 0.0;
+  for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+    cudaEventRecord(a, s);
+    e = launch_tc_peak_probe(sms, iters, err, s);
+    cudaEventRecord(b, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float ms = 0.0f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, a, b);
+    if (rep > 0 && ms > 0.0f)
+      best = std::max(best, (double)sms * iters * 2.0 * 128 * 128 * 64 / (ms * 1e-3));
+  }
+  int h_err = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFreeAsync(err, s);
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (e != cudaSuccess) return cuda_error(e, "tensor-pipe probe");
+  if (h_err) return set_error(RNJ_ERR_TIMEOUT, "tensor-pipe probe: a bounded wait ran out");
+  *fp4_flops_per_s = best;
+  return RNJ_OK;
+}

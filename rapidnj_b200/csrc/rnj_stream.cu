@@ -137,7 +137,10 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
       L > kMaxTcColumns || (model != RNJ_JC && model != RNJ_KIMURA))
     return RNJ_ERR_UNSUPPORTED;
   const int nt = tiles_of(n);
-  const int g = band_tiles > 0 ? band_tiles : default_band_tiles(nt);
+  const TuneParams tp = tune_lookup(n, L, RNJ_DNA, flags);
+  if (tp.dna_kernel != 0) return RNJ_ERR_UNSUPPORTED;  // this bucket counts on the bit planes
+  const int g = band_tiles > 0 ? band_tiles
+                               : (tp.stream_band > 0 ? tp.stream_band : default_band_tiles(nt));
   const std::vector<int> bounds = band_bounds(nt, g);
   const int nbands = (int)bounds.size() - 1;
   if (nbands < 2) return RNJ_ERR_UNSUPPORTED;
@@ -173,6 +176,10 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   p.Np = nt * kTile;
   p.NP = 0;
   p.Lk = std::max(256, (L + 255) / 256 * 256);
+
+  const int transform_ctas = tp.transform_ctas > 0
+                                 ? std::min(tp.transform_ctas, kTransformCtasPerSm)
+                                 : kTransformCtasPerSm;
 
   // Work items, band by band, last band first; within a band column by
   // column, so that the CTAs running at one time share the band's row tiles.
@@ -253,7 +260,7 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
             "tensor-core kernel");
     RNJ_TRY(launch_tc_transform(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
                                 (int)cnt, ctx->d_packed,
-                                (int)std::min<long long>(cnt, (long long)kTransformCtasPerSm *
+                                (int)std::min<long long>(cnt, (long long)transform_ctas *
                                                                   ctx->num_sms),
                                 ctx->stream),
             "transform kernel");

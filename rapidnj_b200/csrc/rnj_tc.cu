@@ -337,12 +337,12 @@ __device__ __forceinline__ void item_tile(const AlnDesc &d, int tile, int &ti, i
 // and 148 / kBand column tiles of operands instead of two rows and every
 // column, which keeps the operand working set of the running tiles in L2.
 // Returns the tile's row-major triangle index (the index of its saturation flag).
-constexpr int kBand = 12;
+constexpr int kBand = 12;  // default band height (the autotuner may choose another)
 
-__device__ __forceinline__ int banded_tile(int it, int nt) {
+__device__ __forceinline__ int banded_tile(int it, int nt, int band) {
   int r0 = 0;
   while (true) {
-    const int g = min(kBand, nt - r0);
+    const int g = min(band, nt - r0);
     const int tri = g * (g + 1) / 2;
     const int count = tri + (nt - r0 - g) * g;
     if (it < count || r0 + g >= nt) {
@@ -369,7 +369,8 @@ __device__ __forceinline__ WorkItem item_at(const AlnDesc *descs, const WorkItem
   if (items) return items[it];
   WorkItem w;
   w.aln = 0;
-  w.tile = descs[0].full ? it : banded_tile(it, descs[0].nt);
+  const int band = descs[0].band > 0 ? descs[0].band : kBand;
+  w.tile = descs[0].full ? it : banded_tile(it, descs[0].nt, band);
   return w;
 }
 
@@ -716,6 +717,75 @@ cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
   if (grid <= 0) return cudaSuccess;
   tc_transform_kernel<<<(unsigned)grid, kTransformThreads, kTransformSmem, s>>>(
       d_descs, d_items, d_nitems, nitems, item0, count, packed);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------ tensor-pipe probe
+//
+// The FP4 tensor-pipe throughput of the device: one CTA per SM, one thread
+// issuing `iters` back-to-back 128 x 128 x 64 kind::mxf4 MMAs into one
+// accumulator with loop-invariant descriptors (zero operands in shared
+// memory, unit scale factors), then one commit.  The counting kernel's
+// roofline is reported against this rate beside the 4 x bf16 GEMM figure.
+constexpr int kProbeSmem = 32 * 1024 + 1024;
+
+__global__ void __launch_bounds__(128, 1) tc_peak_probe_kernel(int iters, int *err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem =
+      reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ uint64_t bar;
+  __shared__ uint32_t slot;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < 32 * 1024 / 16; i += 128)
+    reinterpret_cast<uint4 *>(smem)[i] = make_uint4(0, 0, 0, 0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(&slot, kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = slot;
+  {
+    const uint32_t base = tmem + ((uint32_t)(32 * warp) << 16) + kTmemSfa;
+    tmem_st32(base, 0x7F7F7F7Fu);
+    tmem_st32(base + 32, 0x7F7F7F7Fu);
+    tmem_st32(base + 64, 0x7F7F7F7Fu);
+    tmem_st32(base + 96, 0x7F7F7F7Fu);
+    tmem_st_wait();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) {
+    const uint64_t ad = smem_desc_sw128(smem_u32(smem));
+    const uint64_t bd = smem_desc_sw128(smem_u32(smem) + kTcTileBytes);
+    for (int i = 0; i < iters; i += 4) {
+      tc_mma_fp4_elect(tmem, ad, bd, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, i > 0);
+      tc_mma_fp4_elect(tmem, ad + 2, bd + 2, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+      tc_mma_fp4_elect(tmem, ad + 4, bd + 4, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+      tc_mma_fp4_elect(tmem, ad + 6, bd + 6, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+    }
+    tc_commit_elect(&bar);
+    if (tid == 0 && !mbar_wait_bounded(&bar, 0)) atomicOr(err, 1);
+    __syncwarp();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+cudaError_t launch_tc_peak_probe(int grid, int iters, int *err, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(tc_peak_probe_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kProbeSmem);
+  if (e != cudaSuccess) return e;
+  tc_peak_probe_kernel<<<grid, 128, kProbeSmem, s>>>(iters, err);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,87 @@
+"""Autotuned launch choices change the time of a distance call, never its
+result: every choice (tensor cores or bit planes for DNA, a K split of the
+bit-plane kernel, the tile-order band and transform occupancy of the
+tensor-core kernel, the streamed call's band height) gives the same bits as
+the defaults, and rnj_tune stores a choice that the next calls use."""
+import numpy as np
+import pytest
+
+from rapidnj_b200 import api, synth
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(autouse=True)
+def empty_table():
+    api.tune_clear()
+    yield
+    api.tune_clear()
+
+
+def device_matrix(ctx, seqs, typ, model):
+    aln = ctx.alignment(seqs, typ)
+    mat = ctx.distance(aln, model)
+    out, mx = mat.to_numpy(), mat.max
+    mat.close()
+    aln.close()
+    return out, mx
+
+
+def same(a, b):
+    assert np.array_equal(a[0].view(np.int32), b[0].view(np.int32)) and a[1] == b[1]
+
+
+@pytest.mark.parametrize("fields", [
+    dict(dna_kernel=1),
+    dict(dna_kernel=1, ksplit=4),
+    dict(tile_band=4, transform_ctas=3),
+    dict(tile_band=1, transform_ctas=1),
+])
+@pytest.mark.parametrize("model", ["kim", "jc"])
+def test_dna_choices_give_default_bits(ctx, fields, model):
+    seqs = synth.tree_dna(700, 3000, seed=4, mean_branch=0.05)
+    ref = device_matrix(ctx, seqs, 0, model)
+    api.tune_set(700, 3000, "dna", **fields)
+    same(device_matrix(ctx, seqs, 0, model), ref)
+
+
+@pytest.mark.parametrize("ksplit", [2, 3, 8, 16])
+def test_protein_k_split_gives_default_bits(ctx, ksplit):
+    seqs = synth.tree_protein(300, 2500, seed=6, mean_branch=0.2)
+    ref = device_matrix(ctx, seqs, 1, "kim")
+    api.tune_set(300, 2500, "protein", ksplit=ksplit)
+    same(device_matrix(ctx, seqs, 1, "kim"), ref)
+
+
+def test_stream_band_gives_default_bits(ctx):
+    seqs = synth.tree_dna(1500, 1200, seed=9)
+    out = torch.empty((1500, 1500), dtype=torch.float32).pin_memory().numpy()
+    ref = ctx.distance_matrix_host(seqs, "kim", "dna", band_tiles=-1)
+    for band in (2, 5):
+        api.tune_set(1500, 1200, "dna", stream_band=band)
+        got = ctx.distance_matrix_host(seqs, "kim", "dna", out=out)
+        same(got, ref)
+
+
+@pytest.mark.parametrize("n,L,typ", [(600, 4000, "dna"), (260, 3000, "protein")])
+def test_tune_stores_a_choice_that_later_calls_use(ctx, n, L, typ):
+    p = ctx.tune(n, L, typ)
+    assert p.ms > 0
+    got = api.tune_get(n, L, typ)
+    assert got is not None and got.as_dict() == p.as_dict()
+    # the tuned bucket computes the same distances as the defaults
+    seqs = synth.tree_dna(n, L, seed=1) if typ == "dna" else synth.tree_protein(n, L, seed=1)
+    t = 0 if typ == "dna" else 1
+    tuned = device_matrix(ctx, seqs, t, "kim")
+    api.tune_clear()
+    same(tuned, device_matrix(ctx, seqs, t, "kim"))
+
+
+def test_k_split_helps_few_long_sequences(ctx):
+    # 256 protein sequences x 20,000 columns: 3 triangle tiles, so one CTA per
+    # tile uses 3 of 148 SMs; the tuner must find that splitting the columns
+    # is faster.
+    p = ctx.tune(256, 20000, "protein")
+    assert p.ksplit > 1
