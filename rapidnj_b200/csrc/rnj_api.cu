@@ -294,11 +294,7 @@ int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, s
 
 }  // namespace
 
-int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
-                  int flags, int kind, const uint8_t lut[256], rnj_aln **out) {
-  rnj_aln *a = new rnj_aln();
-  a->ctx = ctx;
-  Packed &p = a->p;
+size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind) {
   p.n = n;
   p.L = L;
   p.type = type;
@@ -313,7 +309,20 @@ int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
     p.kind = KIND_DNA_TC;
     p.NP = 0;
     p.Lk = std::max(256, (L + 255) / 256 * 256);
-    const size_t fbytes = (size_t)p.Np * 4 * p.Lk / 2;
+    return (size_t)p.Np * 4 * p.Lk / 2;
+  }
+  p.NP = planes_of(kind);
+  return (size_t)p.NP * p.Wp * p.Np * sizeof(uint32_t);
+}
+
+int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
+                  int flags, int kind, const uint8_t lut[256], rnj_aln **out) {
+  rnj_aln *a = new rnj_aln();
+  a->ctx = ctx;
+  Packed &p = a->p;
+  const size_t pbytes = packed_layout(p, n, L, type, flags, kind);
+  if (p.kind == KIND_DNA_TC) {
+    const size_t fbytes = pbytes;
     cudaError_t e = cudaMallocAsync((void **)&p.feat, fbytes, ctx->stream);
     if (e != cudaSuccess) {
       delete a;
@@ -331,8 +340,7 @@ int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
     *out = a;
     return RNJ_OK;
   }
-  p.NP = planes_of(kind);
-  const size_t bytes = (size_t)p.NP * p.Wp * p.Np * sizeof(uint32_t);
+  const size_t bytes = pbytes;
   cudaError_t e = cudaMallocAsync((void **)&p.planes, bytes, ctx->stream);
   if (e != cudaSuccess) {
     delete a;
@@ -798,8 +806,8 @@ int rnj_aln_info(const rnj_aln *aln, int *n, int *L, int *type) {
 int rnj_aln_destroy(rnj_aln *aln) {
   if (!aln) return RNJ_OK;
   DeviceGuard g(aln->ctx->device);
-  if (aln->p.planes) cudaFreeAsync(aln->p.planes, aln->ctx->stream);
-  if (aln->p.feat) cudaFreeAsync(aln->p.feat, aln->ctx->stream);
+  if (aln->owns_mem && aln->p.planes) cudaFreeAsync(aln->p.planes, aln->ctx->stream);
+  if (aln->owns_mem && aln->p.feat) cudaFreeAsync(aln->p.feat, aln->ctx->stream);
   delete aln;
   return RNJ_OK;
 }

@@ -62,6 +62,7 @@ struct rnj_batch {
   std::vector<Entry> entries;
   long long tiles_used = 0;
   bool join = true;  // make the context stream wait for each run's completion
+  std::vector<void *> arenas;  // packed alignments of rnj_batch_add_many, freed by clear
   std::vector<int> host_max;  // maxima of the last run, read once per run
   bool host_max_valid = false;
 };
@@ -78,6 +79,7 @@ void free_batch(rnj_batch *b) {
     if (e.owned && e.out) cudaFreeAsync(e.out, b->ctx->stream);
     if (e.owns_aln) rnj_aln_destroy(e.aln);
   }
+  for (void *a : b->arenas) cudaFreeAsync(a, b->ctx->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   cudaFree(b->d_descs);
@@ -228,41 +230,143 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
     if (n[k] < 1 || L[k] < 0 || ld[k] < (size_t)L[k])
       return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
   }
-  // Residue alphabets of every protein alignment: one presence scan each, one
-  // copy and one synchronisation for all.
+  // Residue alphabets of every protein alignment: one presence launch over all
+  // of them, one copy and one synchronisation.
   std::vector<int> pidx(count, -1);
-  int np = 0;
-  for (int k = 0; k < count; ++k)
-    if (type[k] == RNJ_PROTEIN) pidx[k] = np++;
+  std::vector<PackJob> pres;
+  long long pres_units = 0;
+  for (int k = 0; k < count; ++k) {
+    if (type[k] != RNJ_PROTEIN) continue;
+    pidx[k] = (int)pres.size();
+    PackJob j;
+    memset(&j, 0, sizeof j);
+    j.chars = (const uint8_t *)d_chars[k];
+    j.ld = ld[k];
+    j.n = n[k];
+    j.L = L[k];
+    j.unit0 = pres_units;
+    pres_units += (long long)n[k] * ((L[k] + 1023) / 1024);
+    pres.push_back(j);
+  }
+  const int np = (int)pres.size();
   std::vector<uint32_t> masks((size_t)np * 8, 0);
   if (np > 0) {
-    uint32_t *d_masks = nullptr;
-    RNJ_CUDA(cudaMallocAsync((void **)&d_masks, (size_t)np * 8 * sizeof(uint32_t), ctx->stream),
+    uint8_t *d_buf = nullptr;
+    const size_t jbytes = pres.size() * sizeof(PackJob);
+    RNJ_CUDA(cudaMallocAsync((void **)&d_buf, jbytes + masks.size() * sizeof(uint32_t), ctx->stream),
              "mask buffer");
-    cudaError_t e = cudaMemsetAsync(d_masks, 0, (size_t)np * 8 * sizeof(uint32_t), ctx->stream);
-    for (int k = 0; k < count && e == cudaSuccess; ++k)
-      if (pidx[k] >= 0 && L[k] > 0)
-        e = launch_presence((const uint8_t *)d_chars[k], ld[k], n[k], L[k], d_masks + 8 * pidx[k],
-                            ctx->stream);
+    PackJob *d_jobs = (PackJob *)d_buf;
+    uint32_t *d_masks = (uint32_t *)(d_buf + jbytes);
+    cudaError_t e = cudaMemcpyAsync(d_jobs, pres.data(), jbytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(d_masks, 0, masks.size() * sizeof(uint32_t), ctx->stream);
+    if (e == cudaSuccess) e = launch_presence_multi(d_jobs, np, pres_units, d_masks, ctx->stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(masks.data(), d_masks, masks.size() * sizeof(uint32_t),
                           cudaMemcpyDeviceToHost, ctx->stream);
-    cudaFreeAsync(d_masks, ctx->stream);
+    cudaFreeAsync(d_buf, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_error(e, "residue presence");
   }
+  // Layouts of all alignments in one device arena; one pack launch for the bit
+  // planes of all of them and one for the tensor-core features.
+  std::vector<rnj_aln *> alns(count, nullptr);
+  std::vector<size_t> offs(count, 0);
+  std::vector<PackJob> planes, feats;
+  long long plane_units = 0, feat_units = 0;
+  size_t total = 0;
   for (int k = 0; k < count; ++k) {
     uint8_t lut[256];
     int kind;
     lut_for(type[k], flags, pidx[k] >= 0 ? masks.data() + 8 * pidx[k] : nullptr, lut, &kind);
-    rnj_aln *a = nullptr;
-    int rc = pack_prepared(ctx, (const uint8_t *)d_chars[k], n[k], L[k], ld[k], type[k], flags, kind,
-                           lut, &a);
-    if (rc != RNJ_OK) return rc;
-    int slot = -1;
-    rc = rnj_batch_add(b, a, model[k], d_out ? d_out[k] : nullptr, ld_out ? ld_out[k] : 0, &slot);
+    rnj_aln *a = new rnj_aln();
+    a->ctx = ctx;
+    a->owns_mem = false;
+    const size_t bytes = packed_layout(a->p, n[k], L[k], type[k], flags, kind);
+    alns[k] = a;
+    offs[k] = total;
+    total += (bytes + 255) / 256 * 256;
+    PackJob j;
+    memset(&j, 0, sizeof j);
+    j.chars = (const uint8_t *)d_chars[k];
+    j.ld = ld[k];
+    j.n = n[k];
+    j.L = L[k];
+    j.Np = a->p.Np;
+    j.kind = a->p.kind;
+    if (a->p.kind == KIND_DNA_TC) {
+      j.W = a->p.Lk;
+      j.unit0 = feat_units;
+      feat_units += (long long)a->p.Np * (a->p.Lk / 32);
+      feats.push_back(j);
+    } else {
+      j.W = a->p.Wp;
+      memcpy(j.lut, lut, 256);
+      j.unit0 = plane_units;
+      plane_units += (long long)(a->p.Np / 32) * (a->p.Wp / 8);
+      planes.push_back(j);
+    }
+  }
+  auto drop = [&](uint8_t *arena) {
+    for (rnj_aln *a : alns) delete a;
+    if (arena) cudaFreeAsync(arena, ctx->stream);
+  };
+  uint8_t *arena = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&arena, std::max<size_t>(total, 256), ctx->stream);
+  if (e != cudaSuccess) {
+    drop(nullptr);
+    return cuda_error(e, "batch pack arena");
+  }
+  {
+    size_t pi = 0, fi = 0;
+    for (int k = 0; k < count; ++k) {
+      Packed &p = alns[k]->p;
+      if (p.kind == KIND_DNA_TC) {
+        p.feat = arena + offs[k];
+        feats[fi++].dst = p.feat;
+      } else {
+        p.planes = (uint32_t *)(arena + offs[k]);
+        planes[pi++].dst = p.planes;
+      }
+    }
+  }
+  {
+    const size_t pb = planes.size() * sizeof(PackJob), fb = feats.size() * sizeof(PackJob);
+    uint8_t *d_jobs = nullptr;
+    e = cudaMallocAsync((void **)&d_jobs, std::max<size_t>(pb + fb, 16), ctx->stream);
+    if (e == cudaSuccess && pb)
+      e = cudaMemcpyAsync(d_jobs, planes.data(), pb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && fb)
+      e = cudaMemcpyAsync(d_jobs + pb, feats.data(), fb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = launch_pack_chars_multi((const PackJob *)d_jobs, (int)planes.size(), plane_units,
+                                  ctx->stream);
+    if (e == cudaSuccess)
+      e = launch_pack_features_multi((const PackJob *)(d_jobs + pb), (int)feats.size(), feat_units,
+                                     ctx->stream);
+    if (d_jobs) cudaFreeAsync(d_jobs, ctx->stream);
+    if (e != cudaSuccess) {
+      drop(arena);
+      return cuda_error(e, "batch pack kernels");
+    }
+  }
+  for (int k = 0; k < count; ++k) {
+    const int rc = alns[k]->p.kind == KIND_DNA_TC ? encode_features_map(alns[k]->p)
+                                                   : encode_planes_map(alns[k]->p);
     if (rc != RNJ_OK) {
-      rnj_aln_destroy(a);
+      drop(arena);
+      return rc;
+    }
+  }
+  b->arenas.push_back(arena);
+  for (int k = 0; k < count; ++k) {
+    int slot = -1;
+    const int rc = rnj_batch_add(b, alns[k], model[k], d_out ? d_out[k] : nullptr,
+                                 ld_out ? ld_out[k] : 0, &slot);
+    if (rc != RNJ_OK) {
+      // Alignments already added stay in the batch (its arena is the batch's);
+      // the rest are released here.
+      for (int r = k; r < count; ++r) delete alns[r];
       return rc;
     }
     b->entries[slot].owns_aln = true;
@@ -428,6 +532,8 @@ int rnj_batch_clear(rnj_batch *b) {
     if (e.owned && e.out) cudaFreeAsync(e.out, b->ctx->stream);
     if (e.owns_aln) rnj_aln_destroy(e.aln);
   }
+  for (void *a : b->arenas) cudaFreeAsync(a, b->ctx->stream);
+  b->arenas.clear();
   b->entries.clear();
   b->tiles_used = 0;
   return RNJ_OK;

@@ -125,11 +125,33 @@ struct TuneParams {
 // the defaults.
 TuneParams tune_lookup(int n, int L, int type, int flags);
 
+// One alignment of a batched pack (rnj_batch_add_many): the multi-alignment
+// pack kernels take an array of these and find the alignment of each work unit
+// by its first unit (unit0, ascending).
+struct alignas(16) PackJob {
+  const uint8_t *chars;
+  unsigned long long ld;
+  void *dst;              // bit planes (uint32 words) or FP4 features (bytes)
+  long long unit0;        // first work unit of this alignment
+  int n, L, Np, W;        // W: Wp words (bit planes) or Lk columns (features)
+  int kind, pad[3];
+  uint8_t lut[256];       // bit planes: the per-byte table of lut_for
+};
+
 // Launchers (rnj_kernels.cu).
 cudaError_t launch_pack_chars(const uint8_t *d_chars, size_t ld, const Packed &p,
                               const uint8_t lut[256], cudaStream_t s);
 cudaError_t launch_presence(const uint8_t *d_chars, size_t ld, int n, int L,
                             uint32_t *d_mask /*8 words*/, cudaStream_t s);
+// Many alignments in one launch each.  Presence: units = sum of n * ceil(L/1024)
+// (1 KB row segments), 8 mask words per job.  Planes: units = sum of
+// (Np/32) * (Wp/8) pack tiles.  Features (rnj_tc.cu): units = sum of Np * Lk/32.
+cudaError_t launch_presence_multi(const PackJob *d_jobs, int njobs, long long units,
+                                  uint32_t *d_masks, cudaStream_t s);
+cudaError_t launch_pack_chars_multi(const PackJob *d_jobs, int njobs, long long units,
+                                    cudaStream_t s);
+cudaError_t launch_pack_features_multi(const PackJob *d_jobs, int njobs, long long units,
+                                       cudaStream_t s);
 cudaError_t launch_pack_bitstrings_dna(const uint32_t *d_bits, const uint32_t *d_gaps,
                                        int bs_words, const Packed &p, cudaStream_t s);
 // kchunk > 0: words of K per CTA (EPI_ATOMIC splits K over grid.y).

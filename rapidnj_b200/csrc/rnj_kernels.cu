@@ -65,6 +65,34 @@ __device__ __forceinline__ void pack_word(const uint8_t *src, int cnt, int kind,
 // grid covers the padded Np x Wp area, so padding rows and words come out zero.
 constexpr int kPackRows = 32, kPackWords = 8;
 
+// One 32-sequence x 8-word tile (i0, w0) of an alignment into its planes;
+// s_lut holds the alignment's table.  Called by all 256 threads of a block.
+__device__ __forceinline__ void pack_chars_tile(const uint8_t *__restrict__ chars, size_t ld,
+                                                int n, int L, int Np, int Wp, int kind,
+                                                const uint8_t *s_lut,
+                                                uint32_t (*s_words)[kPackWords][kPackRows + 1],
+                                                uint32_t *__restrict__ planes, int i0, int w0) {
+  const int np = planes_of(kind);
+  const size_t plane_stride = (size_t)Np * Wp;
+  {
+    const int r = threadIdx.x >> 3, ww = threadIdx.x & 7;
+    const int i = i0 + r, w = w0 + ww;
+    uint32_t p[8];
+    const int cnt = (i < n) ? min(32, L - w * 32) : 0;
+    pack_word(chars + (size_t)i * ld + (size_t)w * 32, cnt, kind, s_lut, p);
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (q < np) s_words[q][ww][r] = p[q];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int pw = warp; pw < np * kPackWords; pw += 8) {
+    const int q = pw / kPackWords, ww = pw % kPackWords;
+    planes[q * plane_stride + (size_t)(w0 + ww) * Np + i0 + lane] = s_words[q][ww][lane];
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) pack_chars_kernel(const uint8_t *__restrict__ chars,
                                                          size_t ld, int n, int L, int Np, int Wp,
                                                          int kind, Lut256 lut,
@@ -73,30 +101,45 @@ __global__ void __launch_bounds__(256) pack_chars_kernel(const uint8_t *__restri
   __shared__ uint32_t s_words[8][kPackWords][kPackRows + 1];
   for (int k = threadIdx.x; k < 256; k += blockDim.x) s_lut[k] = lut.v[k];
   __syncthreads();
-  const int np = planes_of(kind);
-  const size_t plane_stride = (size_t)Np * Wp;
   const int row_tiles = Np / kPackRows, word_tiles = Wp / kPackWords;
   const long long tiles = (long long)row_tiles * word_tiles;
-  for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const int i0 = (int)(t % row_tiles) * kPackRows;
-    const int w0 = (int)(t / row_tiles) * kPackWords;
-    {
-      const int r = threadIdx.x >> 3, ww = threadIdx.x & 7;
-      const int i = i0 + r, w = w0 + ww;
-      uint32_t p[8];
-      const int cnt = (i < n) ? min(32, L - w * 32) : 0;
-      pack_word(chars + (size_t)i * ld + (size_t)w * 32, cnt, kind, s_lut, p);
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        if (q < np) s_words[q][ww][r] = p[q];
+  for (long long t = blockIdx.x; t < tiles; t += gridDim.x)
+    pack_chars_tile(chars, ld, n, L, Np, Wp, kind, s_lut, s_words, planes,
+                    (int)(t % row_tiles) * kPackRows, (int)(t / row_tiles) * kPackWords);
+}
+
+// The job of work unit u: the last job whose first unit is <= u.
+__device__ __forceinline__ int job_of(const PackJob *__restrict__ jobs, int njobs, long long u) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].unit0 <= u) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Planes of many alignments: a block per pack tile of any job (the tiles of
+// job j are units jobs[j].unit0 ..), its table loaded when the job changes.
+__global__ void __launch_bounds__(256) pack_chars_multi_kernel(const PackJob *__restrict__ jobs,
+                                                               int njobs, long long units) {
+  __shared__ uint8_t s_lut[256];
+  __shared__ uint32_t s_words[8][kPackWords][kPackRows + 1];
+  int cur = -1;
+  for (long long t = blockIdx.x; t < units; t += gridDim.x) {
+    const int j = job_of(jobs, njobs, t);
+    const PackJob &jb = jobs[j];
+    if (j != cur) {
+      __syncthreads();
+      for (int k = threadIdx.x; k < 256; k += blockDim.x) s_lut[k] = jb.lut[k];
+      __syncthreads();
+      cur = j;
     }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int pw = warp; pw < np * kPackWords; pw += 8) {
-      const int q = pw / kPackWords, ww = pw % kPackWords;
-      planes[q * plane_stride + (size_t)(w0 + ww) * Np + i0 + lane] = s_words[q][ww][lane];
-    }
-    __syncthreads();
+    const long long local = t - jb.unit0;
+    const int row_tiles = jb.Np / kPackRows;
+    pack_chars_tile(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, jb.kind, s_lut, s_words,
+                    (uint32_t *)jb.dst, (int)(local % row_tiles) * kPackRows,
+                    (int)(local / row_tiles) * kPackWords);
   }
 }
 
@@ -140,6 +183,45 @@ __global__ void __launch_bounds__(256) presence_kernel(const uint8_t *__restrict
     for (int off = 16; off > 0; off >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, off);
     if (lane == 0 && v) atomicOr(&mask[q], v);
   }
+}
+
+// Presence masks of many alignments: a warp per 1 KB row segment of any job,
+// its lane masks merged into the job's 8 words whenever the warp moves on to
+// another job.
+__device__ __forceinline__ void flush_mask(uint32_t (&m)[8], uint32_t *mask, int lane) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    uint32_t v = m[q];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0 && v) atomicOr(&mask[q], v);
+    m[q] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(256) presence_multi_kernel(const PackJob *__restrict__ jobs,
+                                                             int njobs, long long units,
+                                                             uint32_t *__restrict__ masks) {
+  uint32_t m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & 31;
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  int cur = -1;
+  for (long long u = gwarp; u < units; u += nwarps) {
+    const int j = job_of(jobs, njobs, u);
+    if (j != cur) {
+      if (cur >= 0) flush_mask(m, masks + 8 * cur, lane);
+      cur = j;
+    }
+    const PackJob &jb = jobs[j];
+    const int segs = (jb.L + 1023) / 1024;
+    const long long local = u - jb.unit0;
+    const int i = (int)(local / segs), sg = (int)(local % segs);
+    const uint8_t *row = jb.chars + (size_t)i * jb.ld;
+    const int k1 = min(jb.L, (sg + 1) * 1024);
+    for (int k = sg * 1024 + lane; k < k1; k += 32) mask_set(m, row[k]);
+  }
+  if (cur >= 0) flush_mask(m, masks + 8 * cur, lane);
 }
 
 __device__ __forceinline__ uint32_t compress_even_bits(uint32_t x) {
@@ -734,6 +816,21 @@ cudaError_t launch_presence(const uint8_t *d_chars, size_t ld, int n, int L, uin
                             cudaStream_t s) {
   const long long work = (long long)n * L;
   presence_kernel<<<grid_for(work, 256), 256, 0, s>>>(d_chars, ld, n, L, d_mask);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_presence_multi(const PackJob *d_jobs, int njobs, long long units,
+                                  uint32_t *d_masks, cudaStream_t s) {
+  if (njobs <= 0 || units <= 0) return cudaSuccess;
+  presence_multi_kernel<<<grid_for(units * 32, 256), 256, 0, s>>>(d_jobs, njobs, units, d_masks);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_chars_multi(const PackJob *d_jobs, int njobs, long long units,
+                                    cudaStream_t s) {
+  if (njobs <= 0 || units <= 0) return cudaSuccess;
+  const long long g = std::min<long long>(units, 148LL * 16);
+  pack_chars_multi_kernel<<<(unsigned)g, 256, 0, s>>>(d_jobs, njobs, units);
   return cudaGetLastError();
 }
 

@@ -42,6 +42,7 @@ int run_tc_chunks(rnj_ctx *ctx, const rnj::AlnDesc *d_desc, const rnj::WorkItem 
 struct rnj_aln {
   rnj_ctx *ctx = nullptr;
   rnj::Packed p;
+  bool owns_mem = true;  // false: planes / features live in a batch's shared arena
 };
 
 struct rnj_mat {
@@ -60,6 +61,10 @@ struct rnj_mat {
 void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *kind);
 int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
                   int flags, int kind, const uint8_t lut[256], rnj_aln **out);
+// The packed layout of an alignment (kind: from lut_for; the tensor-core layout
+// when the DNA fast path takes it) without allocating; returns the bytes of
+// its planes or features.
+size_t packed_layout(rnj::Packed &p, int n, int L, int type, int flags, int kind);
 
 // Helpers of rnj_api.cu shared with the streamed host-to-host path
 // (rnj_stream.cu): grow the scratch words, transform parameters wired to the

@@ -209,57 +209,88 @@ __device__ __forceinline__ void store_chunk(uint8_t *F, int Np, int Lk, int i, i
 // Valid sites are A/C/G/T in either case (dataloaderFasta.hpp:155-180).  A
 // 256-entry table in shared memory maps each byte to its four FP4 codes
 // (v | r << 4 | t << 8 | u << 12).
+// The 256-entry byte -> FP4 codes table (v | r << 4 | t << 8 | u << 12) in
+// shared memory; thread k fills entry k (256 threads).
+__device__ __forceinline__ void fill_feature_lut(uint16_t *lut) {
+  const int ch = threadIdx.x;
+  int code = -1;
+  switch (ch) {
+    case 'A': case 'a': code = 0; break;
+    case 'G': case 'g': code = 1; break;
+    case 'T': case 't': code = 2; break;
+    case 'C': case 'c': code = 3; break;
+    default: break;
+  }
+  uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, t[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
+  add_site(0, code, v, r, t, u);
+  lut[ch] = (uint16_t)(v[0] | (r[0] << 4) | (t[0] << 8) | (u[0] << 12));
+}
+
+// Row i, 32-column chunk c of the features (zeros for padding rows/columns).
+__device__ __forceinline__ void pack_feature_chunk(const uint8_t *__restrict__ chars, size_t ld,
+                                                   int n, int L, int Np, int Lk, int i, int c,
+                                                   const uint16_t *lut, uint8_t *__restrict__ F) {
+  uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
+  if (i < n) {
+    const bool aligned = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0;
+    const uint8_t *src = chars + (size_t)i * ld + c * 32;
+    // Two 16-byte loads when the rows are 16-byte aligned and the chunk is
+    // whole (a warp then reads 1 KB of a row contiguously).
+    uint4 q[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+    const bool vec = aligned && c * 32 + 32 <= L;
+    if (vec) {
+      q[0] = __ldg(reinterpret_cast<const uint4 *>(src));
+      q[1] = __ldg(reinterpret_cast<const uint4 *>(src) + 1);
+    }
+    const uint8_t *qb = reinterpret_cast<const uint8_t *>(q);
+#pragma unroll
+    for (int b = 0; b < 32; ++b) {
+      if (c * 32 + b >= L) break;
+      const uint32_t e = lut[vec ? qb[b] : src[b]];
+      const int w = b >> 3, sh = (b & 7) * 4;
+      v[w] |= (e & 0xFu) << sh;
+      r[w] |= ((e >> 4) & 0xFu) << sh;
+      tt[w] |= ((e >> 8) & 0xFu) << sh;
+      u[w] |= (e >> 12) << sh;
+    }
+  }
+  store_chunk(F, Np, Lk, i, c, v, r, tt, u);
+}
+
 __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__restrict__ chars,
                                                             size_t ld, int n, int L, int Np, int Lk,
                                                             int row0, int rows,
                                                             uint8_t *__restrict__ F) {
   __shared__ uint16_t lut[256];
-  {
-    const int ch = threadIdx.x;
-    int code = -1;
-    switch (ch) {
-      case 'A': case 'a': code = 0; break;
-      case 'G': case 'g': code = 1; break;
-      case 'T': case 't': code = 2; break;
-      case 'C': case 'c': code = 3; break;
-      default: break;
-    }
-    uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, t[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
-    add_site(0, code, v, r, t, u);
-    lut[ch] = (uint16_t)(v[0] | (r[0] << 4) | (t[0] << 8) | (u[0] << 12));
-  }
+  fill_feature_lut(lut);
   __syncthreads();
   const int chunks = Lk / 32;
   const long long total = (long long)rows * chunks;
-  const bool aligned = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    pack_feature_chunk(chars, ld, n, L, Np, Lk, row0 + (int)(t / chunks), (int)(t % chunks), lut,
+                       F);
+}
+
+// Features of many alignments: a thread per (row, 32-column chunk) of any job.
+__global__ void __launch_bounds__(256) pack_features_multi_kernel(
+    const PackJob *__restrict__ jobs, int njobs, long long units) {
+  __shared__ uint16_t lut[256];
+  fill_feature_lut(lut);
+  __syncthreads();
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < units;
        t += (long long)gridDim.x * blockDim.x) {
-    const int i = row0 + (int)(t / chunks);
-    const int c = (int)(t % chunks);
-    uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
-    if (i < n) {
-      const uint8_t *src = chars + (size_t)i * ld + c * 32;
-      // Two 16-byte loads when the rows are 16-byte aligned and the chunk is
-      // whole (a warp then reads 1 KB of a row contiguously).
-      uint4 q[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-      const bool vec = aligned && c * 32 + 32 <= L;
-      if (vec) {
-        q[0] = __ldg(reinterpret_cast<const uint4 *>(src));
-        q[1] = __ldg(reinterpret_cast<const uint4 *>(src) + 1);
-      }
-      const uint8_t *qb = reinterpret_cast<const uint8_t *>(q);
-#pragma unroll
-      for (int b = 0; b < 32; ++b) {
-        if (c * 32 + b >= L) break;
-        const uint32_t e = lut[vec ? qb[b] : src[b]];
-        const int w = b >> 3, sh = (b & 7) * 4;
-        v[w] |= (e & 0xFu) << sh;
-        r[w] |= ((e >> 4) & 0xFu) << sh;
-        tt[w] |= ((e >> 8) & 0xFu) << sh;
-        u[w] |= (e >> 12) << sh;
-      }
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].unit0 <= t) lo = mid;
+      else hi = mid - 1;
     }
-    store_chunk(F, Np, Lk, i, c, v, r, tt, u);
+    const PackJob &jb = jobs[lo];
+    const int chunks = jb.W / 32;
+    const long long local = t - jb.unit0;
+    pack_feature_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, (int)(local / chunks),
+                       (int)(local % chunks), lut, (uint8_t *)jb.dst);
   }
 }
 
@@ -687,6 +718,15 @@ cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L
   if (g > 148LL * 64) g = 148LL * 64;
   if (g < 1) g = 1;
   pack_features_kernel<<<(unsigned)g, 256, 0, s>>>(d_chars, ld, n, L, Np, Lk, row0, rows, F);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack_features_multi(const PackJob *d_jobs, int njobs, long long units,
+                                       cudaStream_t s) {
+  if (njobs <= 0 || units <= 0) return cudaSuccess;
+  long long g = (units + 255) / 256;
+  if (g > 148LL * 64) g = 148LL * 64;
+  pack_features_multi_kernel<<<(unsigned)g, 256, 0, s>>>(d_jobs, njobs, units);
   return cudaGetLastError();
 }
 
