@@ -64,11 +64,11 @@ enum {
    * dm != NULL).  Only differs for the naive DNA estimator, whose counts are
    * asymmetric. */
   RNJ_FULL_ROWS = 4,
-  /* DNA on the fast path is counted on the tensor cores by default (tcgen05
-   * kind::mxf4: FP4 features in {-1, 0, +1} with unit block scales, exact f32
-   * sums).  This flag selects the bit-plane popcount kernel instead: same
-   * counts, 0.375 instead of 2 bytes of packed input per site.  Protein and -f
-   * alignments always use the popcount kernels. */
+  /* DNA on the fast path and protein (with at most 31 distinct residues) are
+   * counted on the tensor cores by default (tcgen05 kind::mxf4: FP4 features in
+   * {-1, 0, +1} with unit block scales, exact f32 sums).  This flag selects the
+   * bit-plane popcount kernels instead: same counts, far fewer bytes of packed
+   * input per site.  DNA with the -f rules always uses the popcount kernels. */
   RNJ_POPCOUNT = 8
 };
 
@@ -356,7 +356,7 @@ int rnj_write_matrix_text(const char *path, const char *const *names, const floa
  * tensor memory with the scale factors; what varies is how the tiles are
  * scheduled and how the columns are split.  Zero fields mean the default. */
 typedef struct rnj_tune_params {
-  int dna_kernel;      /* DNA, fast rules: 0 tensor cores, 1 bit-plane popcount */
+  int dna_kernel;      /* DNA fast rules and protein: 0 tensor cores, 1 bit-plane popcount */
   int ksplit;          /* bit-plane kernel: columns split over this many CTAs per tile */
   int tile_band;       /* tensor-core kernel: tile-order band height in tile rows (0 = 12) */
   int transform_ctas;  /* tensor-core transform: resident CTAs per SM, 1..5 (0 = 5) */

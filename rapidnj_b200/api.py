@@ -227,12 +227,14 @@ class Context:
                                                       ctypes.byref(m)))
         return out, m.value
 
-    def tune(self, n: int, L: int, type_="dna", fastdist: bool = True) -> "TuneParams":
+    def tune(self, n: int, L: int, type_="dna", fastdist: bool = True,
+             popcount: bool = False) -> "TuneParams":
         """rnj_tune: time the candidate launch choices of the bucket of (n, L) on a
-        seeded synthetic n x L alignment and keep the fastest for later calls."""
+        seeded synthetic n x L alignment and keep the fastest for later calls
+        (popcount: only the bit-plane kernels' choices)."""
         p = TuneParams()
-        check(N.lib().rnj_tune(self.handle, n, L, TYPES[type_], flags_of(fastdist),
-                               ctypes.byref(p)))
+        check(N.lib().rnj_tune(self.handle, n, L, TYPES[type_],
+                               flags_of(fastdist, popcount=popcount), ctypes.byref(p)))
         return p
 
     def close(self) -> None:

@@ -78,7 +78,7 @@ int encode_planes_map(Packed &p) {
 int encode_features_map(Packed &p) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return set_error(RNJ_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
-  cuuint64_t dims[3] = {128, (cuuint64_t)p.Np, (cuuint64_t)(4 * p.Lk / 256)};
+  cuuint64_t dims[3] = {128, (cuuint64_t)p.Np, (cuuint64_t)p.nfb * (p.Lk / 256)};
   cuuint64_t strides[2] = {128, (cuuint64_t)p.Np * 128};
   cuuint32_t box[3] = {128, (cuuint32_t)kTile, 1};
   cuuint32_t estr[3] = {1, 1, 1};
@@ -141,7 +141,7 @@ EpiParams epi_params_for(const Packed &p, int model) {
 AlnDesc desc_for(const Packed &p, const EpiParams &ep) {
   AlnDesc d;
   memset(&d, 0, sizeof(d));
-  d.map = (p.kind == KIND_DNA_TC) ? p.fmap : p.tmap;
+  d.map = is_tc_kind(p.kind) ? p.fmap : p.tmap;
   d.out = ep.out;
   d.counts = ep.counts;
   d.ld = ep.ld;
@@ -151,13 +151,13 @@ AlnDesc desc_for(const Packed &p, const EpiParams &ep) {
   d.n = p.n;
   d.L = p.L;
   d.nt = tiles_of(p.n);
-  d.kdim = (p.kind == KIND_DNA_TC) ? p.Lk : p.Wp;
+  d.kdim = is_tc_kind(p.kind) ? p.Lk : p.Wp;
   d.model = ep.model;
   d.type = ep.type;
   d.compat = ep.compat_wrap;
   d.full = ep.full;
   d.kind = p.kind;
-  d.np = p.NP;
+  d.np = is_tc_kind(p.kind) ? p.nfb : p.NP;
   d.jc_b = ep.jc_b;
   return d;
 }
@@ -294,7 +294,7 @@ int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, s
 
 }  // namespace
 
-size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind) {
+size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind, const uint8_t *lut) {
   p.n = n;
   p.L = L;
   p.type = type;
@@ -308,8 +308,24 @@ size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind) {
     // FP4 feature rows for the tensor-core kernel instead of bit planes.
     p.kind = KIND_DNA_TC;
     p.NP = 0;
+    p.nfb = 4;
     p.Lk = std::max(256, (L + 255) / 256 * 256);
     return (size_t)p.Np * 4 * p.Lk / 2;
+  }
+  if (type == RNJ_PROTEIN && lut && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns &&
+      tune_lookup(n, L, type, flags).dna_kernel == 0) {
+    // Protein on the tensor cores: a valid block and one one-hot block per
+    // residue rank present, when there are at most kMaxTcRanks ranks.
+    int ranks = 0;
+    for (int c = 0; c < 256; ++c)
+      if (lut[c] != 0xFF) ranks = std::max(ranks, lut[c] + 1);
+    if (ranks >= 1 && ranks <= kMaxTcRanks) {
+      p.kind = KIND_PROT_TC;
+      p.NP = 0;
+      p.nfb = 1 + ranks;
+      p.Lk = std::max(256, (L + 255) / 256 * 256);
+      return (size_t)p.Np * p.nfb * (p.Lk / 2);
+    }
   }
   p.NP = planes_of(kind);
   return (size_t)p.NP * p.Wp * p.Np * sizeof(uint32_t);
@@ -320,8 +336,8 @@ int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
   rnj_aln *a = new rnj_aln();
   a->ctx = ctx;
   Packed &p = a->p;
-  const size_t pbytes = packed_layout(p, n, L, type, flags, kind);
-  if (p.kind == KIND_DNA_TC) {
+  const size_t pbytes = packed_layout(p, n, L, type, flags, kind, lut);
+  if (is_tc_kind(p.kind)) {
     const size_t fbytes = pbytes;
     cudaError_t e = cudaMallocAsync((void **)&p.feat, fbytes, ctx->stream);
     if (e != cudaSuccess) {
@@ -329,7 +345,10 @@ int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld,
       return cuda_error(e, "feature allocation");
     }
     mark(ctx, 0, 0);
-    e = launch_pack_features(d_chars, ld, n, L, p.Np, p.Lk, p.feat, ctx->stream);
+    e = p.kind == KIND_DNA_TC
+            ? launch_pack_features(d_chars, ld, n, L, p.Np, p.Lk, p.feat, ctx->stream)
+            : launch_pack_features_prot(d_chars, ld, n, L, p.Np, p.Lk, p.nfb, lut, p.feat,
+                                        ctx->stream);
     mark(ctx, 0, 1);
     int rc = (e == cudaSuccess) ? encode_features_map(p) : cuda_error(e, "feature pack kernel");
     if (rc != RNJ_OK) {
@@ -440,7 +459,7 @@ int run_distance(rnj_ctx *ctx, const Packed &p, int model, float *d_out, size_t 
   if (p.n == 1) RNJ_CUDA(cudaMemsetAsync(d_out, 0, sizeof(float), ctx->stream), "diagonal");
   const int ckind = count_kind_for(p, model);
   const int nk = p.Wp / kKW;
-  if (p.kind == KIND_DNA_TC) {
+  if (is_tc_kind(p.kind)) {
     // Marks stage 1 (the counting kernels) and opens stage 2 (the transforms).
     rc = run_tc_single(ctx, p, ep, EPI_PACKED);
     if (rc != RNJ_OK) return rc;
@@ -879,7 +898,7 @@ int rnj_counts_into(rnj_ctx *ctx, rnj_aln *aln, unsigned int *d_counts) {
   EpiParams ep = epi_for(ctx, p, RNJ_KIMURA);
   ep.full = (p.flags & RNJ_FULL_ROWS) ? 1 : 0;
   ep.counts = d_counts;
-  if (p.kind == KIND_DNA_TC) {
+  if (is_tc_kind(p.kind)) {
     rc = run_tc_single(ctx, p, ep, EPI_COUNTS);
     if (rc != RNJ_OK) return rc;
     return check_device_error(ctx);

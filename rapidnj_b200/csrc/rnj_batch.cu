@@ -186,7 +186,7 @@ int rnj_batch_add(rnj_batch *b, rnj_aln *aln, int model, float *d_out, size_t ld
   if (aln->ctx != b->ctx) return set_error(RNJ_ERR_INVALID, "alignment from another context");
   const Packed &p = aln->p;
   if (p.n < 1) return set_error(RNJ_ERR_INVALID, "empty alignment");
-  if (p.kind != KIND_DNA_TC && p.Wp / kKW > kMaxFusedWords / kKW)
+  if (!is_tc_kind(p.kind) && p.Wp / kKW > kMaxFusedWords / kKW)
     return set_error(RNJ_ERR_INVALID, "alignments longer than 65280 columns on the bit-plane "
                                       "kernels are not batched; use rnj_distance");
   if ((int)b->entries.size() >= b->cap_aln)
@@ -282,7 +282,7 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
     rnj_aln *a = new rnj_aln();
     a->ctx = ctx;
     a->owns_mem = false;
-    const size_t bytes = packed_layout(a->p, n[k], L[k], type[k], flags, kind);
+    const size_t bytes = packed_layout(a->p, n[k], L[k], type[k], flags, kind, lut);
     alns[k] = a;
     offs[k] = total;
     total += (bytes + 255) / 256 * 256;
@@ -294,8 +294,10 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
     j.L = L[k];
     j.Np = a->p.Np;
     j.kind = a->p.kind;
-    if (a->p.kind == KIND_DNA_TC) {
+    if (is_tc_kind(a->p.kind)) {
       j.W = a->p.Lk;
+      j.nfb = a->p.nfb;
+      memcpy(j.lut, lut, 256);
       j.unit0 = feat_units;
       feat_units += (long long)a->p.Np * (a->p.Lk / 32);
       feats.push_back(j);
@@ -321,7 +323,7 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
     size_t pi = 0, fi = 0;
     for (int k = 0; k < count; ++k) {
       Packed &p = alns[k]->p;
-      if (p.kind == KIND_DNA_TC) {
+      if (is_tc_kind(p.kind)) {
         p.feat = arena + offs[k];
         feats[fi++].dst = p.feat;
       } else {
@@ -351,7 +353,7 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
     }
   }
   for (int k = 0; k < count; ++k) {
-    const int rc = alns[k]->p.kind == KIND_DNA_TC ? encode_features_map(alns[k]->p)
+    const int rc = is_tc_kind(alns[k]->p.kind) ? encode_features_map(alns[k]->p)
                                                    : encode_planes_map(alns[k]->p);
     if (rc != RNJ_OK) {
       drop(arena);
@@ -386,9 +388,12 @@ int rnj_batch_run(rnj_batch *b) {
   std::vector<int> order(na);
   for (int a = 0; a < na; ++a) order[a] = a;
   // Cost per tile grows with the columns; longest first.
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return b->entries[x].aln->p.L > b->entries[y].aln->p.L;
-  });
+  // (tensor cores: feature blocks x columns; bit planes: planes x words).
+  auto cost = [&](int a) {
+    const Packed &p = b->entries[a].aln->p;
+    return is_tc_kind(p.kind) ? (long long)p.nfb * p.Lk : (long long)p.NP * p.Wp * 32;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
   for (int a = 0; a < na; ++a) {
     const Entry &en = b->entries[a];
     const Packed &p = en.aln->p;
@@ -403,7 +408,7 @@ int rnj_batch_run(rnj_batch *b) {
   for (int oi = 0; oi < na; ++oi) {
     const int a = order[oi];
     const Entry &en = b->entries[a];
-    const bool tc = en.aln->p.kind == KIND_DNA_TC;
+    const bool tc = is_tc_kind(en.aln->p.kind);
     for (long long t = 0; t < en.ntiles; ++t) {
       WorkItem w;
       w.aln = a;

@@ -19,9 +19,19 @@ namespace rnj {
 //   KIND_MISM5  planes {c0..c4, valid}         -> {mismatch, valid}
 //   KIND_MISM7  planes {c0..c6, valid}         -> {mismatch, valid}
 //   KIND_DNA_TC FP4 features {v | r | t | u}    -> {ts, tv, valid} on tensor cores
+//   KIND_PROT_TC FP4 features {v | one-hot rank 0 | ... | rank R-1}
+//                                              -> {mismatch, valid} on tensor cores
 enum Kind {
-  KIND_DNA = 0, KIND_NAIVE = 1, KIND_MISM2 = 2, KIND_MISM5 = 3, KIND_MISM7 = 4, KIND_DNA_TC = 5
+  KIND_DNA = 0, KIND_NAIVE = 1, KIND_MISM2 = 2, KIND_MISM5 = 3, KIND_MISM7 = 4, KIND_DNA_TC = 5,
+  KIND_PROT_TC = 6
 };
+
+__host__ __device__ inline bool is_tc_kind(int kind) {
+  return kind == KIND_DNA_TC || kind == KIND_PROT_TC;
+}
+// Protein on the tensor cores: at most this many residue ranks (1 + ranks
+// feature blocks); larger alphabets are counted on the bit planes.
+constexpr int kMaxTcRanks = 31;
 
 constexpr int kTile = 128;        // pairs per tile edge (rows and columns)
 constexpr int kWordBits = 32;     // sites per plane word
@@ -61,7 +71,8 @@ struct Packed {
   // block is a contiguous 16 KB run.
   uint8_t *feat = nullptr;
   int Lk = 0;            // L rounded up to 256
-  CUtensorMap fmap;      // 3-D map over (128, Np, 4 * Lk / 256), box (128, 128, 1), 128-byte swizzle
+  int nfb = 4;           // feature blocks of Lk columns: 4 (DNA), 1 + ranks (protein)
+  CUtensorMap fmap;      // 3-D map over (128, Np, nfb * Lk / 256), box (128, 128, 1), 128-byte swizzle
 };
 
 struct EpiParams {
@@ -92,7 +103,8 @@ struct alignas(128) AlnDesc {
   int *err;                   // shared error word
   int n, L, nt, kdim;         // kdim: Lk columns (tensor-core) or Wp words (popcount)
   int model, type, compat, full;
-  int kind, np, band, pad1;    // band: tile-order band height (single alignment), 0 = 12
+  int kind, np, band, pad1;    // np: planes, or feature blocks (tensor-core kinds);
+                               // band: tile-order band height (single alignment), 0 = 12
   double jc_b;
 };
 
@@ -114,7 +126,7 @@ struct Scratch {
 // Tuned launch parameters of one (alphabet, rules, n, L) bucket (rnj_tune.cu).
 // Zero means the built-in default.
 struct TuneParams {
-  int dna_kernel = 0;      // DNA fast rules: 0 tensor cores, 1 bit-plane popcount
+  int dna_kernel = 0;      // DNA fast rules and protein: 0 tensor cores, 1 bit-plane popcount
   int ksplit = 1;          // bit-plane kernel: K (columns) split over this many CTAs per tile
   int tile_band = 0;       // tensor-core kernel: tile-order band height in tile rows (0 = 12)
   int transform_ctas = 0;  // tensor-core transform: resident CTAs per SM (0 = 5)
@@ -134,7 +146,7 @@ struct alignas(16) PackJob {
   void *dst;              // bit planes (uint32 words) or FP4 features (bytes)
   long long unit0;        // first work unit of this alignment
   int n, L, Np, W;        // W: Wp words (bit planes) or Lk columns (features)
-  int kind, pad[3];
+  int kind, nfb, pad[2];  // nfb: feature blocks (tensor-core kinds)
   uint8_t lut[256];       // bit planes: the per-byte table of lut_for
 };
 
@@ -163,6 +175,11 @@ cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s)
 // Rows [row0, row0 + rows) of the feature matrix (rows < 0: through Np).
 cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L, int Np, int Lk,
                                  uint8_t *F, cudaStream_t s, int row0 = 0, int rows = -1);
+// Protein residues -> FP4 features [v | one-hot rank 0 .. nfb-2]: lut = the rank
+// of each byte (0xFF: gap), rows [row0, row0 + rows).
+cudaError_t launch_pack_features_prot(const uint8_t *d_chars, size_t ld, int n, int L, int Np,
+                                      int Lk, int nfb, const uint8_t lut[256], uint8_t *F,
+                                      cudaStream_t s, int row0 = 0, int rows = -1);
 cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_gaps, int bs_words,
                                       int n, int L, int Np, int Lk, uint8_t *F, cudaStream_t s);
 int encode_features_map(Packed &p);

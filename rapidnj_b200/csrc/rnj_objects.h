@@ -61,10 +61,12 @@ struct rnj_mat {
 void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *kind);
 int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
                   int flags, int kind, const uint8_t lut[256], rnj_aln **out);
-// The packed layout of an alignment (kind: from lut_for; the tensor-core layout
-// when the DNA fast path takes it) without allocating; returns the bytes of
-// its planes or features.
-size_t packed_layout(rnj::Packed &p, int n, int L, int type, int flags, int kind);
+// The packed layout of an alignment (kind: from lut_for; a tensor-core layout
+// when DNA or protein takes one) without allocating; returns the bytes of its
+// planes or features.
+// lut (lut_for's table) decides the protein tensor-core layout (its ranks).
+size_t packed_layout(rnj::Packed &p, int n, int L, int type, int flags, int kind,
+                     const uint8_t *lut);
 
 // Helpers of rnj_api.cu shared with the streamed host-to-host path
 // (rnj_stream.cu): grow the scratch words, transform parameters wired to the

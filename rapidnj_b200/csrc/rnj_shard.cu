@@ -121,7 +121,7 @@ int rnj_shard_create(rnj_ctx *ctx, rnj_aln *aln, int model, int shard, int nshar
   const Packed &p = aln->p;
   if (p.n < 1) return set_error(RNJ_ERR_INVALID, "empty alignment");
   if (d_out && ld < (size_t)p.n) return set_error(RNJ_ERR_INVALID, "ld < n");
-  if (p.kind != KIND_DNA_TC && p.Wp / kKW > kMaxFusedWords / kKW)
+  if (!is_tc_kind(p.kind) && p.Wp / kKW > kMaxFusedWords / kKW)
     return set_error(RNJ_ERR_UNSUPPORTED, "alignments longer than 65280 columns on the bit-plane "
                                           "kernels are not sharded; use rnj_distance");
   const int full = (p.kind == KIND_NAIVE && (p.flags & RNJ_FULL_ROWS)) ? 1 : 0;
@@ -190,7 +190,7 @@ int rnj_shard_run(rnj_shard *s, float *local_max) {
     RNJ_CUDA(cudaMemsetAsync(s->out, 0, sizeof(float), st), "diagonal");
   if (nitems > 0) {
     const int grid = (int)std::min<long long>(nitems, ctx->num_sms);
-    if (p.kind == KIND_DNA_TC) {
+    if (is_tc_kind(p.kind)) {
       // Marks stage 1 around the counting kernels.
       int rc = ensure_packed(ctx, std::min<long long>(nitems, kTcChunkTiles));
       if (rc != RNJ_OK) return rc;

@@ -57,6 +57,11 @@ constexpr uint32_t kTmemCols = 512;                       // 3 x 128 accumulator
 constexpr uint32_t kTmemSfa = 384, kTmemSfb = 448;        // scale-factor columns (all 1.0)
 constexpr size_t kTcSmemBytes = (size_t)kTcStages * kTcStageBytes + 1024 + 256;
 
+// A 256-byte table passed by value to a kernel.
+struct Lut8 {
+  uint8_t v[256];
+};
+
 // ---------------------------------------------------------------- tcgen05 PTX
 
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
@@ -257,6 +262,64 @@ __device__ __forceinline__ void pack_feature_chunk(const uint8_t *__restrict__ c
   store_chunk(F, Np, Lk, i, c, v, r, tt, u);
 }
 
+// Row i, 32-column chunk c of the protein features: block 0 is the valid
+// feature (+1 where the residue is not a gap), block 1 + r the one-hot feature
+// of residue rank r (lut: rank of each byte, 0xFF for a gap).  Then for two
+// sites, V = sum v v' counts the columns where both are residues and
+// M = sum over the rank blocks counts those where they are the same residue:
+// mismatches = V - M, the counts of bitDistanceProtein.cpp:31-61.
+__device__ __forceinline__ void pack_prot_chunk(const uint8_t *__restrict__ chars, size_t ld,
+                                                int n, int L, int Np, int Lk, int nfb,
+                                                const uint8_t *lut, int i, int c,
+                                                uint8_t *__restrict__ F) {
+  uint8_t rk[32];
+#pragma unroll
+  for (int b = 0; b < 32; ++b) rk[b] = 0xFF;
+  if (i < n) {
+    const bool aligned = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0;
+    const uint8_t *src = chars + (size_t)i * ld + c * 32;
+    uint4 q[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+    const bool vec = aligned && c * 32 + 32 <= L;
+    if (vec) {
+      q[0] = __ldg(reinterpret_cast<const uint4 *>(src));
+      q[1] = __ldg(reinterpret_cast<const uint4 *>(src) + 1);
+    }
+    const uint8_t *qb = reinterpret_cast<const uint8_t *>(q);
+#pragma unroll
+    for (int b = 0; b < 32; ++b)
+      if (c * 32 + b < L) rk[b] = lut[vec ? qb[b] : src[b]];
+  }
+  uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+  for (int b = 0; b < 32; ++b)
+    if (rk[b] != 0xFF) w[b >> 3] |= fp4_of(1) << ((b & 7) * 4);
+  *feat_chunk(F, Np, Lk, 0, i, c) = make_uint4(w[0], w[1], w[2], w[3]);
+  for (int f = 1; f < nfb; ++f) {
+    const uint8_t r = (uint8_t)(f - 1);
+    w[0] = w[1] = w[2] = w[3] = 0;
+#pragma unroll
+    for (int b = 0; b < 32; ++b)
+      if (rk[b] == r) w[b >> 3] |= fp4_of(1) << ((b & 7) * 4);
+    *feat_chunk(F, Np, Lk, f, i, c) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+__global__ void __launch_bounds__(256) pack_features_prot_kernel(const uint8_t *__restrict__ chars,
+                                                                 size_t ld, int n, int L, int Np,
+                                                                 int Lk, int nfb, Lut8 lut_in,
+                                                                 int row0, int rows,
+                                                                 uint8_t *__restrict__ F) {
+  __shared__ uint8_t lut[256];
+  lut[threadIdx.x] = lut_in.v[threadIdx.x];
+  __syncthreads();
+  const int chunks = Lk / 32;
+  const long long total = (long long)rows * chunks;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x)
+    pack_prot_chunk(chars, ld, n, L, Np, Lk, nfb, lut, row0 + (int)(t / chunks),
+                    (int)(t % chunks), F);
+}
+
 __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__restrict__ chars,
                                                             size_t ld, int n, int L, int Np, int Lk,
                                                             int row0, int rows,
@@ -289,8 +352,12 @@ __global__ void __launch_bounds__(256) pack_features_multi_kernel(
     const PackJob &jb = jobs[lo];
     const int chunks = jb.W / 32;
     const long long local = t - jb.unit0;
-    pack_feature_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, (int)(local / chunks),
-                       (int)(local % chunks), lut, (uint8_t *)jb.dst);
+    if (jb.kind == KIND_PROT_TC)
+      pack_prot_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, jb.nfb, jb.lut,
+                      (int)(local / chunks), (int)(local % chunks), (uint8_t *)jb.dst);
+    else
+      pack_feature_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, (int)(local / chunks),
+                         (int)(local % chunks), lut, (uint8_t *)jb.dst);
   }
 }
 
@@ -321,6 +388,24 @@ __global__ void pack_features_bits_kernel(const uint32_t *__restrict__ bits,
     }
     store_chunk(F, Np, Lk, i, c, v, r, tt, u);
   }
+}
+
+cudaError_t launch_pack_features_prot(const uint8_t *d_chars, size_t ld, int n, int L, int Np,
+                                      int Lk, int nfb, const uint8_t lut[256], uint8_t *F,
+                                      cudaStream_t s, int row0, int rows) {
+  if (rows < 0) rows = Np - row0;
+  if (row0 < 0 || rows < 0 || row0 + rows > Np || nfb < 2 || nfb > kMaxTcRanks + 1)
+    return cudaErrorInvalidValue;
+  if (rows == 0) return cudaSuccess;
+  Lut8 l;
+  for (int k = 0; k < 256; ++k) l.v[k] = lut[k];
+  const long long work = (long long)rows * (Lk / 32);
+  long long g = (work + 255) / 256;
+  if (g > 148LL * 64) g = 148LL * 64;
+  if (g < 1) g = 1;
+  pack_features_prot_kernel<<<(unsigned)g, 256, 0, s>>>(d_chars, ld, n, L, Np, Lk, nfb, l, row0,
+                                                        rows, F);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_gaps, int bs_words,
@@ -472,7 +557,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tensormap_acquire(&d.map);
         int ti, tj;
         item_tile(d, w.tile, ti, tj);
-        const int nkb = 4 * d.kdim / kTcKCols;
+        const int nkb = d.np * d.kdim / kTcKCols;  // feature blocks x K blocks per block
         for (int kb = 0; kb < nkb; ++kb, ++gkb) {
           const int s = gkb % kTcStages;
           if (!tc_wait(&empty_bar[s], ((gkb / kTcStages) & 1) ^ 1, abort_flag)) {
@@ -502,8 +587,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       if (!go) break;
       const WorkItem w = item_at(descs, items, it);
       const AlnDesc &d = descs[w.aln];
-      const int nkb = 4 * d.kdim / kTcKCols;
-      const int seg = d.kdim / kTcKCols;
+      const int nkb = d.np * d.kdim / kTcKCols;
+      const int seg = d.kdim / kTcKCols;  // K blocks per feature block
+      // Accumulators: DNA blocks v, r, t, u -> V, R, T, T; protein blocks
+      // v, rank 0 .. -> V, M, M, ...
+      const bool prot = d.kind == KIND_PROT_TC;
       // The epilogue of the previous item must have read the accumulators.
       int ok = 1;
       if (lane == 0) ok = tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag);
@@ -519,8 +607,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         ok = __shfl_sync(0xffffffffu, ok, 0);
         if (!ok) break;
         tc_fence_after();
-        const int acc = kb < seg ? 0 : (kb < 2 * seg ? 1 : 2);
-        const uint32_t first = (kb == 0) || (kb == seg) || (kb == 2 * seg);
+        const int acc = kb < seg ? 0 : ((prot || kb < 2 * seg) ? 1 : 2);
+        const uint32_t first = (kb == 0) || (kb == seg) || (!prot && kb == 2 * seg);
         const uint64_t adesc = desc0 + (uint64_t)s * kStageStep;
         const uint64_t bdesc = adesc + kBStep;
         const uint32_t dt = tmem + (uint32_t)(acc * kTile);
@@ -560,6 +648,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       tc_fence_after();
       const int n = d.n;
       const int i = ti * kTile + row;
+      const bool prot_tile = d.kind == KIND_PROT_TC;
       uint64_t *dst = packed + (size_t)(it - item0) * (kTile * kTile);
       // Per 32-column chunk: accumulators -> integer counts -> stores.  Tensor
       // memory is handed back as soon as the last chunk is in registers.
@@ -582,8 +671,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           const int vv = __float2int_rn(__uint_as_float(V[k]));
           const int rr = __float2int_rn(__uint_as_float(R[k]));
           const int tu = __float2int_rn(__uint_as_float(T[k]));
-          const uint32_t ts = (uint32_t)((vv + rr - tu) >> 2);
-          const uint32_t tv = (uint32_t)((vv - rr) >> 1);
+          // DNA: transitions, transversions; protein: mismatches (V - M), 0.
+          const uint32_t ts = prot_tile ? (uint32_t)(vv - rr) : (uint32_t)((vv + rr - tu) >> 2);
+          const uint32_t tv = prot_tile ? 0u : (uint32_t)((vv - rr) >> 1);
           if constexpr (EPI == EPI_PACKED) {
             // Column-major within the tile: the 32 lanes (consecutive rows)
             // store 256 contiguous bytes.

@@ -3,7 +3,7 @@
 // A bucket is (alphabet, counting rules, floor(log2 n), floor(log2 L)).  For
 // each bucket the table holds the choices that only change the time of a
 // distance call, never its result:
-//   * DNA with the fast rules: tensor-core or bit-plane popcount counting;
+//   * tensor-core or bit-plane popcount counting (DNA fast rules, protein);
 //   * bit-plane kernel: how many CTAs share the columns of one tile (K split,
 //     counts accumulated atomically, then the transform) -- one CTA per tile
 //     leaves most SMs idle when a long alignment has few sequences;
@@ -311,7 +311,9 @@ extern "C" int rnj_tune(rnj_ctx *ctx, int n, int L, int type, int flags, rnj_tun
 
   const int nt = tiles_of(n);
   const int nk = std::max(1, ((L + 31) / 32 + kKW - 1) / kKW);  // 8-word K blocks of the bit planes
-  const bool tc_ok = type == RNJ_DNA && (flags & RNJ_FASTDIST) && !(flags & RNJ_POPCOUNT) &&
+  // Tensor cores: DNA with the fast rules; protein with either (its synthetic
+  // alphabet has 20 residues, within the tensor-core limit).
+  const bool tc_ok = (type == RNJ_PROTEIN || (flags & RNJ_FASTDIST)) && !(flags & RNJ_POPCOUNT) &&
                      L <= kMaxTcColumns;
   const bool split_ok = (size_t)n * n * 3 * sizeof(uint32_t) <= ((size_t)1 << 30);
   rnj_tune_params best;
@@ -356,14 +358,14 @@ extern "C" int rnj_tune(rnj_ctx *ctx, int n, int L, int type, int flags, rnj_tun
       if (ks > 1 && (!split_ok || ks > nk)) break;
       rnj_tune_params c;
       memset(&c, 0, sizeof c);
-      c.dna_kernel = type == RNJ_DNA && tc_ok ? 1 : 0;
+      c.dna_kernel = tc_ok ? 1 : 0;
       c.ksplit = ks;
       if ((rc = consider(c, false)) != RNJ_OK) break;
     }
   }
   // 3. The streamed host call's band height (tensor-core DNA; the host buffers
   //    are page-locked like a caller's would be for this path).
-  if (rc == RNJ_OK && tc_ok && best.dna_kernel == 0 && nt >= 8 && n <= 16384) {
+  if (rc == RNJ_OK && tc_ok && type == RNJ_DNA && best.dna_kernel == 0 && nt >= 8 && n <= 16384) {
     cudaError_t e = cudaMallocHost((void **)&b.h_chars, (size_t)n * L);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&b.h_out, (size_t)n * n * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpy(b.h_chars, b.d_chars, (size_t)n * L, cudaMemcpyDeviceToHost);

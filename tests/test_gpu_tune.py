@@ -51,7 +51,7 @@ def test_dna_choices_give_default_bits(ctx, fields, model):
 def test_protein_k_split_gives_default_bits(ctx, ksplit):
     seqs = synth.tree_protein(300, 2500, seed=6, mean_branch=0.2)
     ref = device_matrix(ctx, seqs, 1, "kim")
-    api.tune_set(300, 2500, "protein", ksplit=ksplit)
+    api.tune_set(300, 2500, "protein", dna_kernel=1, ksplit=ksplit)
     same(device_matrix(ctx, seqs, 1, "kim"), ref)
 
 
@@ -80,8 +80,8 @@ def test_tune_stores_a_choice_that_later_calls_use(ctx, n, L, typ):
 
 
 def test_k_split_helps_few_long_sequences(ctx):
-    # 256 protein sequences x 20,000 columns: 3 triangle tiles, so one CTA per
-    # tile uses 3 of 148 SMs; the tuner must find that splitting the columns
-    # is faster.
-    p = ctx.tune(256, 20000, "protein")
+    # 256 protein sequences x 20,000 columns on the bit planes: 3 triangle
+    # tiles, so one CTA per tile uses 3 of 148 SMs; the tuner must find that
+    # splitting the columns is faster.
+    p = ctx.tune(256, 20000, "protein", popcount=True)
     assert p.ksplit > 1
