@@ -52,6 +52,13 @@ def make_alignment(name: str, seed: int = 0) -> np.ndarray:
     return getattr(synth, gen)(n, L, seed=seed)
 
 
+def residue_ranks(seqs: np.ndarray) -> int:
+    """Distinct residue bytes of a protein alignment (gap bytes of the reference
+    loader's resolveChar excluded): the one-hot feature blocks it takes."""
+    gaps = set(b"-.XxzZbBJj?")
+    return sum(1 for c in np.unique(seqs) if int(c) not in gaps)
+
+
 def units(n: int, L: int) -> float:
     return n * (n - 1) / 2.0 * L
 
@@ -230,17 +237,19 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
 
     if rank == 0:
         cnt = sum(count_ms) / len(count_ms)
-        if type_ == "dna" and not args.popcount:
-            # tcgen05 kernel: 4 FP4 MACs (8 flops) per pair-column, against the
-            # dense FP4 tensor peak.
+        if not args.popcount and (type_ == "dna" or residue_ranks(seqs) <= 31):
+            # tcgen05 kernel, against the dense FP4 tensor peak: DNA 4 FP4 MACs
+            # (8 flops) per pair-column; protein 1 + R MACs (valid + one-hot of
+            # R residue ranks).
+            fpc = 8 if type_ == "dna" else 2 * (1 + residue_ranks(seqs))
             peak, peak_source = fp4_tensor_peak(local_rank)
-            achieved = 8.0 * units(n, L) * share / (cnt * 1e-3)
+            achieved = fpc * units(n, L) * share / (cnt * 1e-3)
             result["roofline"] = {
                 "bound": "tensor", "achieved": achieved / 1e12, "peak": peak / 1e12,
                 "unit": "TFLOP/s", "format": "fp4 e2m1 operands (tcgen05 kind::mxf4), f32 sums",
                 "frac": achieved / peak, "traffic": traffic_from_profiles(name),
                 "kernel": "tc_batch_kernel", "kernel_ms": cnt, "peak_source": peak_source,
-                "flops_per_pair_column": 8,
+                "flops_per_pair_column": fpc,
             }
             # The raw tensor pipe: back-to-back kind::mxf4 MMAs on every SM with
             # the operands already in shared memory (rnj_probe_tc_peak, this run).
