@@ -5,6 +5,9 @@
 //   * admission: a request is admitted when the device memory it needs (its
 //     bytes, packed operands and output matrix) fits the server's budget;
 //     otherwise it waits (first come, first served);
+//   * a submitted alignment is copied into the server's page-locked staging
+//     area (pageable memory when it is full), so that its upload is an
+//     asynchronous DMA;
 //   * every admitted request is uploaded and packed on the server's stream and
 //     added to the batch being formed;
 //   * up to two batches are in flight: a new batch is launched as soon as it has
@@ -19,10 +22,12 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <iterator>
 #include <map>
 #include <mutex>
 #include <thread>
@@ -42,7 +47,8 @@ enum ReqState { REQ_QUEUED = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3 };
 
 struct Request {
   uint64_t id = 0;
-  std::vector<char> chars;  // host copy of the alignment (n * L)
+  std::vector<char> chars;  // host copy of the alignment (n * L) when not staged
+  size_t pin_off = SIZE_MAX;  // staged: offset of the copy in the server's page-locked area
   int n = 0, L = 0, type = RNJ_DNA, model = RNJ_KIMURA, flags = RNJ_FASTDIST;
   size_t need = 0;          // device bytes reserved while the server holds it
   int state = REQ_QUEUED;
@@ -89,6 +95,14 @@ struct rnj_server {
   std::atomic<bool> stop{false};
   std::thread worker;
   // statistics
+  // Page-locked staging of submitted alignments: submit copies a request into
+  // memory that is already mapped and locked (a fresh host buffer would page
+  // fault on first touch), and the scheduler's upload is then an asynchronous
+  // DMA instead of a pageable copy that blocks it.  First fit over free extents.
+  char *pin = nullptr;
+  size_t pin_cap = 0;
+  std::map<size_t, size_t> pin_free;  // offset -> bytes
+  std::mutex pin_mu;
   uint64_t completed = 0;
   double work_units = 0;  // pair-columns of completed requests
   Clock::time_point t_first, t_last;
@@ -96,6 +110,71 @@ struct rnj_server {
 };
 
 namespace {
+
+constexpr size_t kPinAlign = 256;
+constexpr size_t kPinBytes = (size_t)256 << 20;  // staging area per server
+
+size_t pin_alloc(rnj_server *s, size_t bytes) {
+  if (!s->pin || bytes == 0) return SIZE_MAX;
+  bytes = round_up(bytes, kPinAlign);
+  std::lock_guard<std::mutex> lk(s->pin_mu);
+  for (auto it = s->pin_free.begin(); it != s->pin_free.end(); ++it) {
+    if (it->second < bytes) continue;
+    const size_t off = it->first, left = it->second - bytes;
+    s->pin_free.erase(it);
+    if (left) s->pin_free[off + bytes] = left;
+    return off;
+  }
+  return SIZE_MAX;
+}
+
+void pin_release(rnj_server *s, Request *r) {
+  if (r->pin_off == SIZE_MAX) return;
+  size_t off = r->pin_off, bytes = round_up((size_t)r->n * r->L, kPinAlign);
+  r->pin_off = SIZE_MAX;
+  std::lock_guard<std::mutex> lk(s->pin_mu);
+  auto next = s->pin_free.lower_bound(off);
+  if (next != s->pin_free.end() && off + bytes == next->first) {
+    bytes += next->second;
+    next = s->pin_free.erase(next);
+  }
+  if (next != s->pin_free.begin()) {
+    auto prev = std::prev(next);
+    if (prev->first + prev->second == off) {
+      prev->second += bytes;
+      return;
+    }
+  }
+  s->pin_free[off] = bytes;
+}
+
+// n rows of L bytes (source stride ld) into dst, packed.  Large requests are
+// copied by several threads: one thread's copy bandwidth, not the device,
+// bounds how fast requests can be submitted.
+void copy_rows(char *dst, const char *src, int n, int L, size_t ld) {
+  const size_t bytes = (size_t)n * L;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int T = bytes >= ((size_t)4 << 20) ? (int)std::min<unsigned>(8, std::max(1u, hw / 2)) : 1;
+  auto part = [&](int t) {
+    const int r0 = (int)((long long)n * t / T), r1 = (int)((long long)n * (t + 1) / T);
+    if (ld == (size_t)L)
+      memcpy(dst + (size_t)r0 * L, src + (size_t)r0 * L, (size_t)(r1 - r0) * L);
+    else
+      for (int i = r0; i < r1; ++i) memcpy(dst + (size_t)i * L, src + (size_t)i * ld, L);
+  };
+  if (T == 1) {
+    part(0);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int t = 1; t < T; ++t) pool.emplace_back(part, t);
+  part(0);
+  for (auto &th : pool) th.join();
+}
+
+const char *host_bytes(const rnj_server *s, const Request *r) {
+  return r->pin_off != SIZE_MAX ? s->pin + r->pin_off : r->chars.data();
+}
 
 void finish_batch(rnj_server *s, int b) {
   // Called with s->mu held, after the batch's completion.
@@ -114,6 +193,7 @@ void finish_batch(rnj_server *s, int b) {
       r->error = rnj_last_error();
     }
     r->t_done = now;
+    pin_release(s, r);  // its upload ran before the batch on the same stream
     if (r->d_chars) cudaFreeAsync(r->d_chars, s->ctx->stream);
     r->d_chars = nullptr;
     r->aln = nullptr;  // owned by the batch, freed by rnj_batch_clear
@@ -185,9 +265,11 @@ void scheduler(rnj_server *s) {
       cudaError_t e = cudaMallocAsync((void **)&r->d_chars, std::max<size_t>((size_t)r->n * r->L, 1),
                                       s->ctx->stream);
       if (e == cudaSuccess && r->n * (size_t)r->L > 0)
-        e = cudaMemcpyAsync(r->d_chars, r->chars.data(), (size_t)r->n * r->L,
+        e = cudaMemcpyAsync(r->d_chars, host_bytes(s, r), (size_t)r->n * r->L,
                             cudaMemcpyHostToDevice, s->ctx->stream);
       if (e != cudaSuccess) {
+        cudaStreamSynchronize(s->ctx->stream);
+        pin_release(s, r);
         std::lock_guard<std::mutex> l2(s->mu);
         r->state = REQ_FAILED;
         r->error = cudaGetErrorString(e);
@@ -224,7 +306,9 @@ void scheduler(rnj_server *s) {
       s->queue.push_front(r->id);
     }
     if (rc != RNJ_OK) {
+      cudaStreamSynchronize(s->ctx->stream);
       for (Request *r : same) {
+        pin_release(s, r);
         r->state = REQ_FAILED;
         r->error = rnj_last_error();
         r->t_done = Clock::now();
@@ -272,6 +356,14 @@ int rnj_server_create(int device, size_t memory_budget, int max_batch, rnj_serve
     }
     batch_set_join(s->batch[b], false);
   }
+  // Staging area (best effort: without it requests are copied to pageable memory).
+  if (cudaHostAlloc((void **)&s->pin, kPinBytes, cudaHostAllocDefault) == cudaSuccess) {
+    s->pin_cap = kPinBytes;
+    s->pin_free[0] = kPinBytes;
+  } else {
+    cudaGetLastError();
+    s->pin = nullptr;
+  }
   s->worker = std::thread(scheduler, s);
   *out = s;
   return RNJ_OK;
@@ -293,13 +385,20 @@ int rnj_server_submit(rnj_server *s, const char *chars, int n, int L, size_t ld,
   r->type = type;
   r->model = model;
   r->flags = flags;
-  r->chars.resize((size_t)n * L);
-  for (int i = 0; i < n; ++i) memcpy(r->chars.data() + (size_t)i * L, chars + (size_t)i * ld, L);
+  const size_t bytes = (size_t)n * L;
+  r->pin_off = pin_alloc(s, bytes);
+  char *dst = r->pin_off != SIZE_MAX ? s->pin + r->pin_off : nullptr;
+  if (!dst) {
+    r->chars.resize(bytes);
+    dst = r->chars.data();
+  }
+  copy_rows(dst, chars, n, L, ld);
   r->need = bytes_needed(n, L, type, flags);
   r->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lock(s->mu);
     if (r->need > s->budget) {
+      pin_release(s, r);
       delete r;
       return set_error(RNJ_ERR_BUSY, "request larger than the server's memory budget");
     }
@@ -387,7 +486,8 @@ int rnj_server_destroy(rnj_server *s) {
       delete kv.second;
     }
   }
-  rnj_ctx_destroy(s->ctx);
+  rnj_ctx_destroy(s->ctx);  // synchronises its stream: no upload still reads the staging area
+  if (s->pin) cudaFreeHost(s->pin);
   delete s;
   return RNJ_OK;
 }

@@ -78,3 +78,27 @@ def test_served_rejects_requests_beyond_budget():
     with pytest.raises(RnjError, match="budget"):
         server.submit(synth.tree_dna(512, 4000, seed=1), "kim", 0)
     server.close()
+
+
+def test_served_beyond_the_staging_area(ctx):
+    # 36 requests of 9 MB each (324 MB) submitted at once: more than the
+    # server's 256 MiB page-locked staging area, so the later ones are staged in
+    # pageable memory until extents are freed.  Every result equals the plain call.
+    from rapidnj_b200 import api, synth
+    reqs = [(synth.tree_dna(1500, 6000, seed=100 + k, mean_branch=0.05), 0, "kim")
+            if k % 2 == 0 else (synth.tree_protein(1500, 6000, seed=100 + k), 1, "kim")
+            for k in range(36)]
+    server = api.Server(0, max_batch=6)
+    ids = [server.submit(s, m, t) for s, t, m in reqs]
+    for k, (seqs, typ, model) in enumerate(reqs):
+        server.wait(ids[k])
+        m, _ = server.result(ctx, ids[k])
+        got = m.to_numpy()
+        m.close()
+        aln = ctx.alignment(seqs, typ)
+        ref = ctx.distance(aln, model)
+        want = ref.to_numpy()
+        ref.close()
+        aln.close()
+        assert np.array_equal(got.view(np.int32), want.view(np.int32))
+    server.close()
