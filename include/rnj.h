@@ -250,6 +250,19 @@ int rnj_batch_size(rnj_batch *batch, int *alignments, long long *tiles);
 int rnj_batch_clear(rnj_batch *batch);
 int rnj_batch_destroy(rnj_batch *batch);
 
+/* Bootstrap replicates on the device: the loop of main.cpp:519-532 with the
+ * column resampling of dataloader::sample_fast_dist (dataloader.cpp:16-58).
+ * Replicate r is the alignment whose column k is column cols[r * L + k] of the
+ * original (device bytes d_chars, n rows of stride ld); rapidNJ draws these
+ * columns as rand() % L after srand(0), so a caller that draws them the same
+ * way gets its replicates.  The replicates are gathered on the device and
+ * computed as batches; d_out[r] (device, n rows of stride ld_out floats)
+ * receives replicate r's post-processed matrix and max_out[r] (host, may be
+ * NULL) its maximum distance.  n <= 32,640.  Returns when all are done. */
+int rnj_bootstrap(rnj_ctx *ctx, const void *d_chars, int n, int L, size_t ld, int type,
+                  int model, int flags, int R, const int *cols, float *const *d_out,
+                  size_t ld_out, float *max_out);
+
 /* ------------------------------------------------------------------ serving */
 
 /* Continuous batching of distance requests.  Clients submit host alignments

@@ -70,6 +70,8 @@ SIGNATURES = {
     "rnj_distance_matrix_host_ex": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int,
                                             c_int, c_int, c_int, c_void_p, P(c_float)]),
     "rnj_tune": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+    "rnj_bootstrap": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int, c_int, c_int,
+                              c_int, c_void_p, c_void_p, c_size_t, c_void_p]),
     "rnj_tune_get": (c_int, [c_int, c_int, c_int, c_int, c_void_p]),
     "rnj_tune_set": (c_int, [c_int, c_int, c_int, c_int, c_void_p]),
     "rnj_tune_clear": (c_int, []),

@@ -227,6 +227,27 @@ class Context:
                                                       ctypes.byref(m)))
         return out, m.value
 
+    def bootstrap(self, d_chars, columns: np.ndarray, type_, model="kim", fastdist: bool = True,
+                  outs=None):
+        """rnj_bootstrap: replicate r of the device alignment d_chars (a CUDA uint8
+        tensor, n x L) takes column columns[r, k] as its column k.  Returns the
+        list of R device matrices (n x n float32 tensors) and their maxima."""
+        import torch
+        n, L = d_chars.shape
+        cols = np.ascontiguousarray(columns, dtype=np.int32)
+        R = cols.shape[0]
+        assert cols.shape == (R, L)
+        if outs is None:
+            outs = [torch.empty((n, n), dtype=torch.float32, device=d_chars.device)
+                    for _ in range(R)]
+        ptrs = (ctypes.c_void_p * max(R, 1))(*[o.data_ptr() for o in outs])
+        mx = np.zeros(max(R, 1), dtype=np.float32)
+        check(N.lib().rnj_bootstrap(self.handle, ctypes.c_void_p(d_chars.data_ptr()), n, L,
+                                    d_chars.stride(0), TYPES[type_], MODELS[model],
+                                    flags_of(fastdist), R, cols.ctypes.data, ptrs, n,
+                                    mx.ctypes.data))
+        return outs, mx[:R]
+
     def tune(self, n: int, L: int, type_="dna", fastdist: bool = True,
              popcount: bool = False) -> "TuneParams":
         """rnj_tune: time the candidate launch choices of the bucket of (n, L) on a
