@@ -496,6 +496,50 @@ def run_served(args, local_rank: int = 0, rate: float = 1000.0, seconds: float =
                         "alignments, host input (H2D inside)"}
 
 
+def run_bootstrap(args, local_rank: int = 0, n: int = 2000, L: int = 2000, R: int = 100):
+    """Bootstrap replicates (rapidNJ -b): R replicates of a resident DNA K2P
+    alignment (tree-evolved, n x L) with seeded random columns, by rnj_bootstrap
+    (gather + batches) against one plain call per replicate on bytes gathered on
+    the device; identical matrices required."""
+    import torch
+    from rapidnj_b200 import api, synth
+    ctx = api.Context(local_rank)
+    dev = f"cuda:{local_rank}"
+    seqs = torch.from_numpy(synth.tree_dna(n, L, seed=3)).to(dev)
+    cols = np.random.default_rng(0).integers(0, L, size=(R, L))
+    cols_t = torch.from_numpy(cols).to(dev)
+    outs_a = [torch.empty((n, n), device=dev) for _ in range(R)]
+    outs_b = [torch.empty((n, n), device=dev) for _ in range(R)]
+
+    def plain():
+        for r in range(R):
+            a = ctx.alignment(seqs[:, cols_t[r]].contiguous(), 0)
+            ctx.distance_into(a, "kim", outs_a[r])
+            a.close()
+        ctx.synchronize()
+
+    def boot():
+        ctx.bootstrap(seqs, cols, 0, "kim", outs=outs_b)
+
+    for fn in (plain, boot):
+        fn()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    boot()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    W = R * units(n, L)
+    identical = all(torch.equal(x, y) for x, y in zip(outs_a, outs_b))
+    ctx.close()
+    return {"value": W / (t2 - t1), "unit": "pair-columns/s", "ms": 1e3 * (t2 - t1),
+            "plain_ms": 1e3 * (t1 - t0), "speedup_vs_plain": (t1 - t0) / (t2 - t1),
+            "identical_to_plain": identical,
+            "workload": f"{R} replicates of DNA K2P {n} x {L} (tree-evolved), seeded columns"}
+
+
 def fp4_tensor_peak(device: int):
     """Dense FP4 tensor throughput (flop/s) of a library GEMM on this device, and
     how it was obtained: an MXFP4 GEMM (torch._scaled_mm, unit block scales,
@@ -556,8 +600,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--popcount", action="store_true",
                     help="count DNA with the bit-plane popcount kernel instead of tensor cores")
-    ap.add_argument("--mode", default="all", choices=["all", "plain", "batched", "served"],
-                    help="all: the plain workload line plus the batched and served figures")
+    ap.add_argument("--mode", default="all",
+                    choices=["all", "plain", "batched", "served", "bootstrap"],
+                    help="all: the plain workload line plus the batched, served and bootstrap "
+                         "figures")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -603,7 +649,10 @@ def main():
                 "vs_baseline": None, "dtype": "fp4" if config["kernel"] == "tcgen05" else "u32",
                 "data": "synthetic", "config": config, "roofline": res["roofline"],
                 "e2e": res["e2e"], "clocks": res["clocks"], "stages_ms": res["stages_ms"],
-                "gpu_launches": (4 if type_ == "protein" else 3) * args.steps}
+                # per step: (protein: presence scan) + pack + count (+ transform on
+                # the tensor cores) + fix-up
+                "gpu_launches": ((1 if type_ == "protein" else 0) + 3 +
+                                 (1 if config["kernel"] == "tcgen05" else 0)) * args.steps}
         if not args.no_cpu_baseline and world == 1:
             seqs = make_alignment(args.workload)
             cpu = cpu_reference(seqs, model, type_, 0, 1)
@@ -614,6 +663,8 @@ def main():
             line["batched"] = run_batched(args, local_rank)
         if args.mode in ("all", "served") and world == 1:
             line["served"] = run_served(args, local_rank)
+        if args.mode in ("all", "bootstrap") and world == 1:
+            line["bootstrap"] = run_bootstrap(args, local_rank)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
