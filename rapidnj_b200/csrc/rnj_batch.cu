@@ -479,14 +479,18 @@ int rnj_batch_output(rnj_batch *b, int slot, float **d_out, size_t *ld, float *m
   if (d_out) *d_out = en.out;
   if (ld) *ld = en.ld;
   if (max_out) {
+    // The maxima of all slots are read once per run (one copy, one wait).
     DeviceGuard g(b->ctx->device);
     RNJ_CUDA(cudaEventSynchronize(b->ev_done), "batch sync");
-    int bits = 0;
-    RNJ_CUDA(cudaMemcpyAsync(&bits, b->d_max + slot, sizeof(int), cudaMemcpyDeviceToHost,
-                             b->stream),
-             "max copy");
-    RNJ_CUDA(cudaStreamSynchronize(b->stream), "max copy");
-    memcpy(max_out, &bits, sizeof(float));
+    if (!b->host_max_valid) {
+      b->host_max.assign(b->entries.size(), 0);
+      RNJ_CUDA(cudaMemcpyAsync(b->host_max.data(), b->d_max, sizeof(int) * b->entries.size(),
+                               cudaMemcpyDeviceToHost, b->stream),
+               "max copy");
+      RNJ_CUDA(cudaStreamSynchronize(b->stream), "max copy");
+      b->host_max_valid = true;
+    }
+    memcpy(max_out, &b->host_max[slot], sizeof(float));
   }
   return RNJ_OK;
 }
@@ -541,6 +545,7 @@ int rnj_batch_clear(rnj_batch *b) {
   b->arenas.clear();
   b->entries.clear();
   b->tiles_used = 0;
+  b->host_max_valid = false;
   return RNJ_OK;
 }
 
