@@ -523,7 +523,8 @@ def read_alignment(path: str, fmt: str | None = None):
             k += 1
         ptr = N.lib().rnj_msa_chars(h)
         size = n.value * L.value
-        chars = np.frombuffer(ctypes.string_at(ptr, size), dtype=np.uint8).reshape(n.value, L.value).copy() \
+        chars = np.ctypeslib.as_array((ctypes.c_uint8 * size).from_address(ptr)) \
+            .reshape(n.value, L.value).copy() \
             if size else np.zeros((n.value, L.value), np.uint8)
         return names, chars, t.value
     finally:

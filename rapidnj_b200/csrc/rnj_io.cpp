@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -31,12 +32,39 @@ namespace {
 
 using rnj::set_error;
 
-bool read_file(const char *path, std::vector<char> &data) {
+// The whole file in one uninitialised buffer (a zero-filled one would cost
+// another pass over it).
+struct FileData {
+  std::unique_ptr<char[]> buf;
+  size_t n = 0;
+  size_t size() const { return n; }
+  char operator[](size_t i) const { return buf[i]; }
+  const char *data() const { return buf.get(); }
+};
+
+bool read_file(const char *path, FileData &fd) {
   FILE *f = fopen(path, "rb");
   if (!f) return false;
-  char buf[1 << 16];
-  size_t k;
-  while ((k = fread(buf, 1, sizeof(buf), f)) > 0) data.insert(data.end(), buf, buf + k);
+  size_t cap = 0;
+  if (fseek(f, 0, SEEK_END) == 0) {
+    const long size = ftell(f);
+    if (size > 0) cap = (size_t)size;
+  }
+  rewind(f);
+  cap = std::max<size_t>(cap, 1 << 16);
+  fd.buf.reset(new char[cap]);
+  fd.n = 0;
+  while (true) {
+    if (fd.n == cap) {  // the file grew, or its size was unknown
+      std::unique_ptr<char[]> bigger(new char[2 * cap]);
+      memcpy(bigger.get(), fd.buf.get(), fd.n);
+      fd.buf.swap(bigger);
+      cap *= 2;
+    }
+    const size_t k = fread(fd.buf.get() + fd.n, 1, cap - fd.n, f);
+    if (k == 0) break;
+    fd.n += k;
+  }
   fclose(f);
   return true;
 }
@@ -68,42 +96,80 @@ struct Builder {
   }
 };
 
-int parse_fasta(const std::vector<char> &data, rnj_msa *m) {
-  size_t pos = 0;
-  bool eof = false;
-  auto next = [&]() -> char {
-    if (pos < data.size()) return data[pos++];
-    eof = true;
-    return 10;
-  };
-  Builder b{m};
-  std::vector<char> buf;
-  while (!eof) {
-    char c = next();
-    if (eof) break;
-    if (c == ';') {
-      while (c != 10) c = next();
-    } else if (c == '>') {
-      int rc = b.store(buf);
-      if (rc != RNJ_OK) return rc;
-      c = next();
-      std::string name;
-      while (c > 31) {
-        name.push_back(c);
-        c = next();
-      }
-      m->names.push_back(name);
-    } else {
-      while (c != 10) {
-        if (c > 32) buf.push_back(c);
-        c = next();
-      }
-    }
+// FASTA in whole lines: a line is found with memchr, a sequence line whose
+// bytes are all > 32 (the common case) is appended with one copy, any other
+// sequence line byte by byte with the reference's filter (signed chars > 32
+// kept: control bytes, spaces and bytes >= 128 are dropped).  A name is the
+// bytes > 31 after '>' up to the first other byte (dataloaderFasta.hpp:78-133).
+int parse_fasta(const FileData &data, rnj_msa *m) {
+  const char *p = data.data(), *end = p + data.size();
+  // Sequences expected: the '>' that start a line.
+  size_t headers = (p < end && *p == '>') ? 1 : 0;
+  for (const char *q = p; q < end;) {
+    const char *nl = (const char *)memchr(q, '\n', (size_t)(end - q));
+    if (!nl) break;
+    if (nl + 1 < end && nl[1] == '>') ++headers;
+    q = nl + 1;
   }
-  return b.store(buf);
+  // The sequence being read is m->chars[seq0 ..): lines are appended there
+  // directly and its length is checked when it ends.
+  size_t seq0 = 0;
+  bool first = true;
+  auto finish = [&]() -> int {
+    const size_t len = m->chars.size() - seq0;
+    if (len == 0) return RNJ_OK;
+    if (first) {
+      m->L = (int)len;
+      m->type = rnj_detect_type(m->chars.data() + seq0, m->L);
+      first = false;
+      m->chars.reserve(len * std::max<size_t>(headers, 1));
+    } else if (len != (size_t)m->L) {
+      return set_error(RNJ_ERR_FORMAT, "ERROR: Sequence " + std::to_string(m->n) + " has length " +
+                                           std::to_string(len) +
+                                           " while the preceding sequences in the alignment which "
+                                           "have length " + std::to_string(m->L) + ".");
+    }
+    m->n++;
+    seq0 = m->chars.size();
+    return RNJ_OK;
+  };
+  auto append_seq = [&](const char *a, const char *z) {
+    bool clean = true;
+    for (const char *c = a; c < z; ++c) clean &= (signed char)*c > 32;
+    if (clean) {
+      m->chars.insert(m->chars.end(), a, z);
+    } else {
+      for (const char *c = a; c < z; ++c)
+        if ((signed char)*c > 32) m->chars.push_back(*c);
+    }
+  };
+  while (p < end) {
+    const char *nl = (const char *)memchr(p, '\n', (size_t)(end - p));
+    const char *le = nl ? nl : end;  // end of file reads as a newline
+    // A segment of the line: the line itself, or what follows a name that
+    // ended on a control byte before the newline (read as if a line began
+    // there, as the reference's character loop does).
+    for (const char *q = p; q < le;) {
+      if (*q == ';') break;  // comment: the rest of the line
+      if (*q == '>') {
+        int rc = finish();
+        if (rc != RNJ_OK) return rc;
+        const char *a = q + 1, *c = a;
+        while (c < le && (signed char)*c > 31) ++c;
+        m->names.emplace_back(a, c);
+        if (c >= le) break;
+        q = c + 1;
+        continue;
+      }
+      append_seq(q, le);
+      break;
+    }
+    p = nl ? nl + 1 : end;
+  }
+  return finish();
 }
 
-int parse_stockholm(const std::vector<char> &data, rnj_msa *m) {
+int parse_stockholm(const FileData &data, rnj_msa *m) {
   size_t pos = 0;
   bool eof = false;
   auto next = [&]() -> char {
@@ -171,7 +237,7 @@ int rnj_msa_read(const char *path, const char *format, rnj_msa **out) {
                                         "the '-i' option to indicate the format.");
   }
   if (fmt != "fa" && fmt != "sth") return set_error(RNJ_ERR_UNSUPPORTED, "Unkown input format " + fmt);
-  std::vector<char> data;
+  FileData data;
   if (!read_file(path, data)) return set_error(RNJ_ERR_IO, std::string("ERROR: Could not read file: ") + path);
   rnj_msa *m = new rnj_msa();
   int rc = (fmt == "fa") ? parse_fasta(data, m) : parse_stockholm(data, m);

@@ -91,6 +91,19 @@ def test_reader_fasta_rules(tmp_path):
     assert chars.tobytes() == b"ACGTACACGTAC"
 
 
+def test_reader_fasta_name_terminators(tmp_path):
+    """A name ends at the first byte <= 31 (or >= 128); the rest of its line is
+    read as if a line began there, as the reference's character loop
+    (dataloaderFasta.hpp:78-133) reads it: a ';' there starts a comment, a '>'
+    another name; sequence bytes >= 128 are dropped like control bytes."""
+    from rapidnj_b200 import api
+    f = tmp_path / "t.fa"
+    f.write_bytes(b">a\t;comment\nACGT\n>b\r\nAC\x80GT\n>c\t>d\nACGT")
+    names, chars, t = api.read_alignment(str(f))
+    assert names == ["a", "b", "c", "d"]
+    assert chars.shape == (3, 4) and chars.tobytes() == b"ACGTACGTACGT"
+
+
 @pytest.mark.parametrize("fixture", ["fixture_LGT_70", "fixture_PF15224_full"])
 @pytest.mark.parametrize("model", ["jc", "kim"])
 def test_matrix_text_matches_reference_binary(fixture, model, tmp_path):
