@@ -551,6 +551,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       // ----------------------------------------------------------- producer
       uint32_t gkb = 0;
+      int ps = 0;           // stage of the next load and the parity of its fill
+      uint32_t pph = 0;
       for (int it = item0 + blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x) {
         const WorkItem w = item_at(descs, items, it);
         const AlnDesc &d = descs[w.aln];
@@ -559,8 +561,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         item_tile(d, w.tile, ti, tj);
         const int nkb = d.np * d.kdim / kTcKCols;  // feature blocks x K blocks per block
         for (int kb = 0; kb < nkb; ++kb, ++gkb) {
-          const int s = gkb % kTcStages;
-          if (!tc_wait(&empty_bar[s], ((gkb / kTcStages) & 1) ^ 1, abort_flag)) {
+          const int s = ps;
+          if (!tc_wait(&empty_bar[s], pph ^ 1u, abort_flag)) {
             *abort_flag = 1;
             break;
           }
@@ -569,6 +571,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
           tma_load_3d(a, &d.map, &full_bar[s], 0, ti * kTile, kb);
           tma_load_3d(a + kTcTileBytes, &d.map, &full_bar[s], 0, tj * kTile, kb);
           issued = gkb + 1;
+          if (++ps == kTcStages) {
+            ps = 0;
+            pph ^= 1u;
+          }
         }
       }
     }
