@@ -183,8 +183,10 @@ int rnj_mat_destroy(rnj_mat *mat);
  * RNJ_ERR_INVALID with the size needed.  All calls share the array and keep the
  * last call's contents (each call clears what must start at zero): calls whose
  * work overlaps on the GPU race, so issue them one after another on one stream.
- * The first call on a device looks up the array's device address; make it
- * before any stream capture.  max_out (host, may be NULL) receives the maximum
+ * The first call on a device looks up the array's device address and loads
+ * the kernels the entry point launches (under CUDA's lazy module loading a
+ * kernel's first launch would otherwise take device memory for its code); make
+ * it before any stream capture.  max_out (host, may be NULL) receives the maximum
  * distance and synchronises the stream. */
 int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld, int type, int model,
                          int flags, float *d_out, size_t ld_out, void *stream, float *max_out);

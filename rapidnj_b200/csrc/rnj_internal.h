@@ -170,6 +170,11 @@ cudaError_t launch_pack_bitstrings_dna(const uint32_t *d_bits, const uint32_t *d
 cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode,
                                const EpiParams &ep, cudaStream_t s, int kchunk = 0);
 cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s);
+// Loads every bit-plane kernel a fused distance call can launch (pack, presence
+// scan, counts of each plane layout, fix-up).  Under CUDA's lazy module loading a
+// kernel's code is loaded, into device memory, at its first launch or attribute
+// query; the no-allocation entry point does this at its set-up instead.
+cudaError_t preload_bitplane_kernels();
 cudaError_t launch_transform_counts(const EpiParams &ep, int nt, cudaStream_t s);
 // Tensor-core DNA path (rnj_tc.cu).
 // Rows [row0, row0 + rows) of the feature matrix (rows < 0: through Np).

@@ -866,6 +866,19 @@ static cudaError_t launch_kind(int kind, const Packed &p, const EpiParams &ep, d
   return cudaErrorInvalidValue;
 }
 
+cudaError_t preload_bitplane_kernels() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, pack_chars_kernel);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, presence_kernel);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, fixup_kernel);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, count_tiles_kernel<KIND_DNA, EPI_DIST>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, count_tiles_kernel<KIND_NAIVE, EPI_DIST>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, count_tiles_kernel<KIND_MISM2, EPI_DIST>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, count_tiles_kernel<KIND_MISM5, EPI_DIST>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, count_tiles_kernel<KIND_MISM7, EPI_DIST>);
+  return e;
+}
+
 cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode, const EpiParams &ep,
                                cudaStream_t s, int kchunk_words) {
   const int nt = tiles_of(p.n);

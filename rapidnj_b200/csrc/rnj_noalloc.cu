@@ -25,7 +25,9 @@
 //     that must start at zero are cleared at the start of each call.
 //   * The first call on each device looks the array's device address up with
 //     cudaGetSymbolAddress (host code cannot use the array's name as a device
-//     address).  Make that first call before any stream capture begins.
+//     address) and loads the kernels the entry point launches, so that no later
+//     call takes device memory for kernel code.  Make that first call before any
+//     stream capture begins.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -59,6 +61,11 @@ int scratch_address(void **out) {
     void *p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(no-allocation scratch)");
+    // Load now every kernel a later call may launch: with lazy module loading
+    // (CUDA's default) a kernel's first launch would take device memory for its
+    // code in the middle of a call that promises to take none.
+    e = preload_bitplane_kernels();
+    if (e != cudaSuccess) return cuda_error(e, "kernel loading (no-allocation set-up)");
     g_scratch_addr[dev] = p;
   }
   *out = g_scratch_addr[dev];

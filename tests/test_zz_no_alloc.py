@@ -76,7 +76,7 @@ def test_noalloc_matches_allocating_entry_on_two_calls():
         stream.synchronize()
         free_after = torch.cuda.mem_get_info()[0]
         assert st == 0
-        if k == 1:  # same kernels as call 1: no device memory may be taken
+        if k == 1:  # the first call's set-up loaded every kernel: no device memory taken
             assert free_after >= free_before
         ref, rmx = existing(dev, typ, model, RNJ_FASTDIST)
         got = out[:, :n].cpu().numpy()
