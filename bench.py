@@ -521,21 +521,22 @@ def run_bootstrap(args, local_rank: int = 0, n: int = 2000, L: int = 2000, R: in
     def boot():
         ctx.bootstrap(seqs, cols, 0, "kim", outs=outs_b)
 
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
     for fn in (plain, boot):
         fn()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    plain()
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    boot()
-    torch.cuda.synchronize()
-    t2 = time.perf_counter()
+    tp = statistics.median(timed(plain) for _ in range(3))
+    tb = statistics.median(timed(boot) for _ in range(3))
     W = R * units(n, L)
     identical = all(torch.equal(x, y) for x, y in zip(outs_a, outs_b))
     ctx.close()
-    return {"value": W / (t2 - t1), "unit": "pair-columns/s", "ms": 1e3 * (t2 - t1),
-            "plain_ms": 1e3 * (t1 - t0), "speedup_vs_plain": (t1 - t0) / (t2 - t1),
+    return {"value": W / tb, "unit": "pair-columns/s", "ms": 1e3 * tb,
+            "plain_ms": 1e3 * tp, "speedup_vs_plain": tp / tb,
             "identical_to_plain": identical,
             "workload": f"{R} replicates of DNA K2P {n} x {L} (tree-evolved), seeded columns"}
 

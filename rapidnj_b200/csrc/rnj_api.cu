@@ -605,6 +605,7 @@ int rnj_ctx_create(int device, rnj_ctx **out) {
 int rnj_ctx_destroy(rnj_ctx *ctx) {
   if (!ctx) return RNJ_OK;
   DeviceGuard g(ctx->device);
+  if (ctx->boot) rnj_batch_destroy(ctx->boot);  // uses the context's stream
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->scratch.words) cudaFree(ctx->scratch.words);
   if (ctx->d_mask) cudaFree(ctx->d_mask);

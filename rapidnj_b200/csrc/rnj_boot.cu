@@ -80,9 +80,18 @@ extern "C" int rnj_bootstrap(rnj_ctx *ctx, const void *d_chars, int n, int L, si
   const long long rep_tiles = tri_tiles(tiles_of(n));
   int chunk = (int)std::max<long long>(1, std::min<long long>(R, (1LL << 30) / rep_bytes));
   chunk = (int)std::min<long long>(chunk, std::max<long long>(1, (8LL * kTcChunkTiles) / rep_tiles));
-  rnj_batch *b = nullptr;
-  int rc = rnj_batch_create(ctx, chunk, (long long)chunk * rep_tiles, &b);
-  if (rc != RNJ_OK) return rc;
+  // The context keeps the batch (its graph and buffers) for later calls of the
+  // same or a smaller size.
+  int rc = RNJ_OK;
+  if (!ctx->boot || ctx->boot_aln < chunk || ctx->boot_tiles < (long long)chunk * rep_tiles) {
+    if (ctx->boot) rnj_batch_destroy(ctx->boot);
+    ctx->boot = nullptr;
+    rc = rnj_batch_create(ctx, chunk, (long long)chunk * rep_tiles, &ctx->boot);
+    if (rc != RNJ_OK) return rc;
+    ctx->boot_aln = chunk;
+    ctx->boot_tiles = (long long)chunk * rep_tiles;
+  }
+  rnj_batch *b = ctx->boot;
   uint8_t *d_rep = nullptr;
   int *d_cols = nullptr;
   cudaError_t e = cudaMallocAsync((void **)&d_rep, (size_t)chunk * rep_bytes, ctx->stream);
@@ -115,7 +124,7 @@ extern "C" int rnj_bootstrap(rnj_ctx *ctx, const void *d_chars, int n, int L, si
   if (d_rep) cudaFreeAsync(d_rep, ctx->stream);
   if (d_cols) cudaFreeAsync(d_cols, ctx->stream);
   const cudaError_t es = cudaStreamSynchronize(ctx->stream);
-  rnj_batch_destroy(b);
+  if (rc != RNJ_OK) rnj_batch_clear(b);
   if (rc != RNJ_OK) return rc;
   if (e != cudaSuccess) return cuda_error(e, "bootstrap");
   if (es != cudaSuccess) return cuda_error(es, "bootstrap sync");

@@ -24,6 +24,9 @@ struct rnj_ctx {
   cudaStream_t s_down = nullptr;          // host-to-host calls: downloads
   int *h_words = nullptr;                 // pinned copy of the scratch words (flags, max, error)
   size_t h_words_cap = 0;
+  rnj_batch *boot = nullptr;              // rnj_bootstrap's batch, kept for the next call
+  int boot_aln = 0;                       // its capacity: alignments and tiles
+  long long boot_tiles = 0;
   rnj::AlnDesc *d_desc = nullptr;         // one-alignment work list of the persistent kernel
   uint64_t *d_packed = nullptr;           // packed counts of the tensor-core path
   long long packed_tiles = 0;             // its capacity in tiles
