@@ -612,7 +612,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     gen, n, L, type_, model = WORKLOADS[args.workload]
     config = {"workload": args.workload, "n": n, "L": L, "type": type_, "model": model,
-              "kernel": ("popcount" if (args.popcount or type_ != "dna") else "tcgen05"),
+              "kernel": ("popcount" if (args.popcount or (
+                  type_ != "dna" and residue_ranks(make_alignment(args.workload)) > 31))
+                  else "tcgen05"),
               "generator": gen, "seed": 0, "parallelism": f"tiles/{world}" if world > 1 else "single",
               "l2": "256 MiB buffer written between timed steps (L2 flushed)"}
 

@@ -1015,8 +1015,8 @@ int rnj_distance_matrix_host_ex(rnj_ctx *ctx, const char *chars, int n, int L, s
     return set_error(RNJ_ERR_INVALID, "invalid alignment shape");
   if (model != RNJ_JC && model != RNJ_KIMURA) return set_error(RNJ_ERR_INVALID, "unknown model");
   if (type == RNJ_UNKNOWN && n > 0) type = rnj_detect_type(chars, L);
-  if (type == RNJ_DNA && band_tiles >= 0) {
-    const int rc = distance_host_streamed(ctx, chars, n, L, ld, model, flags, band_tiles, out,
+  if ((type == RNJ_DNA || type == RNJ_PROTEIN) && band_tiles >= 0) {
+    const int rc = distance_host_streamed(ctx, chars, n, L, ld, type, model, flags, band_tiles, out,
                                           max_out);
     if (rc != RNJ_ERR_UNSUPPORTED) return rc;
   }

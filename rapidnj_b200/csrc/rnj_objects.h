@@ -79,11 +79,11 @@ int ctx_scratch(rnj_ctx *ctx, size_t words);
 rnj::EpiParams ctx_epi(rnj_ctx *ctx, const rnj::Packed &p, int model);
 int ctx_check_error(rnj_ctx *ctx);
 bool ctx_block_pinned(const void *p, size_t bytes);
-// The streamed host-to-host distance call of the tensor-core DNA path
-// (rnj_stream.cu).  Returns RNJ_ERR_UNSUPPORTED, having done nothing, when the
+// The streamed host-to-host distance call of the tensor-core path, DNA and
+// protein (rnj_stream.cu).  Returns RNJ_ERR_UNSUPPORTED, having done nothing, when the
 // input does not take that path.
-int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int model,
-                           int flags, int band_tiles, float *out, float *max_out);
+int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int type,
+                           int model, int flags, int band_tiles, float *out, float *max_out);
 
 // Profiling marks on the context stream (stage 0 pack, 1 count, 2 fix-up;
 // end 0 = begin), read back by rnj_ctx_stage_times.

@@ -1,5 +1,5 @@
 // rnj_stream.cu -- the host-to-host distance call (rnj_distance_matrix_host) of
-// the tensor-core DNA path, streamed.
+// the tensor-core path (DNA and protein), streamed.
 //
 // The n x n float matrix is 16x the bytes of the alignment, so a host-in /
 // host-out call is bound by the device-to-host copy, not by the kernels.  This
@@ -129,15 +129,17 @@ cudaError_t copy_block(float *h, const float *d, size_t ld, int n, int r0, int r
 
 }  // namespace
 
-int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int model,
-                           int flags, int band_tiles, float *out, float *max_out) {
-  // Eligibility: DNA with the fast rules on the tensor-core kernel, a
-  // page-locked output and at least two bands.
-  if (n < 2 || L < 1 || !(flags & RNJ_FASTDIST) || (flags & (RNJ_POPCOUNT | RNJ_FULL_ROWS)) ||
-      L > kMaxTcColumns || (model != RNJ_JC && model != RNJ_KIMURA))
+int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int type,
+                           int model, int flags, int band_tiles, float *out, float *max_out) {
+  // Eligibility: DNA with the fast rules, or protein, on the tensor-core
+  // kernel, a page-locked output and at least two bands.
+  const bool prot = type == RNJ_PROTEIN;
+  if (n < 2 || L < 1 || (type != RNJ_DNA && !prot) || (flags & RNJ_POPCOUNT) ||
+      (!prot && (!(flags & RNJ_FASTDIST) || (flags & RNJ_FULL_ROWS))) || L > kMaxTcColumns ||
+      (model != RNJ_JC && model != RNJ_KIMURA))
     return RNJ_ERR_UNSUPPORTED;
   const int nt = tiles_of(n);
-  const TuneParams tp = tune_lookup(n, L, RNJ_DNA, flags);
+  const TuneParams tp = tune_lookup(n, L, type, flags);
   if (tp.dna_kernel != 0) return RNJ_ERR_UNSUPPORTED;  // this bucket counts on the bit planes
   const int g = band_tiles > 0 ? band_tiles
                                : (tp.stream_band > 0 ? tp.stream_band : default_band_tiles(nt));
@@ -168,9 +170,9 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   Packed p;
   p.n = n;
   p.L = L;
-  p.type = RNJ_DNA;
+  p.type = type;
   p.flags = flags;
-  p.kind = KIND_DNA_TC;
+  p.kind = prot ? KIND_PROT_TC : KIND_DNA_TC;
   p.W = (L + 31) / 32;
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = nt * kTile;
@@ -200,8 +202,33 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   band_off[nbands] = (long long)items.size();
 
   CallBuffers buf(ctx);
-  const size_t fbytes = (size_t)p.Np * 4 * p.Lk / 2;
   RNJ_TRY(cudaMallocAsync((void **)&buf.chars, (size_t)n * L, ctx->stream), "upload buffer");
+  // Protein: the residue ranks come from the whole alignment, so its bytes
+  // (small next to the n x n matrix) are uploaded at once and scanned first.
+  uint8_t lut[256];
+  if (prot) {
+    if (ld == (size_t)L)
+      RNJ_TRY(cudaMemcpyAsync(buf.chars, chars, (size_t)n * L, cudaMemcpyHostToDevice, ctx->stream),
+              "alignment upload");
+    else
+      RNJ_TRY(cudaMemcpy2DAsync(buf.chars, (size_t)L, chars, ld, (size_t)L, (size_t)n,
+                                cudaMemcpyHostToDevice, ctx->stream),
+              "alignment upload");
+    RNJ_TRY(cudaMemsetAsync(ctx->d_mask, 0, 8 * sizeof(uint32_t), ctx->stream), "mask clear");
+    RNJ_TRY(launch_presence(buf.chars, (size_t)L, n, L, ctx->d_mask, ctx->stream), "presence kernel");
+    RNJ_TRY(cudaMemcpyAsync(ctx->h_mask, ctx->d_mask, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            ctx->stream),
+            "mask copy");
+    RNJ_TRY(cudaStreamSynchronize(ctx->stream), "mask sync");
+    int kind = 0;
+    lut_for(RNJ_PROTEIN, flags, ctx->h_mask, lut, &kind);
+    int ranks = 0;
+    for (int c = 0; c < 256; ++c)
+      if (lut[c] != 0xFF) ranks = std::max(ranks, lut[c] + 1);
+    if (ranks < 1 || ranks > kMaxTcRanks) return RNJ_ERR_UNSUPPORTED;
+    p.nfb = 1 + ranks;
+  }
+  const size_t fbytes = (size_t)p.Np * p.nfb * (p.Lk / 2);
   RNJ_TRY(cudaMallocAsync((void **)&buf.feat, fbytes, ctx->stream), "feature allocation");
   RNJ_TRY(cudaMallocAsync((void **)&buf.out, (size_t)n * n * sizeof(float), ctx->stream),
           "matrix allocation");
@@ -239,8 +266,9 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
     const int rn1 = std::min(r1, n);                 // output rows
     cudaEvent_t ev_up = ev.ev[1 + 2 * k], ev_done = ev.ev[2 + 2 * k];
     // One contiguous upload when the host rows are packed: a 2-D upload
-    // running beside the downloads slows them down.
-    if (ld == (size_t)L)
+    // running beside the downloads slows them down.  (Protein: uploaded above.)
+    if (prot) {
+    } else if (ld == (size_t)L)
       RNJ_TRY(cudaMemcpyAsync(buf.chars + (size_t)r0 * L, chars + (size_t)r0 * L,
                               (size_t)(rn1 - r0) * L, cudaMemcpyHostToDevice, ctx->s_up),
               "alignment upload");
@@ -250,8 +278,10 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
               "alignment upload");
     RNJ_TRY(cudaEventRecord(ev_up, ctx->s_up), "event");
     RNJ_TRY(cudaStreamWaitEvent(ctx->stream, ev_up, 0), "kernel wait");
-    RNJ_TRY(launch_pack_features(buf.chars, (size_t)L, n, L, p.Np, p.Lk, p.feat, ctx->stream, r0,
-                                 r1 - r0),
+    RNJ_TRY(prot ? launch_pack_features_prot(buf.chars, (size_t)L, n, L, p.Np, p.Lk, p.nfb, lut,
+                                             p.feat, ctx->stream, r0, r1 - r0)
+                 : launch_pack_features(buf.chars, (size_t)L, n, L, p.Np, p.Lk, p.feat,
+                                        ctx->stream, r0, r1 - r0),
             "feature pack kernel");
     const long long i0 = band_off[k], cnt = band_off[k + 1] - band_off[k];
     RNJ_TRY(launch_tc_batch(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0, (int)cnt,

@@ -216,13 +216,13 @@ int time_plain(rnj_ctx *ctx, TuneBuffers &b, int n, int L, int type, int flags, 
 }
 
 // Median host time (ms) of the host-to-host call with band height `band`.
-int time_host(rnj_ctx *ctx, TuneBuffers &b, int n, int L, int flags, int model,
+int time_host(rnj_ctx *ctx, TuneBuffers &b, int n, int L, int type, int flags, int model,
               const rnj_tune_params &p, int reps, float *ms) {
-  rnj_tune_set(n, L, RNJ_DNA, flags, &p);
+  rnj_tune_set(n, L, type, flags, &p);
   std::vector<float> t;
   for (int r = -1; r < reps; ++r) {
     const auto t0 = std::chrono::steady_clock::now();
-    const int rc = rnj_distance_matrix_host_ex(ctx, b.h_chars, n, L, (size_t)L, RNJ_DNA, model,
+    const int rc = rnj_distance_matrix_host_ex(ctx, b.h_chars, n, L, (size_t)L, type, model,
                                                flags, 0, b.h_out, nullptr);
     if (rc != RNJ_OK) return rc;
     const auto t1 = std::chrono::steady_clock::now();
@@ -321,7 +321,7 @@ extern "C" int rnj_tune(rnj_ctx *ctx, int n, int L, int type, int flags, rnj_tun
   best.ms = 1e30f;
   auto consider = [&](rnj_tune_params c, bool host) -> int {
     float ms = 0.0f;
-    const int rc = host ? time_host(ctx, b, n, L, flags, model, c, reps, &ms)
+    const int rc = host ? time_host(ctx, b, n, L, type, flags, model, c, reps, &ms)
                         : time_plain(ctx, b, n, L, type, flags, model, c, reps, &ms);
     if (rc != RNJ_OK) return rc;
     if (ms < best.ms) {
@@ -363,9 +363,9 @@ extern "C" int rnj_tune(rnj_ctx *ctx, int n, int L, int type, int flags, rnj_tun
       if ((rc = consider(c, false)) != RNJ_OK) break;
     }
   }
-  // 3. The streamed host call's band height (tensor-core DNA; the host buffers
-  //    are page-locked like a caller's would be for this path).
-  if (rc == RNJ_OK && tc_ok && type == RNJ_DNA && best.dna_kernel == 0 && nt >= 8 && n <= 16384) {
+  // 3. The streamed host call's band height (tensor-core DNA and protein; the
+  //    host buffers are page-locked like a caller's would be for this path).
+  if (rc == RNJ_OK && tc_ok && best.dna_kernel == 0 && nt >= 8 && n <= 16384) {
     cudaError_t e = cudaMallocHost((void **)&b.h_chars, (size_t)n * L);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&b.h_out, (size_t)n * n * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpy(b.h_chars, b.d_chars, (size_t)n * L, cudaMemcpyDeviceToHost);
@@ -380,7 +380,7 @@ extern "C" int rnj_tune(rnj_ctx *ctx, int n, int L, int type, int flags, rnj_tun
         rnj_tune_params c = plain_best;
         c.stream_band = band;
         float ms = 0.0f;
-        if ((rc = time_host(ctx, b, n, L, flags, model, c, reps, &ms)) != RNJ_OK) break;
+        if ((rc = time_host(ctx, b, n, L, type, flags, model, c, reps, &ms)) != RNJ_OK) break;
         if (ms < host_ms) {
           host_ms = ms;
           host_best = c;

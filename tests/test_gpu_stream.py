@@ -1,5 +1,5 @@
 """The streamed host-to-host call (rnj_distance_matrix_host[_ex] on the
-tensor-core DNA path with a page-locked output): bands of rows computed last
+tensor-core path, DNA and protein, with a page-locked output): bands of rows computed last
 band first, each band's finished rows and mirror columns copied while the next
 band is uploaded and computed, saturated tiles fixed and copied again at the
 end.  Every result must be bit-identical to the unstreamed call (same kernels,
@@ -22,11 +22,11 @@ def locked(n, fill=7.0):
     return torch.full((n, n), fill, dtype=torch.float32).pin_memory().numpy()
 
 
-def streamed_vs_plain(ctx, seqs, model, band_tiles):
+def streamed_vs_plain(ctx, seqs, model, band_tiles, type_="dna", **kw):
     n = seqs.shape[0]
-    got, mx = ctx.distance_matrix_host(seqs, model, type_="dna", out=locked(n),
-                                       band_tiles=band_tiles)
-    ref, rmx = ctx.distance_matrix_host(seqs, model, type_="dna", band_tiles=-1)
+    got, mx = ctx.distance_matrix_host(seqs, model, type_=type_, out=locked(n),
+                                       band_tiles=band_tiles, **kw)
+    ref, rmx = ctx.distance_matrix_host(seqs, model, type_=type_, band_tiles=-1, **kw)
     assert np.array_equal(got.view(np.int32), ref.view(np.int32)), \
         f"cells differ: {np.argwhere(got.view(np.int32) != ref.view(np.int32))[:5]}"
     assert mx == rmx
@@ -108,3 +108,53 @@ def test_streamed_repeated_calls_reuse_context(ctx):
     b = synth.tree_dna(1100, 900, seed=22)
     for seqs in (a, b, a):
         streamed_vs_plain(ctx, seqs, "kim", 2)
+
+
+# Protein: the whole alignment is uploaded and its residues ranked first, then
+# the same bands run on the one-hot tensor-core features.
+@pytest.mark.parametrize("n,L,band_tiles", [
+    (257, 300, 1),
+    (700, 1000, 2),
+    (1000, 513, 3),
+    (1536, 640, 0),     # L % 128 == 0
+])
+@pytest.mark.parametrize("model", ["kim", "jc"])
+def test_streamed_protein_equals_unstreamed(ctx, n, L, band_tiles, model):
+    seqs = synth.tree_protein(n, L, seed=n + 3 * L, mean_branch=0.15)
+    streamed_vs_plain(ctx, seqs, model, band_tiles, type_="protein")
+
+
+def test_streamed_protein_against_oracle(ctx):
+    seqs = synth.tree_protein(600, 700, seed=6, mean_branch=0.2)
+    got, mx = streamed_vs_plain(ctx, seqs, "kim", 1, type_="protein")
+    c = oracle.counts(seqs, oracle.PROTEIN)
+    ref, rmx = oracle.matrix(c, seqs.shape[1], oracle.PROTEIN, oracle.KIMURA)
+    d = np.abs(got.view(np.int32).astype(np.int64) - ref.view(np.int32).astype(np.int64))
+    assert d.max() <= 1 and (d == 1).sum() <= 2
+    assert mx == np.float32(rmx)
+
+
+@pytest.mark.parametrize("fastdist,compat_wrap", [(False, False), (True, True)])
+def test_streamed_protein_flags(ctx, fastdist, compat_wrap):
+    # The naive estimator's rules and the wrapping valid-site arithmetic of the
+    # fast protein estimator (L % 128 == 0) go through the same bands.
+    seqs = synth.tree_protein(900, 512, seed=17, mean_branch=0.3)
+    streamed_vs_plain(ctx, seqs, "kim", 2, type_="protein", fastdist=fastdist,
+                      compat_wrap=compat_wrap)
+
+
+def test_streamed_protein_saturated(ctx):
+    # Unrelated random proteins: distances past the table's end are fixed to
+    # 2 x max after the bands.
+    seqs = synth.iid_protein(800, 400, gap=0.05, seed=4)
+    got, mx = streamed_vs_plain(ctx, seqs, "kim", 2, type_="protein")
+    assert not (got == -1.0).any()
+
+
+def test_streamed_protein_many_residues_falls_back(ctx):
+    # 32 distinct residue bytes exceed the tensor-core features: the call takes
+    # the bit-plane path unstreamed and gives the same matrix.
+    alphabet = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWYOUacdefghikl", dtype=np.uint8)
+    rng = np.random.default_rng(5)
+    seqs = alphabet[rng.integers(0, alphabet.size, (500, 300))]
+    streamed_vs_plain(ctx, seqs, "kim", 1, type_="protein")
