@@ -398,6 +398,61 @@ int rnj_tune_clear(void);
 int rnj_tune_save(const char *path);
 int rnj_tune_load(const char *path);
 
+/* ---------------------------------------------------------------------------
+ * Neighbour-joining set-up over a finished distance matrix (the O(n^2) passes
+ * rapidNJ makes before its first join: rapidNJ::initialize, rapidNJ.cpp:94-141;
+ * rapidNJMem::initialize, rapidNJMem.cpp:92-135; the zero scan of
+ * rdDataInitialiser::processRow, rdDataInitialiser.cpp:174-189).
+ * ------------------------------------------------------------------------- */
+
+/* One entry of a sorted row: the reference's cluster_pair (cluster_pair.h:4-11),
+ * same layout (id, then distance). */
+typedef struct rnj_cluster_pair {
+  unsigned int id;
+  float distance;
+} rnj_cluster_pair;
+
+/* Outputs of rnj_nj_init; every pointer may be NULL (that output is skipped).
+ * Host arrays hold n entries unless stated. */
+typedef struct rnj_nj_data {
+  /* separationsums: row i summed in float, column 0 first (rapidNJ.cpp:107-110). */
+  float *separation_sums;
+  /* separations: separation_sums[i] / (n - 2) in float (rapidNJ.cpp:111). */
+  float *separations;
+  /* maxRowSeparations: the largest separation of the rows before i, FLT_MIN for
+   * row 0 (rapidNJ.cpp:113-118); max_separation (1 float) the largest of all. */
+  float *max_row_separations;
+  float *max_separation;
+  /* possibleRedundantRows: 1 when the row holds a zero off the diagonal. */
+  short *possible_redundant;
+  /* Redundant rows (rapidNJ.cpp:121-131, handleRedundancy :156-167): row j is
+   * redundant when an equal row (float ==, every column) of higher index exists;
+   * it is mapped to the highest such row, its master.  index_to_id: i, or -1 for
+   * a redundant row; redundant_to_master: the master, or i; redundant_count: the
+   * rows of a master's class (itself included), else 1.  A master's redundantMap
+   * list holds its class's other rows in descending order. */
+  int *index_to_id;
+  int *redundant_to_master;
+  int *redundant_count;
+  /* Sorted rows (buildSortedRow, rapidNJ.cpp:134-154; rapidNJMem.cpp:138-153), on
+   * the DEVICE: row i (stride sorted_ld entries) receives the non-redundant j < i
+   * as (j, matrix[i][j]) by ascending distance, equal distances by ascending j
+   * (std::sort leaves their order unspecified); at most sorted_cap entries when
+   * sorted_cap > 0 (rapidNJMem's sortedMatrixSize), all of them when <= 0.
+   * row_lengths (host) receives the entries written (0 for redundant rows). */
+  rnj_cluster_pair *sorted;
+  size_t sorted_ld;
+  int sorted_cap;
+  int *row_lengths;
+} rnj_nj_data;
+
+/* The NJ set-up of the float n x n matrix d_matrix (device, stride ld floats),
+ * as produced by this library (zero diagonal; RNJ_ERR_INVALID otherwise).  One
+ * pass over the matrix computes the separation sums in the reference's order,
+ * the zero scan and a hash of every row; rows of equal hash are compared in
+ * full; the sorted rows are sorted per row on the device.  Returns when done. */
+int rnj_nj_init(rnj_ctx *ctx, const float *d_matrix, int n, size_t ld, rnj_nj_data *out);
+
 #ifdef __cplusplus
 }
 #endif

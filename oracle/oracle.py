@@ -162,3 +162,118 @@ def ref_matrix(path: str, model: str, fmt: str = "fa", type_: str = "auto",
             n = int(np.fromfile(out, dtype=np.int32, count=1)[0])
             m = np.fromfile(out, dtype=np.float32, offset=4).reshape(n, n)
     return m, info
+
+
+# --- neighbour-joining set-up ---------------------------------------------------
+
+FLT_MIN = np.float32(1.17549435e-38)
+
+
+def nj_init(m: np.ndarray, cap: int = 0) -> dict:
+    """Restatement of the reference's NJ initialisation over an n x n float32
+    distance matrix (rapidNJ::initialize, rapidNJ.cpp:94-141; rapidNJMem::initialize,
+    rapidNJMem.cpp:92-135 when cap > 0 is its sortedMatrixSize), for small n.
+
+    * separation sums: float32 sum of row i in column order (rapidNJ.cpp:107-110),
+      separations = sum / (n - 2) in float32 (:111), maxRowSeparations[i] = the
+      largest separation of rows before i, FLT_MIN first (:102,113-118);
+    * redundant rows: i from n-1 down, skipping rows already marked; for j < i with
+      m[i][j] == 0 and rows i and j equal everywhere (float ==), j is marked
+      (indexToId -1), mapped to i and pushed to the front of i's list
+      (:121-131, handleRedundancy :156-167);
+    * sorted rows: for each unmarked row i the unmarked j < i as (id, m[i][j]),
+      sorted by distance (:134-154), the first `cap` kept for rapidNJMem
+      (rapidNJMem.cpp:138-153).  std::sort leaves the order of equal distances
+      unspecified; this restatement keeps them in id order.
+    * possible_redundant: the row has a zero off the diagonal
+      (rdDataInitialiser::processRow, rdDataInitialiser.cpp:174-189).
+    """
+    m = np.ascontiguousarray(m, dtype=np.float32)
+    n = m.shape[0]
+    sums = np.cumsum(m, axis=1, dtype=np.float32)[:, -1] if n else np.zeros(0, np.float32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        seps = (sums / np.float32(n - 2)).astype(np.float32)
+    maxrow = np.empty(n, np.float32)
+    mx = FLT_MIN
+    for i in range(n):
+        maxrow[i] = mx
+        if seps[i] > mx:
+            mx = seps[i]
+    index_to_id = np.arange(n, dtype=np.int32)
+    master = np.arange(n, dtype=np.int32)
+    count = np.ones(n, dtype=np.int32)
+    lists = [[] for _ in range(n)]
+    for i in range(n - 1, -1, -1):
+        if index_to_id[i] == -1:
+            continue
+        for j in np.nonzero(m[i, :i] == 0)[0]:
+            if np.all(m[i] == m[j]):
+                index_to_id[j] = -1
+                master[j] = i
+                lists[i].insert(0, int(j))
+                count[i] += 1
+    keep = index_to_id != -1
+    lengths = np.zeros(n, dtype=np.int32)
+    rows = []
+    for i in range(n):
+        if not keep[i]:
+            rows.append(None)
+            continue
+        ids = np.nonzero(keep[:i])[0].astype(np.uint32)
+        d = m[i, ids]
+        order = np.argsort(d, kind="stable")
+        k = len(ids) if cap <= 0 else min(len(ids), cap)
+        lengths[i] = k
+        rows.append((ids[order][:k], d[order][:k]))
+    zero = (m == 0)
+    np.fill_diagonal(zero, False)
+    return {"sums": sums, "separations": seps, "max_row_separations": maxrow,
+            "max_separation": np.float32(mx), "index_to_id": index_to_id,
+            "redundant_to_master": master, "redundant_count": count, "lists": lists,
+            "row_lengths": lengths, "rows": rows,
+            "possible_redundant": zero.any(axis=1).astype(np.int16)}
+
+
+def ref_nj_init(m: np.ndarray, cap: int = 0, reps: int = 1, want: bool = True):
+    """The reference's own initialize() through _ref/nj_harness; returns the same
+    dictionary as nj_init (without possible_redundant) and the timing line."""
+    m = np.ascontiguousarray(m, dtype=np.float32)
+    n = m.shape[0]
+    with tempfile.TemporaryDirectory() as td:
+        src = os.path.join(td, "m.bin")
+        out = os.path.join(td, "o.bin") if want else "-"
+        with open(src, "wb") as f:
+            np.array([n, cap], dtype=np.int32).tofile(f)
+            m.tofile(f)
+        p = subprocess.run([os.path.join(REF_DIR, "nj_harness"), src, out, str(reps)],
+                           check=True, capture_output=True, text=True)
+        info = json.loads(p.stdout.strip().splitlines()[-1])
+        if not want:
+            return None, info
+        raw = open(out, "rb").read()
+    pos = 4
+    def take(dt, k):
+        nonlocal pos
+        a = np.frombuffer(raw, dtype=dt, count=k, offset=pos).copy()
+        pos += a.nbytes
+        return a
+    res = {"sums": take(np.float32, n), "separations": take(np.float32, n),
+           "max_row_separations": take(np.float32, n),
+           "max_separation": take(np.float32, 1)[0], "index_to_id": take(np.int32, n),
+           "redundant_to_master": take(np.int32, n), "redundant_count": take(np.int32, n),
+           "row_lengths": take(np.int32, n)}
+    lists = []
+    for _ in range(n):
+        k = int(take(np.int32, 1)[0])
+        lists.append([int(x) for x in take(np.int32, k)])
+    res["lists"] = lists
+    rows = []
+    for i in range(n):
+        k = int(res["row_lengths"][i])
+        if res["index_to_id"][i] == -1:
+            rows.append(None)
+            continue
+        pairs = take(np.uint32, 2 * k).reshape(k, 2)
+        rows.append((pairs[:, 0].copy(), pairs[:, 1].view(np.float32).copy()))
+    res["rows"] = rows
+    return res, info

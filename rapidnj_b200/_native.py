@@ -117,7 +117,18 @@ SIGNATURES = {
     "rnj_msa_chars": (c_void_p, [c_void_p]),
     "rnj_msa_destroy": (c_int, [c_void_p]),
     "rnj_write_matrix_text": (c_int, [c_char_p, P(c_char_p), P(c_void_p), c_int, c_int]),
+    "rnj_nj_init": (c_int, [c_void_p, c_void_p, c_int, c_size_t, c_void_p]),
 }
+
+
+class NjData(ctypes.Structure):
+    """rnj_nj_data (include/rnj.h): output pointers of rnj_nj_init."""
+    _fields_ = [("separation_sums", c_void_p), ("separations", c_void_p),
+                ("max_row_separations", c_void_p), ("max_separation", c_void_p),
+                ("possible_redundant", c_void_p), ("index_to_id", c_void_p),
+                ("redundant_to_master", c_void_p), ("redundant_count", c_void_p),
+                ("sorted", c_void_p), ("sorted_ld", c_size_t), ("sorted_cap", c_int),
+                ("row_lengths", c_void_p)]
 
 
 def lib():

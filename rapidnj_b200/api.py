@@ -248,6 +248,44 @@ class Context:
                                     mx.ctypes.data))
         return outs, mx[:R]
 
+    def nj_init(self, d_matrix, cap: int = 0, sorted_rows: bool = True, sorted_out=None):
+        """rnj_nj_init: rapidNJ's set-up over the device distance matrix d_matrix (a
+        CUDA float32 tensor, n x n, row stride >= n).  Returns a dict of host arrays
+        (separation_sums, separations, max_row_separations, max_separation,
+        possible_redundant, index_to_id, redundant_to_master, redundant_count,
+        row_lengths) and, when sorted_rows, ``sorted``: a device int32 tensor
+        (n, ld, 2) of (id, distance bits) pairs (``sorted_distances`` views the
+        distances as float32).  cap > 0 keeps rapidNJMem's first cap entries."""
+        import torch
+        n = d_matrix.shape[0]
+        assert d_matrix.dtype == torch.float32 and d_matrix.shape == (n, n)
+        assert d_matrix.stride(1) == 1
+        res = {"separation_sums": np.zeros(n, np.float32), "separations": np.zeros(n, np.float32),
+               "max_row_separations": np.zeros(n, np.float32),
+               "max_separation": np.zeros(1, np.float32),
+               "possible_redundant": np.zeros(n, np.int16),
+               "index_to_id": np.zeros(n, np.int32), "redundant_to_master": np.zeros(n, np.int32),
+               "redundant_count": np.zeros(n, np.int32), "row_lengths": np.zeros(n, np.int32)}
+        d = N.NjData()
+        for k, a in res.items():
+            setattr(d, k, a.ctypes.data)
+        d.sorted_cap = int(cap)
+        if sorted_rows:
+            width = max(1, min(cap, n - 1) if cap > 0 else n - 1)
+            if sorted_out is None:
+                sorted_out = torch.zeros((n, width, 2), dtype=torch.int32, device=d_matrix.device)
+            assert sorted_out.dtype == torch.int32 and sorted_out.shape[0] == n
+            assert sorted_out.shape[2] == 2 and sorted_out.is_contiguous()
+            d.sorted = sorted_out.data_ptr()
+            d.sorted_ld = sorted_out.shape[1]
+        check(N.lib().rnj_nj_init(self.handle, ctypes.c_void_p(d_matrix.data_ptr()), n,
+                                  d_matrix.stride(0), ctypes.byref(d)))
+        res["max_separation"] = res["max_separation"][0]
+        if sorted_rows:
+            res["sorted"] = sorted_out
+            res["sorted_distances"] = sorted_out[..., 1].view(torch.float32)
+        return res
+
     def tune(self, n: int, L: int, type_="dna", fastdist: bool = True,
              popcount: bool = False) -> "TuneParams":
         """rnj_tune: time the candidate launch choices of the bucket of (n, L) on a
