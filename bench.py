@@ -541,6 +541,53 @@ def run_bootstrap(args, local_rank: int = 0, n: int = 2000, L: int = 2000, R: in
             "workload": f"{R} replicates of DNA K2P {n} x {L} (tree-evolved), seeded columns"}
 
 
+def run_nj_init(args, local_rank: int = 0, n: int = 10000, L: int = 10000):
+    """rapidNJ's NJ set-up (rapidNJ::initialize: separation sums, redundant rows,
+    sorted rows) by rnj_nj_init over the device matrix of the DNA K2P n x L
+    workload, against the reference's own initialize() (oracle/_ref/nj_harness,
+    one host thread, as in the reference) on the same matrix when built."""
+    import torch
+    from rapidnj_b200 import api, synth
+    ctx = api.Context(local_rank)
+    dev = f"cuda:{local_rank}"
+    seqs = synth.tree_dna(n, L, seed=0)
+    aln = ctx.alignment(torch.from_numpy(seqs).to(dev), 0)
+    m = torch.empty((n, n), dtype=torch.float32, device=dev)
+    ctx.distance_into(aln, "kim", m)
+    aln.close()
+    ctx.synchronize()
+    sorted_out = torch.empty((n, n - 1, 2), dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    ts = []
+    for r in range(6):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = ctx.nj_init(m, sorted_out=sorted_out)
+        t1 = time.perf_counter()
+        if r >= 1:
+            ts.append(t1 - t0)
+    out = {"ms": 1e3 * statistics.median(ts), "n": n,
+           "redundant_rows": int((res["index_to_id"] == -1).sum()),
+           "sorted_entries": int(res["row_lengths"].sum()),
+           "workload": f"rapidNJ initialize() over the DNA K2P {n} x {n} matrix of the {n} x {L} "
+                       "tree-evolved alignment (device-resident), sorted rows kept on the device"}
+    if not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+            from oracle import oracle
+            if os.path.exists(os.path.join(oracle.REF_DIR, "nj_harness")):
+                _, info = oracle.ref_nj_init(m.cpu().numpy(), 0, reps=1, want=False)
+                out["cpu_reference_ms"] = 1e3 * info["init_s"][0]
+                out["cpu_reference"] = ("rapidNJ::initialize from the reference sources "
+                                        "(oracle/_ref/nj_harness), 1 thread, same matrix")
+                out["speedup_vs_cpu_reference"] = out["cpu_reference_ms"] / out["ms"]
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_reference_error"] = str(e)[:200]
+    ctx.close()
+    return out
+
+
 def fp4_tensor_peak(device: int):
     """Dense FP4 tensor throughput (flop/s) of a library GEMM on this device, and
     how it was obtained: an MXFP4 GEMM (torch._scaled_mm, unit block scales,
@@ -602,9 +649,11 @@ def main():
     ap.add_argument("--popcount", action="store_true",
                     help="count DNA with the bit-plane popcount kernel instead of tensor cores")
     ap.add_argument("--mode", default="all",
-                    choices=["all", "plain", "batched", "served", "bootstrap"],
-                    help="all: the plain workload line plus the batched, served and bootstrap "
-                         "figures")
+                    choices=["all", "plain", "batched", "served", "bootstrap", "njinit"],
+                    help="all: the plain workload line plus the batched, served, bootstrap and "
+                         "NJ set-up figures")
+    ap.add_argument("--nj-n", type=int, default=10000,
+                    help="sequences (and columns) of the NJ set-up workload (njinit)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -668,6 +717,8 @@ def main():
             line["served"] = run_served(args, local_rank)
         if args.mode in ("all", "bootstrap") and world == 1:
             line["bootstrap"] = run_bootstrap(args, local_rank)
+        if args.mode in ("all", "njinit") and world == 1:
+            line["nj_init"] = run_nj_init(args, local_rank, n=args.nj_n, L=args.nj_n)
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

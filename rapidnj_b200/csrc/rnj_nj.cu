@@ -15,22 +15,24 @@
 //
 // On the device:
 //   * one pass reads the matrix once: a warp owns 32 rows and streams them in
-//     32 x 32 tiles (cp.async into shared memory, four tiles in flight), then
+//     32 x 32 tiles (cp.async into shared memory, eight tiles in its ring), then
 //     every lane walks its own row of the tile in column order, so each row is
-//     summed exactly in the reference's order; the same walk hashes the row
-//     (zero of either sign hashed as +0), and flags a zero off the diagonal
-//     (rdDataInitialiser.cpp:174-189), a NaN and a non-zero diagonal;
+//     summed exactly in the reference's order; the same walk counts the row's
+//     zeros (a second zero besides the diagonal is the zero scan of
+//     rdDataInitialiser.cpp:174-189), and the diagonal entry is checked;
 //   * with a zero diagonal, row equality is an equivalence whose classes are
 //     exactly the reference's redundancy classes (the highest row of a class is
 //     its master; a row equal to another has a zero at that row's column), so
-//     only rows with a zero and no NaN and with an equal hash are candidates:
-//     each candidate is compared in full with the highest row of its hash group
-//     (a warp per pair), and rows that differ (hash collisions) form new groups;
-//   * each unmarked row is sorted by a CTA: 64-bit keys (the distance's bits
-//     made order-preserving, then j), unique, so a bitonic network gives the
-//     reference's order with equal distances in ascending j; rows of up to 8192
-//     entries are sorted in shared memory, longer ones in a global scratch row
-//     with the short strides done in shared memory.
+//     only rows with a zero off the diagonal are candidates: they are hashed
+//     (a warp per row; zero of either sign as +0), each candidate is compared
+//     in full with the highest row of its hash group (a warp per pair), and rows
+//     that differ (hash collisions, NaN entries) form new groups;
+//   * each unmarked row is sorted by a CTA: 64-bit items (the distance's bits
+//     made order-preserving, then j) in ascending j, and a stable LSD radix
+//     sort on the distance's four bytes (ranking inside each warp by ballots;
+//     a pass whose digit is the same for the whole row is skipped) gives the
+//     reference's order with equal distances in ascending j; rows of up to
+//     8192 items in shared memory, longer ones in the CTA's global scratch rows.
 // The O(n) parts (separations, running maximum, the redundancy classes) run on
 // the host from the per-row results.
 #include <cuda_runtime.h>
@@ -49,13 +51,12 @@ using namespace rnj;
 
 namespace {
 
-constexpr int kRowWarps = 2;     // warps per CTA of the row pass
-constexpr int kRowStages = 4;    // 32 x 32 tiles in flight per warp
+constexpr int kRowStages = 8;    // 32 x 32 tiles in the ring of a row-pass warp
 constexpr int kTileLd = 33;      // padded tile row: lane l reads bank (l + k) % 32
 constexpr int kSortBlock = 8192; // entries of a row sorted in shared memory
 constexpr int kSortThreads = 1024;
 
-enum : uint32_t { kRowZero = 1u, kRowNan = 2u, kRowBadDiag = 4u };
+enum : uint32_t { kRowZero = 1u, kRowBadDiag = 4u };
 
 __device__ __forceinline__ void cp_async4(float *smem, const float *gmem, bool valid) {
   const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
@@ -71,21 +72,22 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// Pass 1: per row the float sum in column order, two 32-bit hashes and flags.
-// Warp w of CTA b owns rows [32 (b kRowWarps + w), +32); lane l sums row
-// row0 + l.  Tile t holds columns [32 t, 32 t + 32) of the 32 rows; stage
-// t % kRowStages of the warp's ring.
-__global__ void __launch_bounds__(32 * kRowWarps)
+// Pass 1: per row the float sum in column order, whether it holds a zero off
+// the diagonal, and whether its diagonal entry is non-zero.  A CTA (one warp)
+// owns rows [32 b, 32 b + 32); lane l sums row 32 b + l.  Tile t holds columns
+// [32 t, 32 t + 32) of the 32 rows, in stage t % kRowStages of the ring.  Per
+// entry the lane does no more than the sum needs (a load, the add, a zero
+// test), so that the pass runs at the rate the matrix streams in.
+__global__ void __launch_bounds__(32)
     nj_row_pass_kernel(const float *__restrict__ M, int n, size_t ld, float *__restrict__ sums,
-                       uint2 *__restrict__ hashes, uint32_t *__restrict__ flags) {
-  __shared__ float tiles[kRowWarps][kRowStages][32 * kTileLd];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row0 = (blockIdx.x * kRowWarps + warp) * 32;
-  if (row0 >= n) return;  // the whole warp; the kernel has no CTA-wide barrier
+                       uint32_t *__restrict__ flags) {
+  extern __shared__ float tiles[];  // [kRowStages][32 * kTileLd]
+  const int lane = threadIdx.x;
+  const int row0 = blockIdx.x * 32;
   const int ntile = (n + 31) / 32;
   auto issue = [&](int t) {
     if (t < ntile) {
-      float *dst = tiles[warp][t % kRowStages];
+      float *dst = tiles + (t % kRowStages) * (32 * kTileLd);
       const int c = t * 32 + lane;
 #pragma unroll 8
       for (int r = 0; r < 32; ++r) {
@@ -100,37 +102,61 @@ __global__ void __launch_bounds__(32 * kRowWarps)
   for (int t = 0; t < kRowStages - 1; ++t) issue(t);
   const int my_row = row0 + lane;
   float sum = 0.0f;
-  uint32_t h1 = 2166136261u, h2 = 0x9E3779B9u, fl = 0;
+  int zeros = 0;
   for (int t = 0; t < ntile; ++t) {
     issue(t + kRowStages - 1);
     cp_async_wait<kRowStages - 1>();  // this lane's copies of tile t are done
     __syncwarp();                     // and every lane's are visible
-    const float *row = tiles[warp][t % kRowStages] + lane * kTileLd;
-    const int c0 = t * 32;
-    const int kmax = min(32, n - c0);
-    if (my_row < n) {
-      for (int k = 0; k < kmax; ++k) {
+    const float *row = tiles + (t % kRowStages) * (32 * kTileLd) + lane * kTileLd;
+    if (t * 32 + 32 <= n) {
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
         const float v = row[k];
         sum += v;
-        const uint32_t u = v == 0.0f ? 0u : __float_as_uint(v);
-        h1 = (h1 ^ u) * 16777619u;
-        h2 = h2 * 0x9E3779B1u + (u ^ (u >> 15));
-        if (c0 + k == my_row) {
-          if (!(v == 0.0f)) fl |= kRowBadDiag;
-        } else if (v == 0.0f) {
-          fl |= kRowZero;
-        }
-        if (v != v) fl |= kRowNan;
+        zeros += v == 0.0f;
+      }
+    } else {
+      for (int k = 0; k < n - t * 32; ++k) {
+        const float v = row[k];
+        sum += v;
+        zeros += v == 0.0f;
       }
     }
     __syncwarp();  // the stage is refilled by the next iteration's issue
   }
   cp_async_wait<0>();
   if (my_row < n) {
+    const float diag = M[(size_t)my_row * ld + my_row];
     sums[my_row] = sum;
-    hashes[my_row] = make_uint2(h1, h2);
-    flags[my_row] = fl;
+    // with a zero diagonal, a second zero is one off the diagonal
+    flags[my_row] = (diag == 0.0f ? 0u : kRowBadDiag) | (zeros >= 2 ? kRowZero : 0u);
   }
+}
+
+// Pass 1b: a hash of each candidate row (warp p: row cand[p]): two 32-bit sums
+// over the columns c of a mix of (entry bits, c), zero of either sign as +0, so
+// that rows equal under float == hash equally.
+__global__ void __launch_bounds__(256)
+    nj_row_hash_kernel(const float *__restrict__ M, int n, size_t ld, const int *__restrict__ cand,
+                       int ncand, uint2 *__restrict__ hashes) {
+  const int p = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= ncand) return;  // uniform per warp
+  const float *row = M + (size_t)cand[p] * ld;
+  uint32_t ha = 0, hb = 0;
+  for (int c = lane; c < n; c += 32) {
+    const float v = row[c];
+    const uint32_t u = v == 0.0f ? 0u : __float_as_uint(v);
+    const uint32_t z = u ^ ((uint32_t)c * 0x9E3779B9u);
+    ha += (z ^ (z >> 15)) * 0x85EBCA6Bu;
+    hb += (z ^ (z >> 13)) * 0xC2B2AE35u + z;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ha += __shfl_xor_sync(0xffffffffu, ha, o);
+    hb += __shfl_xor_sync(0xffffffffu, hb, o);
+  }
+  if (lane == 0) hashes[p] = make_uint2(ha, hb);
 }
 
 // Pass 2: warp p compares row a = pairs[p].x (the reference's row i) with row
@@ -163,81 +189,188 @@ __device__ __forceinline__ unsigned long long sort_key(float v, int j) {
   return ((unsigned long long)f << 32) | (uint32_t)j;
 }
 
-// Compare-exchange stages of the bitonic network over a[0, len) (shared memory,
-// or a global row only this CTA touches) for merge size k, strides j0, j0/2,
-// .., jend.  Element t of a is element base + t of the whole row: the direction
-// of its pair is ascending when bit k of that index is clear.
-__device__ __forceinline__ void bitonic_stages(unsigned long long *a, int len, long long base,
-                                               long long k, int j0, int jend) {
-  for (int j = j0; j >= jend; j >>= 1) {
-    for (int q = threadIdx.x; q < (len >> 1); q += blockDim.x) {
-      const int t = ((q & ~(j - 1)) << 1) | (q & (j - 1));  // bit j clear; partner t + j
-      const bool asc = ((base + t) & k) == 0;
-      const unsigned long long x = a[t], y = a[t + j];
-      if ((x > y) == asc) {
-        a[t] = y;
-        a[t + j] = x;
-      }
-    }
-    __syncthreads();
+// Pass 3: a CTA per unmarked row i (rows[], longest first).  The unmarked j < i
+// (rank[j] = unmarked rows below j, rank[i] of them in all) become 64-bit items
+// (order-preserving distance key << 32 | j) in ascending j, and a stable LSD
+// radix sort on the key's four bytes orders them by distance with equal
+// distances in ascending j; the first min(rank[i], cap) are written as
+// (j, matrix[i][j]).  Each pass, chunk by chunk (8192 items: warp w, slot s,
+// lane l holds item w 256 + s 32 + l): a stable rank inside each warp by
+// ballots, the per-(digit, warp) offsets from the digit bases, and the scatter.
+// The digit bases come from the chunk's own counts when the row is one chunk,
+// else from a histogram of the row first; a pass in which one digit holds every
+// item is skipped.  Rows of up to 8192 items live in shared memory, longer ones
+// in the CTA's scratch rows.
+constexpr int kRadixDigits = 256;
+constexpr int kWarpsPerSort = kSortThreads / 32;
+constexpr int kItems = kSortBlock / kSortThreads;  // per thread and chunk
+
+using u64 = unsigned long long;
+
+// The lanes of the warp holding the same 8-bit digit d as this lane (valid:
+// this lane holds an item), from eight ballots: the hardware match instruction
+// is far slower than ballots on this part.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool valid) {
+  uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const uint32_t m = __ballot_sync(0xffffffffu, bit);
+    peers &= bit ? m : ~m;
   }
+  return peers;
 }
 
-// Pass 3: a CTA per unmarked row i (rows[], longest first): the unmarked j < i
-// (rank[j] = unmarked rows below j, rank[i] of them in all) as keys, sorted, and
-// the first min(rank[i], cap) written as (j, matrix[i][j]).  Rows longer than
-// kSortBlock entries are sorted in this CTA's scratch row (P entries, P the
-// next power of two): blocks of kSortBlock in shared memory first, then each
-// merge's long strides in global memory and its short ones block by block.
-__global__ void __launch_bounds__(kSortThreads)
+struct SortShared {
+  u64 a[kSortBlock];
+  u64 b[kSortBlock];
+  uint32_t wcnt[kWarpsPerSort * kRadixDigits];  // [warp][digit]
+  uint32_t dtot[kRadixDigits];
+  uint32_t dbase[kRadixDigits];
+  int skip;
+};
+
+// Warp 0: the exclusive scan of the digit totals into the digit bases (eight
+// digits a lane) and the skip flag (one digit holds every item).
+__device__ __forceinline__ void scan_digits(SortShared &S, int cnt, int warp, int lane) {
+  if (warp != 0) return;
+  uint32_t v[8], s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    v[k] = S.dtot[lane * 8 + k];
+    s += v[k];
+  }
+  uint32_t incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  uint32_t run = incl - s;
+  bool one = false;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    S.dbase[lane * 8 + k] = run;
+    run += v[k];
+    one |= v[k] == (uint32_t)cnt;
+  }
+  one = __any_sync(0xffffffffu, one);
+  if (lane == 0) S.skip = one;
+}
+
+__global__ void __launch_bounds__(kSortThreads, 1)
     nj_sort_rows_kernel(const float *__restrict__ M, size_t ld, const int *__restrict__ rank,
                         const uint8_t *__restrict__ keep, const int *__restrict__ rows, int nrows,
-                        unsigned long long *__restrict__ scratch, size_t scratch_per_cta,
+                        u64 *__restrict__ scratch, size_t scratch_per_cta,
                         rnj_cluster_pair *__restrict__ out, size_t out_ld, int cap) {
-  extern __shared__ unsigned long long sk[];
+  extern __shared__ __align__(16) unsigned char nj_sort_smem[];
+  SortShared &S = *reinterpret_cast<SortShared *>(nj_sort_smem);
+  const int th = threadIdx.x, lane = th & 31, warp = th >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
   for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = rows[r];
     const int cnt = rank[i];
     if (cnt == 0) continue;  // uniform over the CTA
-    int P = 1;
-    while (P < cnt) P <<= 1;
     const float *row = M + (size_t)i * ld;
-    unsigned long long *a = P <= kSortBlock ? sk : scratch + (size_t)blockIdx.x * scratch_per_cta;
-    for (int t = cnt + threadIdx.x; t < P; t += blockDim.x) a[t] = ~0ull;
-    for (int j = threadIdx.x; j < i; j += blockDim.x)
-      if (keep[j]) a[rank[j]] = sort_key(row[j], j);
-    __syncthreads();
-    if (P <= kSortBlock) {
-      for (int k = 2; k <= P; k <<= 1) bitonic_stages(sk, P, 0, k, k >> 1, 1);
+    u64 *A, *B;
+    if (cnt <= kSortBlock) {
+      A = S.a;
+      B = S.b;
     } else {
-      for (int b0 = 0; b0 < P; b0 += kSortBlock) {
-        for (int t = threadIdx.x; t < kSortBlock; t += blockDim.x) sk[t] = a[b0 + t];
+      A = scratch + (size_t)blockIdx.x * 2 * scratch_per_cta;
+      B = A + scratch_per_cta;
+    }
+    for (int j = th; j < i; j += blockDim.x)
+      if (keep[j]) A[rank[j]] = sort_key(row[j], j);
+    __syncthreads();
+    for (int pass = 0; pass < 4; ++pass) {
+      const int shift = 32 + 8 * pass;
+      const bool chunked = cnt > kSortBlock;
+      if (chunked) {
+        // Histogram of the row's digits (warp-aggregated shared atomics); a row
+        // of one chunk takes its totals from the ranking instead.
+        for (int d = th; d < kRadixDigits; d += blockDim.x) S.dtot[d] = 0;
         __syncthreads();
-        for (int k = 2; k <= kSortBlock; k <<= 1) bitonic_stages(sk, kSortBlock, b0, k, k >> 1, 1);
-        for (int t = threadIdx.x; t < kSortBlock; t += blockDim.x) a[b0 + t] = sk[t];
-        __syncthreads();
-      }
-      for (long long k = 2LL * kSortBlock; k <= P; k <<= 1) {
-        for (int j = (int)(k >> 1); j >= kSortBlock; j >>= 1) bitonic_stages(a, P, 0, k, j, j);
-        for (int b0 = 0; b0 < P; b0 += kSortBlock) {
-          for (int t = threadIdx.x; t < kSortBlock; t += blockDim.x) sk[t] = a[b0 + t];
-          __syncthreads();
-          bitonic_stages(sk, kSortBlock, b0, k, kSortBlock >> 1, 1);
-          for (int t = threadIdx.x; t < kSortBlock; t += blockDim.x) a[b0 + t] = sk[t];
-          __syncthreads();
+        for (int t0 = 0; t0 < cnt; t0 += blockDim.x) {
+          const int t = t0 + th;
+          const bool ok = t < cnt;
+          const uint32_t d = ok ? (uint32_t)((A[t] >> shift) & 255u) : 0u;
+          const uint32_t peers = digit_peers(d, ok);
+          if (ok && (peers & lt) == 0) atomicAdd(&S.dtot[d], (uint32_t)__popc(peers));
         }
+        __syncthreads();
+        scan_digits(S, cnt, warp, lane);
+        __syncthreads();
+        if (S.skip) continue;  // uniform: every item has the same digit
       }
+      for (int c0 = 0; c0 < cnt; c0 += kSortBlock) {
+        for (int k = th; k < kWarpsPerSort * kRadixDigits; k += blockDim.x) S.wcnt[k] = 0;
+        __syncthreads();
+        u64 x[kItems];
+        uint32_t rk[kItems];
+#pragma unroll
+        for (int s = 0; s < kItems; ++s) {
+          const int t = c0 + warp * (32 * kItems) + s * 32 + lane;
+          const bool ok = t < cnt;
+          x[s] = ok ? A[t] : 0ull;
+          const uint32_t d = ok ? (uint32_t)((x[s] >> shift) & 255u) : 0u;
+          const uint32_t peers = digit_peers(d, ok);
+          const uint32_t before = ok ? S.wcnt[warp * kRadixDigits + d] : 0u;
+          __syncwarp();
+          if (ok && (peers & lt) == 0) S.wcnt[warp * kRadixDigits + d] = before + __popc(peers);
+          __syncwarp();
+          rk[s] = before + __popc(peers & lt);
+        }
+        __syncthreads();
+        if (!chunked) {
+          // One chunk: digit totals from the warps' counts, then the bases.
+          for (int d = th; d < kRadixDigits; d += blockDim.x) {
+            uint32_t t = 0;
+            for (int w = 0; w < kWarpsPerSort; ++w) t += S.wcnt[w * kRadixDigits + d];
+            S.dtot[d] = t;
+          }
+          __syncthreads();
+          scan_digits(S, cnt, warp, lane);
+          __syncthreads();
+          if (S.skip) break;  // uniform; the pass leaves the items in place
+        }
+        // Offsets: digit base, then the warps in order; the base moves on by the
+        // chunk's items of that digit.
+        for (int d = th; d < kRadixDigits; d += blockDim.x) {
+          uint32_t run = S.dbase[d];
+          for (int w = 0; w < kWarpsPerSort; ++w) {
+            const uint32_t v = S.wcnt[w * kRadixDigits + d];
+            S.wcnt[w * kRadixDigits + d] = run;
+            run += v;
+          }
+          S.dbase[d] = run;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < kItems; ++s) {
+          const int t = c0 + warp * (32 * kItems) + s * 32 + lane;
+          if (t < cnt) {
+            const uint32_t d = (uint32_t)((x[s] >> shift) & 255u);
+            B[S.wcnt[warp * kRadixDigits + d] + rk[s]] = x[s];
+          }
+        }
+        __syncthreads();
+      }
+      if (!chunked && S.skip) continue;
+      u64 *tmp = A;
+      A = B;
+      B = tmp;
     }
     const int keepn = cap > 0 ? min(cnt, cap) : cnt;
     rnj_cluster_pair *o = out + (size_t)i * out_ld;
-    for (int t = threadIdx.x; t < keepn; t += blockDim.x) {
-      const uint32_t id = (uint32_t)a[t];
+    for (int t = th; t < keepn; t += blockDim.x) {
+      const uint32_t id = (uint32_t)A[t];
       rnj_cluster_pair cp;
       cp.id = id;
       cp.distance = row[id];  // the stored value, -0 kept
       o[t] = cp;
     }
-    __syncthreads();  // the next row reuses the keys
+    __syncthreads();  // the next row reuses the buffers
   }
 }
 
@@ -280,21 +413,18 @@ extern "C" int rnj_nj_init(rnj_ctx *ctx, const float *d_matrix, int n, size_t ld
 
   // Pass 1.
   float *d_sums = nullptr;
-  uint2 *d_hash = nullptr;
   uint32_t *d_flags = nullptr;
   NJ_CUDA(buf.alloc(&d_sums, (size_t)n * sizeof(float)), "nj buffers");
-  NJ_CUDA(buf.alloc(&d_hash, (size_t)n * sizeof(uint2)), "nj buffers");
   NJ_CUDA(buf.alloc(&d_flags, (size_t)n * sizeof(uint32_t)), "nj buffers");
-  const int warps = (n + 31) / 32;
-  nj_row_pass_kernel<<<(warps + kRowWarps - 1) / kRowWarps, 32 * kRowWarps, 0, st>>>(
-      d_matrix, n, ld, d_sums, d_hash, d_flags);
+  const int row_smem = kRowStages * 32 * kTileLd * (int)sizeof(float);
+  NJ_CUDA(cudaFuncSetAttribute(nj_row_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               row_smem),
+          "nj row pass attribute");
+  nj_row_pass_kernel<<<(n + 31) / 32, 32, row_smem, st>>>(d_matrix, n, ld, d_sums, d_flags);
   NJ_CUDA(cudaGetLastError(), "nj row pass");
   std::vector<float> sums(n);
-  std::vector<uint2> hash(n);
   std::vector<uint32_t> flags(n);
   NJ_CUDA(cudaMemcpyAsync(sums.data(), d_sums, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st),
-          "nj copy");
-  NJ_CUDA(cudaMemcpyAsync(hash.data(), d_hash, (size_t)n * sizeof(uint2), cudaMemcpyDeviceToHost, st),
           "nj copy");
   NJ_CUDA(cudaMemcpyAsync(flags.data(), d_flags, (size_t)n * sizeof(uint32_t),
                           cudaMemcpyDeviceToHost, st),
@@ -327,9 +457,30 @@ extern "C" int rnj_nj_init(rnj_ctx *ctx, const float *d_matrix, int n, size_t ld
   std::vector<int> master(n);
   for (int i = 0; i < n; ++i) master[i] = i;
   {
+    // Candidates: rows with a zero off the diagonal (a row equal to another
+    // has one, in that row's column).  Their hashes (pass 1b).
     std::vector<int> cand;
     for (int i = 0; i < n; ++i)
-      if ((flags[i] & kRowZero) && !(flags[i] & kRowNan)) cand.push_back(i);
+      if (flags[i] & kRowZero) cand.push_back(i);
+    std::vector<uint2> hash(n, make_uint2(0u, 0u));
+    if (cand.size() >= 2) {
+      int *d_cand = nullptr;
+      uint2 *d_hash = nullptr;
+      NJ_CUDA(buf.alloc(&d_cand, cand.size() * sizeof(int)), "nj buffers");
+      NJ_CUDA(buf.alloc(&d_hash, cand.size() * sizeof(uint2)), "nj buffers");
+      NJ_CUDA(cudaMemcpyAsync(d_cand, cand.data(), cand.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              st),
+              "nj copy");
+      const size_t threads = cand.size() * 32;
+      nj_row_hash_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+          d_matrix, n, ld, d_cand, (int)cand.size(), d_hash);
+      NJ_CUDA(cudaGetLastError(), "nj row hash");
+      std::vector<uint2> h(cand.size());
+      NJ_CUDA(cudaMemcpyAsync(h.data(), d_hash, h.size() * sizeof(uint2), cudaMemcpyDeviceToHost, st),
+              "nj copy");
+      NJ_CUDA(cudaStreamSynchronize(st), "nj row hash sync");
+      for (size_t k = 0; k < cand.size(); ++k) hash[cand[k]] = h[k];
+    }
     auto same = [&](int a, int b) { return hash[a].x == hash[b].x && hash[a].y == hash[b].y; };
     std::sort(cand.begin(), cand.end(), [&](int a, int b) {
       if (hash[a].x != hash[b].x) return hash[a].x < hash[b].x;
@@ -419,20 +570,25 @@ extern "C" int rnj_nj_init(rnj_ctx *ctx, const float *d_matrix, int n, size_t ld
     NJ_CUDA(cudaMemcpyAsync(d_rows, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice,
                             st),
             "nj copy");
-    const int grid = (int)std::min<size_t>(rows.size(), (size_t)2 * ctx->num_sms);
-    size_t pmax = 1;
-    while (pmax < (size_t)rank[rows[0]]) pmax <<= 1;
-    unsigned long long *d_scratch = nullptr;
-    size_t per_cta = 0;
-    if (pmax > (size_t)kSortBlock) {
-      per_cta = pmax;
-      NJ_CUDA(buf.alloc(&d_scratch, (size_t)grid * per_cta * sizeof(unsigned long long)),
-              "nj sort scratch");
-    }
-    const int smem = kSortBlock * (int)sizeof(unsigned long long);
+    const int smem = (int)sizeof(SortShared);
     NJ_CUDA(cudaFuncSetAttribute(nj_sort_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  smem),
             "nj sort attribute");
+    int per_sm = 1;
+    NJ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nj_sort_rows_kernel, kSortThreads,
+                                                          smem),
+            "nj sort occupancy");
+    const int grid =
+        (int)std::min<size_t>(rows.size(), (size_t)std::max(1, per_sm) * ctx->num_sms);
+    // Rows of more than kSortBlock items: two scratch rows per CTA.
+    const size_t longest = (size_t)rank[rows[0]];
+    u64 *d_scratch = nullptr;
+    size_t per_cta = 0;
+    if (longest > (size_t)kSortBlock) {
+      per_cta = longest;
+      NJ_CUDA(buf.alloc(&d_scratch, (size_t)grid * 2 * per_cta * sizeof(u64)),
+              "nj sort scratch");
+    }
     nj_sort_rows_kernel<<<grid, kSortThreads, smem, st>>>(d_matrix, ld, d_rank, d_keep, d_rows,
                                                          (int)rows.size(), d_scratch, per_cta,
                                                          o->sorted, o->sorted_ld, cap);
