@@ -355,6 +355,22 @@ const char *rnj_msa_name(const rnj_msa *msa, int i);
 const char *rnj_msa_chars(const rnj_msa *msa);
 int rnj_msa_destroy(rnj_msa *msa);
 
+/* Reads an alignment file onto the device of ctx (the input side of
+ * dataloaderFasta::parseData, dataloaderFasta.hpp:78-133,201-276, run on the
+ * GPU): the file's bytes are read by several host threads into page-locked
+ * memory and copied once; kernels find the lines, count each line's kept bytes
+ * (> 32), assign lines to sequences, check the lengths and compact the bytes
+ * into an n x L array on the device.  Names and results are the host reader's
+ * (rnj_msa_read) for every input; FASTA files whose names end on a control byte
+ * other than a final '\r', that hold data before the first name or names
+ * without data, and Stockholm files, are parsed by the host rules and then
+ * copied to the device.  rnj_msa_info / _name work as for rnj_msa_read;
+ * rnj_msa_chars copies the bytes to the host on first use. */
+int rnj_msa_read_device(rnj_ctx *ctx, const char *path, const char *format, rnj_msa **out);
+/* The device bytes of an alignment read by rnj_msa_read_device (n rows of
+ * stride *ld = L bytes); RNJ_ERR_INVALID for one read on the host. */
+int rnj_msa_device_chars(const rnj_msa *msa, const void **d_chars, size_t *ld);
+
 /* Writes the "-o m" text matrix of main.cpp:212-221 ("\t<n>", then per row the
  * name, a tab and n values printed with six fixed decimals, each followed by a
  * space).  rows[i] are n floats; path NULL writes to stdout. */

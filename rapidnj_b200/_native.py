@@ -116,6 +116,8 @@ SIGNATURES = {
     "rnj_msa_name": (c_char_p, [c_void_p, c_int]),
     "rnj_msa_chars": (c_void_p, [c_void_p]),
     "rnj_msa_destroy": (c_int, [c_void_p]),
+    "rnj_msa_read_device": (c_int, [c_void_p, c_char_p, c_char_p, P(c_void_p)]),
+    "rnj_msa_device_chars": (c_int, [c_void_p, P(c_void_p), P(c_size_t)]),
     "rnj_write_matrix_text": (c_int, [c_char_p, P(c_char_p), P(c_void_p), c_int, c_int]),
     "rnj_nj_init": (c_int, [c_void_p, c_void_p, c_int, c_size_t, c_void_p]),
 }

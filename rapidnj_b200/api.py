@@ -248,6 +248,31 @@ class Context:
                                     mx.ctypes.data))
         return outs, mx[:R]
 
+    def read_alignment_device(self, path: str, fmt: str | None = None):
+        """rnj_msa_read_device: the file parsed on this context's device.  Returns
+        (names, chars: CUDA uint8 tensor (n, L), detected type), the same names and
+        bytes as read_alignment."""
+        import torch
+        h = ctypes.c_void_p()
+        check(N.lib().rnj_msa_read_device(self.handle, path.encode(),
+                                          fmt.encode() if fmt else None, ctypes.byref(h)))
+        try:
+            names, n, L, t = _msa_header(h)
+            if n * L == 0:
+                return names, torch.zeros((n, L), dtype=torch.uint8, device=f"cuda:{self.device}"), t
+            p, ld = ctypes.c_void_p(), ctypes.c_size_t()
+            check(N.lib().rnj_msa_device_chars(h, ctypes.byref(p), ctypes.byref(ld)))
+
+            class _View:  # the library's device bytes, copied before the handle goes
+                __cuda_array_interface__ = {"shape": (n, L), "typestr": "|u1",
+                                            "data": (p.value, False), "version": 3,
+                                            "strides": (ld.value, 1)}
+            with torch.cuda.device(self.device):
+                chars = torch.as_tensor(_View(), device=f"cuda:{self.device}").clone()
+            return names, chars, t
+        finally:
+            N.lib().rnj_msa_destroy(h)
+
     def nj_init(self, d_matrix, cap: int = 0, sorted_rows: bool = True, sorted_out=None):
         """rnj_nj_init: rapidNJ's set-up over the device distance matrix d_matrix (a
         CUDA float32 tensor, n x n, row stride >= n).  Returns a dict of host arrays
@@ -544,27 +569,32 @@ class Server:
 
 # --- alignment files (host only) -------------------------------------------------
 
+def _msa_header(h):
+    """(names, n, L, detected type) of an rnj_msa handle."""
+    n, L, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    check(N.lib().rnj_msa_info(h, ctypes.byref(n), ctypes.byref(L), ctypes.byref(t)))
+    names = []
+    k = 0
+    while True:
+        nm = N.lib().rnj_msa_name(h, k)
+        if nm is None:
+            break
+        names.append(nm.decode("latin-1"))
+        k += 1
+    return names, n.value, L.value, t.value
+
+
 def read_alignment(path: str, fmt: str | None = None):
     """(names, chars (n, L) uint8, detected type) with the reference loaders' rules."""
     h = ctypes.c_void_p()
     check(N.lib().rnj_msa_read(path.encode(), fmt.encode() if fmt else None, ctypes.byref(h)))
     try:
-        n, L, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        check(N.lib().rnj_msa_info(h, ctypes.byref(n), ctypes.byref(L), ctypes.byref(t)))
-        names = []
-        k = 0
-        while True:
-            nm = N.lib().rnj_msa_name(h, k)
-            if nm is None:
-                break
-            names.append(nm.decode("latin-1"))
-            k += 1
+        names, n, L, t = _msa_header(h)
         ptr = N.lib().rnj_msa_chars(h)
-        size = n.value * L.value
+        size = n * L
         chars = np.ctypeslib.as_array((ctypes.c_uint8 * size).from_address(ptr)) \
-            .reshape(n.value, L.value).copy() \
-            if size else np.zeros((n.value, L.value), np.uint8)
-        return names, chars, t.value
+            .reshape(n, L).copy() if size else np.zeros((n, L), np.uint8)
+        return names, chars, t
     finally:
         N.lib().rnj_msa_destroy(h)
 

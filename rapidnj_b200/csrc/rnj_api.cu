@@ -618,6 +618,7 @@ int rnj_ctx_destroy(rnj_ctx *ctx) {
   for (int k = 0; k < 6; ++k)
     if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
   if (ctx->h_words) cudaFreeHost(ctx->h_words);
+  if (ctx->h_file) cudaFreeHost(ctx->h_file);
   if (ctx->s_up) {
     cudaStreamSynchronize(ctx->s_up);
     cudaStreamDestroy(ctx->s_up);

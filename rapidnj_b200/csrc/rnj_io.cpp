@@ -17,29 +17,25 @@
 #include <thread>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "rnj.h"
 #include "rnj_internal.h"
-
-struct rnj_msa {
-  std::vector<std::string> names;
-  std::vector<char> chars;  // n * L
-  int n = 0;
-  int L = 0;
-  int type = RNJ_DNA;
-};
-
-namespace {
+#include "rnj_objects.h"
 
 using rnj::set_error;
 
-// The whole file in one uninitialised buffer (a zero-filled one would cost
-// another pass over it).
+namespace {
+
+// The file's bytes: read into one uninitialised buffer (a zero-filled one would
+// cost another pass over it), or a caller's buffer viewed in place.
 struct FileData {
   std::unique_ptr<char[]> buf;
+  const char *view = nullptr;
   size_t n = 0;
   size_t size() const { return n; }
-  char operator[](size_t i) const { return buf[i]; }
-  const char *data() const { return buf.get(); }
+  char operator[](size_t i) const { return data()[i]; }
+  const char *data() const { return view ? view : buf.get(); }
 };
 
 bool read_file(const char *path, FileData &fd) {
@@ -221,10 +217,16 @@ inline int format_fixed6(char *out, float v) { return snprintf(out, 64, "%.6f ",
 
 }  // namespace
 
-extern "C" {
+// Parses bytes already in memory (the device reader's fallback for inputs its
+// kernels leave to the host rules).
+int msa_parse_buffer(const char *bytes, size_t size, bool fasta, rnj_msa *m) {
+  FileData data;
+  data.view = bytes;
+  data.n = size;
+  return fasta ? parse_fasta(data, m) : parse_stockholm(data, m);
+}
 
-int rnj_msa_read(const char *path, const char *format, rnj_msa **out) {
-  if (!path || !out) return set_error(RNJ_ERR_INVALID, "null argument");
+int msa_format(const char *path, const char *format, bool *fasta) {
   std::string fmt = format ? format : "";
   std::string p(path);
   if (fmt.empty()) {
@@ -237,10 +239,21 @@ int rnj_msa_read(const char *path, const char *format, rnj_msa **out) {
                                         "the '-i' option to indicate the format.");
   }
   if (fmt != "fa" && fmt != "sth") return set_error(RNJ_ERR_UNSUPPORTED, "Unkown input format " + fmt);
+  *fasta = fmt == "fa";
+  return RNJ_OK;
+}
+
+extern "C" {
+
+int rnj_msa_read(const char *path, const char *format, rnj_msa **out) {
+  if (!path || !out) return set_error(RNJ_ERR_INVALID, "null argument");
+  bool fasta = true;
+  int rc = msa_format(path, format, &fasta);
+  if (rc != RNJ_OK) return rc;
   FileData data;
   if (!read_file(path, data)) return set_error(RNJ_ERR_IO, std::string("ERROR: Could not read file: ") + path);
   rnj_msa *m = new rnj_msa();
-  int rc = (fmt == "fa") ? parse_fasta(data, m) : parse_stockholm(data, m);
+  rc = fasta ? parse_fasta(data, m) : parse_stockholm(data, m);
   if (rc != RNJ_OK) {
     delete m;
     return rc;
@@ -262,9 +275,42 @@ const char *rnj_msa_name(const rnj_msa *msa, int i) {
   return msa->names[i].c_str();
 }
 
-const char *rnj_msa_chars(const rnj_msa *msa) { return msa && !msa->chars.empty() ? msa->chars.data() : ""; }
+const char *rnj_msa_chars(const rnj_msa *msa) {
+  if (!msa) return "";
+  if (msa->chars.empty() && msa->d_chars && msa->n > 0 && msa->L > 0) {
+    // An alignment read on the device: its bytes come to the host on first use.
+    msa->chars.resize((size_t)msa->n * msa->L);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != msa->device) cudaSetDevice(msa->device);
+    const cudaError_t e = cudaMemcpy(msa->chars.data(), msa->d_chars, msa->chars.size(),
+                                     cudaMemcpyDeviceToHost);
+    if (prev >= 0 && prev != msa->device) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+      msa->chars.clear();
+      rnj::cuda_error(e, "alignment download");
+      return nullptr;
+    }
+  }
+  return !msa->chars.empty() ? msa->chars.data() : "";
+}
+
+int rnj_msa_device_chars(const rnj_msa *msa, const void **d_chars, size_t *ld) {
+  if (!msa || !d_chars) return set_error(RNJ_ERR_INVALID, "null argument");
+  if (!msa->d_chars) return set_error(RNJ_ERR_INVALID, "the alignment was read on the host");
+  *d_chars = msa->d_chars;
+  if (ld) *ld = (size_t)msa->L;
+  return RNJ_OK;
+}
 
 int rnj_msa_destroy(rnj_msa *msa) {
+  if (msa && msa->d_chars) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != msa->device) cudaSetDevice(msa->device);
+    cudaFree(msa->d_chars);
+    if (prev >= 0 && prev != msa->device) cudaSetDevice(prev);
+  }
   delete msa;
   return RNJ_OK;
 }

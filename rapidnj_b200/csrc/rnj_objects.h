@@ -4,8 +4,29 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+#include <vector>
+
 #include "rnj.h"
 #include "rnj_internal.h"
+
+// A parsed alignment: names and n * L bytes (row-major), on the host, or on the
+// device when read by rnj_msa_read_device (its host bytes are then copied on
+// the first rnj_msa_chars).
+struct rnj_msa {
+  std::vector<std::string> names;
+  mutable std::vector<char> chars;  // n * L (host)
+  int n = 0;
+  int L = 0;
+  int type = RNJ_DNA;
+  uint8_t *d_chars = nullptr;  // n * L on device `device` (owned), or null
+  int device = -1;
+};
+
+// Parses a FASTA (fasta) or Stockholm file's bytes already in memory with the
+// host rules (rnj_io.cpp); the format of a path as rnj_msa_read picks it.
+int msa_parse_buffer(const char *bytes, size_t size, bool fasta, rnj_msa *m);
+int msa_format(const char *path, const char *format, bool *fasta);
 
 struct rnj_ctx {
   int device = 0;
@@ -30,6 +51,8 @@ struct rnj_ctx {
   rnj::AlnDesc *d_desc = nullptr;         // one-alignment work list of the persistent kernel
   uint64_t *d_packed = nullptr;           // packed counts of the tensor-core path
   long long packed_tiles = 0;             // its capacity in tiles
+  char *h_file = nullptr;                 // pinned file bytes of rnj_msa_read_device
+  size_t h_file_cap = 0;
 };
 
 // Grows the context's packed-count buffer to `tiles` tiles (rnj_api.cu).
