@@ -588,6 +588,79 @@ def run_nj_init(args, local_rank: int = 0, n: int = 10000, L: int = 10000):
     return out
 
 
+def run_parse(args, local_rank: int = 0):
+    """Reading the workload's alignment from a FASTA file (60 columns a line): the
+    device reader (rnj_msa_read_device: page-locked threaded read, parse on the
+    GPU) against the host reader (rnj_msa_read), both through the C ABI with the
+    file in the page cache; and file -> distance matrix in page-locked host memory
+    through the device reader (read, pack, distances, one download)."""
+    import ctypes
+    import torch
+    from rapidnj_b200 import _native as N
+    from rapidnj_b200 import api, synth
+    _, n, L, type_, model = WORKLOADS[args.workload]
+    seqs = make_alignment(args.workload)
+    lib = N.lib()
+    dev = f"cuda:{local_rank}"
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "aln.fa").encode()
+        synth.write_fasta(path.decode(), seqs, width=60)
+        size = os.path.getsize(path)
+        ctx = api.Context(local_rank)
+
+        def read(device: bool):
+            h = ctypes.c_void_p()
+            t0 = time.perf_counter()
+            if device:
+                N.check(lib.rnj_msa_read_device(ctx.handle, path, b"fa", ctypes.byref(h)))
+            else:
+                N.check(lib.rnj_msa_read(path, b"fa", ctypes.byref(h)))
+            return h, time.perf_counter() - t0
+
+        out_d = torch.empty((n, n), dtype=torch.float32, device=dev)
+        out_h = torch.empty((n, n), dtype=torch.float32).pin_memory()
+
+        def file_to_matrix():
+            t0 = time.perf_counter()
+            h, _ = read(True)
+            p, ld = ctypes.c_void_p(), ctypes.c_size_t()
+            N.check(lib.rnj_msa_device_chars(h, ctypes.byref(p), ctypes.byref(ld)))
+            nn, LL, tt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+            N.check(lib.rnj_msa_info(h, ctypes.byref(nn), ctypes.byref(LL), ctypes.byref(tt)))
+            a = ctypes.c_void_p()
+            N.check(lib.rnj_aln_from_device(ctx.handle, p, nn.value, LL.value, ld.value, tt.value,
+                                            N.RNJ_FASTDIST, ctypes.byref(a)))
+            N.check(lib.rnj_distance_into(ctx.handle, a, api.MODELS[model],
+                                          ctypes.c_void_p(out_d.data_ptr()), n, None))
+            lib.rnj_aln_destroy(a)
+            ctx.synchronize()
+            out_h.copy_(out_d)
+            torch.cuda.synchronize()
+            lib.rnj_msa_destroy(h)
+            return time.perf_counter() - t0
+
+        for dv in (True, False):  # warm-up: page cache, page-locked buffer
+            h, _ = read(dv)
+            lib.rnj_msa_destroy(h)
+        tdv, thv = [], []
+        for _ in range(4):
+            h, t = read(True)
+            lib.rnj_msa_destroy(h)
+            tdv.append(t)
+            h, t = read(False)
+            lib.rnj_msa_destroy(h)
+            thv.append(t)
+        file_to_matrix()
+        tf = statistics.median(file_to_matrix() for _ in range(3))
+        ctx.close()
+    return {"file_mb": size / 1e6, "device_reader_ms": 1e3 * statistics.median(tdv),
+            "host_reader_ms": 1e3 * statistics.median(thv),
+            "speedup_vs_host_reader": statistics.median(thv) / statistics.median(tdv),
+            "file_to_host_matrix_ms": 1e3 * tf,
+            "workload": f"FASTA file of the {args.workload} alignment, 60 columns a line, "
+                        "names s0.., file in the page cache"}
+
+
 def fp4_tensor_peak(device: int):
     """Dense FP4 tensor throughput (flop/s) of a library GEMM on this device, and
     how it was obtained: an MXFP4 GEMM (torch._scaled_mm, unit block scales,
@@ -649,9 +722,9 @@ def main():
     ap.add_argument("--popcount", action="store_true",
                     help="count DNA with the bit-plane popcount kernel instead of tensor cores")
     ap.add_argument("--mode", default="all",
-                    choices=["all", "plain", "batched", "served", "bootstrap", "njinit"],
-                    help="all: the plain workload line plus the batched, served, bootstrap and "
-                         "NJ set-up figures")
+                    choices=["all", "plain", "batched", "served", "bootstrap", "njinit", "parse"],
+                    help="all: the plain workload line plus the batched, served, bootstrap, "
+                         "parse and NJ set-up figures")
     ap.add_argument("--nj-n", type=int, default=10000,
                     help="sequences (and columns) of the NJ set-up workload (njinit)")
     args = ap.parse_args()
@@ -717,6 +790,8 @@ def main():
             line["served"] = run_served(args, local_rank)
         if args.mode in ("all", "bootstrap") and world == 1:
             line["bootstrap"] = run_bootstrap(args, local_rank)
+        if args.mode in ("all", "parse") and world == 1:
+            line["parse"] = run_parse(args, local_rank)
         if args.mode in ("all", "njinit") and world == 1:
             line["nj_init"] = run_nj_init(args, local_rank, n=args.nj_n, L=args.nj_n)
         print(json.dumps(line))

@@ -18,8 +18,9 @@
 //      a sequence line's bytes > 32 are counted; a name line is checked to hold
 //      no control byte but a final '\r' (else the line's rest would be a unit of
 //      its own);
-//   3. one CTA scans the lines (names count up, kept bytes sum up per sequence)
-//      into each line's sequence and offset, each sequence's length and name
+//   3. a scan over the lines (names count up, kept bytes sum up per sequence;
+//      block totals, their scan on the host, then each block from its prefix)
+//      gives each line's sequence and offset, each sequence's length and name
 //      line;
 //   4. after the host has checked the lengths, a warp per sequence line
 //      compacts its kept bytes (ballot + prefix count) into the n x L array.
@@ -211,28 +212,29 @@ __device__ __forceinline__ Seg seg_shfl_up(Seg v, int o) {
   return r;
 }
 
-// Pass 3 (one CTA of 1024 threads, a contiguous run of lines each): line w's
-// sequence rec[w] (-1 before the first name) and offset off[w] in it; sequence
-// r's length rec_len[r] and name line span rec_start[r] .. rec_end[r].
-__global__ void __launch_bounds__(1024)
-    record_scan_kernel(const uint8_t *__restrict__ type, const uint32_t *__restrict__ cnt,
-                       const uint32_t *__restrict__ pos, uint32_t nnl, size_t S,
-                       int *__restrict__ rec, uint32_t *__restrict__ off,
-                       uint32_t *__restrict__ rec_len, uint32_t *__restrict__ rec_start,
-                       uint32_t *__restrict__ rec_end, uint32_t *__restrict__ flags) {
-  __shared__ Seg wsum[32];
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const uint32_t lines = nnl + 1;
-  const uint32_t per = (lines + blockDim.x - 1) / blockDim.x;
-  const uint32_t a = min(lines, (uint32_t)t * per), b = min(lines, a + per);
-  Seg mine = {0u, 0u};
-  for (uint32_t i = a; i < b; ++i) {
-    Seg e;
-    e.h = type[i] == kLineName ? 1u : 0u;
-    e.s = type[i] == kLineSeq ? cnt[i] : 0u;
-    mine = seg_combine(mine, e);
-  }
-  Seg incl = mine;
+// Pass 3, over blocks of kScanLines lines (a CTA each, kScanPer consecutive
+// lines a thread): the scan of (names, kept bytes since the last name).  3a
+// writes each block's total; the host scans the totals; 3b rescans a block from
+// its prefix and walks its lines: line w's sequence rec[w] (-1 before the first
+// name) and offset off[w], sequence r's length rec_len[r] and name line span
+// rec_start[r] .. rec_end[r].
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;
+constexpr uint32_t kScanLines = kScanThreads * kScanPer;
+
+__device__ __forceinline__ Seg line_seg(const uint8_t *type, const uint32_t *cnt, uint32_t i) {
+  Seg e;
+  const uint8_t t = type[i];
+  e.h = t == kLineName ? 1u : 0u;
+  e.s = t == kLineSeq ? cnt[i] : 0u;
+  return e;
+}
+
+// The CTA's exclusive scan of v (identity (0, 0)); *total the CTA's sum.
+__device__ __forceinline__ Seg block_seg_exclusive(Seg v, Seg *total) {
+  __shared__ Seg wsum[kScanThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  Seg incl = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const Seg y = seg_shfl_up(incl, o);
@@ -240,25 +242,47 @@ __global__ void __launch_bounds__(1024)
   }
   if (lane == 31) wsum[warp] = incl;
   __syncthreads();
-  if (warp == 0) {
-    Seg v = lane < (int)(blockDim.x >> 5) ? wsum[lane] : Seg{0u, 0u};
-    Seg inc = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const Seg y = seg_shfl_up(inc, o);
-      if (lane >= o) inc = seg_combine(y, inc);
-    }
-    Seg ex = seg_shfl_up(inc, 1);
-    if (lane == 0) ex = Seg{0u, 0u};
-    __syncwarp();
-    wsum[lane] = ex;
+  Seg before = {0u, 0u}, all = {0u, 0u};
+  for (int w = 0; w < kScanThreads / 32; ++w) {
+    if (w < warp) before = seg_combine(before, wsum[w]);
+    all = seg_combine(all, wsum[w]);
   }
-  __syncthreads();
-  Seg ex_warp = seg_shfl_up(incl, 1);
-  if (lane == 0) ex_warp = Seg{0u, 0u};
-  Seg run = seg_combine(wsum[warp], ex_warp);
+  *total = all;
+  Seg ex = seg_shfl_up(incl, 1);
+  if (lane == 0) ex = Seg{0u, 0u};
+  return seg_combine(before, ex);
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    seq_scan_totals_kernel(const uint8_t *__restrict__ type, const uint32_t *__restrict__ cnt,
+                           uint32_t lines, uint2 *__restrict__ block_total) {
+  const uint32_t a = min(lines, blockIdx.x * kScanLines + threadIdx.x * kScanPer);
+  const uint32_t b = min(lines, a + kScanPer);
+  Seg mine = {0u, 0u};
+  for (uint32_t i = a; i < b; ++i) mine = seg_combine(mine, line_seg(type, cnt, i));
+  Seg total;
+  block_seg_exclusive(mine, &total);
+  if (threadIdx.x == 0) block_total[blockIdx.x] = make_uint2(total.h, total.s);
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    seq_scan_walk_kernel(const uint8_t *__restrict__ type, const uint32_t *__restrict__ cnt,
+                         const uint32_t *__restrict__ pos, uint32_t nnl, size_t S,
+                         const uint2 *__restrict__ block_prefix, int *__restrict__ rec,
+                         uint32_t *__restrict__ off, uint32_t *__restrict__ rec_len,
+                         uint32_t *__restrict__ rec_start, uint32_t *__restrict__ rec_end,
+                         uint32_t *__restrict__ flags) {
+  const uint32_t lines = nnl + 1;
+  const uint32_t a = min(lines, blockIdx.x * kScanLines + threadIdx.x * kScanPer);
+  const uint32_t b = min(lines, a + kScanPer);
+  Seg mine = {0u, 0u};
+  for (uint32_t i = a; i < b; ++i) mine = seg_combine(mine, line_seg(type, cnt, i));
+  Seg total;
+  const Seg ex = block_seg_exclusive(mine, &total);
+  Seg run = seg_combine(Seg{block_prefix[blockIdx.x].x, block_prefix[blockIdx.x].y}, ex);
   for (uint32_t i = a; i < b; ++i) {
-    if (type[i] == kLineName) {
+    const uint8_t t = type[i];
+    if (t == kLineName) {
       if (run.h >= 1) rec_len[run.h - 1] = run.s;
       else if (run.s > 0) atomicOr(&flags[0], kFlagLeadingData);
       size_t s0, e0;
@@ -272,7 +296,7 @@ __global__ void __launch_bounds__(1024)
     } else {
       rec[i] = (int)run.h - 1;
       off[i] = run.s;
-      if (type[i] == kLineSeq) run.s += cnt[i];
+      if (t == kLineSeq) run.s += cnt[i];
     }
   }
   if (a < b && b == lines) {  // the last line's thread closes the last sequence
@@ -472,8 +496,28 @@ extern "C" int rnj_msa_read_device(rnj_ctx *ctx, const char *path, const char *f
       PARSE_CUDA(buf.alloc(&d_len, (size_t)H * sizeof(uint32_t)), "parse buffers");
       PARSE_CUDA(buf.alloc(&d_rs, (size_t)H * sizeof(uint32_t)), "parse buffers");
       PARSE_CUDA(buf.alloc(&d_re, (size_t)H * sizeof(uint32_t)), "parse buffers");
-      record_scan_kernel<<<1, 1024, 0, st>>>(d_type, d_cnt, d_pos, nnl, S, d_rec, d_off, d_len, d_rs,
-                                             d_re, d_flags);
+      const unsigned nblk = (unsigned)((lines + kScanLines - 1) / kScanLines);
+      uint2 *d_blk = nullptr;
+      PARSE_CUDA(buf.alloc(&d_blk, (size_t)nblk * sizeof(uint2)), "parse buffers");
+      seq_scan_totals_kernel<<<nblk, kScanThreads, 0, st>>>(d_type, d_cnt, lines, d_blk);
+      PARSE_CUDA(cudaGetLastError(), "sequence scan");
+      std::vector<uint2> blk(nblk);
+      PARSE_CUDA(cudaMemcpyAsync(blk.data(), d_blk, (size_t)nblk * sizeof(uint2),
+                                 cudaMemcpyDeviceToHost, st),
+                 "parse copy");
+      PARSE_CUDA(cudaStreamSynchronize(st), "sequence scan sync");
+      uint2 run = make_uint2(0u, 0u);  // exclusive scan of the block totals
+      for (unsigned k = 0; k < nblk; ++k) {
+        const uint2 v = blk[k];
+        blk[k] = run;
+        run.y = v.x ? v.y : run.y + v.y;
+        run.x += v.x;
+      }
+      PARSE_CUDA(cudaMemcpyAsync(d_blk, blk.data(), (size_t)nblk * sizeof(uint2),
+                                 cudaMemcpyHostToDevice, st),
+                 "parse copy");
+      seq_scan_walk_kernel<<<nblk, kScanThreads, 0, st>>>(d_type, d_cnt, d_pos, nnl, S, d_blk, d_rec,
+                                                          d_off, d_len, d_rs, d_re, d_flags);
       PARSE_CUDA(cudaGetLastError(), "sequence scan");
       std::vector<uint32_t> len(H), rs(H), re(H);
       PARSE_CUDA(cudaMemcpyAsync(len.data(), d_len, (size_t)H * 4, cudaMemcpyDeviceToHost, st), "parse copy");
