@@ -371,6 +371,16 @@ int rnj_msa_read_device(rnj_ctx *ctx, const char *path, const char *format, rnj_
  * stride *ld = L bytes); RNJ_ERR_INVALID for one read on the host. */
 int rnj_msa_device_chars(const rnj_msa *msa, const void **d_chars, size_t *ld);
 
+/* The "-o m" text of an n x n DEVICE matrix (rows of stride ld floats), as
+ * rnj_write_matrix_text writes it (byte-identical), formatted on the device: the
+ * six-decimal digits of a float are computed exactly (v * 10^6 is exact in
+ * double; rounded to an integer with ties to even, as the C library prints),
+ * rows are formatted in bands of up to 64 MB and written while the next band is
+ * formatted.  Rows holding values of 8e9 or more in magnitude, infinities or
+ * NaNs are printed by the host.  path NULL writes to stdout. */
+int rnj_write_matrix_text_device(rnj_ctx *ctx, const char *path, const char *const *names,
+                                 const float *d_matrix, size_t ld, int n);
+
 /* Writes the "-o m" text matrix of main.cpp:212-221 ("\t<n>", then per row the
  * name, a tab and n values printed with six fixed decimals, each followed by a
  * space).  rows[i] are n floats; path NULL writes to stdout. */

@@ -120,6 +120,8 @@ SIGNATURES = {
     "rnj_msa_device_chars": (c_int, [c_void_p, P(c_void_p), P(c_size_t)]),
     "rnj_write_matrix_text": (c_int, [c_char_p, P(c_char_p), P(c_void_p), c_int, c_int]),
     "rnj_nj_init": (c_int, [c_void_p, c_void_p, c_int, c_size_t, c_void_p]),
+    "rnj_write_matrix_text_device": (c_int, [c_void_p, c_char_p, P(c_char_p), c_void_p, c_size_t,
+                                             c_int]),
 }
 
 

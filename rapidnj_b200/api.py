@@ -599,6 +599,18 @@ def read_alignment(path: str, fmt: str | None = None):
         N.lib().rnj_msa_destroy(h)
 
 
+def write_matrix_text_device(ctx: "Context", path: str | None, names, d_matrix) -> None:
+    """rnj_write_matrix_text_device: the "-o m" text of a CUDA float32 (n, n) tensor
+    (row stride >= n), formatted on the device; byte-identical to
+    write_matrix_text."""
+    n = d_matrix.shape[0]
+    assert d_matrix.shape == (n, n) and d_matrix.stride(1) == 1
+    nm = (ctypes.c_char_p * max(n, 1))(*[x.encode("latin-1") for x in names[:n]])
+    check(N.lib().rnj_write_matrix_text_device(ctx.handle, path.encode() if path else None, nm,
+                                               ctypes.c_void_p(d_matrix.data_ptr()),
+                                               d_matrix.stride(0), n))
+
+
 def write_matrix_text(path: str | None, names, matrix: np.ndarray, threads: int = 0) -> None:
     m = np.ascontiguousarray(matrix, dtype=np.float32)
     n = m.shape[0]

@@ -93,30 +93,43 @@ int main(int argc, char **argv) {
   if (!path) usage();
 
   double t0 = now();
+  rnj_ctx *ctx = nullptr;
+  if (rnj_ctx_create(device, &ctx) != RNJ_OK) die("GPU context");
+  // The alignment is parsed on the device, the matrix stays there and is
+  // formatted there; only its text comes back.
   rnj_msa *msa = nullptr;
-  if (rnj_msa_read(path, fmt, &msa) != RNJ_OK) die("could not read the alignment");
+  if (rnj_msa_read_device(ctx, path, fmt, &msa) != RNJ_OK) die("could not read the alignment");
   int n = 0, L = 0, detected = RNJ_DNA;
   rnj_msa_info(msa, &n, &L, &detected);
   if (type == RNJ_UNKNOWN) type = detected;
   double t1 = now();
 
-  rnj_ctx *ctx = nullptr;
-  if (rnj_ctx_create(device, &ctx) != RNJ_OK) die("GPU context");
-  std::vector<float> m((size_t)n * n);
-  float mx = 0.0f;
-  if (rnj_distance_matrix_host(ctx, rnj_msa_chars(msa), n, L, (size_t)L, type, model,
-                               fast ? RNJ_FASTDIST : 0, m.data(), &mx) != RNJ_OK)
-    die("distance computation");
-  double t2 = now();
-
   std::vector<const char *> names(n);
-  std::vector<const float *> rows(n);
-  for (int i = 0; i < n; ++i) {
-    names[i] = rnj_msa_name(msa, i);
-    rows[i] = m.data() + (size_t)i * n;
+  for (int i = 0; i < n; ++i) names[i] = rnj_msa_name(msa, i);
+  float mx = 0.0f;
+  double t2 = t1;
+  if (n == 0) {
+    if (rnj_write_matrix_text(out, names.data(), nullptr, 0, threads) != RNJ_OK)
+      die("writing the matrix");
+  } else {
+    const void *d_chars = nullptr;
+    size_t ld = 0;
+    rnj_aln *aln = nullptr;
+    rnj_mat *mat = nullptr;
+    if (rnj_msa_device_chars(msa, &d_chars, &ld) != RNJ_OK ||
+        rnj_aln_from_device(ctx, d_chars, n, L, ld, type, fast ? RNJ_FASTDIST : 0, &aln) != RNJ_OK ||
+        rnj_distance(ctx, aln, model, &mat) != RNJ_OK)
+      die("distance computation");
+    float *d_m = nullptr;
+    size_t ldm = 0;
+    if (rnj_mat_device_ptr(mat, &d_m, &ldm) != RNJ_OK || rnj_mat_info(mat, nullptr, &mx) != RNJ_OK)
+      die("distance computation");
+    t2 = now();
+    if (rnj_write_matrix_text_device(ctx, out, names.data(), d_m, ldm, n) != RNJ_OK)
+      die("writing the matrix");
+    rnj_mat_destroy(mat);
+    rnj_aln_destroy(aln);
   }
-  if (rnj_write_matrix_text(out, names.data(), rows.data(), n, threads) != RNJ_OK)
-    die("writing the matrix");
   double t3 = now();
   if (verbose)
     fprintf(stderr, "read %.3f s, distances %.3f s (max %g), text %.3f s; %d sequences x %d columns\n",
