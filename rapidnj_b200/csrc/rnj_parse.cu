@@ -11,7 +11,7 @@
 // its newline.
 //
 // Here the file's bytes are read by several host threads into page-locked
-// memory and copied to the device once, and:
+// memory, each 4 MB chunk copied to the device as soon as it is read, and:
 //   1. the newlines are found by a two-pass compaction over 64 KB chunks (count
 //      per chunk, scan on the host, positions in order);
 //   2. a warp per line reads its first byte: names, comments and sequence lines;
@@ -36,6 +36,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <thread>
 #include <vector>
@@ -356,16 +357,23 @@ struct ParseBuffers {
   }
 };
 
-// The file into the context's page-locked buffer, T threads reading a range each.
-int read_pinned(rnj_ctx *ctx, const char *path, size_t *size) {
+// The file into the context's page-locked buffer: up to eight threads read
+// 4 MB chunks in turn and, when d_raw is given (room for the file's bytes on the
+// context's device), each copies its chunk there as soon as it is read, so that
+// the copies overlap the reading.  *size: the file's bytes.
+constexpr size_t kReadChunk = (size_t)4 << 20;
+
+int file_size(const char *path, size_t *size) {
+  struct stat st;
+  if (stat(path, &st) != 0 || !S_ISREG(st.st_mode))
+    return set_error(RNJ_ERR_IO, std::string("ERROR: Could not read file: ") + path);
+  *size = (size_t)st.st_size;
+  return RNJ_OK;
+}
+
+int read_pinned(rnj_ctx *ctx, const char *path, size_t S, uint8_t *d_raw) {
   const int fd = open(path, O_RDONLY);
   if (fd < 0) return set_error(RNJ_ERR_IO, std::string("ERROR: Could not read file: ") + path);
-  struct stat st;
-  if (fstat(fd, &st) != 0 || !S_ISREG(st.st_mode)) {
-    close(fd);
-    return set_error(RNJ_ERR_IO, std::string("ERROR: Could not read file: ") + path);
-  }
-  const size_t S = (size_t)st.st_size;
   if (S + 16 > ctx->h_file_cap) {
     if (ctx->h_file) cudaFreeHost(ctx->h_file);
     ctx->h_file = nullptr;
@@ -378,18 +386,35 @@ int read_pinned(rnj_ctx *ctx, const char *path, size_t *size) {
     }
     ctx->h_file_cap = cap;
   }
+  const size_t chunks = (S + kReadChunk - 1) / kReadChunk;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const int T = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, S >> 22));
+  const int T = (int)std::max<size_t>(1, std::min<size_t>(std::min(8u, hw), chunks));
+  std::atomic<size_t> next{0};
   std::vector<int> ok(T, 1);
+  std::vector<cudaError_t> err(T, cudaSuccess);
   auto work = [&](int k) {
-    size_t a = S * k / T, b = S * (k + 1) / T;
-    while (a < b) {
-      const ssize_t r = pread(fd, ctx->h_file + a, b - a, (off_t)a);
-      if (r <= 0) {
-        ok[k] = 0;
-        return;
+    if (d_raw && k > 0) cudaSetDevice(ctx->device);  // the current device is per thread
+    for (;;) {
+      const size_t c = next.fetch_add(1);
+      if (c >= chunks) return;
+      size_t a = c * kReadChunk;
+      const size_t a0 = a, b = std::min(S, a + kReadChunk);
+      while (a < b) {
+        const ssize_t r = pread(fd, ctx->h_file + a, b - a, (off_t)a);
+        if (r <= 0) {
+          ok[k] = 0;
+          return;
+        }
+        a += (size_t)r;
       }
-      a += (size_t)r;
+      if (d_raw) {
+        const cudaError_t e =
+            cudaMemcpyAsync(d_raw + a0, ctx->h_file + a0, b - a0, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) {
+          err[k] = e;
+          return;
+        }
+      }
     }
   };
   std::vector<std::thread> th;
@@ -397,9 +422,10 @@ int read_pinned(rnj_ctx *ctx, const char *path, size_t *size) {
   work(0);
   for (auto &x : th) x.join();
   close(fd);
-  for (int k = 0; k < T; ++k)
+  for (int k = 0; k < T; ++k) {
     if (!ok[k]) return set_error(RNJ_ERR_IO, std::string("ERROR: Could not read file: ") + path);
-  *size = S;
+    if (err[k] != cudaSuccess) return cuda_error(err[k], "file upload");
+  }
   return RNJ_OK;
 }
 
@@ -436,9 +462,13 @@ extern "C" int rnj_msa_read_device(rnj_ctx *ctx, const char *path, const char *f
   if (rc != RNJ_OK) return rc;
   DeviceGuard guard(ctx->device);
   size_t S = 0;
-  rc = read_pinned(ctx, path, &S);
+  rc = file_size(path, &S);
   if (rc != RNJ_OK) return rc;
-  if (!fasta || S == 0 || S >= ((size_t)1 << 32) - 1) return host_parse_to_device(ctx, S, fasta, out);
+  if (!fasta || S == 0 || S >= ((size_t)1 << 32) - 1) {
+    rc = read_pinned(ctx, path, S, nullptr);
+    if (rc != RNJ_OK) return rc;
+    return host_parse_to_device(ctx, S, fasta, out);
+  }
 
   cudaStream_t st = ctx->stream;
   int fallback = 0;
@@ -447,7 +477,8 @@ extern "C" int rnj_msa_read_device(rnj_ctx *ctx, const char *path, const char *f
     ParseBuffers buf(st);
     uint8_t *d_raw = nullptr;
     PARSE_CUDA(buf.alloc(&d_raw, S + 16), "parse buffers");
-    PARSE_CUDA(cudaMemcpyAsync(d_raw, ctx->h_file, S, cudaMemcpyHostToDevice, st), "file upload");
+    rc = read_pinned(ctx, path, S, d_raw);
+    if (rc != RNJ_OK) return rc;
     const unsigned nchunks = (unsigned)((S + kChunk - 1) / kChunk);
     uint32_t *d_chunk = nullptr;
     PARSE_CUDA(buf.alloc(&d_chunk, (size_t)nchunks * sizeof(uint32_t)), "parse buffers");
