@@ -661,6 +661,44 @@ def run_parse(args, local_rank: int = 0):
                         "names s0.., file in the page cache"}
 
 
+def run_text(args, local_rank: int = 0):
+    """The "-o m" text of the workload's distance matrix (rapidNJ's
+    printDistanceMatrix): rnj_write_matrix_text_device (formatted on the device)
+    against rnj_write_matrix_text (host, all cores), files compared byte for byte."""
+    import torch
+    from rapidnj_b200 import api
+    _, n, L, type_, model = WORKLOADS[args.workload]
+    seqs = make_alignment(args.workload)
+    dev = f"cuda:{local_rank}"
+    ctx = api.Context(local_rank)
+    aln = ctx.alignment(torch.from_numpy(np.ascontiguousarray(seqs)).to(dev), api.TYPES[type_])
+    m = torch.empty((n, n), dtype=torch.float32, device=dev)
+    ctx.distance_into(aln, model, m)
+    aln.close()
+    ctx.synchronize()
+    names = [f"s{i}" for i in range(n)]
+    with tempfile.TemporaryDirectory() as td:
+        pd, ph = os.path.join(td, "d.txt"), os.path.join(td, "h.txt")
+        api.write_matrix_text_device(ctx, pd, names, m)  # warm-up
+        tdv = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            api.write_matrix_text_device(ctx, pd, names, m)
+            tdv.append(time.perf_counter() - t0)
+        host = m.cpu().numpy()
+        t0 = time.perf_counter()
+        api.write_matrix_text(ph, names, host)
+        th = time.perf_counter() - t0
+        size = os.path.getsize(pd)
+        with open(pd, "rb") as a, open(ph, "rb") as b:
+            same = a.read() == b.read()
+    ctx.close()
+    return {"text_mb": size / 1e6, "device_writer_ms": 1e3 * statistics.median(tdv),
+            "host_writer_ms": 1e3 * th, "speedup_vs_host_writer": th / statistics.median(tdv),
+            "identical": same, "host_threads": os.cpu_count(),
+            "workload": f"-o m text of the {args.workload} matrix into a file (page cache)"}
+
+
 def fp4_tensor_peak(device: int):
     """Dense FP4 tensor throughput (flop/s) of a library GEMM on this device, and
     how it was obtained: an MXFP4 GEMM (torch._scaled_mm, unit block scales,
@@ -722,9 +760,10 @@ def main():
     ap.add_argument("--popcount", action="store_true",
                     help="count DNA with the bit-plane popcount kernel instead of tensor cores")
     ap.add_argument("--mode", default="all",
-                    choices=["all", "plain", "batched", "served", "bootstrap", "njinit", "parse"],
+                    choices=["all", "plain", "batched", "served", "bootstrap", "njinit", "parse",
+                             "text"],
                     help="all: the plain workload line plus the batched, served, bootstrap, "
-                         "parse and NJ set-up figures")
+                         "parse, text and NJ set-up figures")
     ap.add_argument("--nj-n", type=int, default=10000,
                     help="sequences (and columns) of the NJ set-up workload (njinit)")
     args = ap.parse_args()
@@ -792,6 +831,8 @@ def main():
             line["bootstrap"] = run_bootstrap(args, local_rank)
         if args.mode in ("all", "parse") and world == 1:
             line["parse"] = run_parse(args, local_rank)
+        if args.mode in ("all", "text") and world == 1:
+            line["text"] = run_text(args, local_rank)
         if args.mode in ("all", "njinit") and world == 1:
             line["nj_init"] = run_nj_init(args, local_rank, n=args.nj_n, L=args.nj_n)
         print(json.dumps(line))
