@@ -3,8 +3,9 @@
 
 One unit = one (i < j, column) comparison; an alignment of n sequences and L
 columns is n (n - 1) / 2 * L units.  A step is one pass of the path over one
-alignment: pack the resident bytes into bit planes, count every pair, apply the
-transform, post-process (mirror, diagonal, saturation fix-up).
+alignment: pack the resident bytes (FP4 features for the tensor cores, or bit
+planes), count every pair, apply the transform, post-process (mirror, diagonal,
+saturation fix-up).
 
 Default workload (one B200): DNA Kimura-2P, 10,000 x 10,000, tree-evolved
 synthetic alignment.  Output: one JSON line on rank 0.
@@ -40,8 +41,9 @@ WORKLOADS = {
     "dna-k2p-4096x10000": ("tree_dna", 4096, 10000, "dna", "kim"),
 }
 DEFAULT = "dna-k2p-10000x10000"
-# Algorithmic integer operations per pair per 32-column word:
-# (POPC, LOP3) of the counting kernel for each (type, model).
+# Algorithmic integer operations per pair per 32-column word of the bit-plane
+# counting kernel, (POPC, LOP3) for each (type, model): its roofline when the
+# bit planes are used (--popcount, or protein alphabets of more than 31 residues).
 OPS_PER_WORD = {("dna", "kim"): (3, 4), ("dna", "jc"): (2, 4), ("protein", "kim"): (2, 7),
                 ("protein", "jc"): (2, 7)}
 
@@ -822,19 +824,19 @@ def main():
             cpu = cpu_reference(seqs, model, type_, 0, 1)
             line["cpu_baseline"] = ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
                                     if cpu else None)
-        # the batched and served forms are single-GPU (replicas at N > 1)
-        if args.mode in ("all", "batched") and world == 1:
-            line["batched"] = run_batched(args, local_rank)
-        if args.mode in ("all", "served") and world == 1:
-            line["served"] = run_served(args, local_rank)
-        if args.mode in ("all", "bootstrap") and world == 1:
-            line["bootstrap"] = run_bootstrap(args, local_rank)
-        if args.mode in ("all", "parse") and world == 1:
-            line["parse"] = run_parse(args, local_rank)
-        if args.mode in ("all", "text") and world == 1:
-            line["text"] = run_text(args, local_rank)
-        if args.mode in ("all", "njinit") and world == 1:
-            line["nj_init"] = run_nj_init(args, local_rank, n=args.nj_n, L=args.nj_n)
+        # the batched and served forms are single-GPU (replicas at N > 1); an
+        # extra figure that fails is reported as such, the line still printed
+        extras = (("batched", run_batched), ("served", run_served),
+                  ("bootstrap", run_bootstrap), ("parse", run_parse), ("text", run_text),
+                  ("nj_init", lambda a, r: run_nj_init(a, r, n=a.nj_n, L=a.nj_n)))
+        modes = {"batched": "batched", "served": "served", "bootstrap": "bootstrap",
+                 "parse": "parse", "text": "text", "nj_init": "njinit"}
+        for key, fn in extras:
+            if args.mode in ("all", modes[key]) and world == 1:
+                try:
+                    line[key] = fn(args, local_rank)
+                except Exception as e:  # noqa: BLE001
+                    line[key] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist
