@@ -30,6 +30,7 @@
 // are parsed by rnj_io.cpp's reader from the same bytes and copied to the
 // device, so that every input gives the host reader's result.
 #include <cuda_runtime.h>
+#include <errno.h>
 #include <fcntl.h>
 #include <stdint.h>
 #include <sys/stat.h>
@@ -401,6 +402,7 @@ int read_pinned(rnj_ctx *ctx, const char *path, size_t S, uint8_t *d_raw) {
       const size_t a0 = a, b = std::min(S, a + kReadChunk);
       while (a < b) {
         const ssize_t r = pread(fd, ctx->h_file + a, b - a, (off_t)a);
+        if (r < 0 && errno == EINTR) continue;
         if (r <= 0) {
           ok[k] = 0;
           return;
