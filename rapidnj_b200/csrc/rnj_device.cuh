@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "rnj_logtab.h"
+
 namespace rnj {
 
 // ------------------------------------------------------------------ PTX helpers
@@ -85,7 +87,40 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
 // Each transform restates the reference's float/double arithmetic operation by
 // operation with explicitly rounded intrinsics, so that no multiply-add is
 // contracted (the reference is compiled for SSE2 without FMA).  The logarithm
-// is CUDA's double log().
+// is CUDA's double log(), except on the K2P fast path (ln_table, below), whose
+// result is only used where a rounding check with a proven error bound decides.
+
+// ln(x) for x in [2^-1022, 1] by Tang's table-driven method (ACM TOMS 16(4),
+// 1990): x = 2^k m, m in [1, 2); F = 1 + j/128 with j the top 7 bits of m's
+// fraction, so f = m - F is exact and in [0, 2^-7); r = f * (1/F) (table);
+// ln x = k ln 2 + ln F + ln(1 + r), the last by its series to r^6.  Error:
+//   series remainder        |r|^7 / 7 < 2^-51.8
+//   r against f / F         <= 2^-52 |f / F| < 2^-59   (so is ln(1 + r) against ln(1 + f/F))
+//   series arithmetic       < 2^-58 (terms below 2^-7, each fma rounded once)
+//   ln F from the table     <= 2^-54 (nearest double, ln F < 1)
+//   k ln 2                  k * kLn2Hi exact (42-bit kLn2Hi, |k| < 2^11), k * kLn2Lo
+//                           and the table sum rounded: < 2^-52
+//   final fma               <= 2^-53 |ln x|
+// so |ln_table(x) - ln x| < 2^-50.5 + 2^-53 |ln x|.
+__device__ __forceinline__ double ln_table(double x) {
+  const long long bits = __double_as_longlong(x);
+  const int k = (int)((bits >> 52) & 0x7FF) - 1023;
+  const int j = (int)((bits >> 45) & 127);
+  const double m = __longlong_as_double((bits & 0x000FFFFFFFFFFFFFLL) | 0x3FF0000000000000LL);
+  const double F = __longlong_as_double(0x3FF0000000000000LL | ((long long)j << 45));
+  const double lnF = __ldg(&c_log_tab[j][0]);
+  const double inv = __ldg(&c_log_tab[j][1]);
+  const double r = __dmul_rn(__dsub_rn(m, F), inv);
+  double p = -1.0 / 6.0;
+  p = __fma_rn(p, r, 0.2);
+  p = __fma_rn(p, r, -0.25);
+  p = __fma_rn(p, r, 1.0 / 3.0);
+  p = __fma_rn(p, r, -0.5);
+  p = __fma_rn(p, r, 1.0);
+  p = __dmul_rn(p, r);
+  const double dk = (double)k;
+  return __fma_rn(dk, kLn2Hi, __dadd_rn(__fma_rn(dk, kLn2Lo, lnF), p));
+}
 
 // Valid-site count as the fast protein estimator reports it for L % 128 == 0
 // (bitDistanceProtein.cpp:15-16,59): padded length minus the gaps counted over
@@ -139,18 +174,20 @@ __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
   // a, b in (0, 1], so D >= 0 and 0.5|log a| + 0.25|log b| = D.
   //   reference  d_ref = (-0.5 log a) - (0.25 log b), each log within 1 ulp,
   //              one rounded subtraction:   |d_ref - D| <= 1.5 * 2^-52 * D
-  //   this path  dd = -0.25 log(fl(fl(a a) b)): the product is within 2^-52
-  //              (relative) of a^2 b, so its log within 2^-52 + 1 ulp:
-  //                                          |dd - D| <= 2^-54 + 2^-52 * D
-  // so |dd - d_ref| <= 2^-52 (0.25 + 2.5 D) < eps = 2^-50 (1 + 4 dd).  (a^2 b
+  //   this path  dd = -0.25 ln_table(fl(fl(a a) b)): the product is within
+  //              2^-52 (relative) of a^2 b, so its log within 2^-52 of log(a^2 b);
+  //              ln_table adds < 2^-50.5 + 2^-53 |log x| (its comment), and the
+  //              scaling by -0.25 is exact:
+  //                                  |dd - D| < 2^-52.5 + 2^-54 + 2^-53 (D + ...)
+  // so |dd - d_ref| < 2^-51.9 + 2^-50.4 D < eps = 2^-49 (1 + 4 dd).  (a^2 b
   // stays far from the double underflow range: a, b >= 2^-46 when positive.)
   // If dd - eps and dd + eps round to the same float, so does every value
   // between them (rounding is monotone), d_ref included: the float result is
   // the reference's.  Otherwise -- about one pair in 10^7 -- the reference's
-  // own two-logarithm formula decides.
+  // own two-logarithm formula decides (with CUDA's log).
   const double x = __dmul_rn(__dmul_rn(a, a), b);
-  const double dd = __dmul_rn(-0.25, log(x));
-  const double eps = __dmul_rn(0x1p-50, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
+  const double dd = __dmul_rn(-0.25, ln_table(x));
+  const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
   const float lo = __double2float_rn(__dsub_rn(dd, eps));
   const float hi = __double2float_rn(__dadd_rn(dd, eps));
   if (__float_as_int(lo) == __float_as_int(hi)) return lo;

@@ -1,5 +1,5 @@
 """The one-logarithm fast path of the device K2P transform (rnj_device.cuh,
-k2p_distance), restated in numpy with the host's log, checked against the
+k2p_distance), restated in numpy with its table logarithm, checked against the
 reference's two-logarithm arithmetic (KimuraDistance.cpp:339-349, as the oracle
 computes it): whenever the fast path's rounding check accepts, its float must
 be the reference's float.  This pins the error bound the check relies on; the
@@ -23,15 +23,56 @@ def reference_k2p(P, Q, n):
     return np.where(ok, d, np.float32(-1.0)), a, b, ok
 
 
+def _log_table():
+    """The table of rnj_logtab.h (its header, generated by gen_log_table.py)."""
+    import os
+    import re
+    path = os.path.join(os.path.dirname(__file__), "..", "rapidnj_b200", "csrc", "rnj_logtab.h")
+    text = open(path).read()
+    rows = re.findall(r"\{(-?0x[0-9a-fp.+-]+), (0x[0-9a-fp.+-]+)\}", text)
+    tab = np.array([[float.fromhex(a), float.fromhex(b)] for a, b in rows])
+    hi = float.fromhex(re.search(r"kLn2Hi = (\S+);", text).group(1))
+    lo = float.fromhex(re.search(r"kLn2Lo = (\S+);", text).group(1))
+    return tab, hi, lo
+
+
+def ln_table(x):
+    """rnj_device.cuh ln_table in numpy (each fused multiply-add done as a multiply
+    and an add: two roundings, within the same error bound)."""
+    tab, hi, lo = _log_table()
+    bits = x.view(np.int64)
+    k = ((bits >> 52) & 0x7FF) - 1023
+    j = (bits >> 45) & 127
+    m = ((bits & 0x000FFFFFFFFFFFFF) | 0x3FF0000000000000).view(np.float64)
+    F = (0x3FF0000000000000 | (j << 45)).view(np.float64)
+    r = (m - F) * tab[j, 1]
+    p = np.full_like(r, -1.0 / 6.0)
+    for c in (0.2, -0.25, 1.0 / 3.0, -0.5, 1.0):
+        p = p * r + c
+    p = p * r
+    dk = k.astype(np.float64)
+    return dk * hi + ((dk * lo + tab[j, 0]) + p)
+
+
 def fast_k2p(a, b):
     """The device fast path: (accepted, float)."""
     with np.errstate(divide="ignore", invalid="ignore"):
         x = (a * a) * b
-        dd = -0.25 * np.log(x)
-        eps = 2.0 ** -50 * (1.0 + 4.0 * dd)
+        dd = -0.25 * ln_table(x)
+        eps = 2.0 ** -49 * (1.0 + 4.0 * dd)
         lo = (dd - eps).astype(np.float32)
         hi = (dd + eps).astype(np.float32)
     return lo.view(np.int32) == hi.view(np.int32), lo
+
+
+def test_ln_table_error_bound():
+    # |ln_table(x) - ln x| < 2^-50.5 + 2^-53 |ln x| over x in [2^-138, 1]
+    rng = np.random.default_rng(1)
+    x = np.exp2(-rng.random(2_000_000) * 138.0)
+    x = np.concatenate([x, 1.0 - rng.random(200_000) * 2.0 ** -7, [1.0, 0.5, 2.0 ** -138]])
+    err = np.abs(ln_table(x) - np.log(x))
+    bound = 2.0 ** -50.5 + 2.0 ** -53 * np.abs(np.log(x)) + 2.0 ** -52 * np.abs(np.log(x))
+    assert (err <= bound).all()  # np.log itself within 1 ulp: the last term
 
 
 @pytest.mark.parametrize("n", [7, 100, 997, 1000, 2048])
