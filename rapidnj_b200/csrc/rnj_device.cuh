@@ -132,6 +132,21 @@ __device__ __forceinline__ unsigned long long protein_fast_valid(unsigned long l
   return (unsigned long long)(padded - gaps_total);
 }
 
+// The float nearest to -c ln(arg), arg in (0, 1], c in {0.75, 0.95, 1}, when
+// the table logarithm decides it; else NaN.  The reference evaluates
+// (float)(-c log(arg)) in double (log within 1 ulp, one rounded product):
+// |d_ref - D| <= 1.5 * 2^-52 D for D = -c ln(arg) >= 0.  Here dd = fl(-c
+// ln_table(arg)) with |dd - D| < 2^-50.5 + 2^-52 D (ln_table's bound, c <= 1),
+// so |dd - d_ref| < eps = 2^-49 (1 + 4 dd) and, as on the K2P fast path, if
+// dd - eps and dd + eps round to the same float so does d_ref.
+__device__ __forceinline__ float neg_log_checked(double c, double arg) {
+  const double dd = __dmul_rn(-c, ln_table(arg));
+  const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
+  const float lo = __double2float_rn(__dsub_rn(dd, eps));
+  const float hi = __double2float_rn(__dadd_rn(dd, eps));
+  return __float_as_int(lo) == __float_as_int(hi) ? lo : __int_as_float(0x7fc00000);
+}
+
 // JCdistance.cpp:171-183.  b = (alpha - 1) / alpha in double, alpha 4 or 20.
 __device__ __forceinline__ float jc_distance(unsigned long long total,
                                              unsigned long long valid, double b) {
@@ -140,7 +155,11 @@ __device__ __forceinline__ float jc_distance(unsigned long long total,
   else distance = __fdiv_rn(__ll2float_rn((long long)total), __ull2float_rn(valid));
   const double q = __ddiv_rn((double)distance, b);
   if (q >= 1.0) return -1.0f;
-  return __double2float_rn(__dmul_rn(-b, log(__dsub_rn(1.0, q))));
+  const double arg = __dsub_rn(1.0, q);
+  if (arg == 1.0) return __double2float_rn(__dmul_rn(-b, 0.0));  // -0.0, as the reference
+  const float fast = neg_log_checked(b, arg);
+  if (fast == fast) return fast;
+  return __double2float_rn(__dmul_rn(-b, log(arg)));
 }
 
 // KimuraDistance.cpp:339-349.
@@ -205,7 +224,8 @@ __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism
     if (dd > 0.0) {
       const double sq = (double)__fmul_rn(distance, distance);
       const double arg = __dsub_rn(__dsub_rn(1.0, dd), __dmul_rn(sq, 0.20));
-      distance = __double2float_rn(-log(arg));
+      const float fast = neg_log_checked(1.0, arg);
+      distance = fast == fast ? fast : __double2float_rn(-log(arg));
     }
   } else {
     if (dd > 0.930) {

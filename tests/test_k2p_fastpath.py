@@ -113,3 +113,46 @@ def test_fast_path_matches_oracle_transform():
     assert np.array_equal(want.view(np.int32), ref.view(np.int32))
     acc, got = fast_k2p(a[ok], b[ok])
     assert np.array_equal(got[acc].view(np.int32), ref[ok][acc].view(np.int32))
+
+
+def neg_log_checked(c, arg):
+    """rnj_device.cuh neg_log_checked in numpy: (accepted, float)."""
+    dd = -c * ln_table(arg)
+    eps = 2.0 ** -49 * (1.0 + 4.0 * dd)
+    lo = (dd - eps).astype(np.float32)
+    hi = (dd + eps).astype(np.float32)
+    return lo.view(np.int32) == hi.view(np.int32), lo
+
+
+@pytest.mark.parametrize("n", [1, 7, 100, 997, 10000, 65536])
+@pytest.mark.parametrize("alpha", [4, 20])
+def test_jc_checked_log_agrees_with_reference(n, alpha):
+    # JCdistance.cpp:171-183: p = (float) total / valid, q = p / b in double,
+    # (float)(-b log(1 - q)) unless q >= 1
+    b = (alpha - 1.0) / alpha
+    total = np.arange(n + 1)
+    p = (total.astype(np.float32) / np.float32(n)).astype(np.float32)
+    q = p.astype(np.float64) / b
+    keep = (q < 1.0) & (q > 0.0)
+    arg = 1.0 - q[keep]
+    ref = (-b * np.log(arg)).astype(np.float32)
+    acc, got = neg_log_checked(b, arg)
+    assert np.array_equal(got[acc].view(np.int32), ref[acc].view(np.int32))
+    if acc.size:  # n = 1 leaves no pair with 0 < q < 1
+        assert (~acc).mean() < 1e-3
+
+
+def test_protein_kimura_checked_log_agrees_with_reference():
+    # KimuraDistance.cpp:322-338, p < 0.75: (float)(-log(1 - p - (float)(p*p) * 0.2))
+    rng = np.random.default_rng(3)
+    v = rng.integers(1, 200_000, size=3_000_000)
+    m = (rng.random(v.size) * 0.75 * v).astype(np.int64)
+    p = (m.astype(np.float32) / v.astype(np.float32)).astype(np.float32)
+    keep = (p > 0) & (p.astype(np.float64) < 0.75)
+    p = p[keep]
+    sq = (p * p).astype(np.float32).astype(np.float64)
+    arg = (1.0 - p.astype(np.float64)) - sq * 0.2
+    ref = (-np.log(arg)).astype(np.float32)
+    acc, got = neg_log_checked(1.0, arg)
+    assert np.array_equal(got[acc].view(np.int32), ref[acc].view(np.int32))
+    assert (~acc).mean() < 1e-5
