@@ -783,12 +783,18 @@ __global__ void __launch_bounds__(kTransformThreads, kTransformCtasPerSm)
 #pragma unroll 1
       for (int k0 = 0; k0 < 32; k0 += 4) {
         float x[4];
+        // The four packed counts first: the mirror stores below go through a
+        // pointer the compiler cannot tell apart from src, so loads written
+        // after a store would wait for it.
+        uint64_t pk[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pk[u] = src[(size_t)(cb + k0 + u) * kTile];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int c = cb + k0 + u;
           const int j = j0 + c;
           uint32_t ts, tv, vv;
-          unpack_counts(src[(size_t)c * kTile], ts, tv, vv);
+          unpack_counts(pk[u], ts, tv, vv);
           x[u] = 0.0f;
           if (i < j && j < n) {
             x[u] = pair_distance(ep, ts, tv, vv);
