@@ -92,6 +92,23 @@ int rnj_ctx_destroy(rnj_ctx *ctx);
 int rnj_ctx_stream(rnj_ctx *ctx, void **stream);
 int rnj_ctx_synchronize(rnj_ctx *ctx);
 
+/* Every pipeline wait in the counting kernels (a warp waiting for a copy into
+ * shared memory, for the tensor cores, or for tensor memory to be read) is
+ * bounded: when it runs out, the kernel stops, lets its own copies land, frees
+ * its tensor memory and sets the context's device error word, and the next call
+ * that waits for the GPU (rnj_ctx_synchronize, any call returning a maximum)
+ * returns RNJ_ERR_TIMEOUT and clears the word.  rnj_set_wait_limit sets that
+ * bound for kernels launched from now on in this process, in microseconds
+ * (0: the default, 2 seconds).  No counterpart in the reference, which has no
+ * device code in its build. */
+int rnj_set_wait_limit(unsigned int microseconds);
+/* For tests of that failure path: while `on` is non-zero, the consumer warps of
+ * the single-alignment counting kernels first wait on a barrier that nothing
+ * completes, so that their bounded wait runs out (after the wait limit) and the
+ * call reports RNJ_ERR_TIMEOUT; nothing faults or hangs, and the context stays
+ * usable.  Off by default. */
+int rnj_test_wait_on_unset_flag(int on);
+
 /* Stage timing: when on, the library records CUDA events around its kernels
  * (pack, count, transform/fix-up) on the context's stream;
  * rnj_ctx_stage_times() synchronises and returns the last call's milliseconds
@@ -149,7 +166,9 @@ int rnj_aln_destroy(rnj_aln *aln);
 int rnj_distance(rnj_ctx *ctx, rnj_aln *aln, int model, rnj_mat **out);
 /* Same into a caller-owned device buffer of n rows with stride ld (floats).
  * max_out (host, may be NULL) receives the maximum distance; reading it
- * synchronises the context's stream. */
+ * synchronises the context's stream and reports a device timeout.  With
+ * max_out NULL the call returns without waiting for the GPU: a timeout is then
+ * reported by the next call on the context that waits (rnj_ctx_synchronize). */
 int rnj_distance_into(rnj_ctx *ctx, rnj_aln *aln, int model, float *d_out, size_t ld,
                       float *max_out);
 /* Raw per-pair counts, the DistanceEstimate::computeDistance contract
@@ -186,8 +205,11 @@ int rnj_mat_destroy(rnj_mat *mat);
  * The first call on a device looks up the array's device address and loads
  * the kernels the entry point launches (under CUDA's lazy module loading a
  * kernel's first launch would otherwise take device memory for its code); make
- * it before any stream capture.  max_out (host, may be NULL) receives the maximum
- * distance and synchronises the stream. */
+ * it before any stream capture.  The call returns once the GPU has finished its
+ * work (it synchronises `stream`), so that a device timeout is reported in its
+ * return value (RNJ_ERR_TIMEOUT) whether or not max_out is given; on a stream
+ * that is being captured it returns RNJ_ERR_UNSUPPORTED before doing anything.
+ * max_out (host, may be NULL) receives the maximum distance. */
 int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld, int type, int model,
                          int flags, float *d_out, size_t ld_out, void *stream, float *max_out);
 

@@ -32,17 +32,25 @@ JC, KIMURA = 0, 1
 _lib = None
 
 
+def reference_tree() -> str | None:
+    """The rapidNJ source tree the harnesses are compiled from: $RNJ_REFERENCE, else a
+    ``reference`` folder beside this repository; None when neither exists."""
+    env = os.environ.get("RNJ_REFERENCE")
+    if env:
+        return env if os.path.isdir(env) else None
+    beside = os.path.abspath(os.path.join(HERE, "..", "..", "reference"))
+    return beside if os.path.isdir(os.path.join(beside, "src")) else None
+
+
 def build() -> None:
     """Compile liborc.so (and the reference harness when the reference tree is
     present)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if os.path.isdir(os.environ.get("RNJ_REFERENCE", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref",
-                        "REF=" + os.environ.get("RNJ_REFERENCE", "/root/reference")], check=True)
+    ref = reference_tree()
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + ref], check=True)
         if os.path.exists(os.path.join(HERE, "..", "rapidnj_b200", "librnjgpu.so")):
-            subprocess.run(["make", "-s", "-C", HERE, "dropin",
-                            "REF=" + os.environ.get("RNJ_REFERENCE", "/root/reference")],
-                           check=True)
+            subprocess.run(["make", "-s", "-C", HERE, "dropin", "REF=" + ref], check=True)
 
 
 def lib():
@@ -56,6 +64,10 @@ def lib():
         L.orc_counts.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                  ctypes.c_int, ctypes.c_int, u32p]
         L.orc_counts.restype = None
+        L.orc_counts_rows.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_void_p]
+        L.orc_counts_rows.restype = None
         L.orc_matrix.argtypes = [u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                  ctypes.c_int, ctypes.c_int, f32p]
         L.orc_matrix.restype = ctypes.c_float
@@ -86,13 +98,29 @@ def detect_type(seqs: np.ndarray) -> int:
     return lib().orc_detect_type(row.tobytes(), row.size)
 
 
-def counts(seqs: np.ndarray, type_: int, naive: bool = False, full: bool = False) -> np.ndarray:
+def counts(seqs: np.ndarray, type_: int, naive: bool = False, full: bool = False,
+           threads: int = 1) -> np.ndarray:
     """(n, n, 3) uint32: {ts, tv, valid} (DNA) or {mismatch, 0, valid} (protein)
-    for j > i (every pair when ``full``)."""
+    for j > i (every pair when ``full``).  ``threads`` > 1 splits the rows into
+    ranges of equal pair count, one host thread each (the C calls release the GIL)."""
     s = np.ascontiguousarray(seqs, dtype=np.uint8)
     n, L = s.shape
     out = np.zeros((n, n, 3), dtype=np.uint32)
-    lib().orc_counts(s.tobytes(), n, L, type_, int(naive), int(full), out.reshape(-1))
+    if threads <= 1 or n < 4:
+        lib().orc_counts(s.tobytes(), n, L, type_, int(naive), int(full), out.reshape(-1))
+        return out
+    from concurrent.futures import ThreadPoolExecutor
+    raw = s.tobytes()
+    # row i holds n - 1 - i pairs (n with ``full``): cut at equal cumulative work
+    work = np.full(n, n, np.float64) if full else np.arange(n - 1, -1, -1, dtype=np.float64)
+    cum = np.concatenate([[0.0], np.cumsum(work)])
+    cuts = [int(np.searchsorted(cum, cum[-1] * k / threads)) for k in range(threads + 1)]
+    cuts[0], cuts[-1] = 0, n
+    ptr = out.ctypes.data
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda k: lib().orc_counts_rows(raw, n, L, type_, int(naive), int(full),
+                                                    cuts[k], cuts[k + 1], ptr)
+                    if cuts[k + 1] > cuts[k] else None, range(threads)))
     return out
 
 

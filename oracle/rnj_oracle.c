@@ -166,7 +166,13 @@ void orc_pair_counts(const char *a, const char *b, int L, int type, int naive,
 
 void orc_counts(const char *seqs, int n, int L, int type, int naive, int full,
                 uint32_t *out) {
-  for (int i = 0; i < n; i++) {
+  orc_counts_rows(seqs, n, L, type, naive, full, 0, n, out);
+}
+
+/* Rows [row0, row1) of orc_counts (several host threads can each take a range). */
+void orc_counts_rows(const char *seqs, int n, int L, int type, int naive, int full, int row0,
+                     int row1, uint32_t *out) {
+  for (int i = row0; i < row1; i++) {
     for (int j = full ? 0 : i + 1; j < n; j++) {
       uint64_t c[3];
       orc_pair_counts(seqs + (size_t)i * L, seqs + (size_t)j * L, L, type, naive, c);

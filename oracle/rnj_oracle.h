@@ -19,6 +19,8 @@ uint64_t orc_protein_fast_valid(uint64_t valid, int L);
 void orc_pair_counts(const char *a, const char *b, int L, int type, int naive, uint64_t out[3]);
 /* seqs: n*L bytes row-major.  out: n*n*3 uint32, filled for j>i (or every j when full). */
 void orc_counts(const char *seqs, int n, int L, int type, int naive, int full, uint32_t *out);
+void orc_counts_rows(const char *seqs, int n, int L, int type, int naive, int full, int row0,
+                     int row1, uint32_t *out);
 
 float orc_jc(uint64_t c0, uint64_t c1, uint64_t valid, int type);
 float orc_k2p(uint64_t ts, uint64_t tv, uint64_t valid);

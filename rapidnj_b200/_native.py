@@ -16,6 +16,8 @@ RNJ_OK = 0
 RNJ_DNA, RNJ_PROTEIN, RNJ_UNKNOWN = 0, 1, 2
 RNJ_JC, RNJ_KIMURA = 0, 1
 RNJ_FASTDIST, RNJ_COMPAT_PROTEIN_WRAP, RNJ_FULL_ROWS, RNJ_POPCOUNT = 1, 2, 4, 8
+(RNJ_ERR_INVALID, RNJ_ERR_CUDA, RNJ_ERR_NOMEM, RNJ_ERR_IO, RNJ_ERR_FORMAT, RNJ_ERR_TIMEOUT,
+ RNJ_ERR_BUSY, RNJ_ERR_UNSUPPORTED, RNJ_ERR_NOTREADY) = range(1, 10)
 
 STATUS_NAMES = {
     0: "RNJ_OK", 1: "RNJ_ERR_INVALID", 2: "RNJ_ERR_CUDA", 3: "RNJ_ERR_NOMEM", 4: "RNJ_ERR_IO",
@@ -44,6 +46,8 @@ SIGNATURES = {
     "rnj_ctx_destroy": (c_int, [c_void_p]),
     "rnj_ctx_stream": (c_int, [c_void_p, P(c_void_p)]),
     "rnj_ctx_synchronize": (c_int, [c_void_p]),
+    "rnj_set_wait_limit": (c_int, [ctypes.c_uint]),
+    "rnj_test_wait_on_unset_flag": (c_int, [c_int]),
     "rnj_detect_type": (c_int, [c_char_p, c_int]),
     "rnj_ctx_set_profiling": (c_int, [c_void_p, c_int]),
     "rnj_ctx_stage_times": (c_int, [c_void_p, P(c_float)]),

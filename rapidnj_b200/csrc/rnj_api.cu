@@ -7,6 +7,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -124,8 +125,19 @@ void dna_lut(bool naive, uint8_t lut[256]) {
 }
 
 // Transform parameters of a packed alignment (scratch pointers left null).
+namespace {
+std::atomic<uint32_t> g_wait_us{0};
+std::atomic<int> g_wait_stall{0};
+}  // namespace
+
+void apply_wait_settings(EpiParams &ep) {
+  ep.wait_us = g_wait_us.load(std::memory_order_relaxed);
+  ep.stall = g_wait_stall.load(std::memory_order_relaxed);
+}
+
 EpiParams epi_params_for(const Packed &p, int model) {
   EpiParams ep;
+  apply_wait_settings(ep);
   ep.n = p.n;
   ep.L = p.L;
   ep.model = model;
@@ -158,6 +170,8 @@ AlnDesc desc_for(const Packed &p, const EpiParams &ep) {
   d.full = ep.full;
   d.kind = p.kind;
   d.np = is_tc_kind(p.kind) ? p.nfb : p.NP;
+  d.wait_us = (int)ep.wait_us;
+  d.stall = ep.stall;
   d.jc_b = ep.jc_b;
   return d;
 }
@@ -393,10 +407,23 @@ int count_kind_for(const Packed &p, int model) {
 EpiParams epi_for(rnj_ctx *ctx, const Packed &p, int model) {
   EpiParams ep = epi_params_for(p, model);
   ep.max_bits = ctx->scratch.words;
-  ep.err = ctx->scratch.words + 1;
+  ep.err = ctx->d_err;
   ep.tile_flags = ctx->scratch.words + 2;
   return ep;
 }
+
+}  // namespace
+
+// The error word copied to h_max[1] by a finished stream: RNJ_ERR_TIMEOUT (and
+// the device word cleared) when a bounded wait ran out.
+int take_device_error(rnj_ctx *ctx) {
+  if (ctx->h_max[1] == 0) return RNJ_OK;
+  ctx->h_max[1] = 0;
+  cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
+  return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out (pipeline stage lost)");
+}
+
+namespace {
 
 // One alignment through the persistent tensor-core kernel: its triangle tiles
 // are the work list, one CTA per SM.  Distances go through the packed counts
@@ -424,18 +451,15 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
                        tp.transform_ctas);
 }
 
+// Waits for the context's stream and reports (and clears) the sticky device
+// error word: a timeout of any earlier call on this context, including calls
+// that returned without waiting.
 int check_device_error(rnj_ctx *ctx) {
-  if (!ctx->scratch.words) {  // no single-call distance ran on this context yet
-    RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "distance sync");
-    return RNJ_OK;
-  }
-  RNJ_CUDA(cudaMemcpyAsync(ctx->h_max + 1, ctx->scratch.words + 1, sizeof(int),
-                           cudaMemcpyDeviceToHost, ctx->stream),
+  RNJ_CUDA(cudaMemcpyAsync(ctx->h_max + 1, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream),
            "error word copy");
   RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "distance sync");
-  if (ctx->h_max[1] != 0)
-    return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out (pipeline stage lost)");
-  return RNJ_OK;
+  return take_device_error(ctx);
 }
 
 int run_popcount(rnj_ctx *ctx, const Packed &p, int ckind, int nk, int nt, EpiParams &ep);
@@ -581,6 +605,9 @@ int rnj_ctx_create(int device, rnj_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_mask, 8 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_mask, 8 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_max, 4 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) memset(c->h_max, 0, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_desc, sizeof(AlnDesc));
   if (e != cudaSuccess) {
     rnj_ctx_destroy(c);
@@ -609,6 +636,7 @@ int rnj_ctx_destroy(rnj_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->scratch.words) cudaFree(ctx->scratch.words);
   if (ctx->d_mask) cudaFree(ctx->d_mask);
+  if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->d_desc) cudaFree(ctx->d_desc);
   if (ctx->d_packed) cudaFree(ctx->d_packed);
   if (ctx->h_mask) cudaFreeHost(ctx->h_mask);
@@ -660,11 +688,20 @@ int rnj_ctx_stage_times(rnj_ctx *ctx, float *ms) {
   return RNJ_OK;
 }
 
+int rnj_set_wait_limit(unsigned int microseconds) {
+  g_wait_us.store(microseconds, std::memory_order_relaxed);
+  return RNJ_OK;
+}
+
+int rnj_test_wait_on_unset_flag(int on) {
+  g_wait_stall.store(on ? 1 : 0, std::memory_order_relaxed);
+  return RNJ_OK;
+}
+
 int rnj_ctx_synchronize(rnj_ctx *ctx) {
   if (!ctx) return set_error(RNJ_ERR_INVALID, "null context");
   DeviceGuard g(ctx->device);
-  RNJ_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
-  return RNJ_OK;
+  return check_device_error(ctx);
 }
 
 int rnj_detect_type(const char *seq0, int L) {

@@ -49,18 +49,25 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   return t;
 }
 
-// A wait on an mbarrier phase that gives up after kWaitLimitNs of wall time (or
-// an iteration cap), so that a lost transfer turns into an error status instead
-// of a hung GPU.
+// A wait on an mbarrier phase that gives up after limit_ns of wall time (or an
+// iteration cap), so that a lost transfer turns into an error status instead of
+// a hung GPU.  Pipeline waits take the limit the host chose (rnj_set_wait_limit,
+// wait_limit_ns below); the drains that let a CTA's own copies land before it
+// exits always allow the full default.
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 constexpr uint32_t kWaitIterCap = 1u << 26;
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ uint64_t wait_limit_ns(uint32_t us) {
+  return us ? (uint64_t)us * 1000ull : kWaitLimitNs;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 0; it < kWaitIterCap; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 255u && global_timer_ns() - t0 > kWaitLimitNs) break;
+    if ((it & 255u) == 255u && global_timer_ns() - t0 > limit_ns) break;
   }
   return false;
 }

@@ -89,6 +89,8 @@ struct EpiParams {
   int *tile_flags = nullptr;  // per tile: 1 if it holds a saturated (-1) entry
   uint32_t *counts = nullptr; // n*n*3 counts (count-output and split modes)
   int *err = nullptr;         // device error word (bit 0: a bounded wait ran out)
+  uint32_t wait_us = 0;       // bound of the pipeline waits in microseconds (0: 2 s)
+  int stall = 0;              // test of the failure path: wait on a barrier nothing completes
 };
 
 // One alignment of a work list, as the persistent kernels read it from device
@@ -103,8 +105,10 @@ struct alignas(128) AlnDesc {
   int *err;                   // shared error word
   int n, L, nt, kdim;         // kdim: Lk columns (tensor-core) or Wp words (popcount)
   int model, type, compat, full;
-  int kind, np, band, pad1;    // np: planes, or feature blocks (tensor-core kinds);
-                               // band: tile-order band height (single alignment), 0 = 12
+  int kind, np, band, wait_us; // np: planes, or feature blocks (tensor-core kinds);
+                               // band: tile-order band height (single alignment), 0 = 12;
+                               // wait_us: bound of the pipeline waits (0: 2 s)
+  int stall, pad2;             // stall: as EpiParams::stall
   double jc_b;
 };
 
@@ -194,6 +198,9 @@ cudaError_t launch_count_batch(const AlnDesc *d_descs, const WorkItem *d_items, 
 cudaError_t launch_fixup_batch(const AlnDesc *d_descs, const WorkItem *items_a, const int *n_a,
                                const WorkItem *items_b, const int *n_b, int grid, cudaStream_t s);
 // Host helpers shared by the single and batched paths (rnj_api.cu).
+// The process-wide wait settings (rnj_set_wait_limit, rnj_test_wait_on_unset_flag)
+// copied into a kernel's parameters.
+void apply_wait_settings(EpiParams &ep);
 EpiParams epi_params_for(const Packed &p, int model);
 AlnDesc desc_for(const Packed &p, const EpiParams &ep);
 // Persistent over work items [item0, min(n, item0 + count)); d_items == nullptr

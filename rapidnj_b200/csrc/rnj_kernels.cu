@@ -283,9 +283,11 @@ template <>
 struct KT<KIND_MISM5> { static constexpr int NP = 6, NC = 2, ST = 3; };
 template <>
 struct KT<KIND_MISM7> { static constexpr int NP = 8, NC = 2, ST = 3; };
+static_assert(8 * (4 + 1) <= 64, "the barriers of count_tiles_kernel fit its 64 bytes");
 
 template <int KIND>
 constexpr size_t count_smem_bytes() {
+  // stages, alignment slack, ST + 1 barriers
   return (size_t)KT<KIND>::ST * 2 * KT<KIND>::NP * kKW * kTile * 4 + 1024 + 64;
 }
 
@@ -349,13 +351,16 @@ __global__ void __launch_bounds__(256, 1)
   const int nks = min(nk, kc0 + kchunk) - kc0;
 
   const int tid = threadIdx.x;
+  // full_bar[ST]: a barrier that nothing completes, waited on only by the test
+  // of the failure path (ep.stall).
   if (tid == 0) {
 #pragma unroll
-    for (int s = 0; s < ST; ++s) mbar_init(&full_bar[s], 1);
+    for (int s = 0; s <= ST; ++s) mbar_init(&full_bar[s], 1);
     fence_mbar_init();
     prefetch_tmap(&tmap);
   }
   __syncthreads();
+  const uint64_t limit = wait_limit_ns(ep.wait_us);
 
   auto issue = [&](int k) {
     const int s = k % ST;
@@ -386,7 +391,8 @@ __global__ void __launch_bounds__(256, 1)
   for (int k = 0; k < nks; ++k) {
     if (tid == 0 && issued < nks) issue(issued++);
     const int s = k % ST;
-    const bool ok = mbar_wait_bounded(&full_bar[s], (uint32_t)((k / ST) & 1));
+    bool ok = !(ep.stall && k == 0) || mbar_wait_bounded(&full_bar[ST], 0, limit);
+    if (ok) ok = mbar_wait_bounded(&full_bar[s], (uint32_t)((k / ST) & 1), limit);
     if (ok) {
       const uint32_t *A = smem + s * 2 * TILE_WORDS;
       const uint32_t *B = A + TILE_WORDS;
@@ -599,7 +605,7 @@ __device__ __forceinline__ bool batch_tile(const AlnDesc &d, int tile, uint32_t 
     if (tid == 0 && issued < nks) issue(issued++);
     const uint32_t g = gk + (uint32_t)k;
     const int s = g % kBatchST;
-    const bool ok = mbar_wait_bounded(&full_bar[s], (g / kBatchST) & 1);
+    const bool ok = mbar_wait_bounded(&full_bar[s], (g / kBatchST) & 1, wait_limit_ns(d.wait_us));
     if (ok) {
       const uint32_t *A = smem + s * RING_WORDS;
       const uint32_t *B = A + TILE_WORDS;

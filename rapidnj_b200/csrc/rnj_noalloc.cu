@@ -2,9 +2,9 @@
 //
 // Some hosts of this library own every byte of device memory themselves: a
 // process that runs under a fixed memory budget with its own pool (an inference
-// or database server that reserves the GPU up front), code inside a CUDA graph
-// being built by someone else, or an embedding where cudaMalloc is forbidden
-// because it synchronises the device.  rnj_distance_noalloc serves them: it runs
+// or database server that reserves the GPU up front), or an embedding where
+// cudaMalloc is forbidden because it synchronises the device.
+// rnj_distance_noalloc serves them: it runs
 // the same pack -> count -> fix-up kernels as rnj_distance_into, on the caller's
 // stream, with every intermediate buffer (the packed bit planes, the running
 // maximum, the error word and the per-tile saturation flags) placed in one
@@ -28,6 +28,11 @@
 //     address) and loads the kernels the entry point launches, so that no later
 //     call takes device memory for kernel code.  Make that first call before any
 //     stream capture begins.
+//   * Every call waits for its work on the caller's stream to finish, then reads
+//     the array's error word, so that a bounded device wait that ran out is
+//     returned as RNJ_ERR_TIMEOUT whether or not the caller asked for the
+//     maximum.  On a stream that is being captured the call returns
+//     RNJ_ERR_UNSUPPORTED before it touches the stream.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -94,6 +99,15 @@ extern "C" int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld
     if (max_out) *max_out = 0.0f;
     return RNJ_OK;
   }
+  // The call ends by waiting for the stream; a stream being captured cannot be
+  // waited for, and trying would invalidate the caller's capture.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t ce = cudaStreamIsCapturing(s, &cap);
+  if (ce != cudaSuccess) return cuda_error(ce, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return set_error(RNJ_ERR_UNSUPPORTED,
+                     "rnj_distance_noalloc waits for the GPU before it returns; it cannot be "
+                     "called on a stream that is being captured");
 
   // Size check against the worst plane count of the type, before any work.
   const bool naive = (flags & RNJ_FASTDIST) == 0;
@@ -170,6 +184,7 @@ extern "C" int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld
   ep.max_bits = words;
   ep.err = words + 1;
   ep.tile_flags = tile_flags;
+  apply_wait_settings(ep);
   if (n == 1) {
     e = cudaMemsetAsync(d_out, 0, sizeof(float), s);
     if (e != cudaSuccess) return cuda_error(e, "diagonal");
@@ -178,13 +193,12 @@ extern "C" int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld
   e = launch_count_tiles(p, ckind, EPI_DIST, ep, s);
   if (e == cudaSuccess) e = launch_fixup(ep, nt, s);
   if (e != cudaSuccess) return cuda_error(e, "distance kernels");
-  if (max_out) {
-    int hw[2];
-    e = cudaMemcpyAsync(hw, words, sizeof(hw), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_error(e, "max copy");
-    if (hw[1] != 0) return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out");
-    memcpy(max_out, &hw[0], sizeof(float));
-  }
+  // The maximum and the error word, always: a timeout must not pass as success.
+  int hw[2];
+  e = cudaMemcpyAsync(hw, words, sizeof(hw), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_error(e, "max copy");
+  if (hw[1] != 0) return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out");
+  if (max_out) memcpy(max_out, &hw[0], sizeof(float));
   return RNJ_OK;
 }

@@ -36,6 +36,10 @@ struct rnj_ctx {
   uint32_t *d_mask = nullptr;             // presence mask (8 words)
   uint32_t *h_mask = nullptr;             // pinned
   int *h_max = nullptr;                   // pinned max bits / error word
+  // Device error word of the single-alignment calls (bit 0: a bounded wait ran
+  // out).  Sticky: a call that does not wait for the GPU leaves it set, and the
+  // next call that does (rnj_ctx_synchronize, a max read) reports and clears it.
+  int *d_err = nullptr;
   void *h_stage[2] = {nullptr, nullptr};  // pinned staging for copy-out / upload
   size_t stage_cap = 0;
   bool profiling = false;
@@ -101,6 +105,9 @@ size_t packed_layout(rnj::Packed &p, int n, int L, int type, int flags, int kind
 int ctx_scratch(rnj_ctx *ctx, size_t words);
 rnj::EpiParams ctx_epi(rnj_ctx *ctx, const rnj::Packed &p, int model);
 int ctx_check_error(rnj_ctx *ctx);
+// After the stream has finished with ctx->d_err copied into ctx->h_max[1]: the
+// timeout status of that word (clearing it), else RNJ_OK (rnj_api.cu).
+int take_device_error(rnj_ctx *ctx);
 bool ctx_block_pinned(const void *p, size_t bytes);
 // The streamed host-to-host distance call of the tensor-core path, DNA and
 // protein (rnj_stream.cu).  Returns RNJ_ERR_UNSUPPORTED, having done nothing, when the

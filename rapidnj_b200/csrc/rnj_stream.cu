@@ -332,9 +332,12 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   RNJ_TRY(cudaMemcpyAsync(ctx->h_words, ctx->scratch.words, ((size_t)ntiles + 2) * sizeof(int),
                           cudaMemcpyDeviceToHost, ctx->stream),
           "flag copy");
+  RNJ_TRY(cudaMemcpyAsync(ctx->h_max + 1, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream),
+          "error word copy");
   RNJ_TRY(cudaStreamSynchronize(ctx->stream), "band sync");
-  if (ctx->h_words[1] != 0)
-    return set_error(RNJ_ERR_TIMEOUT, "a bounded device wait ran out (pipeline stage lost)");
+  rc = take_device_error(ctx);
+  if (rc != RNJ_OK) return rc;
   std::vector<int> flagged;
   if (!deferred)
     for (long long t = 0; t < ntiles; ++t)

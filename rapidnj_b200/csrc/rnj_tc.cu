@@ -158,15 +158,16 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
 constexpr uint32_t kIdescFp4 = (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) | (1u << 23) |
                                ((uint32_t)(kTile >> 4) << 24);
 
-// A bounded wait that also gives up early once another role has aborted.
-__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+// A bounded wait (limit_ns) that also gives up early once another role has aborted.
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                        uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 0; it < kWaitIterCap; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 255u) == 255u) {
       if (*abort_flag) return false;
-      if (global_timer_ns() - t0 > kWaitLimitNs) break;
+      if (global_timer_ns() - t0 > limit_ns) break;
     }
   }
   return false;
@@ -506,8 +507,13 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   uint64_t *acc_full = empty_bar + kTcStages;
   uint64_t *tmem_empty = acc_full + 1;
   uint64_t *drain_bar = tmem_empty + 1;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain_bar + 1);
+  uint64_t *never_bar = drain_bar + 1;  // nothing completes it: the failure-path test waits here
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(never_bar + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  // The pipeline waits' bound and the failure-path test switch (the same for
+  // every alignment of a launch).
+  const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);
+  const int stall = descs[0].stall;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nitems = (int)min((long long)(nitems_ptr ? *nitems_ptr : nitems_direct),
@@ -522,6 +528,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     mbar_init(acc_full, 1);
     mbar_init(tmem_empty, 256);
     mbar_init(drain_bar, 1);
+    mbar_init(never_bar, 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -562,7 +569,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         const int nkb = d.np * d.kdim / kTcKCols;  // feature blocks x K blocks per block
         for (int kb = 0; kb < nkb; ++kb, ++gkb) {
           const int s = ps;
-          if (!tc_wait(&empty_bar[s], pph ^ 1u, abort_flag)) {
+          if (!tc_wait(&empty_bar[s], pph ^ 1u, abort_flag, limit)) {
             *abort_flag = 1;
             break;
           }
@@ -602,7 +609,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const bool prot = d.kind == KIND_PROT_TC;
       // The epilogue of the previous item must have read the accumulators.
       int ok = 1;
-      if (lane == 0) ok = tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag);
+      if (lane == 0) ok = tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag, limit);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) {
         if (lane == 0) *abort_flag = 1;
@@ -619,7 +626,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       for (int kb = 0; kb < nkb; ++kb) {
         const int s = ring;
         if (!__all_sync(0xffffffffu, mbar_try_wait(&full_bar[s], ring_ph))) {
-          if (lane == 0) ok = tc_wait(&full_bar[s], ring_ph, abort_flag);
+          if (lane == 0) ok = tc_wait(&full_bar[s], ring_ph, abort_flag, limit);
           ok = __shfl_sync(0xffffffffu, ok, 0);
           if (!ok) break;
         }
@@ -666,7 +673,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const AlnDesc &d = descs[w.aln];
       int ti, tj;
       item_tile(d, w.tile, ti, tj);
-      if (!tc_wait(acc_full, titer & 1, abort_flag)) {
+      if ((stall && titer == 0 && !tc_wait(never_bar, 0, abort_flag, limit)) ||
+          !tc_wait(acc_full, titer & 1, abort_flag, limit)) {
         *abort_flag = 1;
         break;
       }

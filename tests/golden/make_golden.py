@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 
 from oracle import oracle  # noqa: E402  (test infrastructure)
 
-REF = os.environ.get("RNJ_REFERENCE", "/root/reference")
+REF = oracle.reference_tree()  # $RNJ_REFERENCE, else a `reference` folder beside the repo
 OUT = os.path.join(ROOT, "tests", "golden")
 
 
@@ -193,6 +193,8 @@ def save(name, names, seqs, outputs, fmt="fa", t="auto"):
 
 
 def main():
+    if REF is None:
+        sys.exit("the rapidNJ source tree was not found: set RNJ_REFERENCE")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "ref", f"REF={REF}"],
                    check=True)
     rng = np.random.default_rng(20240611)

@@ -8,6 +8,7 @@ import ctypes.util
 import numpy as np
 import pytest
 
+from oracle import oracle
 from rapidnj_b200 import synth
 
 pytestmark = pytest.mark.gpu
@@ -24,14 +25,33 @@ def plain(ctx, seqs, typ, model, fastdist=True):
     return out, mx
 
 
-def check_replicates(ctx, seqs, typ, model, cols, fastdist=True, which=None):
+def ulp_diff(a, b):
+    a = np.ascontiguousarray(a, np.float32).view(np.int32).astype(np.int64)
+    b = np.ascontiguousarray(b, np.float32).view(np.int32).astype(np.int64)
+    a = np.where(a < 0, -(a & 0x7FFFFFFF), a)
+    b = np.where(b < 0, -(b & 0x7FFFFFFF), b)
+    return np.abs(a - b)
+
+
+def check_replicates(ctx, seqs, typ, model, cols, fastdist=True, which=None, vs_oracle=2):
+    """Every checked replicate equals the plain call on the host-resampled
+    alignment bit for bit; the first `vs_oracle` of them also equal the oracle's
+    matrix of that alignment (counts and transform restated from the reference,
+    the same <= 1 ulp rule as the other parity tests)."""
     d = torch.from_numpy(seqs).cuda()
     outs, mx = ctx.bootstrap(d, cols, typ, model, fastdist=fastdist)
-    for r in (range(cols.shape[0]) if which is None else which):
-        want, wmx = plain(ctx, np.ascontiguousarray(seqs[:, cols[r]]), typ, model, fastdist)
+    for k, r in enumerate(range(cols.shape[0]) if which is None else which):
+        rep = np.ascontiguousarray(seqs[:, cols[r]])
+        want, wmx = plain(ctx, rep, typ, model, fastdist)
         got = outs[r].cpu().numpy()
         assert np.array_equal(got.view(np.int32), want.view(np.int32)), f"replicate {r}"
         assert mx[r] == np.float32(wmx)
+        if k < vs_oracle:
+            c = oracle.counts(rep, typ, naive=not fastdist, threads=8)
+            ref, rmx = oracle.matrix(c, rep.shape[1], typ, oracle.JC if model == "jc" else
+                                     oracle.KIMURA, naive=not fastdist)
+            dd = ulp_diff(got, ref)
+            assert dd.max() <= 1 and (dd == 1).sum() <= 2, f"replicate {r} vs the oracle"
 
 
 @pytest.mark.parametrize("typ,model,fastdist", [(0, "kim", True), (0, "jc", True),

@@ -307,6 +307,57 @@ def test_full_size_k2p_properties(ctx):
     assert ulp_diff(got, exp).max() <= 1
 
 
+def test_full_size_k2p_matrix_vs_reference(ctx, tmp_path):
+    """The whole 10,000 x 10,000 Kimura-2P matrix of the benchmark workload, cell
+    for cell against the float matrix of the reference's own driver
+    (KimuraDistance::computeDistances, KimuraDistance.cpp:300-395, compiled from
+    the reference sources into oracle/_ref/ref_harness, all host threads)."""
+    import os
+    from rapidnj_b200 import synth
+    if not oracle.ref_available():
+        pytest.skip("reference harness not built")
+    n, L = 10000, 10000
+    seqs = synth.tree_dna(n, L, seed=0)
+    path = str(tmp_path / "bench.fa")
+    synth.write_fasta(path, seqs)
+    ref, info = oracle.ref_matrix(path, "kim", "fa", "d", True, threads=os.cpu_count() or 1)
+    assert ref.shape == (n, n) and info["n"] == n and info["L"] == L
+    aln = ctx.alignment(torch.from_numpy(seqs).cuda(), oracle.DNA)
+    out = torch.empty((n, n), dtype=torch.float32, device="cuda")
+    ctx.distance_into(aln, "kim", out)
+    aln.close()
+    got = out.cpu().numpy()
+    del out
+    worst, ones = 0, 0
+    for r0 in range(0, n, 1000):  # row bands: the ulp arithmetic needs int64 copies
+        d = ulp_diff(got[r0:r0 + 1000], ref[r0:r0 + 1000])
+        worst = max(worst, int(d.max()))
+        ones += int((d == 1).sum())
+    assert worst <= 1, f"a cell differs by {worst} ulp"
+    assert ones <= max(2, int(1e-6 * n * n)), f"{ones} one-ulp cells"
+
+
+def test_tensor_core_exact_at_column_cap(ctx):
+    """The tensor-core path takes DNA up to 2^21 - 1 columns, where the f32 sums
+    of the FP4 products reach 2L ~ 2^22 in magnitude: nearly identical sequences
+    without gaps (and exact copies, whose T sum is exactly 2L) must still give the
+    oracle's integer counts and distances."""
+    import os
+    from rapidnj_b200 import synth
+    n, L = 130, (1 << 21) - 1
+    seqs = synth.tree_dna(n, L, seed=17, mean_branch=0.0004, gap=0.0)
+    seqs[1] = seqs[0]                      # identical: V = R = L, T = 2L
+    seqs[2, : L // 2] = seqs[3, : L // 2]  # half copied
+    seqs[4, 1::2] = ord("-")               # every other site a gap
+    c = oracle.counts(seqs, oracle.DNA, threads=os.cpu_count() or 1)
+    assert c[0, 1, 2] == L and c[0, 1, 0] == 0 and c[0, 1, 1] == 0
+    got = gpu_counts(ctx, seqs, oracle.DNA)
+    assert np.array_equal(got, c)
+    ref, _ = oracle.matrix(c, L, oracle.DNA, oracle.KIMURA)
+    m, _ = gpu_matrix(ctx, seqs, oracle.DNA, "kim")
+    assert_matrix_parity(m, ref)
+
+
 # ------------------------------------------------- tensor-core DNA kernel
 
 TC_SHAPES = [(2, 1), (3, 31), (17, 127), (128, 128), (129, 129), (200, 1000), (257, 4097),
