@@ -445,6 +445,19 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
              "tensor-core kernel");
     return RNJ_OK;
   }
+  if (tp.tc_epilogue == 0 && p.L <= kMaxFusedColumns) {
+    // Counts and transform in one launch (rnj_tcf.cu).
+    int rc = ensure_recip(ctx, p.L);
+    if (rc != RNJ_OK) return rc;
+    mark(ctx, 1, 0);
+    RNJ_CUDA(launch_tc_fused(ctx->d_desc, nullptr, nullptr, (int)ntiles, 0, (int)ntiles,
+                             ctx->d_recip, (int)std::min<long long>(ntiles, ctx->num_sms),
+                             ctx->stream),
+             "fused tensor-core kernel");
+    mark(ctx, 1, 1);
+    mark(ctx, 2, 0);
+    return RNJ_OK;
+  }
   int rc = ensure_packed(ctx, std::min<long long>(ntiles, kTcChunkTiles));
   if (rc != RNJ_OK) return rc;
   return run_tc_chunks(ctx, ctx->d_desc, nullptr, ntiles, ctx->d_packed, ctx->stream,
@@ -562,6 +575,26 @@ int ensure_packed(rnj_ctx *ctx, long long tiles) {
   return RNJ_OK;
 }
 
+int ensure_recip(rnj_ctx *ctx, int L) {
+  if (ctx->d_recip && ctx->recip_L >= L) return RNJ_OK;
+  // At least every 16-bit count: the fused kernel's counts are 16-bit fields.
+  const int cap = std::max(65535, (L + 4095) / 4096 * 4096);
+  std::vector<double> h((size_t)cap + 1);
+  h[0] = 0.0;
+  for (int k = 1; k <= cap; ++k) h[k] = 1.0 / (double)k;  // IEEE division: the nearest double
+  if (ctx->d_recip) cudaFreeAsync(ctx->d_recip, ctx->stream);
+  ctx->d_recip = nullptr;
+  ctx->recip_L = 0;
+  RNJ_CUDA(cudaMallocAsync((void **)&ctx->d_recip, h.size() * sizeof(double), ctx->stream),
+           "reciprocal table");
+  // From pageable memory: the bytes are taken before the call returns.
+  RNJ_CUDA(cudaMemcpyAsync(ctx->d_recip, h.data(), h.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->stream),
+           "reciprocal table upload");
+  ctx->recip_L = cap;
+  return RNJ_OK;
+}
+
 int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, long long nitems,
                   uint64_t *packed, cudaStream_t s, int transform_ctas) {
   const int ctas = transform_ctas > 0 ? std::min(transform_ctas, kTransformCtasPerSm)
@@ -639,6 +672,7 @@ int rnj_ctx_destroy(rnj_ctx *ctx) {
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->d_desc) cudaFree(ctx->d_desc);
   if (ctx->d_packed) cudaFree(ctx->d_packed);
+  if (ctx->d_recip) cudaFree(ctx->d_recip);
   if (ctx->h_mask) cudaFreeHost(ctx->h_mask);
   if (ctx->h_max) cudaFreeHost(ctx->h_max);
   for (int b = 0; b < 2; ++b)

@@ -154,11 +154,40 @@ __device__ __forceinline__ float neg_log_checked(double c, double arg) {
   return __float_as_int(lo) == __float_as_int(hi) ? lo : __int_as_float(0x7fc00000);
 }
 
+// The float quotient fl32(num / den) of integers 0 <= num <= den < 2^24, the
+// value of both (float)num / (float)den and (float)((double)num / (double)den)
+// in the reference.  With rn = the double nearest to 1 / den (a per-context
+// table, filled on the host), d = fl64(num * rn) is within 2^-52 (relative) of
+// num / den.  A float rounding boundary m (the midpoint of two floats) has 25
+// significant bits, m = (2k + 1) 2^-s with 2k + 1 >= 2^24; num / den = m would
+// need 2k + 1 to divide num < 2^24, so num / den != m and
+// |num / den - m| >= 1 / (den 2^s), at least 2^-49 relative to m.  d therefore
+// lies on the same side of every boundary as num / den and rounds to the same
+// float.  rn == 0 (no table) divides instead.
+__device__ __forceinline__ float ratio_f32(unsigned long long num, unsigned long long den,
+                                           double rn) {
+  if (rn != 0.0) return __double2float_rn(__dmul_rn((double)num, rn));
+  return __fdiv_rn(__ull2float_rn(num), __ull2float_rn(den));
+}
+
+// The undecided cases of the table logarithm (about one pair in 10^6): the
+// reference's own formulas with CUDA's log, kept out of line so that the
+// registers they need do not weigh on the common path.
+static __device__ __noinline__ float neg_log_slow(double c, double arg) {
+  return __double2float_rn(__dmul_rn(-c, log(arg)));
+}
+static __device__ __noinline__ float k2p_two_logs(double a, double b) {
+  return __double2float_rn(__dsub_rn(__dmul_rn(-0.5, log(a)), __dmul_rn(0.25, log(b))));
+}
+
 // JCdistance.cpp:171-183.  b = (alpha - 1) / alpha in double, alpha 4 or 20.
+// rn: the reciprocal of valid (ratio_f32), or 0.
 __device__ __forceinline__ float jc_distance(unsigned long long total,
-                                             unsigned long long valid, double b) {
+                                             unsigned long long valid, double b,
+                                             double rn = 0.0) {
   float distance;
   if (valid == 0) distance = 0.0f;
+  else if (rn != 0.0) distance = ratio_f32(total, valid, rn);
   else distance = __fdiv_rn(__ll2float_rn((long long)total), __ull2float_rn(valid));
   const double q = __ddiv_rn((double)distance, b);
   if (q >= 1.0) return -1.0f;
@@ -166,13 +195,13 @@ __device__ __forceinline__ float jc_distance(unsigned long long total,
   if (arg == 1.0) return __double2float_rn(__dmul_rn(-b, 0.0));  // -0.0, as the reference
   const float fast = neg_log_checked(b, arg);
   if (fast == fast) return fast;
-  return __double2float_rn(__dmul_rn(-b, log(arg)));
+  return neg_log_slow(b, arg);
 }
 
-// KimuraDistance.cpp:339-349.
+// KimuraDistance.cpp:339-349.  rn: the reciprocal of valid (ratio_f32), or 0.
 __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
                                               unsigned long long tv_count,
-                                              unsigned long long valid) {
+                                              unsigned long long valid, double rn = 0.0) {
   if (valid == 0) return -1.0f;
   // ts = (float)((double)P / (double)n): for integers P <= n < 2^24 this equals
   // the float quotient rounded once.  A float midpoint m has at most 25
@@ -180,7 +209,10 @@ __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
   // 1 / (n * 2^25) > 2^-49 (relative) away from it, while the double rounding
   // moves it by at most 2^-53: both roundings land on the same float.
   float ts, tv;
-  if (valid < (1u << 24)) {
+  if (rn != 0.0) {
+    ts = ratio_f32(ts_count, valid, rn);
+    tv = ratio_f32(tv_count, valid, rn);
+  } else if (valid < (1u << 24)) {
     const float fn = (float)valid;
     ts = __fdiv_rn((float)ts_count, fn);
     tv = __fdiv_rn((float)tv_count, fn);
@@ -217,22 +249,25 @@ __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
   const float lo = __double2float_rn(__dsub_rn(dd, eps));
   const float hi = __double2float_rn(__dadd_rn(dd, eps));
   if (__float_as_int(lo) == __float_as_int(hi)) return lo;
-  return __double2float_rn(__dsub_rn(__dmul_rn(-0.5, log(a)), __dmul_rn(0.25, log(b))));
+  return k2p_two_logs(a, b);
 }
 
 // KimuraDistance.cpp:322-338 with the Dayhoff table of KimuraDistance.cpp:30-49.
+// rn: the reciprocal of valid (ratio_f32), or 0.
 __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism,
                                                          unsigned long long valid,
-                                                         const int *pam) {
+                                                         const int *pam, double rn = 0.0) {
   float distance = -1.0f;
-  if (valid != 0) distance = __fdiv_rn(__ll2float_rn((long long)mism), __ull2float_rn(valid));
+  if (valid != 0)
+    distance = rn != 0.0 ? ratio_f32(mism, valid, rn)
+                         : __fdiv_rn(__ll2float_rn((long long)mism), __ull2float_rn(valid));
   const double dd = (double)distance;
   if (dd < 0.75) {
     if (dd > 0.0) {
       const double sq = (double)__fmul_rn(distance, distance);
       const double arg = __dsub_rn(__dsub_rn(1.0, dd), __dmul_rn(sq, 0.20));
       const float fast = neg_log_checked(1.0, arg);
-      distance = fast == fast ? fast : __double2float_rn(-log(arg));
+      distance = fast == fast ? fast : neg_log_slow(1.0, arg);
     }
   } else {
     if (dd > 0.930) {

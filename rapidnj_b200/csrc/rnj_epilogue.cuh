@@ -47,13 +47,19 @@ __device__ __forceinline__ void tri_coords(int t, int nt, int &ti, int &tj) {
 __device__ __forceinline__ int row_of(int rbase, int r) { return rbase + (r < 4 ? r : 12 + r); }
 __device__ __forceinline__ int col_of(int cbase, int c) { return cbase + (c < 4 ? c : 28 + c); }
 
+// The exact distance of one pair from its counts.  recip (may be null): the
+// context's table of reciprocals 1 / k for k = 0 .. L (entry 0 unused, 0.0),
+// which replaces the float divisions by a multiply (ratio_f32); the wrapping
+// valid count of RNJ_COMPAT_PROTEIN_WRAP divides.
 __device__ __forceinline__ float pair_distance(const EpiParams &ep, uint32_t c0, uint32_t c1,
-                                               uint32_t valid) {
+                                               uint32_t valid, const double *recip = nullptr) {
   unsigned long long v = valid;
+  double rn = 0.0;
   if (ep.compat_wrap) v = protein_fast_valid(v, ep.L);
-  if (ep.model == RNJ_JC) return jc_distance((unsigned long long)c0 + c1, v, ep.jc_b);
-  if (ep.type == RNJ_PROTEIN) return kimura_protein_distance(c0, v, c_pam);
-  return k2p_distance(c0, c1, v);
+  else if (recip) rn = __ldg(recip + valid);
+  if (ep.model == RNJ_JC) return jc_distance((unsigned long long)c0 + c1, v, ep.jc_b, rn);
+  if (ep.type == RNJ_PROTEIN) return kimura_protein_distance(c0, v, c_pam, rn);
+  return k2p_distance(c0, c1, v, rn);
 }
 
 // Row stride (floats) of the distance tile staged in shared memory: 129 keeps

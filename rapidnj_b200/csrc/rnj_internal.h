@@ -41,6 +41,9 @@ constexpr int kMaxFusedWords = 2047;  // 16-bit packed accumulators: L <= 65504 
 // 2^24, and the packed counts hold 21 bits; longer DNA alignments are counted on
 // the bit-plane kernels.
 constexpr int kMaxTcColumns = (1 << 21) - 1;
+// The fused tensor-core kernel keeps each pair's counts in 16 bits between the
+// accumulators and the transform; longer alignments take the two-kernel form.
+constexpr int kMaxFusedColumns = 65535;
 
 __host__ __device__ inline int planes_of(int kind) {
   switch (kind) {
@@ -135,6 +138,8 @@ struct TuneParams {
   int tile_band = 0;       // tensor-core kernel: tile-order band height in tile rows (0 = 12)
   int transform_ctas = 0;  // tensor-core transform: resident CTAs per SM (0 = 5)
   int stream_band = 0;     // streamed host call: band height in tile rows (0 = automatic)
+  int tc_epilogue = 0;     // tensor-core distances: 0 transform fused into the counting
+                           // kernel, 1 packed counts + separate transform kernel
 };
 // The parameters of the bucket of (n, L, type, flags): the tuned entry if the
 // table (filled by rnj_tune / rnj_tune_load / RNJ_TUNE_CACHE) holds one, else
@@ -215,6 +220,15 @@ cudaError_t launch_tc_peak_probe(int grid, int iters, int *err, cudaStream_t s);
 cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
                                 const int *d_nitems, int nitems, int item0, int count,
                                 const uint64_t *packed, int grid, cudaStream_t s);
+// The fused form (rnj_tcf.cu): counts and the exact transform in one persistent
+// launch over work items [item0, min(n, item0 + count)) (d_items == nullptr: the
+// banded tiles of d_descs[0]; d_nitems == nullptr: n = nitems); distances
+// straight into each alignment's output, with its max slot and saturation
+// flags.  recip: reciprocals 1 / k for k = 0 .. max L (entry 0 = 0).  Every
+// alignment has at most kMaxFusedColumns columns.
+cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
+                            int nitems, int item0, int count, const double *recip, int grid,
+                            cudaStream_t s);
 
 enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2, EPI_PACKED = 3 };
 

@@ -153,7 +153,10 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
     const long long t0 = bounds[k + 1], h = bounds[k] - bounds[k + 1];
     max_band_tiles = std::max(max_band_tiles, h * (nt - t0) - h * (h - 1) / 2);
   }
-  if (max_band_tiles > kTcChunkTiles) return RNJ_ERR_UNSUPPORTED;
+  // Counts and transform in one kernel (rnj_tcf.cu), or through the packed
+  // counts (one pass per band) and the transform kernel.
+  const bool fused = tp.tc_epilogue == 0 && L <= kMaxFusedColumns;
+  if (!fused && max_band_tiles > kTcChunkTiles) return RNJ_ERR_UNSUPPORTED;
   if (!ctx_block_pinned(out, (size_t)n * n * sizeof(float))) return RNJ_ERR_UNSUPPORTED;
 
   DeviceGuard guard(ctx->device);
@@ -161,7 +164,7 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   if (rc != RNJ_OK) return rc;
   rc = ensure_host_words(ctx, (size_t)ntiles + 2);
   if (rc != RNJ_OK) return rc;
-  rc = ensure_packed(ctx, max_band_tiles);
+  rc = fused ? ensure_recip(ctx, L) : ensure_packed(ctx, max_band_tiles);
   if (rc != RNJ_OK) return rc;
   rc = ctx_scratch(ctx, (size_t)ntiles + 2);
   if (rc != RNJ_OK) return rc;
@@ -284,16 +287,23 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
                                         ctx->stream, r0, r1 - r0),
             "feature pack kernel");
     const long long i0 = band_off[k], cnt = band_off[k + 1] - band_off[k];
-    RNJ_TRY(launch_tc_batch(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0, (int)cnt,
-                            ctx->d_packed, (int)std::min<long long>(cnt, ctx->num_sms), EPI_PACKED,
-                            ctx->stream),
-            "tensor-core kernel");
-    RNJ_TRY(launch_tc_transform(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
-                                (int)cnt, ctx->d_packed,
-                                (int)std::min<long long>(cnt, (long long)transform_ctas *
-                                                                  ctx->num_sms),
-                                ctx->stream),
-            "transform kernel");
+    if (fused) {
+      RNJ_TRY(launch_tc_fused(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
+                              (int)cnt, ctx->d_recip, (int)std::min<long long>(cnt, ctx->num_sms),
+                              ctx->stream),
+              "fused tensor-core kernel");
+    } else {
+      RNJ_TRY(launch_tc_batch(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
+                              (int)cnt, ctx->d_packed, (int)std::min<long long>(cnt, ctx->num_sms),
+                              EPI_PACKED, ctx->stream),
+              "tensor-core kernel");
+      RNJ_TRY(launch_tc_transform(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
+                                  (int)cnt, ctx->d_packed,
+                                  (int)std::min<long long>(cnt, (long long)transform_ctas *
+                                                                    ctx->num_sms),
+                                  ctx->stream),
+              "transform kernel");
+    }
     RNJ_TRY(cudaEventRecord(ev_done, ctx->stream), "event");
     if (deferred) return RNJ_OK;
     RNJ_TRY(cudaStreamWaitEvent(ctx->s_down, ev_done, 0), "download wait");

@@ -44,134 +44,14 @@
 #include "rnj_device.cuh"
 #include "rnj_epilogue.cuh"
 #include "rnj_internal.h"
+#include "rnj_tcgen05.cuh"
 
 namespace rnj {
-
-constexpr int kTcStages = 7;
-constexpr int kTcKBlock = 128;                            // bytes of K per stage (256 FP4 columns)
-constexpr int kTcKCols = 256;                             // feature columns per stage
-constexpr uint32_t kTcTileBytes = kTile * kTcKBlock;      // 16 KB per operand tile
-constexpr uint32_t kTcStageBytes = 2 * kTcTileBytes;      // A + B
-constexpr int kTcThreads = 320;
-constexpr uint32_t kTmemCols = 512;                       // 3 x 128 accumulators + scale factors
-constexpr uint32_t kTmemSfa = 384, kTmemSfb = 448;        // scale-factor columns (all 1.0)
-constexpr size_t kTcSmemBytes = (size_t)kTcStages * kTcStageBytes + 1024 + 256;
 
 // A 256-byte table passed by value to a kernel.
 struct Lut8 {
   uint8_t v[256];
 };
-
-// ---------------------------------------------------------------- tcgen05 PTX
-
-__device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
-               "r"(ncols)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_relinquish() {
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
-               : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-// D (f32, tensor memory) (+)= A x B^T with FP4 operands from shared memory and
-// block scale factors from tensor memory (block of 32 columns), issued by one
-// elected lane of a converged warp.  The whole warp runs the issue loop, so the
-// descriptor and tensor-memory operands are warp-uniform values; issued from a
-// single divergent lane with per-instruction operand arithmetic, the MMA issue
-// rate, not the tensor pipe, bounded the kernel (about 150 instead of 64
-// cycles per 128 x 128 x 64 instruction).
-__device__ __forceinline__ void tc_mma_fp4_elect(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                                 uint32_t idesc, uint32_t sfa_tmem,
-                                                 uint32_t sfb_tmem, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p, e;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "elect.sync _|e, 0xffffffff;\n\t"
-      "@e tcgen05.mma.cta_group::1.kind::mxf4.block_scale.block32 [%0], %1, %2, %3, [%5], [%6], p;\n\t}"
-      ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(sfa_tmem),
-      "r"(sfb_tmem)
-      : "memory");
-}
-__device__ __forceinline__ void tc_commit_elect(uint64_t *bar) {
-  asm volatile(
-      "{\n\t.reg .pred e;\n\t"
-      "elect.sync _|e, 0xffffffff;\n\t"
-      "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}"
-      ::"r"(smem_u32(bar))
-      : "memory");
-}
-// 32 lanes x 32 columns of 32-bit words from registers into tensor memory.
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, uint32_t x) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
-      "%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1};"
-      ::"r"(taddr), "r"(x)
-      : "memory");
-}
-__device__ __forceinline__ void tmem_st_wait() {
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
-      "%30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
-        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
-        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr)
-      : "memory");
-}
-__device__ __forceinline__ void tmem_ld_wait() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void named_barrier(int id, int threads) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
-}
-
-// Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, 8-row
-// groups 1024 bytes apart (stride byte offset), descriptor version 1.
-__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;                   // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1u << 46;                   // version
-  d |= (uint64_t)2u << 61;                   // SWIZZLE_128B
-  return d;
-}
-
-// Instruction descriptor, kind::mxf4 (block-scaled layout): A and B E2M1
-// (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bits 17-22, scale factors
-// UE8M0 (bit 23), M >> 4 at bits 24-28, scale-factor ids 0, dense K = 64.
-constexpr uint32_t kIdescFp4 = (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) | (1u << 23) |
-                               ((uint32_t)(kTile >> 4) << 24);
-
-// A bounded wait (limit_ns) that also gives up early once another role has aborted.
-__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
-                                        uint64_t limit_ns) {
-  if (mbar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = global_timer_ns();
-  for (uint32_t it = 0; it < kWaitIterCap; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 255u) {
-      if (*abort_flag) return false;
-      if (global_timer_ns() - t0 > limit_ns) break;
-    }
-  }
-  return false;
-}
 
 // --------------------------------------------------------------- feature pack
 
@@ -421,75 +301,11 @@ cudaError_t launch_pack_features_bits(const uint32_t *d_bits, const uint32_t *d_
 
 // ----------------------------------------------------------------- the kernel
 //
-// Persistent over a work list of (alignment, triangle tile) items: CTA b takes
-// items b, b + G, b + 2G, ... (the list is ordered by decreasing cost, so this
-// round robin balances).  Stage counters run on across items, so the producer
-// streams the next tile's operands while the epilogue of the current one runs
-// (the epilogue works from tensor memory and registers only, never from the
-// stage buffers); the MMA warp waits for the epilogue's hand-back of tensor
-// memory before it overwrites the accumulators.
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *map) {
-  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
-                   reinterpret_cast<uint64_t>(map))
-               : "memory");
-}
-
-__device__ __forceinline__ void item_tile(const AlnDesc &d, int tile, int &ti, int &tj) {
-  if (d.full) {
-    ti = tile / d.nt;
-    tj = tile % d.nt;
-  } else {
-    tri_coords(tile, d.nt, ti, tj);
-  }
-}
-
-// Work order of a single alignment's triangle (no explicit work list): bands of
-// kBand tile rows, each walked column by column (within a column, its rows of
-// the band).  The kernels resident at one time then share about kBand row tiles
-// and 148 / kBand column tiles of operands instead of two rows and every
-// column, which keeps the operand working set of the running tiles in L2.
-// Returns the tile's row-major triangle index (the index of its saturation flag).
-constexpr int kBand = 12;  // default band height (the autotuner may choose another)
-
-__device__ __forceinline__ int banded_tile(int it, int nt, int band) {
-  int r0 = 0;
-  while (true) {
-    const int g = min(band, nt - r0);
-    const int tri = g * (g + 1) / 2;
-    const int count = tri + (nt - r0 - g) * g;
-    if (it < count || r0 + g >= nt) {
-      int ti, tj;
-      if (it < tri) {
-        int c = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
-        while (c * (c + 1) / 2 > it) --c;
-        while ((c + 1) * (c + 2) / 2 <= it) ++c;
-        tj = r0 + c;
-        ti = r0 + (it - c * (c + 1) / 2);
-      } else {
-        const int k = it - tri;
-        tj = r0 + g + k / g;
-        ti = r0 + k % g;
-      }
-      return ti * nt - ti * (ti - 1) / 2 + (tj - ti);
-    }
-    it -= count;
-    r0 += g;
-  }
-}
-
-__device__ __forceinline__ WorkItem item_at(const AlnDesc *descs, const WorkItem *items, int it) {
-  if (items) return items[it];
-  WorkItem w;
-  w.aln = 0;
-  const int band = descs[0].band > 0 ? descs[0].band : kBand;
-  w.tile = descs[0].full ? it : banded_tile(it, descs[0].nt, band);
-  return w;
-}
+// The counting pipeline of rnj_tcgen05.cuh (producer, MMA issuer) with an
+// epilogue of eight warps that turns the accumulators into integer counts:
+// packed per tile for the separate transform kernel (EPI_PACKED), or the
+// n x n x 3 count matrix (EPI_COUNTS).  The epilogue works from tensor memory
+// and registers only, never from the stage buffers.
 
 // Items [item0, min(nitems, item0 + count)) of the work list.  EPI_PACKED: the
 // counts of item it go to packed[(it - item0) * 128 * 128 ...] (see
@@ -500,16 +316,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
                     uint64_t *__restrict__ packed) {
   extern __shared__ uint8_t smem_raw[];
-  uint8_t *smem =
-      reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + kTcStages * kTcStageBytes);
-  uint64_t *empty_bar = full_bar + kTcStages;
-  uint64_t *acc_full = empty_bar + kTcStages;
-  uint64_t *tmem_empty = acc_full + 1;
-  uint64_t *drain_bar = tmem_empty + 1;
-  uint64_t *never_bar = drain_bar + 1;  // nothing completes it: the failure-path test waits here
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(never_bar + 1);
-  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+  const TcShared sh = tc_shared(smem_raw);
   // The pipeline waits' bound and the failure-path test switch (the same for
   // every alignment of a launch).
   const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);
@@ -520,147 +327,15 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                               (long long)item0 + count);
   if (item0 + (int)blockIdx.x >= nitems) return;  // no item for this CTA (before any setup)
 
-  if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) {
-      mbar_init(&full_bar[s], 1);
-      mbar_init(&empty_bar[s], 1);
-    }
-    mbar_init(acc_full, 1);
-    mbar_init(tmem_empty, 256);
-    mbar_init(drain_bar, 1);
-    mbar_init(never_bar, 1);
-    *abort_flag = 0;
-    fence_mbar_init();
-  }
-  if (warp == 1) {
-    tmem_alloc(tmem_slot, kTmemCols);
-    tmem_relinquish();
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  // Block scale factors: every byte of columns kTmemSfa..511 of all 128 lanes is
-  // UE8M0 127 (2^0); the MMAs read theirs from kTmemSfa and kTmemSfb.
-  if (warp >= 2) {
-    const uint32_t base = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + kTmemSfa +
-                          64u * (uint32_t)((warp - 2) >> 2);
-    tmem_st32(base, 0x7F7F7F7Fu);
-    tmem_st32(base + 32, 0x7F7F7F7Fu);
-    tmem_st_wait();
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
+  // tmem_empty: one arrival per epilogue thread (warps 2..9)
+  const uint32_t tmem = tc_setup(sh, 256, 2);
   uint32_t issued = 0;  // producer: k-blocks issued in total (thread 0 only)
 
   if (warp == 0) {
-    if (lane == 0) {
-      // ----------------------------------------------------------- producer
-      uint32_t gkb = 0;
-      int ps = 0;           // stage of the next load and the parity of its fill
-      uint32_t pph = 0;
-      for (int it = item0 + blockIdx.x; it < nitems && !*abort_flag; it += gridDim.x) {
-        const WorkItem w = item_at(descs, items, it);
-        const AlnDesc &d = descs[w.aln];
-        tensormap_acquire(&d.map);
-        int ti, tj;
-        item_tile(d, w.tile, ti, tj);
-        const int nkb = d.np * d.kdim / kTcKCols;  // feature blocks x K blocks per block
-        for (int kb = 0; kb < nkb; ++kb, ++gkb) {
-          const int s = ps;
-          if (!tc_wait(&empty_bar[s], pph ^ 1u, abort_flag, limit)) {
-            *abort_flag = 1;
-            break;
-          }
-          uint8_t *a = smem + s * kTcStageBytes;
-          mbar_arrive_expect_tx(&full_bar[s], kTcStageBytes);
-          tma_load_3d(a, &d.map, &full_bar[s], 0, ti * kTile, kb);
-          tma_load_3d(a + kTcTileBytes, &d.map, &full_bar[s], 0, tj * kTile, kb);
-          issued = gkb + 1;
-          if (++ps == kTcStages) {
-            ps = 0;
-            pph ^= 1u;
-          }
-        }
-      }
-    }
+    if (lane == 0)
+      issued = tc_produce(sh, descs, items, item0 + blockIdx.x, nitems, gridDim.x, limit);
   } else if (warp == 1) {
-    // ---------------------------------------------------------- MMA issuer
-    // The whole warp runs this loop (lane 0 waits, the result is broadcast);
-    // one elected lane issues each MMA and commit.  Descriptors are the stage
-    // base descriptors plus constant offsets: the 14-bit start-address field
-    // (16-byte units) of a shared address below 228 KB cannot carry out.
-    const uint64_t desc0 = smem_desc_sw128(smem_u32(smem));
-    constexpr uint64_t kStageStep = kTcStageBytes >> 4, kBStep = kTcTileBytes >> 4;
-    uint32_t titer = 0;
-    int ring = 0;           // stage of the ring the next K block is in
-    uint32_t ring_ph = 0;   // and the parity of its current fill
-    for (int it = item0 + blockIdx.x;; it += gridDim.x, ++titer) {
-      int go = it < nitems && !*abort_flag;
-      go = __shfl_sync(0xffffffffu, go, 0);
-      if (!go) break;
-      const WorkItem w = item_at(descs, items, it);
-      const AlnDesc &d = descs[w.aln];
-      const int nkb = d.np * d.kdim / kTcKCols;
-      const int seg = d.kdim / kTcKCols;  // K blocks per feature block
-      // Accumulators: DNA blocks v, r, t, u -> V, R, T, T; protein blocks
-      // v, rank 0 .. -> V, M, M, ...
-      const bool prot = d.kind == KIND_PROT_TC;
-      // The epilogue of the previous item must have read the accumulators.
-      int ok = 1;
-      if (lane == 0) ok = tc_wait(tmem_empty, (titer & 1) ^ 1, abort_flag, limit);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) {
-        if (lane == 0) *abort_flag = 1;
-        break;
-      }
-      tc_fence_after();
-      // Per K block: every lane tests the stage's full barrier (one warp vote
-      // when it is already complete, the common case; otherwise lane 0 waits,
-      // bounded); the stage, its parity, the accumulator and whether the block
-      // starts that accumulator's sum follow from counters.  Measured: the
-      // per-block division, modulo and broadcast cost 15 % of the kernel.
-      const int last_acc = prot ? 1 : 2;
-      int kin = 0, blk = 0;  // K block within its feature block, feature block
-      for (int kb = 0; kb < nkb; ++kb) {
-        const int s = ring;
-        if (!__all_sync(0xffffffffu, mbar_try_wait(&full_bar[s], ring_ph))) {
-          if (lane == 0) ok = tc_wait(&full_bar[s], ring_ph, abort_flag, limit);
-          ok = __shfl_sync(0xffffffffu, ok, 0);
-          if (!ok) break;
-        }
-        tc_fence_after();
-        const int acc = blk < last_acc ? blk : last_acc;
-        const uint32_t first = (kin == 0) && (blk <= last_acc);
-        if (++kin == seg) {
-          kin = 0;
-          ++blk;
-        }
-        if (++ring == kTcStages) {
-          ring = 0;
-          ring_ph ^= 1u;
-        }
-        const uint64_t adesc = desc0 + (uint64_t)s * kStageStep;
-        const uint64_t bdesc = adesc + kBStep;
-        const uint32_t dt = tmem + (uint32_t)(acc * kTile);
-        // 32 bytes = 64 columns per MMA, four per 128-byte stage.
-        tc_mma_fp4_elect(dt, adesc, bdesc, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, first ^ 1u);
-        tc_mma_fp4_elect(dt, adesc + 2, bdesc + 2, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
-        tc_mma_fp4_elect(dt, adesc + 4, bdesc + 4, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
-        tc_mma_fp4_elect(dt, adesc + 6, bdesc + 6, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
-        tc_commit_elect(&empty_bar[s]);
-      }
-      if (!ok) {
-        if (lane == 0) *abort_flag = 1;
-        break;
-      }
-      tc_commit_elect(acc_full);
-    }
-    // Every MMA issued has completed before tensor memory is released.
-    tc_commit_elect(drain_bar);
-    if (lane == 0) mbar_wait_bounded(drain_bar, 0);
-    __syncwarp();
+    tc_issue(sh, tmem, descs, items, item0 + blockIdx.x, nitems, gridDim.x, limit);
   } else {
     // ----------------------------------------------------------- epilogue
     // Warps 2..9: TMEM lane quarter = warp % 4 (row block), column half by group.
@@ -673,9 +348,9 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       const AlnDesc &d = descs[w.aln];
       int ti, tj;
       item_tile(d, w.tile, ti, tj);
-      if ((stall && titer == 0 && !tc_wait(never_bar, 0, abort_flag, limit)) ||
-          !tc_wait(acc_full, titer & 1, abort_flag, limit)) {
-        *abort_flag = 1;
+      if ((stall && titer == 0 && !tc_wait(sh.never_bar, 0, sh.abort_flag, limit)) ||
+          !tc_wait(sh.acc_full, titer & 1, sh.abort_flag, limit)) {
+        *sh.abort_flag = 1;
         break;
       }
       tc_fence_after();
@@ -696,7 +371,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         tmem_ld_wait();
         if (cc == 1) {
           tc_fence_before();
-          mbar_arrive(tmem_empty);
+          mbar_arrive(sh.tmem_empty);
         }
         const int jb = tj * kTile + cbase;
 #pragma unroll
@@ -725,19 +400,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
   }
 
-  __syncthreads();
-  if (tid == 0 && *abort_flag) {
-    // Loads may still be in flight into stages the MMA never consumed: let the
-    // last ring's worth land (bounded) before shared memory is released.
-    for (uint32_t k = issued > (uint32_t)kTcStages ? issued - kTcStages : 0; k < issued; ++k)
-      mbar_wait_bounded(&full_bar[k % kTcStages], (k / kTcStages) & 1);
-    atomicOr(descs[0].err, 1);
-  }
-  __syncthreads();
-  if (warp == 1) {
-    tc_fence_after();
-    tmem_dealloc(tmem, kTmemCols);
-  }
+  tc_teardown(sh, tmem, issued, descs[0].err);
 }
 
 // ------------------------------------------------------------ the transform

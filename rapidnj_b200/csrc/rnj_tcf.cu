@@ -1,0 +1,232 @@
+// rnj_tcf.cu -- the fused tensor-core distance kernel: per-pair counts on the
+// tensor cores and the exact transform in the same CTA, straight from tensor
+// memory to the distance matrix.
+//
+// The counting pipeline is the one of rnj_tcgen05.cuh (warp 0 TMA producer,
+// warp 1 MMA issuer, three f32 accumulators V, R, T of 128 x 128 in tensor
+// memory).  Sixteen epilogue warps (2 .. 17) replace the packed-count round
+// trip of the two-kernel form (8 bytes per pair written and read again, then a
+// separate transform launch):
+//   * warp w reads tensor-memory lane quarter w % 4 (32 tile rows, lane = row)
+//     and columns 32 ((w - 2) / 4) .. + 31 of the three accumulators, 16
+//     columns at a time, converts them to integer counts (16 bits each: the
+//     fused form takes alignments of at most 65535 columns) and hands tensor
+//     memory back to the MMA warp at once;
+//   * it then computes the 32 distances of each lane from registers
+//     (pair_distance with the context's reciprocal table, the same float
+//     result as the reference's divisions, ratio_f32) while the tensor cores
+//     already count the next tile;
+//   * stores: the mirror entries out[j][i] as coalesced 128-byte row segments
+//     (lanes are consecutive i), the tile entries out[i][j .. j + 3] as 16-byte
+//     vectors, the diagonal as 0; the tile's maximum goes to the alignment's
+//     max slot (atomicMax on the float bits) and a saturated pair (-1) sets
+//     the tile's flag for the fix-up kernel.
+// Sixteen warps run the transform at four warps per scheduler, enough to hide
+// the double-precision latency, and its instructions overlap the MMAs of the
+// next tile instead of following them in a second kernel.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rnj_device.cuh"
+#include "rnj_epilogue.cuh"
+#include "rnj_internal.h"
+#include "rnj_tcgen05.cuh"
+
+namespace rnj {
+
+constexpr int kTcfEpiWarps = 16;
+constexpr int kTcfThreads = 64 + 32 * kTcfEpiWarps;  // producer, MMA issuer, epilogue
+constexpr int kTcfGroup = 8;                         // pairs per transform group
+
+// Transform variants of the fused epilogue, one loop each so that only the
+// model's own parameters stay in registers.
+enum { kFusedK2p = 0, kFusedJc = 1, kFusedProtein = 2, kFusedGeneric = 3 };
+
+template <int M>
+__device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint32_t tv,
+                                            uint32_t vv, const double *__restrict__ recip) {
+  const double rn = __ldg(recip + vv);  // 1 / valid (0 for valid == 0)
+  if constexpr (M == kFusedK2p) {
+    return k2p_distance(ts, tv, vv, rn);
+  } else if constexpr (M == kFusedJc) {
+    return jc_distance((unsigned long long)ts + tv, vv, d.jc_b, rn);
+  } else if constexpr (M == kFusedProtein) {
+    return kimura_protein_distance(ts, vv, c_pam, rn);
+  } else {
+    EpiParams ep;
+    ep.n = d.n;
+    ep.L = d.L;
+    ep.model = d.model;
+    ep.type = d.type;
+    ep.compat_wrap = d.compat;
+    ep.jc_b = d.jc_b;
+    return pair_distance(ep, ts, tv, vv, recip);
+  }
+}
+
+// The 32 distances of row i, columns jb .. jb + 31 (counts pq / pv, see the
+// epilogue): the mirror entries out[j][i], the row entries out[i][j] for j >= i
+// (0 on the diagonal), the running maximum and whether a pair saturated.
+template <int M>
+__device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint32_t (&pq)[32],
+                                           uint32_t (&pv)[16], const double *__restrict__ recip,
+                                           float &tmax, bool &sat) {
+  const int n = d.n;
+  float *const out = d.out;
+  const size_t ld = d.ld;
+  const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+  float *const orow = out + (size_t)i * ld;  // dereferenced only for i < n
+#pragma unroll 1
+  for (int g = 0; g < 32 / kTcfGroup; ++g) {
+    const int j0 = jb + kTcfGroup * g;
+    float x[kTcfGroup];
+#pragma unroll
+    for (int k = 0; k < kTcfGroup; ++k) {
+      const int j = j0 + k;
+      x[k] = 0.0f;
+      if (i < j && j < n) {
+        const uint32_t vv = (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
+        x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv, recip);
+        tmax = fmaxf(tmax, x[k]);
+        sat |= (x[k] == -1.0f);
+        out[(size_t)j * ld + i] = x[k];  // mirror: consecutive i across lanes
+      }
+    }
+    // Row i, columns j0 .. j0 + 7 (j >= i; the diagonal is 0).
+    if (i < n) {
+#pragma unroll
+      for (int h = 0; h < kTcfGroup / 4; ++h) {
+        const int jj = j0 + 4 * h;
+        if (vec && i < jj && jj + 3 < n) {
+          *reinterpret_cast<float4 *>(orow + jj) =
+              make_float4(x[4 * h], x[4 * h + 1], x[4 * h + 2], x[4 * h + 3]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int j = jj + k;
+            if (j < n && i <= j) orow[j] = (i == j) ? 0.0f : x[4 * h + k];
+          }
+        }
+      }
+    }
+    // The next group's counts into registers 0 .. 7.
+#pragma unroll
+    for (int k = 0; k < 32 - kTcfGroup; ++k) pq[k] = pq[k + kTcfGroup];
+#pragma unroll
+    for (int k = 0; k < (32 - kTcfGroup) / 2; ++k) pv[k] = pv[k + kTcfGroup / 2];
+  }
+}
+
+__global__ void __launch_bounds__(kTcfThreads, 1)
+    tc_fused_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
+                    const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
+                    const double *__restrict__ recip) {
+  extern __shared__ uint8_t smem_raw[];
+  const TcShared sh = tc_shared(smem_raw);
+  const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);
+  const int stall = descs[0].stall;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // items [item0, min(nitems, item0 + count))
+  const int nitems = (int)min((long long)(nitems_ptr ? *nitems_ptr : nitems_direct),
+                              (long long)item0 + count);
+  const int it0 = item0 + (int)blockIdx.x;
+  if (it0 >= nitems) return;  // no item for this CTA (before any setup)
+
+  // tmem_empty: one arrival per epilogue warp
+  const uint32_t tmem = tc_setup(sh, kTcfEpiWarps, 2);
+  uint32_t issued = 0;
+
+  if (warp == 0) {
+    if (lane == 0) issued = tc_produce(sh, descs, items, it0, nitems, gridDim.x, limit);
+  } else if (warp == 1) {
+    tc_issue(sh, tmem, descs, items, it0, nitems, gridDim.x, limit);
+  } else {
+    // ----------------------------------------------------------- epilogue
+    const int q = warp & 3;              // tensor-memory lane quarter
+    const int cofs = 32 * ((warp - 2) >> 2);  // first tile column of this warp
+    const int row = 32 * q + lane;       // tile row of this lane
+    uint32_t titer = 0;
+    for (int it = it0; it < nitems; it += gridDim.x, ++titer) {
+      const WorkItem w = item_at(descs, items, it);
+      const AlnDesc &d = descs[w.aln];
+      int ti, tj;
+      item_tile(d, w.tile, ti, tj);
+      if ((stall && titer == 0 && !tc_wait(sh.never_bar, 0, sh.abort_flag, limit)) ||
+          !tc_wait(sh.acc_full, titer & 1, sh.abort_flag, limit)) {
+        *sh.abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const bool prot = d.kind == KIND_PROT_TC;
+      // Accumulators -> integer counts (DNA: transitions, transversions, valid;
+      // protein: mismatches = V - M, 0, valid), 16 columns at a time, 16 bits
+      // each (the fused form takes L < 65536): pq[k] = ts | tv << 16, and the
+      // valid counts two to a register.
+      uint32_t pq[32], pv[16];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint32_t V[16], R[16], T[16];
+        const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(cofs + 16 * h);
+        tmem_ld16(base, V);
+        tmem_ld16(base + kTile, R);
+        tmem_ld16(base + 2 * kTile, T);
+        tmem_ld_wait();
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int vv = __float2int_rn(__uint_as_float(V[k]));
+          const int rr = __float2int_rn(__uint_as_float(R[k]));
+          const int tu = __float2int_rn(__uint_as_float(T[k]));
+          const uint32_t ts = prot ? (uint32_t)(vv - rr) : (uint32_t)((vv + rr - tu) >> 2);
+          const uint32_t tv = prot ? 0u : (uint32_t)((vv - rr) >> 1);
+          pq[16 * h + k] = ts | (tv << 16);
+          if (k & 1) pv[8 * h + (k >> 1)] |= (uint32_t)vv << 16;
+          else pv[8 * h + (k >> 1)] = (uint32_t)vv;
+        }
+      }
+      // Tensor memory back to the MMA warp: the next tile's MMAs start now.
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(sh.tmem_empty);
+
+      const int i = ti * kTile + row;
+      const int jb = tj * kTile + cofs;
+      float tmax = 0.0f;
+      bool sat = false;
+      if (d.compat) {
+        fused_rows<kFusedGeneric>(d, i, jb, pq, pv, recip, tmax, sat);
+      } else if (d.model == RNJ_JC) {
+        fused_rows<kFusedJc>(d, i, jb, pq, pv, recip, tmax, sat);
+      } else if (d.type == RNJ_PROTEIN) {
+        fused_rows<kFusedProtein>(d, i, jb, pq, pv, recip, tmax, sat);
+      } else {
+        fused_rows<kFusedK2p>(d, i, jb, pq, pv, recip, tmax, sat);
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1)
+        tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, off));
+      const bool any_sat = __any_sync(0xffffffffu, sat);
+      if (lane == 0) {
+        if (tmax > 0.0f) atomicMax(d.max_bits, __float_as_int(tmax));
+        if (any_sat) d.tile_flags[w.tile] = 1;
+      }
+    }
+  }
+
+  tc_teardown(sh, tmem, issued, descs[0].err);
+}
+
+cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
+                            int nitems, int item0, int count, const double *recip, int grid,
+                            cudaStream_t s) {
+  if (grid <= 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(tc_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kTcSmemBytes);
+  if (e != cudaSuccess) return e;
+  tc_fused_kernel<<<(unsigned)grid, kTcfThreads, kTcSmemBytes, s>>>(d_descs, d_items, d_nitems,
+                                                                   nitems, item0, count, recip);
+  return cudaGetLastError();
+}
+
+}  // namespace rnj
