@@ -41,6 +41,8 @@ WORKLOADS = {
     "dna-k2p-4096x10000": ("tree_dna", 4096, 10000, "dna", "kim"),
 }
 DEFAULT = "dna-k2p-10000x10000"
+# The other single-GPU configurations, measured in the default run beside it.
+OTHER_CONFIGS = ("dna-jc-512x2000", "dna-k2p-50000x1000", "protein-kimura-5000x1500")
 # Algorithmic integer operations per pair per 32-column word of the bit-plane
 # counting kernel, (POPC, LOP3) for each (type, model): its roofline when the
 # bit planes are used (--popcount, or protein alphabets of more than 31 residues).
@@ -83,7 +85,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -168,14 +170,17 @@ def cpu_reference(seqs: np.ndarray, model: str, type_: str, warmup: int, steps: 
 
 # ------------------------------------------------------------------ GPU arm
 
-def run_gpu(args, rank: int, world: int, local_rank: int):
+def measure_workload(name: str, steps: int, warmup: int, rank: int = 0, world: int = 1,
+                     local_rank: int = 0, popcount: bool = False, with_e2e: bool = True,
+                     clocks: bool = True):
+    """One workload through the library: W warm-up steps, then K timed steps
+    (CUDA events on the library's stream, a 256 MiB buffer written between
+    steps so that L2 starts cold).  Returns the figures of the JSON line."""
     import torch
     import torch.distributed as dist
     from rapidnj_b200 import api, sharded
 
-    name = args.workload
     gen, n, L, type_, model = WORKLOADS[name]
-    torch.cuda.set_device(local_rank)
     seqs = make_alignment(name, seed=0)
     typ = 0 if type_ == "dna" else 1
     ctx = api.Context(local_rank)
@@ -187,7 +192,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
 
     def step():
-        aln = ctx.alignment(d_chars, typ, popcount=args.popcount)
+        aln = ctx.alignment(d_chars, typ, popcount=popcount)
         if world > 1:
             # this rank's contiguous range of tiles; one float MAX all-reduce
             sh = api.Shard(ctx, aln, model, rank, world, out)
@@ -197,15 +202,17 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             ctx.distance_into(aln, model, out)
         aln.close()
 
-    for _ in range(args.warmup):
+    # The clock record covers the warm-up and the timed steps (the timed region
+    # alone can be shorter than one nvidia-smi sample).
+    sampler = ClockSampler(local_rank).start() if clocks else None
+    for _ in range(warmup):
         step()
     ctx.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local_rank).start()
     total_ms, count_ms, post_ms, pack_ms = 0.0, [], [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         with torch.cuda.stream(stream):
             flush.zero_()  # L2 flush between timed steps (outside the events)
         a = torch.cuda.Event(enable_timing=True)
@@ -220,44 +227,55 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         post_ms.append(st[2])
         pack_ms.append(st[0])
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = sampler.stop() if sampler else None
     if world > 1:
         t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
         dist.barrier()
-    ms_per_step = total_ms / args.steps
+    ms_per_step = total_ms / steps
     W = units(n, L)  # the whole matrix, whatever the number of ranks
     # this rank's share of the tiles (all of them on one GPU)
     t0, t1, ntiles = api.shard_tiles(n, rank, world)
     share = (t1 - t0) / ntiles
     mean = lambda x: sum(x) / len(x)  # noqa: E731
+    tc = not popcount and (type_ == "dna" or residue_ranks(seqs) <= 31)
+    fused = tc and L <= 65535 and world == 1
     result = {"ms_per_step": ms_per_step, "value": W / (ms_per_step * 1e-3), "clocks": clk,
-              "count_ms": count_ms,
-              "stages_ms": {"pack": mean(pack_ms), "count": mean(count_ms),
-                            "transform_and_fixup": mean(post_ms)}}
+              "stages_ms": {"pack": mean(pack_ms),
+                            "count_and_transform" if fused else "count": mean(count_ms),
+                            "fixup" if fused else "transform_and_fixup": mean(post_ms)},
+              "kernel": "tcgen05" if tc else "popcount",
+              # per step: (protein: presence scan) + pack + counting kernel(s) + fix-up
+              "gpu_launches_per_step": (1 if type_ == "protein" else 0) + 3 +
+                                       (0 if (fused or not tc) else 1)}
 
     if rank == 0:
-        cnt = sum(count_ms) / len(count_ms)
-        if not args.popcount and (type_ == "dna" or residue_ranks(seqs) <= 31):
-            # tcgen05 kernel, against the dense FP4 tensor peak: DNA 4 FP4 MACs
-            # (8 flops) per pair-column; protein 1 + R MACs (valid + one-hot of
-            # R residue ranks).
+        cnt = mean(count_ms)
+        if tc:
+            # tcgen05 kernel, against the FP4 tensor pipe measured live on this
+            # device (back-to-back kind::mxf4 MMAs, rnj_probe_tc_peak): DNA 4 FP4
+            # MACs (8 flops) per pair-column; protein 1 + R MACs (valid + one-hot
+            # of R residue ranks).
             fpc = 8 if type_ == "dna" else 2 * (1 + residue_ranks(seqs))
-            peak, peak_source = fp4_tensor_peak(local_rank)
-            achieved = fpc * units(n, L) * share / (cnt * 1e-3)
-            result["roofline"] = {
-                "bound": "tensor", "achieved": achieved / 1e12, "peak": peak / 1e12,
-                "unit": "TFLOP/s", "format": "fp4 e2m1 operands (tcgen05 kind::mxf4), f32 sums",
-                "frac": achieved / peak, "traffic": traffic_from_profiles(name),
-                "kernel": "tc_batch_kernel", "kernel_ms": cnt, "peak_source": peak_source,
-                "flops_per_pair_column": fpc,
-            }
-            # The raw tensor pipe: back-to-back kind::mxf4 MMAs on every SM with
-            # the operands already in shared memory (rnj_probe_tc_peak, this run).
             pipe = ctx.probe_tc_peak()
-            result["roofline"]["tensor_pipe_peak"] = pipe / 1e12
-            result["roofline"]["frac_of_tensor_pipe"] = achieved / pipe
+            bf16x4, bf16_src = fp4_from_bf16()
+            achieved = fpc * units(n, L) * share / (cnt * 1e-3)
+            kname = "tc_fused_kernel" if fused else "tc_batch_kernel"
+            result["roofline"] = {
+                "bound": "tensor", "achieved": achieved / 1e12, "peak": pipe / 1e12,
+                "unit": "TFLOP/s", "frac": achieved / pipe,
+                "format": "fp4 e2m1 operands (tcgen05 kind::mxf4), f32 sums",
+                "peak_source": "FP4 tensor pipe measured on this device in this run "
+                               "(rnj_probe_tc_peak: back-to-back 128x128x64 kind::mxf4 MMAs "
+                               "on every SM); 4 x measured dense bf16 beside it",
+                "peak_4x_bf16": bf16x4 / 1e12, "frac_of_4x_bf16": achieved / bf16x4,
+                "peak_4x_bf16_source": bf16_src,
+                "traffic": traffic_from_profiles(name), "kernel": kname, "kernel_ms": cnt,
+                "flops_per_pair_column": fpc,
+                "kernel_includes": ("counts, exact transform and the matrix stores" if fused
+                                    else "counts (the transform is a second kernel)"),
+            }
         else:
             # Bit-plane popcount kernel: bound by the POPC pipe, against the
             # POPC peak measured on this device.
@@ -275,15 +293,19 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                 "peak_source": "rnj_probe_int_peaks, measured on this device in this run",
                 "ops_per_pair_word": {"popc": popc_w, "lop3": lop3_w},
             }
-    if world > 1:
-        result["e2e"] = run_e2e_sharded(ctx, seqs, typ, model, args, rank, world, local_rank)
-    elif rank == 0:
-        result["e2e"] = run_e2e(ctx, seqs, typ, model, args)
+    if with_e2e:
+        if world > 1:
+            result["e2e"] = run_e2e_sharded(ctx, seqs, typ, model, steps, popcount, rank, world,
+                                            local_rank)
+        elif rank == 0:
+            result["e2e"] = run_e2e(ctx, seqs, typ, model, steps, popcount)
+    del out, flush, d_chars
     ctx.close()
+    torch.cuda.empty_cache()
     return result
 
 
-def run_e2e(ctx, seqs, typ, model, args):
+def run_e2e(ctx, seqs, typ, model, steps, popcount=False):
     """The same metric through the host-facing C ABI call (rnj_distance_matrix_host):
     page-locked host bytes in, the caller's page-locked host n x n float matrix
     out; upload, pack, distances and the device-to-host copy of the whole matrix
@@ -294,12 +316,12 @@ def run_e2e(ctx, seqs, typ, model, args):
     host = pinned.numpy()
     # the caller's result matrix: page-locked host memory, allocated once
     out = torch.empty((n, n), dtype=torch.float32).pin_memory().numpy()
-    steps = max(1, min(args.steps, 10))
-    ctx.distance_matrix_host(host, model, typ, popcount=args.popcount, out=out)  # warm-up
+    steps = max(1, min(steps, 10))
+    ctx.distance_matrix_host(host, model, typ, popcount=popcount, out=out)  # warm-up
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        ctx.distance_matrix_host(host, model, typ, popcount=args.popcount, out=out)
+        ctx.distance_matrix_host(host, model, typ, popcount=popcount, out=out)
         times.append(time.perf_counter() - t0)
     # median step: the host side shares its cores with other jobs on the machine
     med = statistics.median(times)
@@ -309,7 +331,7 @@ def run_e2e(ctx, seqs, typ, model, args):
             "call": "rnj_distance_matrix_host"}
 
 
-def run_e2e_sharded(ctx, seqs, typ, model, args, rank, world, local_rank):
+def run_e2e_sharded(ctx, seqs, typ, model, steps, popcount, rank, world, local_rank):
     """The multi-GPU end to end: every rank uploads the host alignment (pinned),
     packs it, computes its tiles, joins the one MAX all-reduce, applies the cap
     and copies its own tiles into pinned host memory.  Time = max over ranks."""
@@ -320,12 +342,12 @@ def run_e2e_sharded(ctx, seqs, typ, model, args, rank, world, local_rank):
     pinned = torch.from_numpy(seqs).pin_memory()
     host = torch.empty((n, n), dtype=torch.float32).pin_memory().numpy()
     stream = torch.cuda.ExternalStream(ctx.stream)
-    steps = max(1, min(args.steps, 5))
+    steps = max(1, min(steps, 5))
 
     def once():
         with torch.cuda.stream(stream):
             d = pinned.to(f"cuda:{local_rank}", non_blocking=True)
-        aln = ctx.alignment(d, typ, popcount=args.popcount)
+        aln = ctx.alignment(d, typ, popcount=popcount)
         sh = api.Shard(ctx, aln, model, rank, world)
         sharded.run_sharded(sh, None, local_rank)
         nbytes = sh.copy_tiles(host)
@@ -701,41 +723,15 @@ def run_text(args, local_rank: int = 0):
             "workload": f"-o m text of the {args.workload} matrix into a file (page cache)"}
 
 
-def fp4_tensor_peak(device: int):
-    """Dense FP4 tensor throughput (flop/s) of a library GEMM on this device, and
-    how it was obtained: an MXFP4 GEMM (torch._scaled_mm, unit block scales,
-    8192^3) when this torch build offers one, else four times the measured dense
-    bf16 peak of MEASURED_PEAKS.json (the dense FP4 : BF16 rate ratio of B200)."""
-    import torch
-    m = 8192
-    dev = f"cuda:{device}"
+def fp4_from_bf16():
+    """Four times the measured dense bf16 GEMM throughput of MEASURED_PEAKS.json
+    (flop/s; the dense FP4 : BF16 rate ratio of B200), and its source."""
     try:
-        a = torch.randint(0, 256, (m, m // 2), dtype=torch.uint8, device=dev)
-        b = torch.randint(0, 256, (m, m // 2), dtype=torch.uint8, device=dev)
-        a = a.view(torch.float4_e2m1fn_x2)
-        b = b.view(torch.float4_e2m1fn_x2).t()
-        sa = torch.full((m, m // 32), 127, dtype=torch.uint8, device=dev).view(torch.float8_e8m0fnu)
-        sb = torch.full((m, m // 32), 127, dtype=torch.uint8, device=dev).view(torch.float8_e8m0fnu)
-        best = 0.0
-        for k in range(12):
-            s0 = torch.cuda.Event(enable_timing=True)
-            s1 = torch.cuda.Event(enable_timing=True)
-            s0.record()
-            torch._scaled_mm(a, b, sa, sb, out_dtype=torch.bfloat16)
-            s1.record()
-            s1.synchronize()
-            if k >= 2:
-                best = max(best, 2.0 * m ** 3 / (s0.elapsed_time(s1) * 1e-3))
-        return best, "MXFP4 GEMM (torch._scaled_mm, 8192^3, unit scales, best of 10) measured on " \
-                     "this device in this run"
-    except Exception as e:  # no FP4 GEMM in this torch build
-        why = str(e).splitlines()[0][:120] if str(e) else type(e).__name__
-        try:
-            bf16 = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"] * 1e12
-            src = "MEASURED_PEAKS.json bf16_tflops"
-        except Exception:
-            bf16, src = 1.59e15, "fallback bf16 1.59 PFLOP/s"
-        return 4.0 * bf16, f"4 x measured dense bf16 ({src}); FP4 GEMM unavailable: {why}"
+        bf16 = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"] * 1e12
+        src = "4 x MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)"
+    except Exception:
+        bf16, src = 1.59e15, "4 x the fallback bf16 1.59 PFLOP/s"
+    return 4.0 * bf16, src
 
 
 def traffic_from_profiles(name: str):
@@ -762,10 +758,10 @@ def main():
     ap.add_argument("--popcount", action="store_true",
                     help="count DNA with the bit-plane popcount kernel instead of tensor cores")
     ap.add_argument("--mode", default="all",
-                    choices=["all", "plain", "batched", "served", "bootstrap", "njinit", "parse",
-                             "text"],
-                    help="all: the plain workload line plus the batched, served, bootstrap, "
-                         "parse, text and NJ set-up figures")
+                    choices=["all", "plain", "configs", "batched", "served", "bootstrap",
+                             "njinit", "parse", "text"],
+                    help="all: the plain workload line plus the other configurations and the "
+                         "batched, served, bootstrap, parse, text and NJ set-up figures")
     ap.add_argument("--nj-n", type=int, default=10000,
                     help="sequences (and columns) of the NJ set-up workload (njinit)")
     args = ap.parse_args()
@@ -806,24 +802,46 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    res = run_gpu(args, rank, world, local_rank)
+    res = measure_workload(args.workload, args.steps, args.warmup, rank, world, local_rank,
+                           popcount=args.popcount)
     if rank == 0:
+        tc = res["kernel"] == "tcgen05"
         line = {"metric": "pair-column comparisons/s", "value": res["value"],
                 "unit": "pair-columns/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
                 "higher_is_better": True, "scaling": "strong",
-                "vs_baseline": None, "dtype": "fp4" if config["kernel"] == "tcgen05" else "u32",
+                "vs_baseline": None, "dtype": "fp4" if tc else "u32",
+                "dtype_note": ("exact integer counts: the FP4 e2m1 operands hold -1, 0, +1 "
+                               "exactly and every f32 tensor sum is an integer below 2^24; the "
+                               "transform is the reference's float/double arithmetic" if tc else
+                               "exact integer counts from bit planes (POPC/LOP3)"),
                 "data": "synthetic", "config": config, "roofline": res["roofline"],
                 "e2e": res["e2e"], "clocks": res["clocks"], "stages_ms": res["stages_ms"],
-                # per step: (protein: presence scan) + pack + count (+ transform on
-                # the tensor cores) + fix-up
-                "gpu_launches": ((1 if type_ == "protein" else 0) + 3 +
-                                 (1 if config["kernel"] == "tcgen05" else 0)) * args.steps}
+                "gpu_launches": res["gpu_launches_per_step"] * args.steps}
         if not args.no_cpu_baseline and world == 1:
             seqs = make_alignment(args.workload)
             cpu = cpu_reference(seqs, model, type_, 0, 1)
             line["cpu_baseline"] = ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
                                     if cpu else None)
+        # The other single-GPU configurations of the workload list, each with its
+        # own roofline, end-to-end figure and CPU baseline (guarded: a failure is
+        # reported in the line, which is still printed).
+        if args.mode in ("all", "configs") and world == 1:
+            line["configs"] = {}
+            for name in OTHER_CONFIGS:
+                try:
+                    r = measure_workload(name, min(args.steps, 10), 3, local_rank=local_rank,
+                                         popcount=args.popcount)
+                    r.pop("clocks", None)
+                    if not args.no_cpu_baseline:
+                        _, _, _, t_, m_ = WORKLOADS[name]
+                        cpu = cpu_reference(make_alignment(name), m_, t_, 0, 1, budget_s=8.0)
+                        r["cpu_baseline"] = ({k: cpu[k] for k in
+                                              ("value", "unit", "cores", "kind", "sample")}
+                                             if cpu else None)
+                    line["configs"][name] = r
+                except Exception as e:  # noqa: BLE001
+                    line["configs"][name] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
         # the batched and served forms are single-GPU (replicas at N > 1); an
         # extra figure that fails is reported as such, the line still printed
         extras = (("batched", run_batched), ("served", run_served),

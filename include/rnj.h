@@ -213,6 +213,33 @@ int rnj_mat_destroy(rnj_mat *mat);
 int rnj_distance_noalloc(const void *d_chars, int n, int L, size_t ld, int type, int model,
                          int flags, float *d_out, size_t ld_out, void *stream, float *max_out);
 
+/* ------------------------------------------------- matrices beyond device memory */
+
+/* Receives rows [row0, row0 + nrows) of the distance matrix, row k at
+ * rows + k * ld (page-locked host memory, valid during the call).  Returns 0 to
+ * go on, non-zero to stop the computation (the call then fails). */
+typedef int (*rnj_rows_fn)(void *user, int row0, int nrows, const float *rows, size_t ld);
+
+/* The distance matrix of an alignment whose n x n floats need not fit in device
+ * memory: the rows are computed in bands of band_rows (rounded up to 128; 0:
+ * two bands of at most 512 MiB) with device buffers for two bands only, and
+ * handed to fn in row order while the next band computes.  Each row is complete
+ * (j = 0 .. n - 1, every ordered pair counted, as rapidNJ's disk-matrix drivers
+ * compute them, KimuraDistance.cpp:308-354 / JCdistance.cpp:160-195 with
+ * dm != NULL), with 0 on the diagonal and -1 for saturated pairs: the rows
+ * those drivers pass to diskMatrix::writeArray (diskMatrix.cpp:96-117).  When
+ * the call returns, *max_out holds the maximum distance and *saturated_out
+ * (both may be NULL) is 1 if any pair saturated; the caller's post-process then
+ * replaces every -1 by 2 * max (KimuraDistance.cpp:366-395,
+ * JCdistance.cpp:201-230).  Alignments of at most 65535 columns (tensor-core
+ * layouts) or 65280 (bit planes).  Device memory: the packed alignment, two
+ * bands of band_rows x n floats, one int per 128 x 128 tile of the full square. */
+int rnj_distance_rows(rnj_ctx *ctx, rnj_aln *aln, int model, int band_rows, rnj_rows_fn fn,
+                      void *user, float *max_out, int *saturated_out);
+
+/* Free and total memory of the context's device, in bytes (cudaMemGetInfo). */
+int rnj_ctx_memory(rnj_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
+
 /* One call, host in / host out: pack, distances, copy into out (n*n floats,
  * row-major).  max_out may be NULL.  This is what JCdistance::computeDistanceMatrix
  * (JCdistance.cpp:24-44) and KimuraDistance::computeDistances

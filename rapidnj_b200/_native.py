@@ -47,6 +47,9 @@ SIGNATURES = {
     "rnj_ctx_stream": (c_int, [c_void_p, P(c_void_p)]),
     "rnj_ctx_synchronize": (c_int, [c_void_p]),
     "rnj_set_wait_limit": (c_int, [ctypes.c_uint]),
+    "rnj_ctx_memory": (c_int, [c_void_p, P(c_size_t), P(c_size_t)]),
+    "rnj_distance_rows": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                  P(c_float), P(c_int)]),
     "rnj_test_wait_on_unset_flag": (c_int, [c_int]),
     "rnj_detect_type": (c_int, [c_char_p, c_int]),
     "rnj_ctx_set_profiling": (c_int, [c_void_p, c_int]),
@@ -127,6 +130,10 @@ SIGNATURES = {
     "rnj_write_matrix_text_device": (c_int, [c_void_p, c_char_p, P(c_char_p), c_void_p, c_size_t,
                                              c_int]),
 }
+
+
+# rnj_rows_fn: int (*)(void *user, int row0, int nrows, const float *rows, size_t ld)
+ROWS_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_int, c_int, P(c_float), c_size_t)
 
 
 class NjData(ctypes.Structure):

@@ -196,6 +196,39 @@ class Context:
                                         ctypes.byref(m) if want_max else None))
         return m.value if want_max else None
 
+    def distance_rows(self, aln: Alignment, model, on_rows, band_rows: int = 0):
+        """The matrix in bands of full rows (rnj_distance_rows), for matrices larger
+        than device memory: on_rows(row0, rows) receives each band as a float32
+        array view (valid during the call; copy what you keep), rows as the
+        reference's disk-matrix drivers write them (diagonal 0, saturated pairs -1).
+        Returns (max distance, whether a pair saturated)."""
+        err = []
+
+        def cb(_user, row0, nrows, ptr, ld):
+            try:
+                arr = np.ctypeslib.as_array(ptr, shape=(nrows, ld))
+                on_rows(row0, arr[:, :aln.n])
+                return 0
+            except Exception as e:  # noqa: BLE001 -- reported after the call
+                err.append(e)
+                return 1
+
+        fn = N.ROWS_FN(cb)
+        mx, sat = ctypes.c_float(), ctypes.c_int()
+        st = N.lib().rnj_distance_rows(self.handle, aln.handle, MODELS[model], band_rows,
+                                       ctypes.cast(fn, ctypes.c_void_p), None, ctypes.byref(mx),
+                                       ctypes.byref(sat))
+        if err:
+            raise err[0]
+        check(st)
+        return mx.value, bool(sat.value)
+
+    def memory(self):
+        """(free, total) bytes of the context's device."""
+        f, t = ctypes.c_size_t(), ctypes.c_size_t()
+        check(N.lib().rnj_ctx_memory(self.handle, ctypes.byref(f), ctypes.byref(t)))
+        return f.value, t.value
+
     def counts_into(self, aln: Alignment, out) -> None:
         """Raw counts into a CUDA int32/uint32 tensor of n*n*3 elements."""
         check(N.lib().rnj_counts_into(self.handle, aln.handle, ctypes.c_void_p(out.data_ptr())))

@@ -172,6 +172,7 @@ AlnDesc desc_for(const Packed &p, const EpiParams &ep) {
   d.np = is_tc_kind(p.kind) ? p.nfb : p.NP;
   d.wait_us = (int)ep.wait_us;
   d.stall = ep.stall;
+  d.row0 = ep.row0;
   d.jc_b = ep.jc_b;
   return d;
 }
@@ -447,12 +448,10 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
   }
   if (tp.tc_epilogue == 0 && p.L <= kMaxFusedColumns) {
     // Counts and transform in one launch (rnj_tcf.cu).
-    int rc = ensure_recip(ctx, p.L);
-    if (rc != RNJ_OK) return rc;
     mark(ctx, 1, 0);
     RNJ_CUDA(launch_tc_fused(ctx->d_desc, nullptr, nullptr, (int)ntiles, 0, (int)ntiles,
-                             ctx->d_recip, (int)std::min<long long>(ntiles, ctx->num_sms),
-                             ctx->stream),
+                             (int)std::min<long long>(ntiles, ctx->num_sms),
+                             fused_variant_for(ep.model, ep.type, ep.compat_wrap, 0), ctx->stream),
              "fused tensor-core kernel");
     mark(ctx, 1, 1);
     mark(ctx, 2, 0);
@@ -575,26 +574,6 @@ int ensure_packed(rnj_ctx *ctx, long long tiles) {
   return RNJ_OK;
 }
 
-int ensure_recip(rnj_ctx *ctx, int L) {
-  if (ctx->d_recip && ctx->recip_L >= L) return RNJ_OK;
-  // At least every 16-bit count: the fused kernel's counts are 16-bit fields.
-  const int cap = std::max(65535, (L + 4095) / 4096 * 4096);
-  std::vector<double> h((size_t)cap + 1);
-  h[0] = 0.0;
-  for (int k = 1; k <= cap; ++k) h[k] = 1.0 / (double)k;  // IEEE division: the nearest double
-  if (ctx->d_recip) cudaFreeAsync(ctx->d_recip, ctx->stream);
-  ctx->d_recip = nullptr;
-  ctx->recip_L = 0;
-  RNJ_CUDA(cudaMallocAsync((void **)&ctx->d_recip, h.size() * sizeof(double), ctx->stream),
-           "reciprocal table");
-  // From pageable memory: the bytes are taken before the call returns.
-  RNJ_CUDA(cudaMemcpyAsync(ctx->d_recip, h.data(), h.size() * sizeof(double),
-                           cudaMemcpyHostToDevice, ctx->stream),
-           "reciprocal table upload");
-  ctx->recip_L = cap;
-  return RNJ_OK;
-}
-
 int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, long long nitems,
                   uint64_t *packed, cudaStream_t s, int transform_ctas) {
   const int ctas = transform_ctas > 0 ? std::min(transform_ctas, kTransformCtasPerSm)
@@ -672,7 +651,6 @@ int rnj_ctx_destroy(rnj_ctx *ctx) {
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->d_desc) cudaFree(ctx->d_desc);
   if (ctx->d_packed) cudaFree(ctx->d_packed);
-  if (ctx->d_recip) cudaFree(ctx->d_recip);
   if (ctx->h_mask) cudaFreeHost(ctx->h_mask);
   if (ctx->h_max) cudaFreeHost(ctx->h_max);
   for (int b = 0; b < 2; ++b)
@@ -719,6 +697,16 @@ int rnj_ctx_stage_times(rnj_ctx *ctx, float *ms) {
     if (ctx->profiling && ctx->ev_used[k])
       RNJ_CUDA(cudaEventElapsedTime(&ms[k], ctx->ev[2 * k], ctx->ev[2 * k + 1]), "stage time");
   }
+  return RNJ_OK;
+}
+
+int rnj_ctx_memory(rnj_ctx *ctx, size_t *free_bytes, size_t *total_bytes) {
+  if (!ctx) return set_error(RNJ_ERR_INVALID, "null context");
+  DeviceGuard g(ctx->device);
+  size_t f = 0, t = 0;
+  RNJ_CUDA(cudaMemGetInfo(&f, &t), "cudaMemGetInfo");
+  if (free_bytes) *free_bytes = f;
+  if (total_bytes) *total_bytes = t;
   return RNJ_OK;
 }
 

@@ -156,18 +156,36 @@ __device__ __forceinline__ float neg_log_checked(double c, double arg) {
 
 // The float quotient fl32(num / den) of integers 0 <= num <= den < 2^24, the
 // value of both (float)num / (float)den and (float)((double)num / (double)den)
-// in the reference.  With rn = the double nearest to 1 / den (a per-context
-// table, filled on the host), d = fl64(num * rn) is within 2^-52 (relative) of
-// num / den.  A float rounding boundary m (the midpoint of two floats) has 25
-// significant bits, m = (2k + 1) 2^-s with 2k + 1 >= 2^24; num / den = m would
-// need 2k + 1 to divide num < 2^24, so num / den != m and
-// |num / den - m| >= 1 / (den 2^s), at least 2^-49 relative to m.  d therefore
-// lies on the same side of every boundary as num / den and rounds to the same
-// float.  rn == 0 (no table) divides instead.
+// in the reference.  Given rn within 2^-51 (relative) of 1 / den (recip_nr),
+// d = fl64(num * rn) is within 2^-50 of num / den.  A float rounding boundary
+// m (the midpoint of two floats) has 25 significant bits, m = (2k + 1) 2^-s
+// with 2k + 1 >= 2^24; num / den = m would need 2k + 1 to divide num < 2^24, so
+// num / den != m and |num / den - m| >= 1 / (den 2^s), at least 2^-49 relative
+// to m.  d therefore lies on the same side of every boundary as num / den and
+// rounds to the same float.  rn == 0 divides instead.
 __device__ __forceinline__ float ratio_f32(unsigned long long num, unsigned long long den,
                                            double rn) {
   if (rn != 0.0) return __double2float_rn(__dmul_rn((double)num, rn));
   return __fdiv_rn(__ull2float_rn(num), __ull2float_rn(den));
+}
+
+// 1 / n for an integer 1 <= n < 2^24, within 2^-52.9 (relative), by Newton-
+// Raphson iteration for the reciprocal, r <- r + r (1 - n r), from the float
+// reciprocal of n.  With r = (1 / n)(1 - e), one step gives (1 / n)(1 - e^2)
+// before rounding:
+//   r0 = __frcp_rn(n)        |e0| <= 2^-24 (a correctly rounded float)
+//   t0 = fma(-n, r0, 1) = e0 exactly (n r0 has at most 48 significant bits and
+//        lies within 2^-24 of 1, so the product and the difference are exact)
+//   r1 = fma(r0, t0, r0)     |e1| <= 2^-48 + 2^-53
+//   t1 = fma(-n, r1, 1)      = e1 (1 + 2^-53 at most)
+//   r2 = fma(r1, t1, r1)     |e2| <= e1^2 + 2^-53 + ... < 2^-52.9
+// which is well inside the 2^-51 that ratio_f32 needs.  n = 0 gives a NaN
+// (callers treat valid == 0 before any quotient).
+__device__ __forceinline__ double recip_nr(uint32_t n) {
+  const double dn = (double)n;
+  const double r0 = (double)__frcp_rn((float)n);
+  const double r1 = __fma_rn(r0, __fma_rn(-dn, r0, 1.0), r0);
+  return __fma_rn(r1, __fma_rn(-dn, r1, 1.0), r1);
 }
 
 // The undecided cases of the table logarithm (about one pair in 10^6): the
@@ -181,7 +199,7 @@ static __device__ __noinline__ float k2p_two_logs(double a, double b) {
 }
 
 // JCdistance.cpp:171-183.  b = (alpha - 1) / alpha in double, alpha 4 or 20.
-// rn: the reciprocal of valid (ratio_f32), or 0.
+// rn: an approximate reciprocal of valid (recip_nr; see ratio_f32), or 0.
 __device__ __forceinline__ float jc_distance(unsigned long long total,
                                              unsigned long long valid, double b,
                                              double rn = 0.0) {
@@ -198,7 +216,8 @@ __device__ __forceinline__ float jc_distance(unsigned long long total,
   return neg_log_slow(b, arg);
 }
 
-// KimuraDistance.cpp:339-349.  rn: the reciprocal of valid (ratio_f32), or 0.
+// KimuraDistance.cpp:339-349.  rn: an approximate reciprocal of valid
+// (recip_nr; see ratio_f32), or 0.
 __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
                                               unsigned long long tv_count,
                                               unsigned long long valid, double rn = 0.0) {
@@ -252,8 +271,32 @@ __device__ __forceinline__ float k2p_distance(unsigned long long ts_count,
   return k2p_two_logs(a, b);
 }
 
+// The K2P distance of k2p_distance for 1 <= n < 2^24 (the fused kernel's
+// counts), without branches, so that the pairs of a group interleave: the
+// saturated (-1) and identical (-0.0) cases and the one-logarithm value are
+// computed for every pair and selected.  *slow is set when the rounding check
+// cannot decide (about one pair in 10^6-10^7); the caller then evaluates
+// k2p_distance for that pair.  n == 0 gives -1 like k2p_distance.
+__device__ __forceinline__ float k2p_decide(uint32_t P, uint32_t Q, uint32_t n, bool &slow) {
+  const double rn = recip_nr(n == 0 ? 1u : n);
+  const float ts = __double2float_rn(__dmul_rn((double)P, rn));
+  const float tv = __double2float_rn(__dmul_rn((double)Q, rn));
+  const double a = __dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, (double)ts)), (double)tv);
+  const double b = __dsub_rn(1.0, __dmul_rn(2.0, (double)tv));
+  const bool sat = (n == 0) | (__double2float_rn(a) <= 0.0f) | (__double2float_rn(b) <= 0.0f);
+  const bool same = (P | Q) == 0;
+  // a, b in (0, 1] unless saturated: ln_table's argument stays positive.
+  const double x = sat ? 1.0 : __dmul_rn(__dmul_rn(a, a), b);
+  const double dd = __dmul_rn(-0.25, ln_table(x));
+  const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
+  const float lo = __double2float_rn(__dsub_rn(dd, eps));
+  const float hi = __double2float_rn(__dadd_rn(dd, eps));
+  slow = !sat && !same && (__float_as_int(lo) != __float_as_int(hi));
+  return sat ? -1.0f : (same ? -0.0f : lo);
+}
+
 // KimuraDistance.cpp:322-338 with the Dayhoff table of KimuraDistance.cpp:30-49.
-// rn: the reciprocal of valid (ratio_f32), or 0.
+// rn: an approximate reciprocal of valid (recip_nr; see ratio_f32), or 0.
 __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism,
                                                          unsigned long long valid,
                                                          const int *pam, double rn = 0.0) {

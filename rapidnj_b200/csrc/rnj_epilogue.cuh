@@ -47,16 +47,16 @@ __device__ __forceinline__ void tri_coords(int t, int nt, int &ti, int &tj) {
 __device__ __forceinline__ int row_of(int rbase, int r) { return rbase + (r < 4 ? r : 12 + r); }
 __device__ __forceinline__ int col_of(int cbase, int c) { return cbase + (c < 4 ? c : 28 + c); }
 
-// The exact distance of one pair from its counts.  recip (may be null): the
-// context's table of reciprocals 1 / k for k = 0 .. L (entry 0 unused, 0.0),
-// which replaces the float divisions by a multiply (ratio_f32); the wrapping
-// valid count of RNJ_COMPAT_PROTEIN_WRAP divides.
+// The exact distance of one pair from its counts.  nr_quotients: the float
+// quotients by the valid count come from its Newton-Raphson reciprocal
+// (recip_nr, ratio_f32; the same floats) instead of divisions; the wrapping
+// valid count of RNJ_COMPAT_PROTEIN_WRAP always divides.
 __device__ __forceinline__ float pair_distance(const EpiParams &ep, uint32_t c0, uint32_t c1,
-                                               uint32_t valid, const double *recip = nullptr) {
+                                               uint32_t valid, bool nr_quotients = false) {
   unsigned long long v = valid;
   double rn = 0.0;
   if (ep.compat_wrap) v = protein_fast_valid(v, ep.L);
-  else if (recip) rn = __ldg(recip + valid);
+  else if (nr_quotients && valid != 0 && valid < (1u << 24)) rn = recip_nr(valid);
   if (ep.model == RNJ_JC) return jc_distance((unsigned long long)c0 + c1, v, ep.jc_b, rn);
   if (ep.type == RNJ_PROTEIN) return kimura_protein_distance(c0, v, c_pam, rn);
   return k2p_distance(c0, c1, v, rn);
@@ -108,7 +108,7 @@ __device__ __forceinline__ void store_distances(const EpiParams &ep, int ti, int
   for (int r = warp; r < kTile; r += nwarps) {
     const int i = i0 + r;
     if (i >= n) break;
-    float *row = ep.out + (size_t)i * ep.ld + j0;
+    float *row = ep.out + (size_t)(i - ep.row0) * ep.ld + j0;
 #pragma unroll
     for (int q = 0; q < kTile / 32; ++q) {
       const int cl = lane + 32 * q;
@@ -124,7 +124,7 @@ __device__ __forceinline__ void store_distances(const EpiParams &ep, int ti, int
     for (int c = warp; c < kTile; c += nwarps) {
       const int j = j0 + c;
       if (j >= n) break;
-      float *row = ep.out + (size_t)j * ep.ld + i0;
+      float *row = ep.out + (size_t)(j - ep.row0) * ep.ld + i0;
 #pragma unroll
       for (int q = 0; q < kTile / 32; ++q) {
         const int rl = lane + 32 * q;

@@ -94,6 +94,8 @@ struct EpiParams {
   int *err = nullptr;         // device error word (bit 0: a bounded wait ran out)
   uint32_t wait_us = 0;       // bound of the pipeline waits in microseconds (0: 2 s)
   int stall = 0;              // test of the failure path: wait on a barrier nothing completes
+  int row0 = 0;               // output row offset: row i is stored at out + (i - row0) * ld
+  int tile0 = 0;              // bit-plane kernel: tile of block 0 (a band of full-square tiles)
 };
 
 // One alignment of a work list, as the persistent kernels read it from device
@@ -111,7 +113,7 @@ struct alignas(128) AlnDesc {
   int kind, np, band, wait_us; // np: planes, or feature blocks (tensor-core kinds);
                                // band: tile-order band height (single alignment), 0 = 12;
                                // wait_us: bound of the pipeline waits (0: 2 s)
-  int stall, pad2;             // stall: as EpiParams::stall
+  int stall, row0;             // stall, row0: as EpiParams
   double jc_b;
 };
 
@@ -175,9 +177,11 @@ cudaError_t launch_pack_features_multi(const PackJob *d_jobs, int njobs, long lo
                                        cudaStream_t s);
 cudaError_t launch_pack_bitstrings_dna(const uint32_t *d_bits, const uint32_t *d_gaps,
                                        int bs_words, const Packed &p, cudaStream_t s);
-// kchunk > 0: words of K per CTA (EPI_ATOMIC splits K over grid.y).
+// kchunk > 0: words of K per CTA (EPI_ATOMIC splits K over grid.y).  ntiles > 0:
+// only tiles [ep.tile0, ep.tile0 + ntiles) (EPI_DIST; a band of full-square tiles).
 cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode,
-                               const EpiParams &ep, cudaStream_t s, int kchunk = 0);
+                               const EpiParams &ep, cudaStream_t s, int kchunk = 0,
+                               long long ntiles = 0);
 cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s);
 // Loads every bit-plane kernel a fused distance call can launch (pack, presence
 // scan, counts of each plane layout, fix-up).  Under CUDA's lazy module loading a
@@ -224,10 +228,15 @@ cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
 // launch over work items [item0, min(n, item0 + count)) (d_items == nullptr: the
 // banded tiles of d_descs[0]; d_nitems == nullptr: n = nitems); distances
 // straight into each alignment's output, with its max slot and saturation
-// flags.  recip: reciprocals 1 / k for k = 0 .. max L (entry 0 = 0).  Every
-// alignment has at most kMaxFusedColumns columns.
+// flags.  Every alignment has at most kMaxFusedColumns columns.
+// variant: the transform of every item (fused_variant_for), or FUSED_ANY to
+// choose per item from its descriptor.
+enum FusedVariant {
+  FUSED_K2P = 0, FUSED_JC = 1, FUSED_PROTEIN = 2, FUSED_GENERIC = 3, FUSED_FULL = 4, FUSED_ANY = 5
+};
+int fused_variant_for(int model, int type, int compat, int full);
 cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
-                            int nitems, int item0, int count, const double *recip, int grid,
+                            int nitems, int item0, int count, int grid, int variant,
                             cudaStream_t s);
 
 enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2, EPI_PACKED = 3 };

@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(256, 1)
   uint64_t *full_bar = reinterpret_cast<uint64_t *>(smem + ST * 2 * TILE_WORDS);
 
   int ti, tj;
-  const int tile_id = blockIdx.x;
+  const int tile_id = ep.tile0 + (int)blockIdx.x;
   if (ep.full) {
     ti = tile_id / nt;
     tj = tile_id % nt;
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(256) transform_counts_kernel(int nt, EpiParams
   extern __shared__ uint8_t smem_raw[];
   float *S = reinterpret_cast<float *>(smem_raw);
   int ti, tj;
-  const int tile_id = blockIdx.x;
+  const int tile_id = ep.tile0 + (int)blockIdx.x;
   if (ep.full) {
     ti = tile_id / nt;
     tj = tile_id % nt;
@@ -886,9 +886,12 @@ cudaError_t preload_bitplane_kernels() {
 }
 
 cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode, const EpiParams &ep,
-                               cudaStream_t s, int kchunk_words) {
+                               cudaStream_t s, int kchunk_words, long long band_tiles) {
   const int nt = tiles_of(p.n);
-  const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
+  const long long all_tiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
+  if (band_tiles > 0 && (epi_mode != EPI_DIST || ep.tile0 < 0 || ep.tile0 + band_tiles > all_tiles))
+    return cudaErrorInvalidValue;
+  const long long ntiles = band_tiles > 0 ? band_tiles : all_tiles;
   if (ntiles == 0) return cudaSuccess;
   const int nk = p.Wp / kKW;
   const int kmax = kMaxFusedWords / kKW;

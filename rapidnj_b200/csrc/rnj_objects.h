@@ -54,8 +54,6 @@ struct rnj_ctx {
   long long boot_tiles = 0;
   rnj::AlnDesc *d_desc = nullptr;         // one-alignment work list of the persistent kernel
   uint64_t *d_packed = nullptr;           // packed counts of the tensor-core path
-  double *d_recip = nullptr;              // 1 / k for k = 0 .. recip_L (entry 0 = 0)
-  int recip_L = 0;
   long long packed_tiles = 0;             // its capacity in tiles
   char *h_file = nullptr;                 // pinned file bytes of rnj_msa_read_device
   size_t h_file_cap = 0;
@@ -63,9 +61,6 @@ struct rnj_ctx {
 
 // Grows the context's packed-count buffer to `tiles` tiles (rnj_api.cu).
 int ensure_packed(rnj_ctx *ctx, long long tiles);
-// Grows the context's reciprocal table to cover valid counts up to L: entry k
-// is the double nearest to 1 / k, computed on the host (rnj_api.cu).
-int ensure_recip(rnj_ctx *ctx, int L);
 // Counts + transform of work items [0, nitems) of the tensor-core path in
 // passes of at most kTcChunkTiles tiles through `packed` (capacity
 // min(nitems, kTcChunkTiles) tiles), on stream s.  Profiling marks: stage 1
@@ -114,6 +109,8 @@ int ctx_check_error(rnj_ctx *ctx);
 // timeout status of that word (clearing it), else RNJ_OK (rnj_api.cu).
 int take_device_error(rnj_ctx *ctx);
 bool ctx_block_pinned(const void *p, size_t bytes);
+// The context's upload and download streams, created on first use (rnj_stream.cu).
+int ensure_side_streams(rnj_ctx *ctx);
 // The streamed host-to-host distance call of the tensor-core path, DNA and
 // protein (rnj_stream.cu).  Returns RNJ_ERR_UNSUPPORTED, having done nothing, when the
 // input does not take that path.

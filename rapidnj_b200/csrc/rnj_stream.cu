@@ -99,12 +99,6 @@ struct CallBuffers {
   }
 };
 
-int ensure_side_streams(rnj_ctx *ctx) {
-  if (!ctx->s_up) RNJ_TRY(cudaStreamCreateWithFlags(&ctx->s_up, cudaStreamNonBlocking), "upload stream");
-  if (!ctx->s_down)
-    RNJ_TRY(cudaStreamCreateWithFlags(&ctx->s_down, cudaStreamNonBlocking), "download stream");
-  return RNJ_OK;
-}
 
 int ensure_host_words(rnj_ctx *ctx, size_t words) {
   if (ctx->h_words_cap >= words) return RNJ_OK;
@@ -128,6 +122,13 @@ cudaError_t copy_block(float *h, const float *d, size_t ld, int n, int r0, int r
 }
 
 }  // namespace
+
+int ensure_side_streams(rnj_ctx *ctx) {
+  if (!ctx->s_up) RNJ_TRY(cudaStreamCreateWithFlags(&ctx->s_up, cudaStreamNonBlocking), "upload stream");
+  if (!ctx->s_down)
+    RNJ_TRY(cudaStreamCreateWithFlags(&ctx->s_down, cudaStreamNonBlocking), "download stream");
+  return RNJ_OK;
+}
 
 int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld, int type,
                            int model, int flags, int band_tiles, float *out, float *max_out) {
@@ -164,8 +165,10 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   if (rc != RNJ_OK) return rc;
   rc = ensure_host_words(ctx, (size_t)ntiles + 2);
   if (rc != RNJ_OK) return rc;
-  rc = fused ? ensure_recip(ctx, L) : ensure_packed(ctx, max_band_tiles);
-  if (rc != RNJ_OK) return rc;
+  if (!fused) {
+    rc = ensure_packed(ctx, max_band_tiles);
+    if (rc != RNJ_OK) return rc;
+  }
   rc = ctx_scratch(ctx, (size_t)ntiles + 2);
   if (rc != RNJ_OK) return rc;
 
@@ -289,7 +292,8 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
     const long long i0 = band_off[k], cnt = band_off[k + 1] - band_off[k];
     if (fused) {
       RNJ_TRY(launch_tc_fused(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
-                              (int)cnt, ctx->d_recip, (int)std::min<long long>(cnt, ctx->num_sms),
+                              (int)cnt, (int)std::min<long long>(cnt, ctx->num_sms),
+                              fused_variant_for(ep.model, ep.type, ep.compat_wrap, 0),
                               ctx->stream),
               "fused tensor-core kernel");
     } else {

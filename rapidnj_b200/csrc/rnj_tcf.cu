@@ -12,15 +12,18 @@
 //     columns at a time, converts them to integer counts (16 bits each: the
 //     fused form takes alignments of at most 65535 columns) and hands tensor
 //     memory back to the MMA warp at once;
-//   * it then computes the 32 distances of each lane from registers
-//     (pair_distance with the context's reciprocal table, the same float
-//     result as the reference's divisions, ratio_f32) while the tensor cores
-//     already count the next tile;
+//   * it then computes the 32 distances of each lane from registers, eight
+//     pairs at a time (K2P without branches, k2p_decide; the quotients by the
+//     valid count from its Newton-Raphson reciprocal, the same floats as the
+//     reference's divisions, ratio_f32) while the tensor cores already count
+//     the next tile;
 //   * stores: the mirror entries out[j][i] as coalesced 128-byte row segments
 //     (lanes are consecutive i), the tile entries out[i][j .. j + 3] as 16-byte
 //     vectors, the diagonal as 0; the tile's maximum goes to the alignment's
 //     max slot (atomicMax on the float bits) and a saturated pair (-1) sets
-//     the tile's flag for the fix-up kernel.
+//     the tile's flag for the fix-up kernel.  With AlnDesc::full the work items
+//     are full-square tiles of a band of rows (out-of-core delivery): every
+//     ordered pair is stored in its row of the band buffer, no mirror.
 // Sixteen warps run the transform at four warps per scheduler, enough to hide
 // the double-precision latency, and its instructions overlap the MMAs of the
 // next tile instead of following them in a second kernel.
@@ -37,19 +40,21 @@ namespace rnj {
 
 constexpr int kTcfEpiWarps = 16;
 constexpr int kTcfThreads = 64 + 32 * kTcfEpiWarps;  // producer, MMA issuer, epilogue
-constexpr int kTcfGroup = 8;                         // pairs per transform group
+constexpr int kTcfGroup = 4;                         // pairs per transform group
 
 // Transform variants of the fused epilogue, one loop each so that only the
-// model's own parameters stay in registers.
-enum { kFusedK2p = 0, kFusedJc = 1, kFusedProtein = 2, kFusedGeneric = 3 };
+// model's own parameters stay in registers (kFusedK2p .. kFusedAny are the
+// FusedVariant values of rnj_internal.h).
+enum {
+  kFusedK2p = FUSED_K2P, kFusedJc = FUSED_JC, kFusedProtein = FUSED_PROTEIN,
+  kFusedGeneric = FUSED_GENERIC, kFusedFull = FUSED_FULL, kFusedAny = FUSED_ANY
+};
 
 template <int M>
 __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint32_t tv,
-                                            uint32_t vv, const double *__restrict__ recip) {
-  const double rn = __ldg(recip + vv);  // 1 / valid (0 for valid == 0)
-  if constexpr (M == kFusedK2p) {
-    return k2p_distance(ts, tv, vv, rn);
-  } else if constexpr (M == kFusedJc) {
+                                            uint32_t vv) {
+  const double rn = vv ? recip_nr(vv) : 0.0;
+  if constexpr (M == kFusedJc) {
     return jc_distance((unsigned long long)ts + tv, vv, d.jc_b, rn);
   } else if constexpr (M == kFusedProtein) {
     return kimura_protein_distance(ts, vv, c_pam, rn);
@@ -61,8 +66,14 @@ __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint3
     ep.type = d.type;
     ep.compat_wrap = d.compat;
     ep.jc_b = d.jc_b;
-    return pair_distance(ep, ts, tv, vv, recip);
+    return pair_distance(ep, ts, tv, vv, true);
   }
+}
+
+// k2p_distance out of line: the rare pairs whose one-logarithm value the
+// rounding check cannot decide.
+static __device__ __noinline__ float k2p_undecided(uint32_t P, uint32_t Q, uint32_t n) {
+  return k2p_distance(P, Q, n);
 }
 
 // The 32 distances of row i, columns jb .. jb + 31 (counts pq / pv, see the
@@ -70,8 +81,7 @@ __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint3
 // (0 on the diagonal), the running maximum and whether a pair saturated.
 template <int M>
 __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint32_t (&pq)[32],
-                                           uint32_t (&pv)[16], const double *__restrict__ recip,
-                                           float &tmax, bool &sat) {
+                                           uint32_t (&pv)[16], float &tmax, bool &sat) {
   const int n = d.n;
   float *const out = d.out;
   const size_t ld = d.ld;
@@ -81,16 +91,45 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
   for (int g = 0; g < 32 / kTcfGroup; ++g) {
     const int j0 = jb + kTcfGroup * g;
     float x[kTcfGroup];
+    if constexpr (M == kFusedK2p) {
+      // Every pair of the group without branches (they interleave), then the
+      // rare undecided ones through the reference's two-logarithm formula.
+      uint32_t undecided = 0;
 #pragma unroll
-    for (int k = 0; k < kTcfGroup; ++k) {
-      const int j = j0 + k;
-      x[k] = 0.0f;
-      if (i < j && j < n) {
+      for (int k = 0; k < kTcfGroup; ++k) {
         const uint32_t vv = (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
-        x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv, recip);
+        bool slow;
+        x[k] = k2p_decide(pq[k] & 0xFFFFu, pq[k] >> 16, vv, slow);
+        undecided |= (uint32_t)slow << k;
+      }
+      if (undecided) {
+#pragma unroll
+        for (int k = 0; k < kTcfGroup; ++k)
+          if ((undecided >> k) & 1u)
+            x[k] = k2p_undecided(pq[k] & 0xFFFFu, pq[k] >> 16,
+                                 (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
+      }
+#pragma unroll
+      for (int k = 0; k < kTcfGroup; ++k) {
+        const int j = j0 + k;
+        const bool in = i < j && j < n;
+        x[k] = in ? x[k] : 0.0f;
         tmax = fmaxf(tmax, x[k]);
         sat |= (x[k] == -1.0f);
-        out[(size_t)j * ld + i] = x[k];  // mirror: consecutive i across lanes
+        if (in) out[(size_t)j * ld + i] = x[k];  // mirror: consecutive i across lanes
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kTcfGroup; ++k) {
+        const int j = j0 + k;
+        x[k] = 0.0f;
+        if (i < j && j < n) {
+          const uint32_t vv = (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
+          x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv);
+          tmax = fmaxf(tmax, x[k]);
+          sat |= (x[k] == -1.0f);
+          out[(size_t)j * ld + i] = x[k];  // mirror: consecutive i across lanes
+        }
       }
     }
     // Row i, columns j0 .. j0 + 7 (j >= i; the diagonal is 0).
@@ -118,10 +157,57 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
   }
 }
 
+// Full-rows form (a band of full-square tiles, AlnDesc::full): the 32
+// distances of row i, columns jb .. jb + 31, every j != i (0 on the diagonal),
+// into row i - row0 of the band buffer; no mirror.
+template <int M>
+__device__ __forceinline__ void fused_rows_full(const AlnDesc &d, int i, int jb, uint32_t (&pq)[32],
+                                                uint32_t (&pv)[16], float &tmax, bool &sat) {
+  const int n = d.n;
+  if (i >= n) return;
+  const size_t ld = d.ld;
+  float *const orow = d.out + (size_t)(i - d.row0) * ld;
+  const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(d.out) & 15) == 0);
+#pragma unroll 1
+  for (int g = 0; g < 32 / kTcfGroup; ++g) {
+    const int j0 = jb + kTcfGroup * g;
+    float x[kTcfGroup];
+#pragma unroll
+    for (int k = 0; k < kTcfGroup; ++k) {
+      const int j = j0 + k;
+      x[k] = 0.0f;
+      if (j != i && j < n) {
+        const uint32_t vv = (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
+        x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv);
+        tmax = fmaxf(tmax, x[k]);
+        sat |= (x[k] == -1.0f);
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < kTcfGroup / 4; ++h) {
+      const int jj = j0 + 4 * h;
+      if (vec && jj + 3 < n) {
+        *reinterpret_cast<float4 *>(orow + jj) =
+            make_float4(x[4 * h], x[4 * h + 1], x[4 * h + 2], x[4 * h + 3]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (jj + k < n) orow[jj + k] = x[4 * h + k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 32 - kTcfGroup; ++k) pq[k] = pq[k + kTcfGroup];
+#pragma unroll
+    for (int k = 0; k < (32 - kTcfGroup) / 2; ++k) pv[k] = pv[k + kTcfGroup / 2];
+  }
+}
+
+// V: the transform variant of every item (kFused*), or kFusedAny to choose per
+// item (a work list of alignments with different models).
+template <int V>
 __global__ void __launch_bounds__(kTcfThreads, 1)
     tc_fused_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
-                    const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
-                    const double *__restrict__ recip) {
+                    const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count) {
   extern __shared__ uint8_t smem_raw[];
   const TcShared sh = tc_shared(smem_raw);
   const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);
@@ -167,17 +253,17 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
       uint32_t pq[32], pv[16];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        uint32_t V[16], R[16], T[16];
+        uint32_t av[16], ar[16], at[16];  // accumulators V, R, T
         const uint32_t base = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(cofs + 16 * h);
-        tmem_ld16(base, V);
-        tmem_ld16(base + kTile, R);
-        tmem_ld16(base + 2 * kTile, T);
+        tmem_ld16(base, av);
+        tmem_ld16(base + kTile, ar);
+        tmem_ld16(base + 2 * kTile, at);
         tmem_ld_wait();
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
-          const int vv = __float2int_rn(__uint_as_float(V[k]));
-          const int rr = __float2int_rn(__uint_as_float(R[k]));
-          const int tu = __float2int_rn(__uint_as_float(T[k]));
+          const int vv = __float2int_rn(__uint_as_float(av[k]));
+          const int rr = __float2int_rn(__uint_as_float(ar[k]));
+          const int tu = __float2int_rn(__uint_as_float(at[k]));
           const uint32_t ts = prot ? (uint32_t)(vv - rr) : (uint32_t)((vv + rr - tu) >> 2);
           const uint32_t tv = prot ? 0u : (uint32_t)((vv - rr) >> 1);
           pq[16 * h + k] = ts | (tv << 16);
@@ -194,14 +280,19 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
       const int jb = tj * kTile + cofs;
       float tmax = 0.0f;
       bool sat = false;
-      if (d.compat) {
-        fused_rows<kFusedGeneric>(d, i, jb, pq, pv, recip, tmax, sat);
+      if constexpr (V == kFusedFull) {
+        // a band of full rows (out-of-core delivery), every model
+        fused_rows_full<kFusedGeneric>(d, i, jb, pq, pv, tmax, sat);
+      } else if constexpr (V != kFusedAny) {
+        fused_rows<V>(d, i, jb, pq, pv, tmax, sat);
+      } else if (d.compat) {
+        fused_rows<kFusedGeneric>(d, i, jb, pq, pv, tmax, sat);
       } else if (d.model == RNJ_JC) {
-        fused_rows<kFusedJc>(d, i, jb, pq, pv, recip, tmax, sat);
+        fused_rows<kFusedJc>(d, i, jb, pq, pv, tmax, sat);
       } else if (d.type == RNJ_PROTEIN) {
-        fused_rows<kFusedProtein>(d, i, jb, pq, pv, recip, tmax, sat);
+        fused_rows<kFusedProtein>(d, i, jb, pq, pv, tmax, sat);
       } else {
-        fused_rows<kFusedK2p>(d, i, jb, pq, pv, recip, tmax, sat);
+        fused_rows<kFusedK2p>(d, i, jb, pq, pv, tmax, sat);
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1)
@@ -217,16 +308,50 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
   tc_teardown(sh, tmem, issued, descs[0].err);
 }
 
-cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
-                            int nitems, int item0, int count, const double *recip, int grid,
-                            cudaStream_t s) {
-  if (grid <= 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(tc_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <int V>
+static cudaError_t launch_variant(const AlnDesc *d_descs, const WorkItem *d_items,
+                                  const int *d_nitems, int nitems, int item0, int count, int grid,
+                                  cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(tc_fused_kernel<V>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kTcSmemBytes);
   if (e != cudaSuccess) return e;
-  tc_fused_kernel<<<(unsigned)grid, kTcfThreads, kTcSmemBytes, s>>>(d_descs, d_items, d_nitems,
-                                                                   nitems, item0, count, recip);
+  tc_fused_kernel<V><<<(unsigned)grid, kTcfThreads, kTcSmemBytes, s>>>(
+      d_descs, d_items, d_nitems, nitems, item0, count);
   return cudaGetLastError();
+}
+
+int fused_variant_for(int model, int type, int compat, int full) {
+  if (full) return FUSED_FULL;
+  if (compat) return FUSED_GENERIC;
+  if (model == RNJ_JC) return FUSED_JC;
+  return type == RNJ_PROTEIN ? FUSED_PROTEIN : FUSED_K2P;
+}
+
+cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
+                            int nitems, int item0, int count, int grid, int variant,
+                            cudaStream_t s) {
+  if (grid <= 0) return cudaSuccess;
+  switch (variant) {
+    case FUSED_K2P:
+      return launch_variant<kFusedK2p>(d_descs, d_items, d_nitems, nitems, item0, count, grid, s);
+    case FUSED_JC:
+      return launch_variant<kFusedJc>(d_descs, d_items, d_nitems, nitems, item0, count, grid, s);
+    case FUSED_PROTEIN:
+      return launch_variant<kFusedProtein>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
+                                           s);
+    case FUSED_GENERIC:
+      return launch_variant<kFusedGeneric>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
+                                           s);
+    case FUSED_FULL:
+      return launch_variant<kFusedFull>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
+                                        s);
+    case FUSED_ANY:
+      return launch_variant<kFusedAny>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
+                                       s);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace rnj

@@ -20,7 +20,13 @@ namespace rnj_dropin {
 // (RNJ_JC or RNJ_KIMURA), computed on the GPU:
 //   rows != NULL: rows[i][0..n) of the caller's n row arrays receive row i;
 //   dm != NULL:   every full row goes through dm->writeArray(row, i, n), the
-//                 disk-backed mode of the reference (KimuraDistance.cpp:267-281).
+//                 disk-backed mode of the reference (KimuraDistance.cpp:267-281),
+//                 and rows holding saturated pairs are post-processed through
+//                 readArray / writeArray (KimuraDistance.cpp:366-395).
+// With a disk matrix, or when the n x n floats exceed the device budget
+// (RNJ_DEVICE_MATRIX_BUDGET bytes, else 80 % of the free device memory), the
+// rows are computed in bands (rnj_distance_rows) with device buffers for two
+// bands only; otherwise the whole matrix is computed on the device and copied.
 // fastdist reads the loader's bit strings (getBitStrings / getGapFilters /
 // getBitStringsCount), otherwise its sequences with the naive -f rules.
 // numThreads is used for the host copy of the rows.  Returns the maximum

@@ -33,16 +33,17 @@ def fixture(tmp_path, name):
     return str(p)
 
 
-def run(binary, args, tmp_path):
-    r = subprocess.run([binary] + args, capture_output=True, timeout=600, cwd=str(tmp_path))
+def run(binary, args, tmp_path, env=None):
+    r = subprocess.run([binary] + args, capture_output=True, timeout=600, cwd=str(tmp_path),
+                       env=dict(os.environ, **(env or {})))
     assert r.returncode == 0, (binary, args, r.stderr.decode()[-2000:])
     return r.stdout
 
 
-def same_output(args, tmp_path):
+def same_output(args, tmp_path, env=None):
     need_binaries()
     want = run(REF, args, tmp_path)
-    got = run(DROPIN, args, tmp_path)
+    got = run(DROPIN, args, tmp_path, env)
     assert len(want) > 0
     assert got == want, f"output differs for {args}"
 
@@ -80,6 +81,45 @@ def test_synthetic_multi_tile(tmp_path):
     for model in ("jc", "kim"):
         same_output([str(p), "-o", "m", "-a", model], tmp_path)
     same_output([str(p), "-a", "kim"], tmp_path)
+
+
+# A device-matrix budget far below the n x n floats: the drop-in computes the
+# rows in bands of 128 (rnj_distance_rows, two band buffers on the device) and
+# hands them to the disk matrix or to the row arrays, post-processing the rows
+# with saturated pairs as the reference does.
+SMALL_BUDGET = {"RNJ_DEVICE_MATRIX_BUDGET": "100000"}
+
+
+def synthetic_files(tmp_path):
+    from rapidnj_b200 import synth
+    p = tmp_path / "syn.fa"
+    synth.write_fasta(str(p), synth.tree_dna(600, 1500, seed=21, mean_branch=0.05))
+    rng = np.random.default_rng(4)
+    q = tmp_path / "sat.fa"  # unrelated short sequences: many saturated pairs
+    synth.write_fasta(str(q), np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, (300, 40))])
+    return str(p), str(q)
+
+
+@pytest.mark.parametrize("fast", [True, False])
+def test_matrix_beyond_device_budget_disk_mode(tmp_path, fast):
+    """-d: the disk-matrix tree and -o m text of matrices larger than the budget."""
+    syn, sat = synthetic_files(tmp_path)
+    cache = tmp_path / "cache"
+    cache.mkdir()
+    f = [] if fast else ["-f"]
+    for path in (syn, sat):
+        same_output([path, "-a", "kim", "-d", str(cache)] + f, tmp_path, SMALL_BUDGET)
+        same_output([path, "-o", "m", "-a", "jc", "-d", str(cache)] + f, tmp_path, SMALL_BUDGET)
+
+
+def test_matrix_beyond_device_budget_in_memory(tmp_path):
+    """No disk matrix: the banded rows fill rapidNJ's in-memory rows."""
+    syn, sat = synthetic_files(tmp_path)
+    for path in (syn, sat):
+        same_output([path, "-o", "m", "-a", "kim"], tmp_path, SMALL_BUDGET)
+    same_output([syn, "-a", "kim"], tmp_path, SMALL_BUDGET)
+    same_output([fixture(tmp_path, "PF15224_full"), "-o", "m", "-a", "kim"], tmp_path,
+                SMALL_BUDGET)
 
 
 def test_dropin_fails_loudly_on_a_bad_device(tmp_path):

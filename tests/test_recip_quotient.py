@@ -1,0 +1,76 @@
+"""The quotients of the device transforms by the valid count (rnj_device.cuh,
+recip_nr and ratio_f32): for integers 0 <= num <= den < 2^24, rounding
+num * r to float, with r the Newton-Raphson reciprocal of den (a correctly
+rounded float seed, then two steps r + r (1 - den r) as fused multiply-adds in
+double), gives the float quotient num / den that the reference computes with a
+float division (JCdistance.cpp:171-176, KimuraDistance.cpp:324) and with a
+double division rounded to float (KimuraDistance.cpp:341-342).
+
+The reciprocal is restated exactly: each fused multiply-add is the exact
+rational a * b + c rounded once to double (Python's float() of a Fraction is
+correctly rounded).  numpy's float32 division and float64 products are IEEE,
+correctly rounded.  Every den below 2^16 (the fused kernel's 16-bit counts) is
+checked for its error bound, with every num for den <= 2000 and samples beyond;
+random den up to 2^24 exercise the general statement."""
+from fractions import Fraction
+
+import numpy as np
+
+
+def fma(a: float, b: float, c: float) -> float:
+    return float(Fraction(a) * Fraction(b) + Fraction(c))
+
+
+def recip_nr(n: int) -> float:
+    r0 = float(np.float32(1.0) / np.float32(n))  # __frcp_rn: correctly rounded
+    r1 = fma(r0, fma(-float(n), r0, 1.0), r0)
+    return fma(r1, fma(-float(n), r1, 1.0), r1)
+
+
+def quotient(num: np.ndarray, r: np.ndarray) -> np.ndarray:
+    return (num.astype(np.float64) * r).astype(np.float32)
+
+
+def check(num, den, r):
+    got = quotient(num, r)
+    want_f = num.astype(np.float32) / den.astype(np.float32)
+    want_d = (num.astype(np.float64) / den.astype(np.float64)).astype(np.float32)
+    assert np.array_equal(got.view(np.uint32), want_f.view(np.uint32))
+    assert np.array_equal(got.view(np.uint32), want_d.view(np.uint32))
+
+
+def test_reciprocal_error_bound_for_16_bit_counts():
+    dens = np.arange(1, 1 << 16)
+    r = np.array([recip_nr(int(d)) for d in dens])
+    # |r - 1/n| <= 2^-52.9 / n, checked exactly
+    worst = max(abs(Fraction(float(x)) * int(d) - 1) for d, x in zip(dens[::97], r[::97]))
+    assert worst < Fraction(1, 2 ** 52)
+    rel = np.abs(r * dens - 1.0)
+    assert rel.max() <= 2.0 ** -51
+
+
+def test_quotients_exhaustive_small_and_sampled_16_bit():
+    for lo in range(1, 2001, 250):
+        den = np.arange(lo, min(lo + 250, 2001), dtype=np.int64)
+        num = np.concatenate([np.arange(d + 1) for d in den])
+        dd = np.concatenate([np.full(d + 1, d) for d in den])
+        r = np.array([recip_nr(int(d)) for d in den])
+        rr = np.concatenate([np.full(d + 1, x) for d, x in zip(den, r)])
+        check(num, dd, rr)
+    rng = np.random.default_rng(3)
+    den = rng.integers(2001, 1 << 16, 200_000)
+    r_all = {int(d): recip_nr(int(d)) for d in np.unique(den)}
+    r = np.array([r_all[int(d)] for d in den])
+    num = np.minimum((rng.random(den.size) * (den + 1)).astype(np.int64), den)
+    check(num, den, r)
+    for edge in (np.zeros_like(den), np.ones_like(den), den - 1, den):
+        check(edge, den, r)
+
+
+def test_quotients_random_up_to_2_24():
+    rng = np.random.default_rng(11)
+    den = rng.integers(1 << 16, 1 << 24, 3000)
+    r = np.array([recip_nr(int(d)) for d in den])
+    for _ in range(20):
+        num = np.minimum((rng.random(den.size) * (den + 1)).astype(np.int64), den)
+        check(num, den, r)
