@@ -269,8 +269,9 @@ int rnj_distance_matrix_host_ex(rnj_ctx *ctx, const char *chars, int n, int L, s
  * alignment (JCdistance / KimuraDistance per input, or per bootstrap replicate
  * of main.cpp:519-532).  Capacities bound the alignments and the total tiles
  * (128 x 128 pairs each, (ceil(n/128)+1)*ceil(n/128)/2 per alignment).  The
- * alignments added must stay alive until the run has completed.  Bit-plane
- * alignments longer than 65280 columns are not batched (use rnj_distance). */
+ * alignments added must stay alive until the run has completed.  Alignments
+ * longer than 65535 columns (tensor cores) or 65280 (bit planes) are not
+ * batched (use rnj_distance). */
 typedef struct rnj_batch rnj_batch;
 int rnj_batch_create(rnj_ctx *ctx, int max_alignments, long long max_tiles, rnj_batch **out);
 /* Adds an alignment; d_out NULL lets the batch allocate the n x n output.  The

@@ -446,21 +446,7 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
              "tensor-core kernel");
     return RNJ_OK;
   }
-  if (tp.tc_epilogue == 0 && p.L <= kMaxFusedColumns) {
-    // Counts and transform in one launch (rnj_tcf.cu).
-    mark(ctx, 1, 0);
-    RNJ_CUDA(launch_tc_fused(ctx->d_desc, nullptr, nullptr, (int)ntiles, 0, (int)ntiles,
-                             (int)std::min<long long>(ntiles, ctx->num_sms),
-                             fused_variant_for(ep.model, ep.type, ep.compat_wrap, 0), ctx->stream),
-             "fused tensor-core kernel");
-    mark(ctx, 1, 1);
-    mark(ctx, 2, 0);
-    return RNJ_OK;
-  }
-  int rc = ensure_packed(ctx, std::min<long long>(ntiles, kTcChunkTiles));
-  if (rc != RNJ_OK) return rc;
-  return run_tc_chunks(ctx, ctx->d_desc, nullptr, ntiles, ctx->d_packed, ctx->stream,
-                       tp.transform_ctas);
+  return run_tc_distances(ctx, p, ep, ctx->d_desc, nullptr, ntiles, ctx->stream, tp);
 }
 
 // Waits for the context's stream and reports (and clears) the sticky device
@@ -572,6 +558,25 @@ int ensure_packed(rnj_ctx *ctx, long long tiles) {
            "packed-count buffer");
   ctx->packed_tiles = tiles;
   return RNJ_OK;
+}
+
+int run_tc_distances(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, const AlnDesc *d_desc,
+                     const WorkItem *d_items, long long nitems, cudaStream_t s,
+                     const TuneParams &tp) {
+  if (tp.tc_epilogue == 0 && p.L <= kMaxFusedColumns) {
+    // Counts and transform in one launch (rnj_tcf.cu).
+    mark(ctx, 1, 0);
+    RNJ_CUDA(launch_tc_fused(d_desc, d_items, nullptr, (int)nitems, 0, (int)nitems,
+                             (int)std::min<long long>(nitems, ctx->num_sms),
+                             fused_variant_for(ep.model, ep.type, ep.compat_wrap, 0), s),
+             "fused tensor-core kernel");
+    mark(ctx, 1, 1);
+    mark(ctx, 2, 0);
+    return RNJ_OK;
+  }
+  int rc = ensure_packed(ctx, std::min<long long>(nitems, kTcChunkTiles));
+  if (rc != RNJ_OK) return rc;
+  return run_tc_chunks(ctx, d_desc, d_items, nitems, ctx->d_packed, s, tp.transform_ctas);
 }
 
 int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, long long nitems,

@@ -51,7 +51,6 @@ struct rnj_batch {
   int *d_ints = nullptr;  // [0] tensor-core items, [1] popcount items, [2] item counter, [3] error
   int *d_max = nullptr;   // per-alignment max bits
   int *d_flags = nullptr; // per-tile saturation flags of all alignments
-  uint64_t *d_packed = nullptr;  // packed counts of one pass of tensor-core tiles
   // pinned host staging of the uploads
   AlnDesc *h_descs = nullptr;
   WorkItem *h_items_tc = nullptr, *h_items_pc = nullptr;
@@ -88,7 +87,6 @@ void free_batch(rnj_batch *b) {
   cudaFree(b->d_ints);
   cudaFree(b->d_max);
   cudaFree(b->d_flags);
-  cudaFree(b->d_packed);
   cudaFreeHost(b->h_descs);
   cudaFreeHost(b->h_items_tc);
   cudaFreeHost(b->h_items_pc);
@@ -100,26 +98,18 @@ void free_batch(rnj_batch *b) {
   delete b;
 }
 
-// Tensor-core passes of the graph: the work list may fill the capacity, and
-// each pass covers kTcChunkTiles items (passes beyond the run's items exit at once).
-long long tc_chunk(const rnj_batch *b) { return std::min<long long>(b->cap_tiles, kTcChunkTiles); }
-
-// Captures: clear scratch -> tensor-core passes (counts, transform) -> popcount
-// kernel -> fix-up.
+// Captures: clear scratch -> the fused tensor-core kernel over every
+// tensor-core item (counts and transform, per-item model) -> popcount kernel ->
+// fix-up.
 int capture_graph(rnj_batch *b) {
   const int sms = b->ctx->num_sms;
   RNJ_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
   cudaError_t e = cudaMemsetAsync(b->d_max, 0, sizeof(int) * b->cap_aln, b->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_flags, 0, sizeof(int) * b->cap_tiles, b->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ints + 2, 0, 2 * sizeof(int), b->stream);
-  const long long chunk = tc_chunk(b);
-  for (long long i0 = 0; e == cudaSuccess && i0 < b->cap_tiles; i0 += chunk) {
-    e = launch_tc_batch(b->d_descs, b->d_items_tc, b->d_ints + 0, 0, (int)i0, (int)chunk,
-                        b->d_packed, sms, EPI_PACKED, b->stream);
-    if (e == cudaSuccess)
-      e = launch_tc_transform(b->d_descs, b->d_items_tc, b->d_ints + 0, 0, (int)i0, (int)chunk,
-                              b->d_packed, kTransformCtasPerSm * sms, b->stream);
-  }
+  if (e == cudaSuccess)
+    e = launch_tc_fused(b->d_descs, b->d_items_tc, b->d_ints + 0, 0, 0, (int)b->cap_tiles, sms,
+                        FUSED_ANY, b->stream);
   if (e == cudaSuccess)
     e = launch_count_batch(b->d_descs, b->d_items_pc, b->d_ints + 1, b->d_ints + 2, sms, EPI_DIST,
                            b->stream);
@@ -160,8 +150,6 @@ int rnj_batch_create(rnj_ctx *ctx, int max_alignments, long long max_tiles, rnj_
   if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_ints, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_max, sizeof(int) * max_alignments);
   if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_flags, sizeof(int) * max_tiles);
-  if (e == cudaSuccess)
-    e = cudaMalloc((void **)&b->d_packed, (size_t)tc_chunk(b) * kPackedTileWords * 8);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_descs, sizeof(AlnDesc) * max_alignments);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_items_tc, sizeof(WorkItem) * max_tiles);
   if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_items_pc, sizeof(WorkItem) * max_tiles);
@@ -189,6 +177,9 @@ int rnj_batch_add(rnj_batch *b, rnj_aln *aln, int model, float *d_out, size_t ld
   if (!is_tc_kind(p.kind) && p.Wp / kKW > kMaxFusedWords / kKW)
     return set_error(RNJ_ERR_INVALID, "alignments longer than 65280 columns on the bit-plane "
                                       "kernels are not batched; use rnj_distance");
+  if (is_tc_kind(p.kind) && p.L > kMaxFusedColumns)
+    return set_error(RNJ_ERR_INVALID, "alignments longer than 65535 columns on the tensor "
+                                      "cores are not batched; use rnj_distance");
   if ((int)b->entries.size() >= b->cap_aln)
     return set_error(RNJ_ERR_BUSY, "batch is full (alignments)");
   const int nt = tiles_of(p.n);

@@ -129,6 +129,47 @@ __device__ __forceinline__ double ln_table(double x) {
   return __fma_rn(dk, kLn2Hi, __dadd_rn(__fma_rn(dk, kLn2Lo, lnF), p));
 }
 
+// The same logarithm with k turned into a double by the 2^52 bias (an integer
+// add and a double subtraction, both exact, instead of a conversion): the
+// arithmetic, and so the result and its error bound, are ln_table's.
+__device__ __forceinline__ double ln_table_k(double x) {
+  const long long bits = __double_as_longlong(x);
+  const int ebits = (int)((bits >> 52) & 0x7FF);  // k + 1023
+  const int j = (int)((bits >> 45) & 127);
+  const double m = __longlong_as_double((bits & 0x000FFFFFFFFFFFFFLL) | 0x3FF0000000000000LL);
+  const double F = __longlong_as_double(0x3FF0000000000000LL | ((long long)j << 45));
+  const double lnF = __ldg(&c_log_tab[j][0]);
+  const double inv = __ldg(&c_log_tab[j][1]);
+  const double r = __dmul_rn(__dsub_rn(m, F), inv);
+  double p = -1.0 / 6.0;
+  p = __fma_rn(p, r, 0.2);
+  p = __fma_rn(p, r, -0.25);
+  p = __fma_rn(p, r, 1.0 / 3.0);
+  p = __fma_rn(p, r, -0.5);
+  p = __fma_rn(p, r, 1.0);
+  p = __dmul_rn(p, r);
+  // 2^52 + ebits, exactly, minus 2^52 + 1023: the double k (|k| < 2^11).
+  const double dk =
+      __dsub_rn(__hiloint2double(0x43300000, ebits), 4503599627370496.0 + 1023.0);
+  return __fma_rn(dk, kLn2Hi, __dadd_rn(__fma_rn(dk, kLn2Lo, lnF), p));
+}
+
+// The double of an integer 0 <= v < 2^32: 2^52 + v has v in its low mantissa
+// bits, so the subtraction of 2^52 is exact.
+__device__ __forceinline__ double u32_to_double(uint32_t v) {
+  return __dsub_rn(__hiloint2double(0x43300000, (int)v), 4503599627370496.0);
+}
+
+// y rounded to 24 significant bits, to nearest, in double arithmetic: Veltkamp
+// splitting with C = 2^29 + 1 (Dekker 1971): g = fl(C y), h = fl(g - fl(g - y))
+// keeps the 53 - 29 = 24 leading bits of y rounded to nearest (Boldo 2006; a
+// tie may round either way).  For 2^-126 <= |y| < 2^127 that is (double)(float)y
+// unless y lies exactly halfway between two floats.
+__device__ __forceinline__ double round_to_float_bits(double y) {
+  const double g = __dmul_rn(y, 536870913.0);
+  return __dsub_rn(g, __dsub_rn(g, y));
+}
+
 // Valid-site count as the fast protein estimator reports it for L % 128 == 0
 // (bitDistanceProtein.cpp:15-16,59): padded length minus the gaps counted over
 // one extra 128-byte block, stored in an unsigned long long.
@@ -288,6 +329,43 @@ __device__ __forceinline__ float k2p_decide(uint32_t P, uint32_t Q, uint32_t n, 
   // a, b in (0, 1] unless saturated: ln_table's argument stays positive.
   const double x = sat ? 1.0 : __dmul_rn(__dmul_rn(a, a), b);
   const double dd = __dmul_rn(-0.25, ln_table(x));
+  const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
+  const float lo = __double2float_rn(__dsub_rn(dd, eps));
+  const float hi = __double2float_rn(__dadd_rn(dd, eps));
+  slow = !sat && !same && (__float_as_int(lo) != __float_as_int(hi));
+  return sat ? -1.0f : (same ? -0.0f : lo);
+}
+
+// k2p_decide for 16-bit counts (the fused kernel): P, Q, n < 2^16 given as
+// integers packed by the epilogue.  The same decision and result, computed
+// with fewer conversions:
+//   * the doubles of P, Q and n by the 2^52 bias (u32_to_double), the float of
+//     n by the 2^23 bias; the reciprocal as recip_nr from them;
+//   * ts, tv: y = fl(P rn) as in ratio_f32 is within 2^-50 of P / n, which lies
+//     at least 2^-49 (relative) from every float midpoint, so y is no midpoint
+//     and lies on the same side of each: its 24-bit rounding to nearest
+//     (round_to_float_bits, y in [2^-16, 1]) is (double)fl32(P / n), the
+//     reference's (double)ts, without a conversion to float and back (P = 0
+//     gives 0);
+//   * temp1 = (float)a <= 0 exactly when a <= 0: a and b are sums of doubles
+//     of floats in [0, 1] with at most 24 significant bits and exponents above
+//     -17, so a nonzero a or b exceeds 2^-70 in magnitude and its float is not 0;
+//   * ln_table_k for the logarithm.
+__device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n, bool &slow) {
+  const uint32_t nn = n == 0 ? 1u : n;
+  const double dn = u32_to_double(nn);
+  const float fn = __fsub_rn(__uint_as_float(0x4B000000u | nn), 8388608.0f);
+  const double r0 = (double)__frcp_rn(fn);
+  const double r1 = __fma_rn(r0, __fma_rn(-dn, r0, 1.0), r0);
+  const double rn = __fma_rn(r1, __fma_rn(-dn, r1, 1.0), r1);
+  const double ts = round_to_float_bits(__dmul_rn(u32_to_double(P), rn));
+  const double tv = round_to_float_bits(__dmul_rn(u32_to_double(Q), rn));
+  const double a = __dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, ts)), tv);
+  const double b = __dsub_rn(1.0, __dmul_rn(2.0, tv));
+  const bool sat = (n == 0) | (a <= 0.0) | (b <= 0.0);
+  const bool same = (P | Q) == 0;
+  const double x = sat ? 1.0 : __dmul_rn(__dmul_rn(a, a), b);
+  const double dd = __dmul_rn(-0.25, ln_table_k(x));
   const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
   const float lo = __double2float_rn(__dsub_rn(dd, eps));
   const float hi = __double2float_rn(__dadd_rn(dd, eps));

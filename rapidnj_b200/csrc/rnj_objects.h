@@ -68,6 +68,13 @@ int ensure_packed(rnj_ctx *ctx, long long tiles);
 // transform_ctas > 0: resident CTAs per SM of the transform grid (else 5).
 int run_tc_chunks(rnj_ctx *ctx, const rnj::AlnDesc *d_desc, const rnj::WorkItem *d_items,
                   long long nitems, uint64_t *packed, cudaStream_t s, int transform_ctas = 0);
+// Distances of work items [0, nitems) of one tensor-core alignment (descriptor
+// d_desc on the device; d_items == nullptr: its banded triangle): the fused
+// kernel (rnj_tcf.cu) when the alignment takes it (at most kMaxFusedColumns
+// columns, and the tuned choice), else run_tc_chunks (rnj_api.cu).
+int run_tc_distances(rnj_ctx *ctx, const rnj::Packed &p, const rnj::EpiParams &ep,
+                     const rnj::AlnDesc *d_desc, const rnj::WorkItem *d_items, long long nitems,
+                     cudaStream_t s, const rnj::TuneParams &tp);
 
 struct rnj_aln {
   rnj_ctx *ctx = nullptr;

@@ -192,9 +192,8 @@ int rnj_shard_run(rnj_shard *s, float *local_max) {
     const int grid = (int)std::min<long long>(nitems, ctx->num_sms);
     if (is_tc_kind(p.kind)) {
       // Marks stage 1 around the counting kernels.
-      int rc = ensure_packed(ctx, std::min<long long>(nitems, kTcChunkTiles));
-      if (rc != RNJ_OK) return rc;
-      rc = run_tc_chunks(ctx, s->d_desc, s->d_items, nitems, ctx->d_packed, st);
+      const int rc = run_tc_distances(ctx, p, epi_params_for(p, s->model), s->d_desc, s->d_items,
+                                      nitems, st, tune_lookup(p.n, p.L, p.type, p.flags));
       if (rc != RNJ_OK) return rc;
     } else {
       ctx_mark(ctx, 1, 0);

@@ -91,34 +91,7 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
   for (int g = 0; g < 32 / kTcfGroup; ++g) {
     const int j0 = jb + kTcfGroup * g;
     float x[kTcfGroup];
-    if constexpr (M == kFusedK2p) {
-      // Every pair of the group without branches (they interleave), then the
-      // rare undecided ones through the reference's two-logarithm formula.
-      uint32_t undecided = 0;
-#pragma unroll
-      for (int k = 0; k < kTcfGroup; ++k) {
-        const uint32_t vv = (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
-        bool slow;
-        x[k] = k2p_decide(pq[k] & 0xFFFFu, pq[k] >> 16, vv, slow);
-        undecided |= (uint32_t)slow << k;
-      }
-      if (undecided) {
-#pragma unroll
-        for (int k = 0; k < kTcfGroup; ++k)
-          if ((undecided >> k) & 1u)
-            x[k] = k2p_undecided(pq[k] & 0xFFFFu, pq[k] >> 16,
-                                 (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
-      }
-#pragma unroll
-      for (int k = 0; k < kTcfGroup; ++k) {
-        const int j = j0 + k;
-        const bool in = i < j && j < n;
-        x[k] = in ? x[k] : 0.0f;
-        tmax = fmaxf(tmax, x[k]);
-        sat |= (x[k] == -1.0f);
-        if (in) out[(size_t)j * ld + i] = x[k];  // mirror: consecutive i across lanes
-      }
-    } else {
+    {
 #pragma unroll
       for (int k = 0; k < kTcfGroup; ++k) {
         const int j = j0 + k;
@@ -128,7 +101,7 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
           x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv);
           tmax = fmaxf(tmax, x[k]);
           sat |= (x[k] == -1.0f);
-          out[(size_t)j * ld + i] = x[k];  // mirror: consecutive i across lanes
+          __stcs(out + (size_t)j * ld + i, x[k]);  // mirror: consecutive i across lanes
         }
       }
     }
@@ -138,13 +111,13 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
       for (int h = 0; h < kTcfGroup / 4; ++h) {
         const int jj = j0 + 4 * h;
         if (vec && i < jj && jj + 3 < n) {
-          *reinterpret_cast<float4 *>(orow + jj) =
-              make_float4(x[4 * h], x[4 * h + 1], x[4 * h + 2], x[4 * h + 3]);
+          __stcs(reinterpret_cast<float4 *>(orow + jj),
+                 make_float4(x[4 * h], x[4 * h + 1], x[4 * h + 2], x[4 * h + 3]));
         } else {
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             const int j = jj + k;
-            if (j < n && i <= j) orow[j] = (i == j) ? 0.0f : x[4 * h + k];
+            if (j < n && i <= j) __stcs(orow + j, (i == j) ? 0.0f : x[4 * h + k]);
           }
         }
       }
@@ -154,6 +127,96 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
     for (int k = 0; k < 32 - kTcfGroup; ++k) pq[k] = pq[k + kTcfGroup];
 #pragma unroll
     for (int k = 0; k < (32 - kTcfGroup) / 2; ++k) pv[k] = pv[k + kTcfGroup / 2];
+  }
+}
+
+// Kimura-2P rows (the variant of the DNA workloads): the 32 distances of row i,
+// columns jb .. jb + 31, in groups of four computed without branches
+// (k2p_decide16), the rare undecided pairs out of line; stores as streaming
+// stores (.cs), so that the output does not push the logarithm table out of
+// L1.  interior: the tile lies above the diagonal and inside the matrix (every
+// pair valid, no masks).
+constexpr int kK2pGroups = 2;  // groups of four pairs computed per loop iteration
+
+__device__ __forceinline__ void fused_rows_k2p(const AlnDesc &d, int i, int jb, bool interior,
+                                               uint32_t (&pq)[32], uint32_t (&pv)[16],
+                                               float &tmax, bool &sat) {
+  const int n = d.n;
+  float *const out = d.out;
+  const size_t ld = d.ld;
+  const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+  float *const orow = out + (size_t)i * ld;  // dereferenced only for i < n
+  float *mp = out + (size_t)jb * ld + i;     // out[jb + c][i], one row further per column
+  constexpr int U = kK2pGroups;
+#pragma unroll 1
+  for (int it = 0; it < 8 / U; ++it) {
+#pragma unroll
+  for (int g = 0; g < U; ++g) {
+    float x[4];
+    uint32_t undecided = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int c = 4 * g + k;
+      bool slow;
+      x[k] = k2p_decide16(pq[c] & 0xFFFFu, pq[c] >> 16, (pv[c >> 1] >> (16 * (c & 1))) & 0xFFFFu,
+                          slow);
+      undecided |= (uint32_t)slow << k;
+    }
+    if (undecided) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int c = 4 * g + k;
+        if ((undecided >> k) & 1u)
+          x[k] = k2p_undecided(pq[c] & 0xFFFFu, pq[c] >> 16,
+                               (pv[c >> 1] >> (16 * (c & 1))) & 0xFFFFu);
+      }
+    }
+    const int j0 = jb + 4 * (U * it + g);
+    if (interior) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        tmax = fmaxf(tmax, x[k]);
+        sat |= (x[k] == -1.0f);
+        __stcs(mp, x[k]);  // mirror: consecutive i across lanes
+        mp += ld;
+      }
+      if (vec) {
+        __stcs(reinterpret_cast<float4 *>(orow + j0), make_float4(x[0], x[1], x[2], x[3]));
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) __stcs(orow + j0 + k, x[k]);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int j = j0 + k;
+        const bool in = i < j && j < n;
+        x[k] = in ? x[k] : 0.0f;
+        tmax = fmaxf(tmax, x[k]);
+        sat |= (x[k] == -1.0f);
+        if (in) __stcs(mp, x[k]);
+        mp += ld;
+      }
+      if (i < n) {
+        if (vec && i < j0 && j0 + 3 < n) {
+          __stcs(reinterpret_cast<float4 *>(orow + j0), make_float4(x[0], x[1], x[2], x[3]));
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int j = j0 + k;
+            if (j < n && i <= j) __stcs(orow + j, (i == j) ? 0.0f : x[k]);
+          }
+        }
+      }
+    }
+  }
+  // The next iteration's counts into registers 0 .. 4U - 1.
+  if constexpr (U < 8) {
+#pragma unroll
+    for (int k = 0; k < 32 - 4 * U; ++k) pq[k] = pq[k + 4 * U];
+#pragma unroll
+    for (int k = 0; k < 16 - 2 * U; ++k) pv[k] = pv[k + 2 * U];
+  }
   }
 }
 
@@ -187,12 +250,12 @@ __device__ __forceinline__ void fused_rows_full(const AlnDesc &d, int i, int jb,
     for (int h = 0; h < kTcfGroup / 4; ++h) {
       const int jj = j0 + 4 * h;
       if (vec && jj + 3 < n) {
-        *reinterpret_cast<float4 *>(orow + jj) =
-            make_float4(x[4 * h], x[4 * h + 1], x[4 * h + 2], x[4 * h + 3]);
+        __stcs(reinterpret_cast<float4 *>(orow + jj),
+               make_float4(x[4 * h], x[4 * h + 1], x[4 * h + 2], x[4 * h + 3]));
       } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k)
-          if (jj + k < n) orow[jj + k] = x[4 * h + k];
+          if (jj + k < n) __stcs(orow + jj + k, x[4 * h + k]);
       }
     }
 #pragma unroll
@@ -259,16 +322,23 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
         tmem_ld16(base + kTile, ar);
         tmem_ld16(base + 2 * kTile, at);
         tmem_ld_wait();
+        // The sums are exact integers in f32 (below 2^24 in magnitude), and so
+        // are P = (V + R - T) / 4 and Q = (V - R) / 2 (DNA) or P = V - M
+        // (protein); x + 2^23 holds x in its low mantissa bits (0 <= x < 2^23),
+        // from which the 16-bit fields are taken without a conversion.
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
-          const int vv = __float2int_rn(__uint_as_float(av[k]));
-          const int rr = __float2int_rn(__uint_as_float(ar[k]));
-          const int tu = __float2int_rn(__uint_as_float(at[k]));
-          const uint32_t ts = prot ? (uint32_t)(vv - rr) : (uint32_t)((vv + rr - tu) >> 2);
-          const uint32_t tv = prot ? 0u : (uint32_t)((vv - rr) >> 1);
-          pq[16 * h + k] = ts | (tv << 16);
-          if (k & 1) pv[8 * h + (k >> 1)] |= (uint32_t)vv << 16;
-          else pv[8 * h + (k >> 1)] = (uint32_t)vv;
+          const float fv = __uint_as_float(av[k]), fr = __uint_as_float(ar[k]);
+          const float ft = __uint_as_float(at[k]);
+          const float fp = prot ? __fsub_rn(fv, fr)
+                                : __fmul_rn(__fsub_rn(__fadd_rn(fv, fr), ft), 0.25f);
+          const float fq = prot ? 0.0f : __fmul_rn(__fsub_rn(fv, fr), 0.5f);
+          const uint32_t bp = __float_as_uint(__fadd_rn(fp, 8388608.0f));
+          const uint32_t bq = __float_as_uint(__fadd_rn(fq, 8388608.0f));
+          const uint32_t bv = __float_as_uint(__fadd_rn(fv, 8388608.0f));
+          pq[16 * h + k] = __byte_perm(bp, bq, 0x5410);  // P | Q << 16
+          if (k & 1) pv[8 * h + (k >> 1)] = __byte_perm(pv[8 * h + (k >> 1)], bv, 0x5410);
+          else pv[8 * h + (k >> 1)] = bv;  // high half replaced by the odd column
         }
       }
       // Tensor memory back to the MMA warp: the next tile's MMAs start now.
@@ -283,6 +353,8 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
       if constexpr (V == kFusedFull) {
         // a band of full rows (out-of-core delivery), every model
         fused_rows_full<kFusedGeneric>(d, i, jb, pq, pv, tmax, sat);
+      } else if constexpr (V == kFusedK2p) {
+        fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat);
       } else if constexpr (V != kFusedAny) {
         fused_rows<V>(d, i, jb, pq, pv, tmax, sat);
       } else if (d.compat) {
@@ -292,7 +364,7 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
       } else if (d.type == RNJ_PROTEIN) {
         fused_rows<kFusedProtein>(d, i, jb, pq, pv, tmax, sat);
       } else {
-        fused_rows<kFusedK2p>(d, i, jb, pq, pv, tmax, sat);
+        fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat);
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1)

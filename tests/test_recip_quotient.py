@@ -74,3 +74,37 @@ def test_quotients_random_up_to_2_24():
     for _ in range(20):
         num = np.minimum((rng.random(den.size) * (den + 1)).astype(np.int64), den)
         check(num, den, r)
+
+
+def round_to_float_bits(y: np.ndarray) -> np.ndarray:
+    """rnj_device.cuh round_to_float_bits: Veltkamp splitting with C = 2^29 + 1
+    (two roundings per operation, as the device's explicitly rounded ops)."""
+    g = y * 536870913.0
+    return g - (g - y)
+
+
+def check_k2p16(num, den, r):
+    """k2p_decide16's ts: the 24-bit rounding of fl(num * r) in double equals the
+    double of the float quotient the reference computes."""
+    y = num.astype(np.float64) * r
+    got = round_to_float_bits(y)
+    want = (num.astype(np.float32) / den.astype(np.float32)).astype(np.float64)
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+
+
+def test_veltkamp_rounding_of_16_bit_quotients():
+    for lo in range(1, 2001, 250):
+        den = np.arange(lo, min(lo + 250, 2001), dtype=np.int64)
+        num = np.concatenate([np.arange(d + 1) for d in den])
+        dd = np.concatenate([np.full(d + 1, d) for d in den])
+        r = np.array([recip_nr(int(d)) for d in den])
+        check_k2p16(num, dd, np.concatenate([np.full(d + 1, x) for d, x in zip(den, r)]))
+    rng = np.random.default_rng(5)
+    den = rng.integers(2001, 1 << 16, 300_000)
+    r_all = {int(d): recip_nr(int(d)) for d in np.unique(den)}
+    r = np.array([r_all[int(d)] for d in den])
+    for _ in range(3):
+        num = np.minimum((rng.random(den.size) * (den + 1)).astype(np.int64), den)
+        check_k2p16(num, den, r)
+    for edge in (np.zeros_like(den), np.ones_like(den), den - 1, den):
+        check_k2p16(edge, den, r)
