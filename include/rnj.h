@@ -452,6 +452,9 @@ typedef struct rnj_tune_params {
   int tile_band;       /* tensor-core kernel: tile-order band height in tile rows (0 = 12) */
   int transform_ctas;  /* tensor-core transform: resident CTAs per SM, 1..5 (0 = 5) */
   int stream_band;     /* rnj_distance_matrix_host: band height in tile rows (0 = automatic) */
+  int tc_epilogue;     /* tensor cores: 0 the exact transform in the counting kernel's own
+                          epilogue warps (one launch), 1 packed counts and a separate
+                          transform kernel at higher occupancy */
   float ms;            /* the tuned configuration's time for the measured shape (output) */
 } rnj_tune_params;
 

@@ -452,7 +452,8 @@ class TuneParams(ctypes.Structure):
     floor(log2 n), floor(log2 L)); zero fields mean the library default."""
     _fields_ = [("dna_kernel", ctypes.c_int), ("ksplit", ctypes.c_int),
                 ("tile_band", ctypes.c_int), ("transform_ctas", ctypes.c_int),
-                ("stream_band", ctypes.c_int), ("ms", ctypes.c_float)]
+                ("stream_band", ctypes.c_int), ("tc_epilogue", ctypes.c_int),
+                ("ms", ctypes.c_float)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -55,7 +55,7 @@ def main():
     print("#pragma once")
     print(f"constexpr double kLn2Hi = {hi.hex()};")
     print(f"constexpr double kLn2Lo = {lo.hex()};")
-    print("static __device__ const double c_log_tab[128][2] = {")
+    print("static __device__ __align__(16) const double c_log_tab[128][2] = {")
     for lnF, inv in rows:
         print(f"    {{{lnF.hex()}, {inv.hex()}}},")
     print("};")

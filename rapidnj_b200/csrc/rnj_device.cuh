@@ -129,18 +129,20 @@ __device__ __forceinline__ double ln_table(double x) {
   return __fma_rn(dk, kLn2Hi, __dadd_rn(__fma_rn(dk, kLn2Lo, lnF), p));
 }
 
-// The same logarithm with k turned into a double by the 2^52 bias (an integer
-// add and a double subtraction, both exact, instead of a conversion): the
-// arithmetic, and so the result and its error bound, are ln_table's.
-__device__ __forceinline__ double ln_table_k(double x) {
+// The same logarithm with the table read from `tab` (a copy of c_log_tab in
+// shared memory: a warp's 32 random entries are one shared-memory request
+// instead of up to 16 L1 lines) and k turned into a double by the 2^52 bias (an
+// integer add and a double subtraction, both exact, instead of a conversion):
+// the arithmetic, and so the result and its error bound, are ln_table's.
+__device__ __forceinline__ double ln_table_k(double x, const double2 *tab) {
   const long long bits = __double_as_longlong(x);
   const int ebits = (int)((bits >> 52) & 0x7FF);  // k + 1023
   const int j = (int)((bits >> 45) & 127);
   const double m = __longlong_as_double((bits & 0x000FFFFFFFFFFFFFLL) | 0x3FF0000000000000LL);
   const double F = __longlong_as_double(0x3FF0000000000000LL | ((long long)j << 45));
-  const double lnF = __ldg(&c_log_tab[j][0]);
-  const double inv = __ldg(&c_log_tab[j][1]);
-  const double r = __dmul_rn(__dsub_rn(m, F), inv);
+  const double2 e = tab[j];  // {ln F, 1 / F}
+  const double r = __dmul_rn(__dsub_rn(m, F), e.y);
+  const double lnF = e.x;
   double p = -1.0 / 6.0;
   p = __fma_rn(p, r, 0.2);
   p = __fma_rn(p, r, -0.25);
@@ -350,8 +352,9 @@ __device__ __forceinline__ float k2p_decide(uint32_t P, uint32_t Q, uint32_t n, 
 //   * temp1 = (float)a <= 0 exactly when a <= 0: a and b are sums of doubles
 //     of floats in [0, 1] with at most 24 significant bits and exponents above
 //     -17, so a nonzero a or b exceeds 2^-70 in magnitude and its float is not 0;
-//   * ln_table_k for the logarithm.
-__device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n, bool &slow) {
+//   * ln_table_k for the logarithm (tab: the table in shared memory).
+__device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n, bool &slow,
+                                              const double2 *tab) {
   const uint32_t nn = n == 0 ? 1u : n;
   const double dn = u32_to_double(nn);
   const float fn = __fsub_rn(__uint_as_float(0x4B000000u | nn), 8388608.0f);
@@ -365,7 +368,7 @@ __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n
   const bool sat = (n == 0) | (a <= 0.0) | (b <= 0.0);
   const bool same = (P | Q) == 0;
   const double x = sat ? 1.0 : __dmul_rn(__dmul_rn(a, a), b);
-  const double dd = __dmul_rn(-0.25, ln_table_k(x));
+  const double dd = __dmul_rn(-0.25, ln_table_k(x, tab));
   const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
   const float lo = __double2float_rn(__dsub_rn(dd, eps));
   const float hi = __double2float_rn(__dadd_rn(dd, eps));

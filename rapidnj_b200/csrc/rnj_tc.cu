@@ -316,7 +316,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                     const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
                     uint64_t *__restrict__ packed) {
   extern __shared__ uint8_t smem_raw[];
-  const TcShared sh = tc_shared(smem_raw);
+  const TcShared<kTcStages> sh = tc_shared<kTcStages>(smem_raw);
   // The pipeline waits' bound and the failure-path test switch (the same for
   // every alignment of a launch).
   const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);

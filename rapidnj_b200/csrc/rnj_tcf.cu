@@ -2,21 +2,22 @@
 // tensor cores and the exact transform in the same CTA, straight from tensor
 // memory to the distance matrix.
 //
-// The counting pipeline is the one of rnj_tcgen05.cuh (warp 0 TMA producer,
-// warp 1 MMA issuer, three f32 accumulators V, R, T of 128 x 128 in tensor
-// memory).  Sixteen epilogue warps (2 .. 17) replace the packed-count round
-// trip of the two-kernel form (8 bytes per pair written and read again, then a
+// The counting pipeline is the one of rnj_tcgen05.cuh (warp 16 TMA producer,
+// warp 17 MMA issuer, three f32 accumulators V, R, T of 128 x 128 in tensor
+// memory, a six-stage ring).  Sixteen epilogue warps (0 .. 15, with 112
+// registers each after a setmaxnreg split) replace the packed-count round trip
+// of the two-kernel form (8 bytes per pair written and read again, then a
 // separate transform launch):
 //   * warp w reads tensor-memory lane quarter w % 4 (32 tile rows, lane = row)
-//     and columns 32 ((w - 2) / 4) .. + 31 of the three accumulators, 16
+//     and columns 32 (w / 4) .. + 31 of the three accumulators, 16
 //     columns at a time, converts them to integer counts (16 bits each: the
 //     fused form takes alignments of at most 65535 columns) and hands tensor
 //     memory back to the MMA warp at once;
-//   * it then computes the 32 distances of each lane from registers, eight
-//     pairs at a time (K2P without branches, k2p_decide; the quotients by the
-//     valid count from its Newton-Raphson reciprocal, the same floats as the
-//     reference's divisions, ratio_f32) while the tensor cores already count
-//     the next tile;
+//   * it then computes the 32 distances of each lane from registers, sixteen
+//     pairs at a time (K2P: k2p_decide16, with the logarithm table copied to
+//     shared memory; the quotients by the valid count from its Newton-Raphson
+//     reciprocal, the same floats as the reference's divisions, ratio_f32)
+//     while the tensor cores already count the next tile;
 //   * stores: the mirror entries out[j][i] as coalesced 128-byte row segments
 //     (lanes are consecutive i), the tile entries out[i][j .. j + 3] as 16-byte
 //     vectors, the diagonal as 0; the tile's maximum goes to the alignment's
@@ -24,9 +25,8 @@
 //     the tile's flag for the fix-up kernel.  With AlnDesc::full the work items
 //     are full-square tiles of a band of rows (out-of-core delivery): every
 //     ordered pair is stored in its row of the band buffer, no mirror.
-// Sixteen warps run the transform at four warps per scheduler, enough to hide
-// the double-precision latency, and its instructions overlap the MMAs of the
-// next tile instead of following them in a second kernel.
+// The transform's instructions overlap the MMAs of the next tile instead of
+// following them in a second kernel.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -38,8 +38,24 @@
 
 namespace rnj {
 
+// Warps 0 .. 15: epilogue (warpgroups 0 .. 3); warp 16: TMA producer; warp 17:
+// MMA issuer and tensor-memory owner; warps 18, 19 complete warpgroup 4.
 constexpr int kTcfEpiWarps = 16;
-constexpr int kTcfThreads = 64 + 32 * kTcfEpiWarps;  // producer, MMA issuer, epilogue
+constexpr int kTcfThreads = 640;
+constexpr int kTcfProducerWarp = 16, kTcfMmaWarp = 17;
+// Registers: launched with 640 threads x 96; warpgroup 4 (producer, issuer)
+// gives back 64 a thread (setmaxnreg.dec to 32), which lets the 512 epilogue
+// threads grow by 16 (setmaxnreg.inc to 112): 128 x 32 + 512 x 112 = 640 x 96,
+// so the increase never waits for registers that are not there.
+constexpr int kTcfRegsLow = 32, kTcfRegsHigh = 112, kTcfRegsLaunch = 96;
+static_assert(128 * kTcfRegsLow + 512 * kTcfRegsHigh <= kTcfThreads * kTcfRegsLaunch,
+              "the register split fits the launch's registers");
+// A six-stage ring (the seventh stage's 32 KB would leave no room) and the
+// logarithm table (128 x {ln F, 1 / F}) after the barrier block.
+constexpr int kTcfStages = 6;
+constexpr size_t kTcfTableBytes = 128 * 2 * sizeof(double);
+constexpr size_t kTcfSmemBytes = tc_smem_bytes(kTcfStages, kTcfTableBytes);
+static_assert(kTcfSmemBytes <= 232448, "fits the shared memory of one CTA");
 constexpr int kTcfGroup = 4;                         // pairs per transform group
 
 // Transform variants of the fused epilogue, one loop each so that only the
@@ -136,11 +152,11 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
 // stores (.cs), so that the output does not push the logarithm table out of
 // L1.  interior: the tile lies above the diagonal and inside the matrix (every
 // pair valid, no masks).
-constexpr int kK2pGroups = 2;  // groups of four pairs computed per loop iteration
+constexpr int kK2pGroups = 4;  // groups of four pairs computed per loop iteration
 
 __device__ __forceinline__ void fused_rows_k2p(const AlnDesc &d, int i, int jb, bool interior,
                                                uint32_t (&pq)[32], uint32_t (&pv)[16],
-                                               float &tmax, bool &sat) {
+                                               float &tmax, bool &sat, const double2 *tab) {
   const int n = d.n;
   float *const out = d.out;
   const size_t ld = d.ld;
@@ -159,7 +175,7 @@ __device__ __forceinline__ void fused_rows_k2p(const AlnDesc &d, int i, int jb, 
       const int c = 4 * g + k;
       bool slow;
       x[k] = k2p_decide16(pq[c] & 0xFFFFu, pq[c] >> 16, (pv[c >> 1] >> (16 * (c & 1))) & 0xFFFFu,
-                          slow);
+                          slow, tab);
       undecided |= (uint32_t)slow << k;
     }
     if (undecided) {
@@ -272,7 +288,8 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
     tc_fused_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
                     const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count) {
   extern __shared__ uint8_t smem_raw[];
-  const TcShared sh = tc_shared(smem_raw);
+  const TcShared<kTcfStages> sh = tc_shared<kTcfStages>(smem_raw);
+  double2 *const tab = reinterpret_cast<double2 *>(tc_extra(sh));
   const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);
   const int stall = descs[0].stall;
 
@@ -283,18 +300,26 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
   const int it0 = item0 + (int)blockIdx.x;
   if (it0 >= nitems) return;  // no item for this CTA (before any setup)
 
-  // tmem_empty: one arrival per epilogue warp
-  const uint32_t tmem = tc_setup(sh, kTcfEpiWarps, 2);
+  for (int e = tid; e < 128; e += kTcfThreads)
+    tab[e] = make_double2(c_log_tab[e][0], c_log_tab[e][1]);
+  // tmem_empty: one arrival per epilogue warp; the scale factors by warps 0 .. 7
+  const uint32_t tmem = tc_setup(sh, kTcfEpiWarps, 0, kTcfMmaWarp);
   uint32_t issued = 0;
 
-  if (warp == 0) {
-    if (lane == 0) issued = tc_produce(sh, descs, items, it0, nitems, gridDim.x, limit);
-  } else if (warp == 1) {
-    tc_issue(sh, tmem, descs, items, it0, nitems, gridDim.x, limit);
+  if (warp >= kTcfProducerWarp) {
+    // The register split is made inside each role's branch, so that the
+    // compiler allocates each role's code within its own limit.
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(kTcfRegsLow) : "memory");
+    if (warp == kTcfProducerWarp) {
+      if (lane == 0) issued = tc_produce(sh, descs, items, it0, nitems, gridDim.x, limit);
+    } else if (warp == kTcfMmaWarp) {
+      tc_issue(sh, tmem, descs, items, it0, nitems, gridDim.x, limit);
+    }
   } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(kTcfRegsHigh) : "memory");
     // ----------------------------------------------------------- epilogue
     const int q = warp & 3;              // tensor-memory lane quarter
-    const int cofs = 32 * ((warp - 2) >> 2);  // first tile column of this warp
+    const int cofs = 32 * (warp >> 2);   // first tile column of this warp
     const int row = 32 * q + lane;       // tile row of this lane
     uint32_t titer = 0;
     for (int it = it0; it < nitems; it += gridDim.x, ++titer) {
@@ -354,7 +379,7 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
         // a band of full rows (out-of-core delivery), every model
         fused_rows_full<kFusedGeneric>(d, i, jb, pq, pv, tmax, sat);
       } else if constexpr (V == kFusedK2p) {
-        fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat);
+        fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat, tab);
       } else if constexpr (V != kFusedAny) {
         fused_rows<V>(d, i, jb, pq, pv, tmax, sat);
       } else if (d.compat) {
@@ -364,7 +389,7 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
       } else if (d.type == RNJ_PROTEIN) {
         fused_rows<kFusedProtein>(d, i, jb, pq, pv, tmax, sat);
       } else {
-        fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat);
+        fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat, tab);
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1)
@@ -377,7 +402,7 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
     }
   }
 
-  tc_teardown(sh, tmem, issued, descs[0].err);
+  tc_teardown(sh, tmem, issued, descs[0].err, kTcfMmaWarp);
 }
 
 template <int V>
@@ -386,9 +411,9 @@ static cudaError_t launch_variant(const AlnDesc *d_descs, const WorkItem *d_item
                                   cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(tc_fused_kernel<V>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kTcSmemBytes);
+                                       (int)kTcfSmemBytes);
   if (e != cudaSuccess) return e;
-  tc_fused_kernel<V><<<(unsigned)grid, kTcfThreads, kTcSmemBytes, s>>>(
+  tc_fused_kernel<V><<<(unsigned)grid, kTcfThreads, kTcfSmemBytes, s>>>(
       d_descs, d_items, d_nitems, nitems, item0, count);
   return cudaGetLastError();
 }

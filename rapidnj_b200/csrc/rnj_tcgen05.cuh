@@ -14,7 +14,7 @@
 
 namespace rnj {
 
-constexpr int kTcStages = 7;
+constexpr int kTcStages = 7;  // ring depth of the two-kernel form (tc_batch_kernel)
 constexpr int kTcKBlock = 128;                            // bytes of K per stage (256 FP4 columns)
 constexpr int kTcKCols = 256;                             // feature columns per stage
 constexpr uint32_t kTcTileBytes = kTile * kTcKBlock;      // 16 KB per operand tile
@@ -22,7 +22,12 @@ constexpr uint32_t kTcStageBytes = 2 * kTcTileBytes;      // A + B
 constexpr int kTcThreads = 320;
 constexpr uint32_t kTmemCols = 512;                       // 3 x 128 accumulators + scale factors
 constexpr uint32_t kTmemSfa = 384, kTmemSfb = 448;        // scale-factor columns (all 1.0)
-constexpr size_t kTcSmemBytes = (size_t)kTcStages * kTcStageBytes + 1024 + 256;
+// Dynamic shared memory of a counting kernel with an ST-stage ring: the ring
+// (1024-byte aligned), the 256-byte barrier block and `extra` bytes after it.
+constexpr size_t tc_smem_bytes(int ST, size_t extra = 0) {
+  return (size_t)ST * kTcStageBytes + 1024 + 256 + extra;
+}
+constexpr size_t kTcSmemBytes = tc_smem_bytes(kTcStages);
 
 // ---------------------------------------------------------------- tcgen05 PTX
 
@@ -214,7 +219,7 @@ __device__ __forceinline__ WorkItem item_at(const AlnDesc *descs, const WorkItem
 // The roles every tensor-core counting kernel shares, over a work list of
 // (alignment, triangle tile) items that CTA b walks as b, b + G, b + 2G, ...:
 //   warp 0, lane 0   TMA producer: per item, the K blocks of its row tile (A)
-//                    and column tile (B) into the kTcStages-deep ring
+//                    and column tile (B) into the stage ring
 //   warp 1           MMA issuer: per item, every K block into the accumulators
 //                    (DNA blocks v, r, t, u -> V, R, T, T; protein blocks v,
 //                    rank 0 .. -> V, M, M, ...), then a commit to acc_full
@@ -224,11 +229,12 @@ __device__ __forceinline__ WorkItem item_at(const AlnDesc *descs, const WorkItem
 // operands while the epilogue of the current one runs; the MMA warp waits for
 // tmem_empty before it overwrites the accumulators.
 
-// The barrier block that follows the stage ring in shared memory.
+// The barrier block that follows the ST-stage ring in shared memory.
+template <int ST>
 struct TcShared {
-  uint8_t *stages;            // kTcStages x (A | B), 1024-byte aligned
-  uint64_t *full_bar;         // [kTcStages] TMA bytes landed
-  uint64_t *empty_bar;        // [kTcStages] MMAs done reading
+  uint8_t *stages;            // ST x (A | B), 1024-byte aligned
+  uint64_t *full_bar;         // [ST] TMA bytes landed
+  uint64_t *empty_bar;        // [ST] MMAs done reading
   uint64_t *acc_full;         // accumulators complete (one per item)
   uint64_t *tmem_empty;       // accumulators read by the epilogue
   uint64_t *drain_bar;        // every issued MMA complete (teardown)
@@ -237,13 +243,14 @@ struct TcShared {
   volatile int *abort_flag;
 };
 
-__device__ __forceinline__ TcShared tc_shared(uint8_t *smem_raw) {
-  TcShared sh;
+template <int ST>
+__device__ __forceinline__ TcShared<ST> tc_shared(uint8_t *smem_raw) {
+  TcShared<ST> sh;
   sh.stages =
       reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  sh.full_bar = reinterpret_cast<uint64_t *>(sh.stages + kTcStages * kTcStageBytes);
-  sh.empty_bar = sh.full_bar + kTcStages;
-  sh.acc_full = sh.empty_bar + kTcStages;
+  sh.full_bar = reinterpret_cast<uint64_t *>(sh.stages + ST * kTcStageBytes);
+  sh.empty_bar = sh.full_bar + ST;
+  sh.acc_full = sh.empty_bar + ST;
   sh.tmem_empty = sh.acc_full + 1;
   sh.drain_bar = sh.tmem_empty + 1;
   sh.never_bar = sh.drain_bar + 1;
@@ -252,17 +259,24 @@ __device__ __forceinline__ TcShared tc_shared(uint8_t *smem_raw) {
   return sh;
 }
 static_assert(8 * (2 * kTcStages + 4) + 8 <= 256, "the barrier block fits its 256 bytes");
+// The extra bytes after the barrier block of an ST-stage ring.
+template <int ST>
+__device__ __forceinline__ uint8_t *tc_extra(const TcShared<ST> &sh) {
+  return sh.stages + ST * kTcStageBytes + 256;
+}
 
 // Barriers, tensor memory and the unit scale factors.  tmem_readers: arrivals
 // that release the accumulators (epilogue threads or warps).  epi_warp0 ..
 // epi_warp0 + 7: the warps that fill the scale-factor columns (two per lane
-// quarter and column half).  Ends with a block barrier; returns the tensor
-// memory base address.
-__device__ __forceinline__ uint32_t tc_setup(const TcShared &sh, uint32_t tmem_readers,
-                                             int epi_warp0) {
+// quarter and column half).  alloc_warp allocates tensor memory (and frees it
+// in tc_teardown).  Ends with a block barrier; returns the tensor memory base
+// address.
+template <int ST>
+__device__ __forceinline__ uint32_t tc_setup(const TcShared<ST> &sh, uint32_t tmem_readers,
+                                             int epi_warp0, int alloc_warp = 1) {
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
-    for (int s = 0; s < kTcStages; ++s) {
+    for (int s = 0; s < ST; ++s) {
       mbar_init(&sh.full_bar[s], 1);
       mbar_init(&sh.empty_bar[s], 1);
     }
@@ -273,7 +287,7 @@ __device__ __forceinline__ uint32_t tc_setup(const TcShared &sh, uint32_t tmem_r
     *sh.abort_flag = 0;
     fence_mbar_init();
   }
-  if (warp == 1) {
+  if (warp == alloc_warp) {
     tmem_alloc(sh.tmem_slot, kTmemCols);
     tmem_relinquish();
   }
@@ -298,7 +312,8 @@ __device__ __forceinline__ uint32_t tc_setup(const TcShared &sh, uint32_t tmem_r
 
 // The producer (one thread): items it0, it0 + step, ... below nitems.  Returns
 // the number of K blocks whose loads it issued.
-__device__ __forceinline__ uint32_t tc_produce(const TcShared &sh, const AlnDesc *descs,
+template <int ST>
+__device__ __forceinline__ uint32_t tc_produce(const TcShared<ST> &sh, const AlnDesc *descs,
                                                const WorkItem *items, int it0, int nitems,
                                                int step, uint64_t limit) {
   uint32_t gkb = 0, issued = 0;
@@ -322,7 +337,7 @@ __device__ __forceinline__ uint32_t tc_produce(const TcShared &sh, const AlnDesc
       tma_load_3d(a, &d.map, &sh.full_bar[s], 0, ti * kTile, kb);
       tma_load_3d(a + kTcTileBytes, &d.map, &sh.full_bar[s], 0, tj * kTile, kb);
       issued = gkb + 1;
-      if (++ps == kTcStages) {
+      if (++ps == ST) {
         ps = 0;
         pph ^= 1u;
       }
@@ -336,7 +351,8 @@ __device__ __forceinline__ uint32_t tc_produce(const TcShared &sh, const AlnDesc
 // Descriptors are the stage base descriptors plus constant offsets: the 14-bit
 // start-address field (16-byte units) of a shared address below 228 KB cannot
 // carry out.  Ends after every MMA it issued has completed.
-__device__ __forceinline__ void tc_issue(const TcShared &sh, uint32_t tmem, const AlnDesc *descs,
+template <int ST>
+__device__ __forceinline__ void tc_issue(const TcShared<ST> &sh, uint32_t tmem, const AlnDesc *descs,
                                          const WorkItem *items, int it0, int nitems, int step,
                                          uint64_t limit) {
   const int lane = threadIdx.x & 31;
@@ -384,7 +400,7 @@ __device__ __forceinline__ void tc_issue(const TcShared &sh, uint32_t tmem, cons
         kin = 0;
         ++blk;
       }
-      if (++ring == kTcStages) {
+      if (++ring == ST) {
         ring = 0;
         ring_ph ^= 1u;
       }
@@ -413,17 +429,20 @@ __device__ __forceinline__ void tc_issue(const TcShared &sh, uint32_t tmem, cons
 // After every role has finished (call from all threads): when a wait ran out,
 // let the loads still in flight land (bounded) before shared memory is
 // released and report through err; then free tensor memory.
-__device__ __forceinline__ void tc_teardown(const TcShared &sh, uint32_t tmem, uint32_t issued,
-                                            int *err) {
+template <int ST>
+__device__ __forceinline__ void tc_teardown(const TcShared<ST> &sh, uint32_t tmem,
+                                            uint32_t issued, int *err, int alloc_warp = 1) {
   const int tid = threadIdx.x, warp = tid >> 5;
   __syncthreads();
-  if (tid == 0 && *sh.abort_flag) {
-    for (uint32_t k = issued > (uint32_t)kTcStages ? issued - kTcStages : 0; k < issued; ++k)
-      mbar_wait_bounded(&sh.full_bar[k % kTcStages], (k / kTcStages) & 1);
-    atomicOr(err, 1);
+  // `issued` is the producer's count; the producer is thread 0 of its warp, so
+  // the drain runs on the thread that knows it.
+  if (issued > 0 && *sh.abort_flag) {
+    for (uint32_t k = issued > (uint32_t)ST ? issued - ST : 0; k < issued; ++k)
+      mbar_wait_bounded(&sh.full_bar[k % ST], (k / ST) & 1);
   }
+  if (tid == 0 && *sh.abort_flag) atomicOr(err, 1);
   __syncthreads();
-  if (warp == 1) {
+  if (warp == alloc_warp) {
     tc_fence_after();
     tmem_dealloc(tmem, kTmemCols);
   }

@@ -56,7 +56,8 @@ Key key_of(int n, int L, int type, int flags) {
 bool valid_params(const rnj_tune_params &p) {
   return (p.dna_kernel == 0 || p.dna_kernel == 1) && p.ksplit >= 0 && p.ksplit <= 64 &&
          p.tile_band >= 0 && p.tile_band <= 4096 && p.transform_ctas >= 0 &&
-         p.transform_ctas <= kTransformCtasPerSm && p.stream_band >= 0 && p.stream_band <= 4096;
+         p.transform_ctas <= kTransformCtasPerSm && p.stream_band >= 0 && p.stream_band <= 4096 &&
+         (p.tc_epilogue == 0 || p.tc_epilogue == 1);
 }
 
 const char *cache_path() {
@@ -66,7 +67,8 @@ const char *cache_path() {
 
 // Text form: a header comment, then one bucket per line:
 //   <dna|protein> <naive 0/1> <log2 n> <log2 L> <dna_kernel> <ksplit> <tile_band>
-//   <transform_ctas> <stream_band> <ms>
+//   <transform_ctas> <stream_band> <tc_epilogue> <ms>
+// (lines of the earlier ten-field form, without tc_epilogue, are read as 0).
 int load_locked(const char *path) {
   FILE *f = fopen(path, "r");
   if (!f) return set_error(RNJ_ERR_IO, std::string("cannot open ") + path);
@@ -79,11 +81,20 @@ int load_locked(const char *path) {
     int naive, ln, ll;
     rnj_tune_params p;
     memset(&p, 0, sizeof p);
-    const int got = sscanf(line, "%15s %d %d %d %d %d %d %d %d %f", type, &naive, &ln, &ll,
-                           &p.dna_kernel, &p.ksplit, &p.tile_band, &p.transform_ctas,
-                           &p.stream_band, &p.ms);
+    float f10 = 0.0f, f11 = 0.0f;
+    int got = sscanf(line, "%15s %d %d %d %d %d %d %d %d %f %f", type, &naive, &ln, &ll,
+                     &p.dna_kernel, &p.ksplit, &p.tile_band, &p.transform_ctas, &p.stream_band,
+                     &f10, &f11);
+    if (got == 11) {  // tc_epilogue, ms
+      p.tc_epilogue = (int)f10;
+      p.ms = f11;
+      if ((float)p.tc_epilogue != f10) got = 0;
+    } else if (got == 10) {  // the ten-field form: ms last
+      p.ms = f10;
+      got = 11;
+    }
     const int t = strcmp(type, "dna") == 0 ? RNJ_DNA : (strcmp(type, "protein") == 0 ? RNJ_PROTEIN : -1);
-    if (got != 10 || t < 0 || (naive != 0 && naive != 1) || ln < 0 || ln > 40 || ll < 0 ||
+    if (got != 11 || t < 0 || (naive != 0 && naive != 1) || ln < 0 || ln > 40 || ll < 0 ||
         ll > 40 || !valid_params(p)) {
       fclose(f);
       return set_error(RNJ_ERR_FORMAT, std::string(path) + ": bad tune entry on line " +
@@ -98,14 +109,14 @@ int load_locked(const char *path) {
 int save_locked(const char *path) {
   FILE *f = fopen(path, "w");
   if (!f) return set_error(RNJ_ERR_IO, std::string("cannot write ") + path);
-  fprintf(f, "# rapidnj-b200 tune table v1: type naive log2n log2L dna_kernel ksplit tile_band "
-             "transform_ctas stream_band ms\n");
+  fprintf(f, "# rapidnj-b200 tune table v2: type naive log2n log2L dna_kernel ksplit tile_band "
+             "transform_ctas stream_band tc_epilogue ms\n");
   for (const auto &kv : g_table) {
     const rnj_tune_params &p = kv.second;
-    fprintf(f, "%s %d %d %d %d %d %d %d %d %.4f\n",
+    fprintf(f, "%s %d %d %d %d %d %d %d %d %d %.4f\n",
             std::get<0>(kv.first) == RNJ_DNA ? "dna" : "protein", std::get<1>(kv.first),
             std::get<2>(kv.first), std::get<3>(kv.first), p.dna_kernel, p.ksplit, p.tile_band,
-            p.transform_ctas, p.stream_band, p.ms);
+            p.transform_ctas, p.stream_band, p.tc_epilogue, p.ms);
   }
   const bool ok = fclose(f) == 0;
   return ok ? RNJ_OK : set_error(RNJ_ERR_IO, std::string("cannot write ") + path);
@@ -138,6 +149,7 @@ TuneParams tune_lookup(int n, int L, int type, int flags) {
   t.tile_band = it->second.tile_band;
   t.transform_ctas = it->second.transform_ctas;
   t.stream_band = it->second.stream_band;
+  t.tc_epilogue = it->second.tc_epilogue;
   return t;
 }
 

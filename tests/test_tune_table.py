@@ -84,3 +84,22 @@ def test_env_cache_is_read_on_first_use(tmp_path):
     out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
                          check=True)
     assert out.stdout.strip() == "4"
+
+
+def test_epilogue_choice_and_earlier_file_form(tmp_path):
+    api.tune_set(10000, 10000, "dna", tc_epilogue=1, ms=1.0)
+    assert api.tune_get(10000, 10000, "dna").tc_epilogue == 1
+    with pytest.raises(RnjError):
+        api.tune_set(100, 100, "dna", tc_epilogue=2)
+    path = str(tmp_path / "t.txt")
+    api.tune_save(path)
+    api.tune_clear()
+    api.tune_load(path)
+    assert api.tune_get(10000, 10000, "dna").tc_epilogue == 1
+    # a table written before the epilogue field existed: ten fields, ms last
+    old = tmp_path / "v1.txt"
+    old.write_text("# v1\ndna 0 13 13 0 1 12 5 16 1.2500\n")
+    api.tune_clear()
+    api.tune_load(str(old))
+    p = api.tune_get(10000, 10000, "dna")
+    assert (p.tile_band, p.stream_band, p.tc_epilogue) == (12, 16, 0) and abs(p.ms - 1.25) < 1e-4
