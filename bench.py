@@ -271,7 +271,7 @@ def measure_workload(name: str, steps: int, warmup: int, rank: int = 0, world: i
                                "on every SM); 4 x measured dense bf16 beside it",
                 "peak_4x_bf16": bf16x4 / 1e12, "frac_of_4x_bf16": achieved / bf16x4,
                 "peak_4x_bf16_source": bf16_src,
-                "traffic": traffic_from_profiles(name), "kernel": kname, "kernel_ms": cnt,
+                "traffic": traffic_from_profiles(kname, name), "kernel": kname, "kernel_ms": cnt,
                 "flops_per_pair_column": fpc,
                 "kernel_includes": ("counts, exact transform and the matrix stores" if fused
                                     else "counts (the transform is a second kernel)"),
@@ -286,7 +286,8 @@ def measure_workload(name: str, steps: int, warmup: int, rank: int = 0, world: i
             result["roofline"] = {
                 "bound": "int", "pipe": "POPC", "achieved": achieved / 1e12,
                 "peak": popc_peak / 1e12, "unit": "Tops/s", "frac": achieved / popc_peak,
-                "traffic": traffic_from_profiles(name),
+                "traffic": traffic_from_profiles(
+                    "count_batch_kernel" if world > 1 else "count_tiles_kernel", name),
                 "kernel": "count_batch_kernel" if world > 1 else "count_tiles_kernel",
                 "kernel_ms": cnt,
                 "lop3_frac": (lop3_w * words / (cnt * 1e-3)) / lop3_peak,
@@ -734,12 +735,13 @@ def fp4_from_bf16():
     return 4.0 * bf16, src
 
 
-def traffic_from_profiles(name: str):
-    """DRAM bytes per launch of the counting kernel for this workload, from the
-    ncu summaries committed under profiles/ (None when there is none)."""
+def traffic_from_profiles(kernel: str, name: str):
+    """DRAM bytes per launch of `kernel` on this workload, measured by one ncu
+    capture and recorded under profiles/ (None when that kernel was not
+    captured on this workload)."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
-        v = json.load(open(p)).get(name)
+        v = json.load(open(p)).get(kernel, {}).get(name)
         return float(v) if isinstance(v, (int, float)) else None
     except Exception:
         return None
