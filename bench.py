@@ -172,7 +172,7 @@ def cpu_reference(seqs: np.ndarray, model: str, type_: str, warmup: int, steps: 
 
 def measure_workload(name: str, steps: int, warmup: int, rank: int = 0, world: int = 1,
                      local_rank: int = 0, popcount: bool = False, with_e2e: bool = True,
-                     clocks: bool = True):
+                     clocks: bool = True, roofline: bool = True):
     """One workload through the library: W warm-up steps, then K timed steps
     (CUDA events on the library's stream, a 256 MiB buffer written between
     steps so that L2 starts cold).  Returns the figures of the JSON line."""
@@ -240,7 +240,10 @@ def measure_workload(name: str, steps: int, warmup: int, rank: int = 0, world: i
     share = (t1 - t0) / ntiles
     mean = lambda x: sum(x) / len(x)  # noqa: E731
     tc = not popcount and (type_ == "dna" or residue_ranks(seqs) <= 31)
-    fused = tc and L <= 65535 and world == 1
+    # the fused kernel unless the tuner's entry for this bucket chose the
+    # two-kernel form
+    entry = api.tune_get(n, L, type_)
+    fused = tc and L <= 65535 and (entry is None or entry.tc_epilogue == 0)
     result = {"ms_per_step": ms_per_step, "value": W / (ms_per_step * 1e-3), "clocks": clk,
               "stages_ms": {"pack": mean(pack_ms),
                             "count_and_transform" if fused else "count": mean(count_ms),
@@ -250,7 +253,7 @@ def measure_workload(name: str, steps: int, warmup: int, rank: int = 0, world: i
               "gpu_launches_per_step": (1 if type_ == "protein" else 0) + 3 +
                                        (0 if (fused or not tc) else 1)}
 
-    if rank == 0:
+    if rank == 0 and roofline:
         cnt = mean(count_ms)
         if tc:
             # tcgen05 kernel, against the FP4 tensor pipe measured live on this
@@ -424,12 +427,27 @@ def run_batched(args, local_rank: int = 0, count: int = 256):
     steps = max(1, min(args.steps, 5))
     t_plain = timed(plain, steps)
     t_batch = timed(batched, steps)
+    # launch shape of the batched pass: each alignment's tile-order band from
+    # its bucket's tuned entry, the ring depth from the bucket with most work
+    depth, tuned = batch.tuning()
     identical = all(torch.equal(x, y) for x, y in zip(outs_a, outs_b))
+
+    def untuned():
+        for _ in range(max(1, args.warmup)):
+            batched()
+        return timed(batched, steps), batch.tuning()
+
+    t_untuned, (depth0, _) = without_tuning(untuned)
+    identical = identical and all(torch.equal(x, y) for x, y in zip(outs_a, outs_b))
     batch.close()
     ctx.close()
     return {"value": W / (t_batch * 1e-3), "unit": "pair-columns/s", "ms_per_step": t_batch,
             "plain_value": W / (t_plain * 1e-3), "plain_ms_per_step": t_plain,
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": identical,
+            "shapes": {"source": "autotuner table " + str(tune_table_source()),
+                       "tuned_alignments": tuned, "ring_depth": depth,
+                       "tile_shape": "128 x 128 pairs (the tcgen05 M and the shared tile order)",
+                       "untuned_ms_per_step": t_untuned, "untuned_ring_depth": depth0},
             "alignments": count, "tiles": tiles, "pair_columns": W,
             "workload": "256 alignments, N~U[32,2048], L~U[300,5000], 70% DNA K2P / 30% "
                         "protein Kimura, tree-evolved, seed 0"}
@@ -724,6 +742,54 @@ def run_text(args, local_rank: int = 0):
             "workload": f"-o m text of the {args.workload} matrix into a file (page cache)"}
 
 
+def tune_table_source():
+    """The tuning table the library read at its first lookup (as it chooses:
+    RNJ_TUNE_CACHE, else the table shipped beside librnjgpu.so unless
+    RNJ_NO_TUNE_TABLE is set), relative to the repository when inside it."""
+    p = os.environ.get("RNJ_TUNE_CACHE")
+    if not p:
+        off = os.environ.get("RNJ_NO_TUNE_TABLE", "")
+        p = None if (off and off != "0") else os.path.join(ROOT, "rapidnj_b200", "tune_b200.txt")
+    if not p or not os.path.exists(p):
+        return None
+    p = os.path.abspath(p)
+    return os.path.relpath(p, ROOT) if p.startswith(ROOT + os.sep) else p
+
+
+def without_tuning(fn):
+    """fn() with the tuning table emptied (every bucket at the library's
+    defaults), the table restored afterwards."""
+    import tempfile
+    from rapidnj_b200 import api
+    fd, path = tempfile.mkstemp(suffix=".tune")
+    os.close(fd)
+    try:
+        api.tune_save(path)
+        api.tune_clear()
+        return fn()
+    finally:
+        api.tune_load(path)
+        os.unlink(path)
+
+
+def tuning_report(name, steps, local_rank, popcount, tuned_ms):
+    """The plain workload at the tuned choice of its bucket against the
+    library's defaults (fewer steps, no roofline or end-to-end run)."""
+    from rapidnj_b200 import api
+    _, n, L, type_, _ = WORKLOADS[name]
+    entry = api.tune_get(n, L, type_)
+    rep = {"table": tune_table_source(), "entry": entry.as_dict() if entry else None,
+           "tuned_ms_per_step": tuned_ms}
+    if entry is None:
+        rep["default_ms_per_step"] = tuned_ms
+        return rep
+    r = without_tuning(lambda: measure_workload(name, max(3, min(steps, 20)), 3,
+                                                local_rank=local_rank, popcount=popcount,
+                                                with_e2e=False, clocks=False, roofline=False))
+    rep["default_ms_per_step"] = r["ms_per_step"]
+    return rep
+
+
 def fp4_from_bf16():
     """Four times the measured dense bf16 GEMM throughput of MEASURED_PEAKS.json
     (flop/s; the dense FP4 : BF16 rate ratio of B200), and its source."""
@@ -820,6 +886,13 @@ def main():
                 "data": "synthetic", "config": config, "roofline": res["roofline"],
                 "e2e": res["e2e"], "clocks": res["clocks"], "stages_ms": res["stages_ms"],
                 "gpu_launches": res["gpu_launches_per_step"] * args.steps}
+        if world == 1:
+            # the bucket's tuned launch choice (the headline) against the defaults
+            try:
+                line["tuning"] = tuning_report(args.workload, args.steps, local_rank,
+                                               args.popcount, res["ms_per_step"])
+            except Exception as e:  # noqa: BLE001
+                line["tuning"] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
         if not args.no_cpu_baseline and world == 1:
             seqs = make_alignment(args.workload)
             cpu = cpu_reference(seqs, model, type_, 0, 1)

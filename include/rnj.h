@@ -298,6 +298,11 @@ int rnj_batch_output(rnj_batch *batch, int slot, float **d_out, size_t *ld, floa
 /* Moves a batch-allocated output into a matrix handle (for rnj_mat_copy_rows). */
 int rnj_batch_take(rnj_batch *batch, int slot, rnj_mat **out);
 int rnj_batch_size(rnj_batch *batch, int *alignments, long long *tiles);
+/* The launch shape of the last run: the tensor-core ring depth it ran with
+ * (the tuned depth of the bucket holding most of its work) and how many of its
+ * alignments had a tuned entry (each one's tile-order band comes from it).
+ * Either pointer may be NULL. */
+int rnj_batch_tuning(rnj_batch *batch, int *ring_depth, int *tuned_alignments);
 /* Forgets the alignments (frees outputs still owned by the batch); the graph stays. */
 int rnj_batch_clear(rnj_batch *batch);
 int rnj_batch_destroy(rnj_batch *batch);
@@ -444,8 +449,11 @@ int rnj_write_matrix_text(const char *path, const char *const *names, const floa
  * No counterpart in the reference (its CPU code has nothing to tune).  The
  * tile edge itself is fixed at 128 pairs: the tensor-core MMA is 128 rows
  * (M = 128) and three 128-column f32 accumulators fill the 512 columns of
- * tensor memory with the scale factors; what varies is how the tiles are
- * scheduled and how the columns are split.  Zero fields mean the default. */
+ * tensor memory with the scale factors, and every path (transform, fix-up,
+ * streamed, sharded, batched, row-band) shares that tile order.  What varies
+ * is how the tiles are scheduled, how the columns are split, which epilogue
+ * form runs and how deep the shared-memory rings of staged K blocks are.
+ * Zero fields mean the default. */
 typedef struct rnj_tune_params {
   int dna_kernel;      /* DNA fast rules and protein: 0 tensor cores, 1 bit-plane popcount */
   int ksplit;          /* bit-plane kernel: columns split over this many CTAs per tile */
@@ -455,6 +463,11 @@ typedef struct rnj_tune_params {
   int tc_epilogue;     /* tensor cores: 0 the exact transform in the counting kernel's own
                           epilogue warps (one launch), 1 packed counts and a separate
                           transform kernel at higher occupancy */
+  int tc_stages;       /* tensor cores: shared-memory ring depth in 256-column K blocks,
+                          2..6 fused, 2..7 two-kernel (0 = the deepest) */
+  int pop_stages;      /* bit-plane kernel: ring depth in 256-site K blocks, raised to the
+                          3 (DNA, 2-bit codes) or 2 (5- and 7-bit codes) its distance
+                          staging needs; 0 = the deepest, 4 (DNA, 2-bit) or 3 */
   float ms;            /* the tuned configuration's time for the measured shape (output) */
 } rnj_tune_params;
 
@@ -465,7 +478,10 @@ typedef struct rnj_tune_params {
  * that every later call of that bucket uses.  Every candidate computes the same
  * distances; only the time differs.  If the environment variable
  * RNJ_TUNE_CACHE names a file, the table is read from it on first use and
- * written back after each rnj_tune.  out (may be NULL) receives the choice. */
+ * written back after each rnj_tune; otherwise the table shipped beside the
+ * library (tune_b200.txt in the directory of librnjgpu.so, measured on a B200
+ * by rapidnj_b200/make_tune_table.py) is read on first use, unless
+ * RNJ_NO_TUNE_TABLE is set.  out (may be NULL) receives the choice. */
 int rnj_tune(rnj_ctx *ctx, int n, int L, int type, int flags, rnj_tune_params *out);
 /* The stored entry of the bucket (RNJ_ERR_NOTREADY if there is none). */
 int rnj_tune_get(int n, int L, int type, int flags, rnj_tune_params *out);

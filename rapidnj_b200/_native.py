@@ -95,6 +95,7 @@ SIGNATURES = {
     "rnj_batch_output": (c_int, [c_void_p, c_int, P(c_void_p), P(c_size_t), P(c_float)]),
     "rnj_batch_take": (c_int, [c_void_p, c_int, P(c_void_p)]),
     "rnj_batch_size": (c_int, [c_void_p, P(c_int), P(ctypes.c_longlong)]),
+    "rnj_batch_tuning": (c_int, [c_void_p, P(c_int), P(c_int)]),
     "rnj_batch_clear": (c_int, [c_void_p]),
     "rnj_batch_destroy": (c_int, [c_void_p]),
     "rnj_batch_poll": (c_int, [c_void_p, P(c_int)]),

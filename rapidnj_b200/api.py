@@ -431,6 +431,12 @@ class Batch:
         check(N.lib().rnj_batch_size(self.handle, ctypes.byref(a), ctypes.byref(t)))
         return a.value, t.value
 
+    def tuning(self):
+        """(ring depth, alignments with a tuned entry) of the last run."""
+        d, t = ctypes.c_int(), ctypes.c_int()
+        check(N.lib().rnj_batch_tuning(self.handle, ctypes.byref(d), ctypes.byref(t)))
+        return d.value, t.value
+
     def clear(self) -> None:
         check(N.lib().rnj_batch_clear(self.handle))
         self._keep = []
@@ -453,6 +459,7 @@ class TuneParams(ctypes.Structure):
     _fields_ = [("dna_kernel", ctypes.c_int), ("ksplit", ctypes.c_int),
                 ("tile_band", ctypes.c_int), ("transform_ctas", ctypes.c_int),
                 ("stream_band", ctypes.c_int), ("tc_epilogue", ctypes.c_int),
+                ("tc_stages", ctypes.c_int), ("pop_stages", ctypes.c_int),
                 ("ms", ctypes.c_float)]
 
     def as_dict(self) -> dict:

@@ -442,7 +442,7 @@ int run_tc_single(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, int epi_mo
   if (epi_mode == EPI_COUNTS) {
     const int grid = (int)std::min<long long>(ntiles, ctx->num_sms);
     RNJ_CUDA(launch_tc_batch(ctx->d_desc, nullptr, nullptr, (int)ntiles, 0, (int)ntiles, nullptr,
-                             grid, EPI_COUNTS, ctx->stream),
+                             grid, EPI_COUNTS, ctx->stream, tp.tc_stages),
              "tensor-core kernel");
     return RNJ_OK;
   }
@@ -508,6 +508,7 @@ int run_popcount(rnj_ctx *ctx, const Packed &p, int ckind, int nk, int nt, EpiPa
   // SMs idle with one CTA per tile; splitting the columns over several CTAs
   // per tile (atomic count accumulation, then the transform) fills them.
   const TuneParams tp = tune_lookup(p.n, p.L, p.type, p.flags);
+  ep.stages = tp.pop_stages;
   const bool split = tp.ksplit > 1 && nk >= 2 && !ep.full &&
                      (size_t)p.n * p.n * 3 * sizeof(uint32_t) <= (size_t)1 << 30;
   if (nk <= kMaxFusedWords / kKW && !split) {
@@ -568,7 +569,8 @@ int run_tc_distances(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, const A
     mark(ctx, 1, 0);
     RNJ_CUDA(launch_tc_fused(d_desc, d_items, nullptr, (int)nitems, 0, (int)nitems,
                              (int)std::min<long long>(nitems, ctx->num_sms),
-                             fused_variant_for(ep.model, ep.type, ep.compat_wrap, 0), s),
+                             fused_variant_for(ep.model, ep.type, ep.compat_wrap, 0), s,
+                             tp.tc_stages),
              "fused tensor-core kernel");
     mark(ctx, 1, 1);
     mark(ctx, 2, 0);
@@ -576,11 +578,12 @@ int run_tc_distances(rnj_ctx *ctx, const Packed &p, const EpiParams &ep, const A
   }
   int rc = ensure_packed(ctx, std::min<long long>(nitems, kTcChunkTiles));
   if (rc != RNJ_OK) return rc;
-  return run_tc_chunks(ctx, d_desc, d_items, nitems, ctx->d_packed, s, tp.transform_ctas);
+  return run_tc_chunks(ctx, d_desc, d_items, nitems, ctx->d_packed, s, tp.transform_ctas,
+                       tp.tc_stages);
 }
 
 int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, long long nitems,
-                  uint64_t *packed, cudaStream_t s, int transform_ctas) {
+                  uint64_t *packed, cudaStream_t s, int transform_ctas, int stages) {
   const int ctas = transform_ctas > 0 ? std::min(transform_ctas, kTransformCtasPerSm)
                                       : kTransformCtasPerSm;
   const int chunk = (int)std::min<long long>(nitems, kTcChunkTiles);
@@ -588,7 +591,7 @@ int run_tc_chunks(rnj_ctx *ctx, const AlnDesc *d_desc, const WorkItem *d_items, 
     const int cnt = (int)std::min<long long>(chunk, nitems - i0);
     if (i0 == 0) mark(ctx, 1, 0);
     RNJ_CUDA(launch_tc_batch(d_desc, d_items, nullptr, (int)nitems, (int)i0, cnt, packed,
-                             std::min(cnt, ctx->num_sms), EPI_PACKED, s),
+                             std::min(cnt, ctx->num_sms), EPI_PACKED, s, stages),
              "tensor-core kernel");
     if (i0 + chunk >= nitems) mark(ctx, 1, 1);
     if (i0 + chunk >= nitems) mark(ctx, 2, 0);

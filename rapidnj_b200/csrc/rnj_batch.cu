@@ -14,6 +14,7 @@
 #include "rnj.h"
 #include "rnj_internal.h"
 #include "rnj_objects.h"
+#include "rnj_tcgen05.cuh"
 
 using namespace rnj;
 
@@ -64,6 +65,12 @@ struct rnj_batch {
   std::vector<void *> arenas;  // packed alignments of rnj_batch_add_many, freed by clear
   std::vector<int> host_max;  // maxima of the last run, read once per run
   bool host_max_valid = false;
+  // Launch shape from the tuner: the fused kernel's ring depth the graph was
+  // captured with (that of the bucket holding most of a run's work; 0 = the
+  // default) and how many alignments of the last run had a tuned entry (their
+  // tile-order band comes from it).
+  int tc_stages = 0;
+  int tuned_alns = 0;
 };
 
 void batch_set_join(rnj_batch *b, bool join) { b->join = join; }
@@ -109,7 +116,7 @@ int capture_graph(rnj_batch *b) {
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ints + 2, 0, 2 * sizeof(int), b->stream);
   if (e == cudaSuccess)
     e = launch_tc_fused(b->d_descs, b->d_items_tc, b->d_ints + 0, 0, 0, (int)b->cap_tiles, sms,
-                        FUSED_ANY, b->stream);
+                        FUSED_ANY, b->stream, b->tc_stages);
   if (e == cudaSuccess)
     e = launch_count_batch(b->d_descs, b->d_items_pc, b->d_ints + 1, b->d_ints + 2, sms, EPI_DIST,
                            b->stream);
@@ -396,14 +403,50 @@ int rnj_batch_run(rnj_batch *b) {
     ep.err = b->d_ints + 3;
     b->h_descs[a] = desc_for(p, ep);
   }
+  // Tuned launch shape: each alignment's tile-order band from its bucket, the
+  // ring depth from the bucket of the tensor-core alignment with the most
+  // work (tiles x K).  A new depth re-captures the graph.
+  std::vector<int> bands(na, 0);
+  {
+    int tuned = 0, depth = 0;
+    long long top = -1;
+    for (int a = 0; a < na; ++a) {
+      const Packed &p = b->entries[a].aln->p;
+      bool found = false;
+      const TuneParams tp = tune_lookup(p.n, p.L, p.type, p.flags, &found);
+      tuned += found ? 1 : 0;
+      bands[a] = tp.tile_band > 0 ? tp.tile_band : kBand;
+      const long long work = b->entries[a].ntiles * cost(a);
+      if (is_tc_kind(p.kind) && work > top) {
+        top = work;
+        depth = tp.tc_stages;
+      }
+    }
+    b->tuned_alns = tuned;
+    if (depth != b->tc_stages) {
+      RNJ_CUDA(cudaStreamSynchronize(b->stream), "batch stream");
+      if (b->exec) cudaGraphExecDestroy(b->exec);
+      if (b->graph) cudaGraphDestroy(b->graph);
+      b->exec = nullptr;
+      b->graph = nullptr;
+      b->tc_stages = depth;
+      const int rc = capture_graph(b);
+      if (rc != RNJ_OK) return rc;
+    }
+  }
   for (int oi = 0; oi < na; ++oi) {
     const int a = order[oi];
     const Entry &en = b->entries[a];
     const bool tc = is_tc_kind(en.aln->p.kind);
+    // tensor-core triangles in the banded order of their bucket's band
+    // height (consecutive items go to consecutive CTAs, which then share row
+    // tiles in L2); full-square and bit-plane items in row-major order
+    const bool banded = tc && !b->h_descs[a].full;
+    const int nt = b->h_descs[a].nt;
     for (long long t = 0; t < en.ntiles; ++t) {
       WorkItem w;
       w.aln = a;
-      w.tile = (int)t;
+      w.tile = banded ? banded_tile((int)t, nt, bands[a]) : (int)t;
       if (tc) b->h_items_tc[ntc++] = w;
       else b->h_items_pc[npc++] = w;
     }
@@ -513,6 +556,13 @@ int rnj_batch_take(rnj_batch *b, int slot, rnj_mat **out) {
   en.owned = false;
   en.out = nullptr;
   *out = m;
+  return RNJ_OK;
+}
+
+int rnj_batch_tuning(rnj_batch *b, int *ring_depth, int *tuned_alignments) {
+  if (!b) return set_error(RNJ_ERR_INVALID, "null batch");
+  if (ring_depth) *ring_depth = fused_ring_depth(b->tc_stages);
+  if (tuned_alignments) *tuned_alignments = b->tuned_alns;
   return RNJ_OK;
 }
 

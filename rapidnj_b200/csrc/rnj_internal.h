@@ -96,6 +96,7 @@ struct EpiParams {
   int stall = 0;              // test of the failure path: wait on a barrier nothing completes
   int row0 = 0;               // output row offset: row i is stored at out + (i - row0) * ld
   int tile0 = 0;              // bit-plane kernel: tile of block 0 (a band of full-square tiles)
+  int stages = 0;             // bit-plane kernel: ring depth (0: its plane layout's deepest)
 };
 
 // One alignment of a work list, as the persistent kernels read it from device
@@ -142,11 +143,13 @@ struct TuneParams {
   int stream_band = 0;     // streamed host call: band height in tile rows (0 = automatic)
   int tc_epilogue = 0;     // tensor-core distances: 0 transform fused into the counting
                            // kernel, 1 packed counts + separate transform kernel
+  int tc_stages = 0;       // tensor-core ring depth (0 = 6 fused, 7 two-kernel)
+  int pop_stages = 0;      // bit-plane kernel ring depth (0 = its plane layout's deepest)
 };
 // The parameters of the bucket of (n, L, type, flags): the tuned entry if the
 // table (filled by rnj_tune / rnj_tune_load / RNJ_TUNE_CACHE) holds one, else
-// the defaults.
-TuneParams tune_lookup(int n, int L, int type, int flags);
+// the defaults (*found, when given, says which).
+TuneParams tune_lookup(int n, int L, int type, int flags, bool *found = nullptr);
 
 // One alignment of a batched pack (rnj_batch_add_many): the multi-alignment
 // pack kernels take an array of these and find the alignment of each work unit
@@ -216,9 +219,10 @@ AlnDesc desc_for(const Packed &p, const EpiParams &ep);
 // means the tiles of d_descs[0] in banded order; d_nitems == nullptr means
 // nitems is n.  EPI_PACKED writes packed counts (kPackedTileWords per item) for
 // launch_tc_transform; EPI_COUNTS writes each alignment's n x n x 3 counts.
+// stages: the ring depth (0: the default, 7; the tuner's tc_stages).
 cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
                             int nitems, int item0, int count, uint64_t *packed, int grid,
-                            int epi_mode, cudaStream_t s);
+                            int epi_mode, cudaStream_t s, int stages = 0);
 // Tensor-pipe probe (rnj_probe_tc_peak): one CTA per SM, `iters` FP4 MMAs each.
 cudaError_t launch_tc_peak_probe(int grid, int iters, int *err, cudaStream_t s);
 cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
@@ -230,14 +234,17 @@ cudaError_t launch_tc_transform(const AlnDesc *d_descs, const WorkItem *d_items,
 // straight into each alignment's output, with its max slot and saturation
 // flags.  Every alignment has at most kMaxFusedColumns columns.
 // variant: the transform of every item (fused_variant_for), or FUSED_ANY to
-// choose per item from its descriptor.
+// choose per item from its descriptor.  stages: the ring depth (0: the
+// default, 6; the tuner's tc_stages).
 enum FusedVariant {
   FUSED_K2P = 0, FUSED_JC = 1, FUSED_PROTEIN = 2, FUSED_GENERIC = 3, FUSED_FULL = 4, FUSED_ANY = 5
 };
 int fused_variant_for(int model, int type, int compat, int full);
 cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
                             int nitems, int item0, int count, int grid, int variant,
-                            cudaStream_t s);
+                            cudaStream_t s, int stages = 0);
+// The ring depth launch_tc_fused runs with for a requested `stages`.
+int fused_ring_depth(int stages);
 
 enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2, EPI_PACKED = 3 };
 

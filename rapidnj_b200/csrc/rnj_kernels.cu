@@ -283,12 +283,28 @@ template <>
 struct KT<KIND_MISM5> { static constexpr int NP = 6, NC = 2, ST = 3; };
 template <>
 struct KT<KIND_MISM7> { static constexpr int NP = 8, NC = 2, ST = 3; };
-static_assert(8 * (4 + 1) <= 64, "the barriers of count_tiles_kernel fit its 64 bytes");
+static_assert(8 * (4 + 1) <= 64, "the barriers of count_tiles_kernel (at most 4 + 1) fit its 64 bytes");
 
+// Shared memory of count_tiles_kernel with an nst-stage ring: the stages,
+// alignment slack, nst + 1 barriers.
 template <int KIND>
-constexpr size_t count_smem_bytes() {
-  // stages, alignment slack, ST + 1 barriers
-  return (size_t)KT<KIND>::ST * 2 * KT<KIND>::NP * kKW * kTile * 4 + 1024 + 64;
+constexpr size_t count_smem_bytes(int nst) {
+  return (size_t)nst * 2 * KT<KIND>::NP * kKW * kTile * 4 + 1024 + 64;
+}
+// The ring depths count_tiles_kernel takes: at most its layout's ST, at least
+// two and enough stages to hold the distance tile the EPI_DIST epilogue stages
+// in the same buffers.
+template <int KIND>
+__host__ __device__ constexpr int count_min_stages() {
+  constexpr size_t stage = 2 * (size_t)KT<KIND>::NP * kKW * kTile * 4;
+  return (int)((kStageBytes + stage - 1) / stage) < 2 ? 2 : (int)((kStageBytes + stage - 1) / stage);
+}
+template <int KIND>
+__host__ __device__ constexpr int count_stages(int requested) {
+  return requested <= 0 ? KT<KIND>::ST
+                        : (requested < count_min_stages<KIND>()
+                               ? count_min_stages<KIND>()
+                               : (requested > KT<KIND>::ST ? KT<KIND>::ST : requested));
 }
 
 template <int KIND>
@@ -329,10 +345,13 @@ __global__ void __launch_bounds__(256, 1)
     count_tiles_kernel(const __grid_constant__ CUtensorMap tmap, int nt, int nk, int kchunk,
                        EpiParams ep) {
   using T = KT<KIND>;
-  constexpr int NP = T::NP, NC = T::NC, ST = T::ST;
+  constexpr int NP = T::NP, NC = T::NC;
   constexpr int TILE_WORDS = NP * kKW * kTile;
   constexpr uint32_t STAGE_BYTES = 2u * TILE_WORDS * 4u;
-  static_assert((size_t)ST * STAGE_BYTES >= kStageBytes, "distance tile must fit the stage buffers");
+  static_assert((size_t)count_min_stages<KIND>() * STAGE_BYTES >= kStageBytes,
+                "distance tile must fit the stage buffers");
+  // ring depth: count_stages() of the launch (the launcher sets ep.stages)
+  const int ST = ep.stages;
 
   extern __shared__ uint8_t smem_raw[];
   uint32_t *smem =
@@ -354,7 +373,6 @@ __global__ void __launch_bounds__(256, 1)
   // full_bar[ST]: a barrier that nothing completes, waited on only by the test
   // of the failure path (ep.stall).
   if (tid == 0) {
-#pragma unroll
     for (int s = 0; s <= ST; ++s) mbar_init(&full_bar[s], 1);
     fence_mbar_init();
     prefetch_tmap(&tmap);
@@ -851,11 +869,13 @@ cudaError_t launch_pack_bitstrings_dna(const uint32_t *d_bits, const uint32_t *d
 template <int KIND, int EPI>
 static cudaError_t launch_one(const Packed &p, const EpiParams &ep, dim3 grid, int nt, int nk,
                               int kchunk, cudaStream_t s) {
-  constexpr size_t smem = count_smem_bytes<KIND>();
+  EpiParams e1 = ep;
+  e1.stages = count_stages<KIND>(ep.stages);
+  const size_t smem = count_smem_bytes<KIND>(e1.stages);
   cudaError_t e = cudaFuncSetAttribute(count_tiles_kernel<KIND, EPI>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  count_tiles_kernel<KIND, EPI><<<grid, 256, smem, s>>>(p.tmap, nt, nk, kchunk, ep);
+  count_tiles_kernel<KIND, EPI><<<grid, 256, smem, s>>>(p.tmap, nt, nk, kchunk, e1);
   return cudaGetLastError();
 }
 

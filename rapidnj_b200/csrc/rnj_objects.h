@@ -65,9 +65,11 @@ int ensure_packed(rnj_ctx *ctx, long long tiles);
 // passes of at most kTcChunkTiles tiles through `packed` (capacity
 // min(nitems, kTcChunkTiles) tiles), on stream s.  Profiling marks: stage 1
 // spans the counting kernels, stage 2 the transforms (rnj_api.cu).
-// transform_ctas > 0: resident CTAs per SM of the transform grid (else 5).
+// transform_ctas > 0: resident CTAs per SM of the transform grid (else 5);
+// stages > 0: the counting kernel's ring depth (else its default).
 int run_tc_chunks(rnj_ctx *ctx, const rnj::AlnDesc *d_desc, const rnj::WorkItem *d_items,
-                  long long nitems, uint64_t *packed, cudaStream_t s, int transform_ctas = 0);
+                  long long nitems, uint64_t *packed, cudaStream_t s, int transform_ctas = 0,
+                  int stages = 0);
 // Distances of work items [0, nitems) of one tensor-core alignment (descriptor
 // d_desc on the device; d_items == nullptr: its banded triangle): the fused
 // kernel (rnj_tcf.cu) when the alignment takes it (at most kMaxFusedColumns

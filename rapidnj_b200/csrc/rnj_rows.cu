@@ -112,6 +112,8 @@ extern "C" int rnj_distance_rows(rnj_ctx *ctx, rnj_aln *aln, int model, int band
   EpiParams ep = ctx_epi(ctx, p, model);
   ep.full = 1;
   ep.ld = (size_t)n;
+  const TuneParams tp = tune_lookup(p.n, p.L, p.type, p.flags);
+  ep.stages = tp.pop_stages;
 
   RowBuffers buf(ctx);
   const size_t band_floats = (size_t)band * n;
@@ -161,8 +163,7 @@ extern "C" int rnj_distance_rows(rnj_ctx *ctx, rnj_aln *aln, int model, int band
               "band descriptor upload");
       RNJ_TRY(launch_tc_fused(buf.d_desc[b], nullptr, nullptr, (int)all_tiles, (int)tile0,
                               (int)btiles, (int)std::min<long long>(btiles, ctx->num_sms),
-                              FUSED_FULL,
-                              ctx->stream),
+                              FUSED_FULL, ctx->stream, tp.tc_stages),
               "fused tensor-core kernel (row band)");
     } else {
       const int ckind = (p.kind == KIND_DNA && model == RNJ_JC) ? KIND_MISM2 : p.kind;

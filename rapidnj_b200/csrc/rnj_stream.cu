@@ -294,12 +294,12 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
       RNJ_TRY(launch_tc_fused(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
                               (int)cnt, (int)std::min<long long>(cnt, ctx->num_sms),
                               fused_variant_for(ep.model, ep.type, ep.compat_wrap, 0),
-                              ctx->stream),
+                              ctx->stream, tp.tc_stages),
               "fused tensor-core kernel");
     } else {
       RNJ_TRY(launch_tc_batch(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
                               (int)cnt, ctx->d_packed, (int)std::min<long long>(cnt, ctx->num_sms),
-                              EPI_PACKED, ctx->stream),
+                              EPI_PACKED, ctx->stream, tp.tc_stages),
               "tensor-core kernel");
       RNJ_TRY(launch_tc_transform(ctx->d_desc, buf.items, nullptr, (int)items.size(), (int)i0,
                                   (int)cnt, ctx->d_packed,

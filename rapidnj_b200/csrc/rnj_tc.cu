@@ -314,9 +314,9 @@ template <int EPI>
 __global__ void __launch_bounds__(kTcThreads, 1)
     tc_batch_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
                     const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
-                    uint64_t *__restrict__ packed) {
+                    uint64_t *__restrict__ packed, int nst) {
   extern __shared__ uint8_t smem_raw[];
-  const TcShared<kTcStages> sh = tc_shared<kTcStages>(smem_raw);
+  const TcShared sh = tc_shared(smem_raw, nst, 0);
   // The pipeline waits' bound and the failure-path test switch (the same for
   // every alignment of a launch).
   const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);
@@ -524,22 +524,15 @@ cudaError_t launch_pack_features_multi(const PackJob *d_jobs, int njobs, long lo
 
 cudaError_t launch_tc_batch(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
                             int nitems, int item0, int count, uint64_t *packed, int grid,
-                            int epi_mode, cudaStream_t s) {
+                            int epi_mode, cudaStream_t s, int stages) {
   if (grid <= 0) return cudaSuccess;
-  cudaError_t e;
-  if (epi_mode == EPI_PACKED) {
-    e = cudaFuncSetAttribute(tc_batch_kernel<EPI_PACKED>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes);
-    if (e != cudaSuccess) return e;
-    tc_batch_kernel<EPI_PACKED><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(
-        d_descs, d_items, d_nitems, nitems, item0, count, packed);
-  } else {
-    e = cudaFuncSetAttribute(tc_batch_kernel<EPI_COUNTS>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes);
-    if (e != cudaSuccess) return e;
-    tc_batch_kernel<EPI_COUNTS><<<(unsigned)grid, kTcThreads, kTcSmemBytes, s>>>(
-        d_descs, d_items, d_nitems, nitems, item0, count, packed);
-  }
+  const int nst = tc_ring_depth(stages, kTcStages, kTcStages);
+  const size_t smem = tc_smem_bytes(nst);
+  auto kernel = epi_mode == EPI_PACKED ? tc_batch_kernel<EPI_PACKED> : tc_batch_kernel<EPI_COUNTS>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<(unsigned)grid, kTcThreads, smem, s>>>(d_descs, d_items, d_nitems, nitems, item0, count,
+                                                  packed, nst);
   return cudaGetLastError();
 }
 

@@ -50,8 +50,9 @@ constexpr int kTcfProducerWarp = 16, kTcfMmaWarp = 17;
 constexpr int kTcfRegsLow = 32, kTcfRegsHigh = 112, kTcfRegsLaunch = 96;
 static_assert(128 * kTcfRegsLow + 512 * kTcfRegsHigh <= kTcfThreads * kTcfRegsLaunch,
               "the register split fits the launch's registers");
-// A six-stage ring (the seventh stage's 32 KB would leave no room) and the
-// logarithm table (128 x {ln F, 1 / F}) after the barrier block.
+// A ring of up to six stages (a seventh stage's 32 KB would leave no room; six
+// is the default, the tuner may choose fewer) and the logarithm table
+// (128 x {ln F, 1 / F}) after the barrier block.
 constexpr int kTcfStages = 6;
 constexpr size_t kTcfTableBytes = 128 * 2 * sizeof(double);
 constexpr size_t kTcfSmemBytes = tc_smem_bytes(kTcfStages, kTcfTableBytes);
@@ -286,9 +287,10 @@ __device__ __forceinline__ void fused_rows_full(const AlnDesc &d, int i, int jb,
 template <int V>
 __global__ void __launch_bounds__(kTcfThreads, 1)
     tc_fused_kernel(const AlnDesc *__restrict__ descs, const WorkItem *__restrict__ items,
-                    const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count) {
+                    const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
+                    int nst) {
   extern __shared__ uint8_t smem_raw[];
-  const TcShared<kTcfStages> sh = tc_shared<kTcfStages>(smem_raw);
+  const TcShared sh = tc_shared(smem_raw, nst, kTcfTableBytes);
   double2 *const tab = reinterpret_cast<double2 *>(tc_extra(sh));
   const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);
   const int stall = descs[0].stall;
@@ -408,13 +410,14 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
 template <int V>
 static cudaError_t launch_variant(const AlnDesc *d_descs, const WorkItem *d_items,
                                   const int *d_nitems, int nitems, int item0, int count, int grid,
-                                  cudaStream_t s) {
+                                  int stages, cudaStream_t s) {
+  const int nst = tc_ring_depth(stages, kTcfStages, kTcfStages);
+  const size_t smem = tc_smem_bytes(nst, kTcfTableBytes);
   cudaError_t e = cudaFuncSetAttribute(tc_fused_kernel<V>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kTcfSmemBytes);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  tc_fused_kernel<V><<<(unsigned)grid, kTcfThreads, kTcfSmemBytes, s>>>(
-      d_descs, d_items, d_nitems, nitems, item0, count);
+  tc_fused_kernel<V><<<(unsigned)grid, kTcfThreads, smem, s>>>(d_descs, d_items, d_nitems, nitems,
+                                                              item0, count, nst);
   return cudaGetLastError();
 }
 
@@ -425,30 +428,20 @@ int fused_variant_for(int model, int type, int compat, int full) {
   return type == RNJ_PROTEIN ? FUSED_PROTEIN : FUSED_K2P;
 }
 
+int fused_ring_depth(int stages) { return tc_ring_depth(stages, kTcfStages, kTcfStages); }
+
 cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, const int *d_nitems,
                             int nitems, int item0, int count, int grid, int variant,
-                            cudaStream_t s) {
+                            cudaStream_t s, int stages) {
   if (grid <= 0) return cudaSuccess;
-  switch (variant) {
-    case FUSED_K2P:
-      return launch_variant<kFusedK2p>(d_descs, d_items, d_nitems, nitems, item0, count, grid, s);
-    case FUSED_JC:
-      return launch_variant<kFusedJc>(d_descs, d_items, d_nitems, nitems, item0, count, grid, s);
-    case FUSED_PROTEIN:
-      return launch_variant<kFusedProtein>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
-                                           s);
-    case FUSED_GENERIC:
-      return launch_variant<kFusedGeneric>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
-                                           s);
-    case FUSED_FULL:
-      return launch_variant<kFusedFull>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
-                                        s);
-    case FUSED_ANY:
-      return launch_variant<kFusedAny>(d_descs, d_items, d_nitems, nitems, item0, count, grid,
-                                       s);
-    default:
-      return cudaErrorInvalidValue;
-  }
+  using Launch = cudaError_t (*)(const AlnDesc *, const WorkItem *, const int *, int, int, int,
+                                 int, int, cudaStream_t);
+  // indexed by FusedVariant
+  static const Launch kLaunch[] = {launch_variant<kFusedK2p>,     launch_variant<kFusedJc>,
+                                   launch_variant<kFusedProtein>, launch_variant<kFusedGeneric>,
+                                   launch_variant<kFusedFull>,    launch_variant<kFusedAny>};
+  if (variant < FUSED_K2P || variant > FUSED_ANY) return cudaErrorInvalidValue;
+  return kLaunch[variant](d_descs, d_items, d_nitems, nitems, item0, count, grid, stages, s);
 }
 
 }  // namespace rnj

@@ -14,7 +14,8 @@
 
 namespace rnj {
 
-constexpr int kTcStages = 7;  // ring depth of the two-kernel form (tc_batch_kernel)
+constexpr int kTcStages = 7;  // deepest ring of the two-kernel form (tc_batch_kernel)
+constexpr int kTcMinStages = 2;
 constexpr int kTcKBlock = 128;                            // bytes of K per stage (256 FP4 columns)
 constexpr int kTcKCols = 256;                             // feature columns per stage
 constexpr uint32_t kTcTileBytes = kTile * kTcKBlock;      // 16 KB per operand tile
@@ -22,12 +23,18 @@ constexpr uint32_t kTcStageBytes = 2 * kTcTileBytes;      // A + B
 constexpr int kTcThreads = 320;
 constexpr uint32_t kTmemCols = 512;                       // 3 x 128 accumulators + scale factors
 constexpr uint32_t kTmemSfa = 384, kTmemSfb = 448;        // scale-factor columns (all 1.0)
-// Dynamic shared memory of a counting kernel with an ST-stage ring: the ring
-// (1024-byte aligned), the 256-byte barrier block and `extra` bytes after it.
-constexpr size_t tc_smem_bytes(int ST, size_t extra = 0) {
-  return (size_t)ST * kTcStageBytes + 1024 + 256 + extra;
+// Dynamic shared memory of a counting kernel with an nst-stage ring: 1024
+// bytes of alignment slack, the 256-byte barrier block, `extra` bytes after it
+// (both padded to 1024), then the ring.  The barriers and the extra bytes sit
+// at fixed offsets before the ring, so the ring depth -- a launch parameter,
+// the tuner's choice per bucket -- moves nothing but the ring's end, and the
+// launch gives the kernel exactly the shared memory of its depth.
+__host__ __device__ constexpr size_t tc_head_bytes(size_t extra) { return (256 + extra + 1023) / 1024 * 1024; }
+constexpr size_t tc_smem_bytes(int nst, size_t extra = 0) {
+  return 1024 + tc_head_bytes(extra) + (size_t)nst * kTcStageBytes;
 }
 constexpr size_t kTcSmemBytes = tc_smem_bytes(kTcStages);
+static_assert(kTcSmemBytes <= 232448, "the deepest two-kernel ring fits the shared memory of one CTA");
 
 // ---------------------------------------------------------------- tcgen05 PTX
 
@@ -179,16 +186,16 @@ __device__ __forceinline__ void item_tile(const AlnDesc &d, int tile, int &ti, i
 // Returns the tile's row-major triangle index (the index of its saturation flag).
 constexpr int kBand = 12;  // default band height (the autotuner may choose another)
 
-__device__ __forceinline__ int banded_tile(int it, int nt, int band) {
+__host__ __device__ __forceinline__ int banded_tile(int it, int nt, int band) {
   int r0 = 0;
   while (true) {
-    const int g = min(band, nt - r0);
+    const int g = band < nt - r0 ? band : nt - r0;
     const int tri = g * (g + 1) / 2;
     const int count = tri + (nt - r0 - g) * g;
     if (it < count || r0 + g >= nt) {
       int ti, tj;
       if (it < tri) {
-        int c = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
+        int c = (int)((sqrtf(8.0f * (float)it + 1.0f) - 1.0f) * 0.5f);
         while (c * (c + 1) / 2 > it) --c;
         while ((c + 1) * (c + 2) / 2 <= it) ++c;
         tj = r0 + c;
@@ -229,40 +236,49 @@ __device__ __forceinline__ WorkItem item_at(const AlnDesc *descs, const WorkItem
 // operands while the epilogue of the current one runs; the MMA warp waits for
 // tmem_empty before it overwrites the accumulators.
 
-// The barrier block that follows the ST-stage ring in shared memory.
-template <int ST>
+// The barrier block at the start of shared memory (before the ring).
 struct TcShared {
-  uint8_t *stages;            // ST x (A | B), 1024-byte aligned
-  uint64_t *full_bar;         // [ST] TMA bytes landed
-  uint64_t *empty_bar;        // [ST] MMAs done reading
+  uint8_t *stages;            // nst x (A | B), 1024-byte aligned
+  uint64_t *full_bar;         // [nst] TMA bytes landed
+  uint64_t *empty_bar;        // [nst] MMAs done reading
   uint64_t *acc_full;         // accumulators complete (one per item)
   uint64_t *tmem_empty;       // accumulators read by the epilogue
   uint64_t *drain_bar;        // every issued MMA complete (teardown)
   uint64_t *never_bar;        // nothing completes it: the failure-path test waits here
   uint32_t *tmem_slot;
   volatile int *abort_flag;
+  int nst;                    // ring depth, kTcMinStages .. the kernel's maximum
 };
 
-template <int ST>
-__device__ __forceinline__ TcShared<ST> tc_shared(uint8_t *smem_raw) {
-  TcShared<ST> sh;
-  sh.stages =
+// extra: the bytes after the barrier block the kernel asked for in
+// tc_smem_bytes (a constant of the kernel).
+__device__ __forceinline__ TcShared tc_shared(uint8_t *smem_raw, int nst, size_t extra) {
+  TcShared sh;
+  sh.nst = nst;
+  uint8_t *const base =
       reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  sh.full_bar = reinterpret_cast<uint64_t *>(sh.stages + ST * kTcStageBytes);
-  sh.empty_bar = sh.full_bar + ST;
-  sh.acc_full = sh.empty_bar + ST;
+  sh.full_bar = reinterpret_cast<uint64_t *>(base);
+  sh.empty_bar = sh.full_bar + kTcStages;
+  sh.acc_full = sh.empty_bar + kTcStages;
   sh.tmem_empty = sh.acc_full + 1;
   sh.drain_bar = sh.tmem_empty + 1;
   sh.never_bar = sh.drain_bar + 1;
   sh.tmem_slot = reinterpret_cast<uint32_t *>(sh.never_bar + 1);
   sh.abort_flag = reinterpret_cast<volatile int *>(sh.tmem_slot + 1);
+  sh.stages = base + tc_head_bytes(extra);
   return sh;
 }
 static_assert(8 * (2 * kTcStages + 4) + 8 <= 256, "the barrier block fits its 256 bytes");
-// The extra bytes after the barrier block of an ST-stage ring.
-template <int ST>
-__device__ __forceinline__ uint8_t *tc_extra(const TcShared<ST> &sh) {
-  return sh.stages + ST * kTcStageBytes + 256;
+// The extra bytes after the barrier block.
+__device__ __forceinline__ uint8_t *tc_extra(const TcShared &sh) {
+  return reinterpret_cast<uint8_t *>(sh.full_bar) + 256;
+}
+// The ring depth a kernel runs with: `requested` (0: the kernel's default
+// `dflt`) within kTcMinStages .. `max_st`.
+__host__ __device__ constexpr int tc_ring_depth(int requested, int dflt, int max_st) {
+  return requested <= 0 ? dflt
+                        : (requested < kTcMinStages ? kTcMinStages
+                                                    : (requested > max_st ? max_st : requested));
 }
 
 // Barriers, tensor memory and the unit scale factors.  tmem_readers: arrivals
@@ -271,12 +287,11 @@ __device__ __forceinline__ uint8_t *tc_extra(const TcShared<ST> &sh) {
 // quarter and column half).  alloc_warp allocates tensor memory (and frees it
 // in tc_teardown).  Ends with a block barrier; returns the tensor memory base
 // address.
-template <int ST>
-__device__ __forceinline__ uint32_t tc_setup(const TcShared<ST> &sh, uint32_t tmem_readers,
+__device__ __forceinline__ uint32_t tc_setup(const TcShared &sh, uint32_t tmem_readers,
                                              int epi_warp0, int alloc_warp = 1) {
   const int tid = threadIdx.x, warp = tid >> 5;
   if (tid == 0) {
-    for (int s = 0; s < ST; ++s) {
+    for (int s = 0; s < sh.nst; ++s) {
       mbar_init(&sh.full_bar[s], 1);
       mbar_init(&sh.empty_bar[s], 1);
     }
@@ -312,8 +327,7 @@ __device__ __forceinline__ uint32_t tc_setup(const TcShared<ST> &sh, uint32_t tm
 
 // The producer (one thread): items it0, it0 + step, ... below nitems.  Returns
 // the number of K blocks whose loads it issued.
-template <int ST>
-__device__ __forceinline__ uint32_t tc_produce(const TcShared<ST> &sh, const AlnDesc *descs,
+__device__ __forceinline__ uint32_t tc_produce(const TcShared &sh, const AlnDesc *descs,
                                                const WorkItem *items, int it0, int nitems,
                                                int step, uint64_t limit) {
   uint32_t gkb = 0, issued = 0;
@@ -337,7 +351,7 @@ __device__ __forceinline__ uint32_t tc_produce(const TcShared<ST> &sh, const Aln
       tma_load_3d(a, &d.map, &sh.full_bar[s], 0, ti * kTile, kb);
       tma_load_3d(a + kTcTileBytes, &d.map, &sh.full_bar[s], 0, tj * kTile, kb);
       issued = gkb + 1;
-      if (++ps == ST) {
+      if (++ps == sh.nst) {
         ps = 0;
         pph ^= 1u;
       }
@@ -351,8 +365,7 @@ __device__ __forceinline__ uint32_t tc_produce(const TcShared<ST> &sh, const Aln
 // Descriptors are the stage base descriptors plus constant offsets: the 14-bit
 // start-address field (16-byte units) of a shared address below 228 KB cannot
 // carry out.  Ends after every MMA it issued has completed.
-template <int ST>
-__device__ __forceinline__ void tc_issue(const TcShared<ST> &sh, uint32_t tmem, const AlnDesc *descs,
+__device__ __forceinline__ void tc_issue(const TcShared &sh, uint32_t tmem, const AlnDesc *descs,
                                          const WorkItem *items, int it0, int nitems, int step,
                                          uint64_t limit) {
   const int lane = threadIdx.x & 31;
@@ -400,7 +413,7 @@ __device__ __forceinline__ void tc_issue(const TcShared<ST> &sh, uint32_t tmem, 
         kin = 0;
         ++blk;
       }
-      if (++ring == ST) {
+      if (++ring == sh.nst) {
         ring = 0;
         ring_ph ^= 1u;
       }
@@ -429,16 +442,16 @@ __device__ __forceinline__ void tc_issue(const TcShared<ST> &sh, uint32_t tmem, 
 // After every role has finished (call from all threads): when a wait ran out,
 // let the loads still in flight land (bounded) before shared memory is
 // released and report through err; then free tensor memory.
-template <int ST>
-__device__ __forceinline__ void tc_teardown(const TcShared<ST> &sh, uint32_t tmem,
+__device__ __forceinline__ void tc_teardown(const TcShared &sh, uint32_t tmem,
                                             uint32_t issued, int *err, int alloc_warp = 1) {
   const int tid = threadIdx.x, warp = tid >> 5;
   __syncthreads();
   // `issued` is the producer's count; the producer is thread 0 of its warp, so
   // the drain runs on the thread that knows it.
   if (issued > 0 && *sh.abort_flag) {
-    for (uint32_t k = issued > (uint32_t)ST ? issued - ST : 0; k < issued; ++k)
-      mbar_wait_bounded(&sh.full_bar[k % ST], (k / ST) & 1);
+    const uint32_t nst = (uint32_t)sh.nst;
+    for (uint32_t k = issued > nst ? issued - nst : 0; k < issued; ++k)
+      mbar_wait_bounded(&sh.full_bar[k % nst], (k / nst) & 1);
   }
   if (tid == 0 && *sh.abort_flag) atomicOr(err, 1);
   __syncthreads();

@@ -38,6 +38,12 @@ def same(a, b):
     dict(dna_kernel=1, ksplit=4),
     dict(tile_band=4, transform_ctas=3),
     dict(tile_band=1, transform_ctas=1),
+    dict(tc_stages=2),
+    dict(tc_stages=4, tile_band=8),
+    dict(tc_epilogue=1, tc_stages=5),
+    dict(tc_epilogue=1, tc_stages=2, transform_ctas=2),
+    dict(dna_kernel=1, pop_stages=3),
+    dict(dna_kernel=1, pop_stages=2, ksplit=2),
 ])
 @pytest.mark.parametrize("model", ["kim", "jc"])
 def test_dna_choices_give_default_bits(ctx, fields, model):
@@ -47,12 +53,52 @@ def test_dna_choices_give_default_bits(ctx, fields, model):
     same(device_matrix(ctx, seqs, 0, model), ref)
 
 
-@pytest.mark.parametrize("ksplit", [2, 3, 8, 16])
-def test_protein_k_split_gives_default_bits(ctx, ksplit):
+@pytest.mark.parametrize("fields", [dict(ksplit=2), dict(ksplit=3), dict(ksplit=8),
+                                    dict(ksplit=16), dict(pop_stages=2), dict(pop_stages=3),
+                                    dict(ksplit=4, pop_stages=2)])
+def test_protein_bit_plane_choices_give_default_bits(ctx, fields):
     seqs = synth.tree_protein(300, 2500, seed=6, mean_branch=0.2)
     ref = device_matrix(ctx, seqs, 1, "kim")
-    api.tune_set(300, 2500, "protein", dna_kernel=1, ksplit=ksplit)
+    api.tune_set(300, 2500, "protein", dna_kernel=1, **fields)
     same(device_matrix(ctx, seqs, 1, "kim"), ref)
+
+
+@pytest.mark.parametrize("stages", [2, 3, 6])
+def test_protein_tensor_core_ring_depth_gives_default_bits(ctx, stages):
+    seqs = synth.tree_protein(400, 1500, seed=8, mean_branch=0.1)
+    ref = device_matrix(ctx, seqs, 1, "kim")
+    api.tune_set(400, 1500, "protein", tc_stages=stages)
+    same(device_matrix(ctx, seqs, 1, "kim"), ref)
+
+
+def test_batch_takes_its_shape_from_the_tuner(ctx):
+    # Two alignments; the larger one's bucket is tuned to a three-stage ring
+    # and band 4: the batch re-captures its graph with that ring depth, and the
+    # results equal the untuned batch's.
+    dna = synth.tree_dna(900, 2000, seed=2)
+    prot = synth.tree_protein(200, 700, seed=3)
+
+    def run():
+        b = api.Batch(ctx, max_alignments=4, max_tiles=4096)
+        slots = [b.add(ctx.alignment(dna, 0), "kim"), b.add(ctx.alignment(prot, 1), "kim")]
+        b.run()
+        b.synchronize()
+        out = []
+        for k in slots:
+            m = b.take(k)
+            out.append((m.to_numpy(), m.max))
+            m.close()
+        shape = b.tuning()
+        b.close()
+        return out, shape
+
+    ref, shape0 = run()
+    assert shape0 == (6, 0)
+    api.tune_set(900, 2000, "dna", tc_stages=3, tile_band=4)
+    got, shape1 = run()
+    assert shape1 == (3, 1)
+    for g, r in zip(got, ref):
+        same(g, r)
 
 
 def test_stream_band_gives_default_bits(ctx):

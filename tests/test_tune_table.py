@@ -103,3 +103,60 @@ def test_epilogue_choice_and_earlier_file_form(tmp_path):
     api.tune_load(str(old))
     p = api.tune_get(10000, 10000, "dna")
     assert (p.tile_band, p.stream_band, p.tc_epilogue) == (12, 16, 0) and abs(p.ms - 1.25) < 1e-4
+
+
+def test_ring_depths_and_eleven_field_form(tmp_path):
+    api.tune_set(10000, 10000, "dna", tc_stages=4, pop_stages=3, ms=1.0)
+    p = api.tune_get(10000, 10000, "dna")
+    assert (p.tc_stages, p.pop_stages) == (4, 3)
+    for field, value in (("tc_stages", 8), ("tc_stages", -1), ("pop_stages", 5)):
+        with pytest.raises(RnjError):
+            api.tune_set(100, 100, "dna", **{field: value})
+    path = str(tmp_path / "t.txt")
+    api.tune_save(path)
+    line = open(path).read().splitlines()[1].split()
+    assert len(line) == 13 and line[10:12] == ["4", "3"]
+    api.tune_clear()
+    api.tune_load(path)
+    assert api.tune_get(10000, 10000, "dna").tc_stages == 4
+    # the form with tc_epilogue but without the ring depths: eleven fields
+    old = tmp_path / "v2.txt"
+    old.write_text("# v2\nprotein 0 12 10 0 2 8 5 0 1 0.5000\n")
+    api.tune_clear()
+    api.tune_load(str(old))
+    p = api.tune_get(5000, 1500, "protein")
+    assert (p.ksplit, p.tile_band, p.tc_epilogue, p.tc_stages, p.pop_stages) == (2, 8, 1, 0, 0)
+    # a fractional integer field is malformed
+    old.write_text("dna 0 13 13 0 1.5 12 5 16 1 0 0 1.0\n")
+    with pytest.raises(RnjError):
+        api.tune_load(str(old))
+
+
+def test_shipped_table_beside_the_library(tmp_path):
+    # A copy of the library with a tune_b200.txt beside it reads that table at
+    # its first lookup; RNJ_NO_TUNE_TABLE turns it off, RNJ_TUNE_CACHE wins.
+    import shutil
+    lib = os.path.join(ROOT, "rapidnj_b200", "librnjgpu.so")
+    shutil.copy(lib, tmp_path / "librnjgpu.so")
+    (tmp_path / "tune_b200.txt").write_text("# shipped\ndna 0 13 13 0 1 8 0 0 0 5 0 1.0\n")
+    other = tmp_path / "other.txt"
+    other.write_text("dna 0 13 13 0 1 24 0 0 0 3 0 1.0\n")
+    code = textwrap.dedent(f"""
+        import ctypes
+        lib = ctypes.CDLL({str(tmp_path / "librnjgpu.so")!r})
+        p = (ctypes.c_int * 9)()
+        rc = lib.rnj_tune_get(10000, 10000, 0, 1, p)
+        print(rc, p[2], p[6])
+    """)
+
+    def run(**env):
+        e = {k: v for k, v in os.environ.items()
+             if k not in ("RNJ_TUNE_CACHE", "RNJ_NO_TUNE_TABLE")}
+        e.update(env)
+        out = subprocess.run([sys.executable, "-c", code], env=e, capture_output=True,
+                             text=True, check=True)
+        return out.stdout.split()
+
+    assert run() == ["0", "8", "5"]
+    assert run(RNJ_NO_TUNE_TABLE="1")[0] != "0"
+    assert run(RNJ_TUNE_CACHE=str(other)) == ["0", "24", "3"]
