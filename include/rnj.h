@@ -326,10 +326,14 @@ int rnj_bootstrap(rnj_ctx *ctx, const void *d_chars, int n, int L, size_t ld, in
  * from any thread; a scheduler thread of the server (with its own context on
  * `device`) admits requests first come, first served while the device memory
  * they need (bytes, packed operands, output) fits `memory_budget` (0: 60 % of
- * the free memory at creation), uploads and packs them, and launches them as a
- * batch; up to two batches are in flight, so requests that arrive while one
- * batch computes form the next, which starts as soon as it has work and
- * overlaps the first on the device.  Packed inputs are freed when a request
+ * the free memory at creation), at most `max_batch` per scheduling pass,
+ * uploads and packs them, and appends their tiles to a live work list that one
+ * persistent kernel consumes while it runs: a request that arrives while
+ * others compute joins the running launch, and completes on its own as soon
+ * as its last tile is done (the kernel then applies its saturation fix-up and
+ * flags it complete to the host).  Requests the tensor-core kernel cannot take
+ * (protein alphabets above 31 residues, the -f rules, RNJ_POPCOUNT, more than
+ * 65,535 columns) run as plain calls.  Packed inputs are freed when a request
  * completes; its output matrix stays on the device until the client takes it.
  * No counterpart in the reference (which computes one matrix per process run). */
 typedef struct rnj_server rnj_server;

@@ -65,10 +65,10 @@ struct rnj_batch {
   std::vector<void *> arenas;  // packed alignments of rnj_batch_add_many, freed by clear
   std::vector<int> host_max;  // maxima of the last run, read once per run
   bool host_max_valid = false;
-  // Launch shape from the tuner: the fused kernel's ring depth the graph was
-  // captured with (that of the bucket holding most of a run's work; 0 = the
-  // default) and how many alignments of the last run had a tuned entry (their
-  // tile-order band comes from it).
+  // Launch shape from the tuner: the fused kernel's ring depth of the last run
+  // (that of the bucket holding most of its work; 0 = the default) and how
+  // many of its alignments had a tuned entry (their tile-order band comes
+  // from it).
   int tc_stages = 0;
   int tuned_alns = 0;
 };
@@ -116,7 +116,7 @@ int capture_graph(rnj_batch *b) {
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ints + 2, 0, 2 * sizeof(int), b->stream);
   if (e == cudaSuccess)
     e = launch_tc_fused(b->d_descs, b->d_items_tc, b->d_ints + 0, 0, 0, (int)b->cap_tiles, sms,
-                        FUSED_ANY, b->stream, b->tc_stages);
+                        FUSED_ANY, b->stream);
   if (e == cudaSuccess)
     e = launch_count_batch(b->d_descs, b->d_items_pc, b->d_ints + 1, b->d_ints + 2, sms, EPI_DIST,
                            b->stream);
@@ -405,7 +405,7 @@ int rnj_batch_run(rnj_batch *b) {
   }
   // Tuned launch shape: each alignment's tile-order band from its bucket, the
   // ring depth from the bucket of the tensor-core alignment with the most
-  // work (tiles x K).  A new depth re-captures the graph.
+  // work (tiles x K).
   std::vector<int> bands(na, 0);
   {
     int tuned = 0, depth = 0;
@@ -423,16 +423,10 @@ int rnj_batch_run(rnj_batch *b) {
       }
     }
     b->tuned_alns = tuned;
-    if (depth != b->tc_stages) {
-      RNJ_CUDA(cudaStreamSynchronize(b->stream), "batch stream");
-      if (b->exec) cudaGraphExecDestroy(b->exec);
-      if (b->graph) cudaGraphDestroy(b->graph);
-      b->exec = nullptr;
-      b->graph = nullptr;
-      b->tc_stages = depth;
-      const int rc = capture_graph(b);
-      if (rc != RNJ_OK) return rc;
-    }
+    // The graph's launch holds the deepest ring; the run's depth travels in
+    // the first descriptor (no re-capture).
+    b->tc_stages = depth;
+    if (na > 0) b->h_descs[0].stages = depth;
   }
   for (int oi = 0; oi < na; ++oi) {
     const int a = order[oi];

@@ -40,6 +40,31 @@ __device__ __forceinline__ void tri_coords(int t, int nt, int &ti, int &tj) {
   tj = r + (int)(t - start(r));
 }
 
+// The saturation fix-up of one tile of d (-1 -> m2 = 2 x the alignment's
+// maximum; KimuraDistance.cpp:366-395, JCdistance.cpp:201-230), threads t0,
+// t0 + nthr, ... of its 128 x 128 entries: a triangle tile's pairs i < j and
+// their mirror entries, or every off-diagonal entry of a full-square tile.
+__device__ __forceinline__ void fixup_tile(const AlnDesc &d, int tile, float m2, int t0, int nthr) {
+  int ti, tj;
+  if (d.full) {
+    ti = tile / d.nt;
+    tj = tile % d.nt;
+  } else {
+    tri_coords(tile, d.nt, ti, tj);
+  }
+  for (int e = t0; e < kTile * kTile; e += nthr) {
+    const int i = ti * kTile + e / kTile;
+    const int j = tj * kTile + e % kTile;
+    if (d.full) {
+      if (i < d.n && j < d.n && i != j && d.out[(size_t)(i - d.row0) * d.ld + j] == -1.0f)
+        d.out[(size_t)(i - d.row0) * d.ld + j] = m2;
+    } else if (i < j && j < d.n && d.out[(size_t)i * d.ld + j] == -1.0f) {
+      d.out[(size_t)i * d.ld + j] = m2;
+      d.out[(size_t)j * d.ld + i] = m2;
+    }
+  }
+}
+
 // Per-thread pair layout inside a 128 x 128 tile (256 threads = 4 x 2 warps, each
 // warp 32 rows x 64 columns, each lane 8 x 8 pairs): rows rbase + {0..3, 16..19},
 // columns cbase + {0..3, 32..35}.  The two 4-wide groups keep every 128-bit

@@ -115,8 +115,11 @@ struct alignas(128) AlnDesc {
                                // band: tile-order band height (single alignment), 0 = 12;
                                // wait_us: bound of the pipeline waits (0: 2 s)
   int stall, row0;             // stall, row0: as EpiParams
+  int stages, pad_;            // stages: the tensor-core ring depth of a work-list launch
+                               // (read from the first descriptor; 0: the launch's own)
   double jc_b;
 };
+static_assert(sizeof(AlnDesc) % 128 == 0, "descriptors of a work list share no 128-byte line");
 
 // A work item: alignment index and linear triangle-tile index within it.
 struct WorkItem {
@@ -245,6 +248,52 @@ cudaError_t launch_tc_fused(const AlnDesc *d_descs, const WorkItem *d_items, con
                             cudaStream_t s, int stages = 0);
 // The ring depth launch_tc_fused runs with for a requested `stages`.
 int fused_ring_depth(int stages);
+
+// The live work list of the served form (rnj_server.cu): triangle tiles of
+// tensor-core alignments appended while tc_live_kernel runs.  The publisher
+// (launch_live_publish, on another stream) writes items [first, first + count)
+// of alignment slot aln and then raises *tail with a release store; the live
+// kernel's CTAs claim indices below *tail (compare-and-swap on *head) and,
+// when there is none, poll *tail for idle_us before they exit.  tiles_done[a]
+// counts the finished tiles of slot a and sat[a] says whether one held a
+// saturated pair.  The CTA that finishes slot a's last tile appends a fix-up
+// item per flagged tile to the second list (fix_items: reserved by
+// atomicAdd on *fix_tail, written with a release store, claimed by any CTA
+// before the main list's items); fix_pending[a] counts the fix-ups not yet
+// done (plus one held by the appending CTA), and whoever brings it to zero --
+// or the last tile's CTA when nothing saturated -- writes done[a] = {1, max
+// bits} (mapped page-locked host memory).  err: the error word of the launch.
+struct LiveList {
+  WorkItem *items;
+  unsigned int *head;
+  unsigned int *tail;
+  unsigned int *tiles_done;
+  int *sat;
+  unsigned long long *fix_items;  // (tile << 32) | (slot + 1); 0 = not yet written
+  unsigned int *fix_head;
+  unsigned int *fix_tail;
+  unsigned int *fix_pending;
+  // The exit vote: a CTA that has found nothing to claim for idle_us counts
+  // itself in *idle_ctas; when every CTA of the launch is counted, *closing is
+  // set and every CTA leaves at its next claim (items published after that go
+  // to the next launch).  Both are cleared before each launch.
+  unsigned int *idle_ctas;
+  unsigned int *closing;
+  int2 *done;
+  int *err;
+  int cap_items, cap_aln;
+  unsigned int idle_us;
+};
+// grid CTAs of the live kernel (fewer than the SMs: the others pack arriving
+// requests); stages: the ring depth (0: 6).
+cudaError_t launch_tc_live(const AlnDesc *d_descs, const LiveList &live, int grid, int stages,
+                           cudaStream_t s);
+// Clears the scratch of slot aln (its max slot, tile flags and counters),
+// appends its count triangle tiles (band order of height band) at items[first
+// ..] and publishes them.
+cudaError_t launch_live_publish(const LiveList &live, int aln, int nt, int band,
+                                unsigned int first, unsigned int count, int *max_bits,
+                                int *tile_flags, cudaStream_t s);
 
 enum EpiMode { EPI_DIST = 0, EPI_COUNTS = 1, EPI_ATOMIC = 2, EPI_PACKED = 3 };
 

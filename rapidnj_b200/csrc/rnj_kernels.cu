@@ -770,25 +770,7 @@ __global__ void __launch_bounds__(256) fixup_batch_kernel(const AlnDesc *__restr
     const WorkItem w = it < na ? items_a[it] : items_b[it - na];
     const AlnDesc &d = descs[w.aln];
     if (d.out == nullptr || d.tile_flags[w.tile] == 0) continue;
-    int ti, tj;
-    if (d.full) {
-      ti = w.tile / d.nt;
-      tj = w.tile % d.nt;
-    } else {
-      tri_coords(w.tile, d.nt, ti, tj);
-    }
-    const float m2 = __fmul_rn(__int_as_float(*d.max_bits), 2.0f);
-    for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
-      const int i = ti * kTile + e / kTile;
-      const int j = tj * kTile + e % kTile;
-      if (d.full) {
-        if (i < d.n && j < d.n && i != j && d.out[(size_t)i * d.ld + j] == -1.0f)
-          d.out[(size_t)i * d.ld + j] = m2;
-      } else if (i < j && j < d.n && d.out[(size_t)i * d.ld + j] == -1.0f) {
-        d.out[(size_t)i * d.ld + j] = m2;
-        d.out[(size_t)j * d.ld + i] = m2;
-      }
-    }
+    fixup_tile(d, w.tile, __fmul_rn(__int_as_float(*d.max_bits), 2.0f), threadIdx.x, blockDim.x);
   }
 }
 

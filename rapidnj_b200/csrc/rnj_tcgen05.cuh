@@ -325,6 +325,36 @@ __device__ __forceinline__ uint32_t tc_setup(const TcShared &sh, uint32_t tmem_r
   return tmem;
 }
 
+// The producer's loads of one item: its K blocks of the row tile (A) and the
+// column tile (B) into the ring.  ps / pph: the ring stage and parity of the
+// next load; gkb / issued: K blocks loaded so far and the count whose loads
+// were issued.  False (abort flag set) when a wait ran out.
+__device__ __forceinline__ bool tc_produce_item(const TcShared &sh, const AlnDesc &d, int tile,
+                                                uint32_t &gkb, uint32_t &issued, int &ps,
+                                                uint32_t &pph, uint64_t limit) {
+  tensormap_acquire(&d.map);
+  int ti, tj;
+  item_tile(d, tile, ti, tj);
+  const int nkb = d.np * d.kdim / kTcKCols;  // feature blocks x K blocks per block
+  for (int kb = 0; kb < nkb; ++kb, ++gkb) {
+    const int s = ps;
+    if (!tc_wait(&sh.empty_bar[s], pph ^ 1u, sh.abort_flag, limit)) {
+      *sh.abort_flag = 1;
+      return false;
+    }
+    uint8_t *a = sh.stages + s * kTcStageBytes;
+    mbar_arrive_expect_tx(&sh.full_bar[s], kTcStageBytes);
+    tma_load_3d(a, &d.map, &sh.full_bar[s], 0, ti * kTile, kb);
+    tma_load_3d(a + kTcTileBytes, &d.map, &sh.full_bar[s], 0, tj * kTile, kb);
+    issued = gkb + 1;
+    if (++ps == sh.nst) {
+      ps = 0;
+      pph ^= 1u;
+    }
+  }
+  return true;
+}
+
 // The producer (one thread): items it0, it0 + step, ... below nitems.  Returns
 // the number of K blocks whose loads it issued.
 __device__ __forceinline__ uint32_t tc_produce(const TcShared &sh, const AlnDesc *descs,
@@ -335,42 +365,93 @@ __device__ __forceinline__ uint32_t tc_produce(const TcShared &sh, const AlnDesc
   uint32_t pph = 0;
   for (int it = it0; it < nitems && !*sh.abort_flag; it += step) {
     const WorkItem w = item_at(descs, items, it);
-    const AlnDesc &d = descs[w.aln];
-    tensormap_acquire(&d.map);
-    int ti, tj;
-    item_tile(d, w.tile, ti, tj);
-    const int nkb = d.np * d.kdim / kTcKCols;  // feature blocks x K blocks per block
-    for (int kb = 0; kb < nkb; ++kb, ++gkb) {
-      const int s = ps;
-      if (!tc_wait(&sh.empty_bar[s], pph ^ 1u, sh.abort_flag, limit)) {
-        *sh.abort_flag = 1;
-        break;
-      }
-      uint8_t *a = sh.stages + s * kTcStageBytes;
-      mbar_arrive_expect_tx(&sh.full_bar[s], kTcStageBytes);
-      tma_load_3d(a, &d.map, &sh.full_bar[s], 0, ti * kTile, kb);
-      tma_load_3d(a + kTcTileBytes, &d.map, &sh.full_bar[s], 0, tj * kTile, kb);
-      issued = gkb + 1;
-      if (++ps == sh.nst) {
-        ps = 0;
-        pph ^= 1u;
-      }
-    }
+    if (!tc_produce_item(sh, descs[w.aln], w.tile, gkb, issued, ps, pph, limit)) break;
   }
   return issued;
 }
 
-// The MMA issuer (a whole warp): the same items as the producer.  Lane 0 waits,
-// the result is broadcast; one elected lane issues each MMA and commit.
-// Descriptors are the stage base descriptors plus constant offsets: the 14-bit
-// start-address field (16-byte units) of a shared address below 228 KB cannot
-// carry out.  Ends after every MMA it issued has completed.
+// The MMA issuer's part of one item (the whole warp): waits until the
+// epilogue has read the previous item's accumulators (titer: items so far),
+// issues every K block into the accumulators (DNA blocks v, r, t, u -> V, R,
+// T, T; protein blocks v, rank 0, .. -> V, M, M, ...) and commits to acc_full.
+// ring / ring_ph: the stage of the next K block and the parity of its fill.
+// Lane 0 waits, the result is broadcast; one elected lane issues each MMA and
+// commit.  Descriptors are the stage base descriptors plus constant offsets:
+// the 14-bit start-address field (16-byte units) of a shared address below
+// 228 KB cannot carry out.  False (abort flag set) when a wait ran out.
+__device__ __forceinline__ bool tc_issue_item(const TcShared &sh, uint32_t tmem, uint64_t desc0,
+                                              const AlnDesc &d, uint32_t titer, int &ring,
+                                              uint32_t &ring_ph, uint64_t limit) {
+  const int lane = threadIdx.x & 31;
+  constexpr uint64_t kStageStep = kTcStageBytes >> 4, kBStep = kTcTileBytes >> 4;
+  const int nkb = d.np * d.kdim / kTcKCols;
+  const int seg = d.kdim / kTcKCols;  // K blocks per feature block
+  const bool prot = d.kind == KIND_PROT_TC;
+  // The epilogue of the previous item must have read the accumulators.
+  int ok = 1;
+  if (lane == 0) ok = tc_wait(sh.tmem_empty, (titer & 1) ^ 1, sh.abort_flag, limit);
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (!ok) {
+    if (lane == 0) *sh.abort_flag = 1;
+    return false;
+  }
+  tc_fence_after();
+  // Per K block: every lane tests the stage's full barrier (one warp vote
+  // when it is already complete, the common case; otherwise lane 0 waits,
+  // bounded); the stage, its parity, the accumulator and whether the block
+  // starts that accumulator's sum follow from counters.  Measured: the
+  // per-block division, modulo and broadcast cost 15 % of the kernel.
+  const int last_acc = prot ? 1 : 2;
+  int kin = 0, blk = 0;  // K block within its feature block, feature block
+  for (int kb = 0; kb < nkb; ++kb) {
+    const int s = ring;
+    if (!__all_sync(0xffffffffu, mbar_try_wait(&sh.full_bar[s], ring_ph))) {
+      if (lane == 0) ok = tc_wait(&sh.full_bar[s], ring_ph, sh.abort_flag, limit);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+    }
+    tc_fence_after();
+    const int acc = blk < last_acc ? blk : last_acc;
+    const uint32_t first = (kin == 0) && (blk <= last_acc);
+    if (++kin == seg) {
+      kin = 0;
+      ++blk;
+    }
+    if (++ring == sh.nst) {
+      ring = 0;
+      ring_ph ^= 1u;
+    }
+    const uint64_t adesc = desc0 + (uint64_t)s * kStageStep;
+    const uint64_t bdesc = adesc + kBStep;
+    const uint32_t dt = tmem + (uint32_t)(acc * kTile);
+    // 32 bytes = 64 columns per MMA, four per 128-byte stage.
+    tc_mma_fp4_elect(dt, adesc, bdesc, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, first ^ 1u);
+    tc_mma_fp4_elect(dt, adesc + 2, bdesc + 2, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+    tc_mma_fp4_elect(dt, adesc + 4, bdesc + 4, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+    tc_mma_fp4_elect(dt, adesc + 6, bdesc + 6, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
+    tc_commit_elect(&sh.empty_bar[s]);
+  }
+  if (!ok) {
+    if (lane == 0) *sh.abort_flag = 1;
+    return false;
+  }
+  tc_commit_elect(sh.acc_full);
+  return true;
+}
+
+// Every MMA the warp issued has completed (before tensor memory is released).
+__device__ __forceinline__ void tc_issue_drain(const TcShared &sh) {
+  tc_commit_elect(sh.drain_bar);
+  if ((threadIdx.x & 31) == 0) mbar_wait_bounded(sh.drain_bar, 0);
+  __syncwarp();
+}
+
+// The MMA issuer (a whole warp): the same items as the producer.  Ends after
+// every MMA it issued has completed.
 __device__ __forceinline__ void tc_issue(const TcShared &sh, uint32_t tmem, const AlnDesc *descs,
                                          const WorkItem *items, int it0, int nitems, int step,
                                          uint64_t limit) {
-  const int lane = threadIdx.x & 31;
   const uint64_t desc0 = smem_desc_sw128(smem_u32(sh.stages));
-  constexpr uint64_t kStageStep = kTcStageBytes >> 4, kBStep = kTcTileBytes >> 4;
   uint32_t titer = 0;
   int ring = 0;           // stage of the ring the next K block is in
   uint32_t ring_ph = 0;   // and the parity of its current fill
@@ -379,64 +460,9 @@ __device__ __forceinline__ void tc_issue(const TcShared &sh, uint32_t tmem, cons
     go = __shfl_sync(0xffffffffu, go, 0);
     if (!go) break;
     const WorkItem w = item_at(descs, items, it);
-    const AlnDesc &d = descs[w.aln];
-    const int nkb = d.np * d.kdim / kTcKCols;
-    const int seg = d.kdim / kTcKCols;  // K blocks per feature block
-    const bool prot = d.kind == KIND_PROT_TC;
-    // The epilogue of the previous item must have read the accumulators.
-    int ok = 1;
-    if (lane == 0) ok = tc_wait(sh.tmem_empty, (titer & 1) ^ 1, sh.abort_flag, limit);
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (!ok) {
-      if (lane == 0) *sh.abort_flag = 1;
-      break;
-    }
-    tc_fence_after();
-    // Per K block: every lane tests the stage's full barrier (one warp vote
-    // when it is already complete, the common case; otherwise lane 0 waits,
-    // bounded); the stage, its parity, the accumulator and whether the block
-    // starts that accumulator's sum follow from counters.  Measured: the
-    // per-block division, modulo and broadcast cost 15 % of the kernel.
-    const int last_acc = prot ? 1 : 2;
-    int kin = 0, blk = 0;  // K block within its feature block, feature block
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = ring;
-      if (!__all_sync(0xffffffffu, mbar_try_wait(&sh.full_bar[s], ring_ph))) {
-        if (lane == 0) ok = tc_wait(&sh.full_bar[s], ring_ph, sh.abort_flag, limit);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) break;
-      }
-      tc_fence_after();
-      const int acc = blk < last_acc ? blk : last_acc;
-      const uint32_t first = (kin == 0) && (blk <= last_acc);
-      if (++kin == seg) {
-        kin = 0;
-        ++blk;
-      }
-      if (++ring == sh.nst) {
-        ring = 0;
-        ring_ph ^= 1u;
-      }
-      const uint64_t adesc = desc0 + (uint64_t)s * kStageStep;
-      const uint64_t bdesc = adesc + kBStep;
-      const uint32_t dt = tmem + (uint32_t)(acc * kTile);
-      // 32 bytes = 64 columns per MMA, four per 128-byte stage.
-      tc_mma_fp4_elect(dt, adesc, bdesc, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, first ^ 1u);
-      tc_mma_fp4_elect(dt, adesc + 2, bdesc + 2, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
-      tc_mma_fp4_elect(dt, adesc + 4, bdesc + 4, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
-      tc_mma_fp4_elect(dt, adesc + 6, bdesc + 6, kIdescFp4, tmem + kTmemSfa, tmem + kTmemSfb, 1u);
-      tc_commit_elect(&sh.empty_bar[s]);
-    }
-    if (!ok) {
-      if (lane == 0) *sh.abort_flag = 1;
-      break;
-    }
-    tc_commit_elect(sh.acc_full);
+    if (!tc_issue_item(sh, tmem, desc0, descs[w.aln], titer, ring, ring_ph, limit)) break;
   }
-  // Every MMA issued has completed before tensor memory is released.
-  tc_commit_elect(sh.drain_bar);
-  if (lane == 0) mbar_wait_bounded(sh.drain_bar, 0);
-  __syncwarp();
+  tc_issue_drain(sh);
 }
 
 // After every role has finished (call from all threads): when a wait ran out,

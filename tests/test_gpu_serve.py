@@ -80,14 +80,16 @@ def test_served_rejects_requests_beyond_budget():
     server.close()
 
 
-def test_served_beyond_the_staging_area(ctx):
-    # 36 requests of 9 MB each (324 MB) submitted at once: more than the
-    # server's 256 MiB page-locked staging area, so the later ones are staged in
-    # pageable memory until extents are freed.  Every result equals the plain call.
+def test_served_beyond_the_staging_area(ctx, monkeypatch):
+    # 36 requests of 9 MB each (324 MB) submitted at once: more than a 256 MiB
+    # page-locked staging area (RNJ_SERVER_STAGING_MB; 1 GiB by default), so the
+    # later ones are staged in pageable memory until extents are freed.  Every
+    # result equals the plain call.
     from rapidnj_b200 import api, synth
     reqs = [(synth.tree_dna(1500, 6000, seed=100 + k, mean_branch=0.05), 0, "kim")
             if k % 2 == 0 else (synth.tree_protein(1500, 6000, seed=100 + k), 1, "kim")
             for k in range(36)]
+    monkeypatch.setenv("RNJ_SERVER_STAGING_MB", "256")
     server = api.Server(0, max_batch=6)
     ids = [server.submit(s, m, t) for s, t, m in reqs]
     for k, (seqs, typ, model) in enumerate(reqs):
@@ -101,4 +103,50 @@ def test_served_beyond_the_staging_area(ctx):
         ref.close()
         aln.close()
         assert np.array_equal(got.view(np.int32), want.view(np.int32))
+    server.close()
+
+
+def test_live_list_mixed_edges_and_generations(ctx):
+    # Requests that join a running live kernel: tiny ones (n = 1, 2, L = 1),
+    # saturated i.i.d. DNA under JC (the last tile's CTA applies the fix-up),
+    # tree DNA and protein under Kimura, an 80-residue alphabet and -f DNA
+    # (plain calls on the server's stream), in two waves so that the work
+    # list starts a new generation of slots and items in between.  Each
+    # result equals the plain call bit for bit, with the same maximum.
+    from rapidnj_b200 import api, synth
+    rng = np.random.default_rng(3)
+    big = np.frombuffer(bytes(range(40, 120)), np.uint8)
+    wave = []
+    for k in range(40):
+        kind = k % 8
+        n = int(rng.integers(2, 900)) if kind else int(rng.integers(1, 4))
+        L = int(rng.integers(1, 2500)) if kind != 1 else 1
+        if kind in (0, 1, 2):
+            wave.append((synth.iid_dna(max(n, 1), max(L, 1), seed=k), 0, "jc", True))
+        elif kind == 3:
+            wave.append((synth.tree_protein(n, L, seed=k), 1, "kim", True))
+        elif kind == 4:
+            s = big[rng.integers(0, big.size, (max(n, 2), 300))]
+            wave.append((s, 1, "kim", True))
+        elif kind == 5:
+            wave.append((synth.tree_dna(n, L, seed=k, mean_branch=0.1), 0, "kim", False))
+        else:
+            wave.append((synth.tree_dna(n, L, seed=k, mean_branch=0.1), 0, "kim", True))
+    server = api.Server(0, max_batch=16)
+    for rnd in range(2):
+        ids = [server.submit(s, m, t, fastdist=f) for s, t, m, f in wave]
+        for rid, (seqs, typ, model, fast) in zip(ids, wave):
+            server.wait(rid)
+            m, lat = server.result(ctx, rid)
+            got, gmax = m.to_numpy(), m.max
+            m.close()
+            aln = ctx.alignment(seqs, typ, fastdist=fast)
+            ref = ctx.distance(aln, model)
+            want, wmax = ref.to_numpy(), ref.max
+            ref.close()
+            aln.close()
+            assert np.array_equal(got.view(np.int32), want.view(np.int32)) and gmax == wmax
+            assert lat > 0
+    st = server.stats()
+    assert st["completed"] == 2 * len(wave) and st["bytes_in_use"] == 0
     server.close()
