@@ -212,21 +212,29 @@ __device__ __forceinline__ float ratio_f32(unsigned long long num, unsigned long
   return __fdiv_rn(__ull2float_rn(num), __ull2float_rn(den));
 }
 
+// The PTX fast reciprocal of a float (rcp.approx: within a couple of ulps of
+// 1 / x; one instruction, where a correctly rounded reciprocal takes several).
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // 1 / n for an integer 1 <= n < 2^24, within 2^-52.9 (relative), by Newton-
-// Raphson iteration for the reciprocal, r <- r + r (1 - n r), from the float
-// reciprocal of n.  With r = (1 / n)(1 - e), one step gives (1 / n)(1 - e^2)
-// before rounding:
-//   r0 = __frcp_rn(n)        |e0| <= 2^-24 (a correctly rounded float)
+// Raphson iteration for the reciprocal, r <- r + r (1 - n r), from the fast
+// float reciprocal of n.  With r = (1 / n)(1 - e), one step gives
+// (1 / n)(1 - e^2) before rounding:
+//   r0 = rcp_approx(n)       |e0| <= 2^-21 (a float within 4 ulps of 1 / n)
 //   t0 = fma(-n, r0, 1) = e0 exactly (n r0 has at most 48 significant bits and
-//        lies within 2^-24 of 1, so the product and the difference are exact)
-//   r1 = fma(r0, t0, r0)     |e1| <= 2^-48 + 2^-53
+//        lies within 2^-21 of 1, so the product and the difference are exact)
+//   r1 = fma(r0, t0, r0)     |e1| <= 2^-42 + 2^-53
 //   t1 = fma(-n, r1, 1)      = e1 (1 + 2^-53 at most)
 //   r2 = fma(r1, t1, r1)     |e2| <= e1^2 + 2^-53 + ... < 2^-52.9
 // which is well inside the 2^-51 that ratio_f32 needs.  n = 0 gives a NaN
 // (callers treat valid == 0 before any quotient).
 __device__ __forceinline__ double recip_nr(uint32_t n) {
   const double dn = (double)n;
-  const double r0 = (double)__frcp_rn((float)n);
+  const double r0 = (double)rcp_approx((float)n);
   const double r1 = __fma_rn(r0, __fma_rn(-dn, r0, 1.0), r0);
   return __fma_rn(r1, __fma_rn(-dn, r1, 1.0), r1);
 }
@@ -358,7 +366,7 @@ __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n
   const uint32_t nn = n == 0 ? 1u : n;
   const double dn = u32_to_double(nn);
   const float fn = __fsub_rn(__uint_as_float(0x4B000000u | nn), 8388608.0f);
-  const double r0 = (double)__frcp_rn(fn);
+  const double r0 = (double)rcp_approx(fn);
   const double r1 = __fma_rn(r0, __fma_rn(-dn, r0, 1.0), r0);
   const double rn = __fma_rn(r1, __fma_rn(-dn, r1, 1.0), r1);
   const double ts = round_to_float_bits(__dmul_rn(u32_to_double(P), rn));

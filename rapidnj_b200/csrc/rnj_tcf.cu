@@ -381,9 +381,10 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
                     const int *__restrict__ nitems_ptr, int nitems_direct, int item0, int count,
                     int nst) {
   extern __shared__ uint8_t smem_raw[];
-  // A work list's first descriptor may ask for a shallower ring than the
-  // launch's shared memory holds (a batch graph is captured once).
-  if (descs[0].stages > 0) nst = max(kTcMinStages, min(nst, descs[0].stages));
+  // A batch's first descriptor may ask for a shallower ring than the launch's
+  // shared memory holds (its graph is captured once; batches launch kFusedAny).
+  if constexpr (V == kFusedAny)
+    if (descs[0].stages > 0) nst = max(kTcMinStages, min(nst, descs[0].stages));
   const TcShared sh = tc_shared(smem_raw, nst, kTcfTableBytes);
   double2 *const tab = reinterpret_cast<double2 *>(tc_extra(sh));
   const uint64_t limit = wait_limit_ns((uint32_t)descs[0].wait_us);

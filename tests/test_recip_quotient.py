@@ -1,8 +1,8 @@
 """The quotients of the device transforms by the valid count (rnj_device.cuh,
 recip_nr and ratio_f32): for integers 0 <= num <= den < 2^24, rounding
-num * r to float, with r the Newton-Raphson reciprocal of den (a correctly
-rounded float seed, then two steps r + r (1 - den r) as fused multiply-adds in
-double), gives the float quotient num / den that the reference computes with a
+num * r to float, with r the Newton-Raphson reciprocal of den (a float seed
+within four ulps of 1 / den, then two steps r + r (1 - den r) as fused
+multiply-adds in double), gives the float quotient num / den that the reference computes with a
 float division (JCdistance.cpp:171-176, KimuraDistance.cpp:324) and with a
 double division rounded to float (KimuraDistance.cpp:341-342).
 
@@ -21,8 +21,19 @@ def fma(a: float, b: float, c: float) -> float:
     return float(Fraction(a) * Fraction(b) + Fraction(c))
 
 
-def recip_nr(n: int) -> float:
-    r0 = float(np.float32(1.0) / np.float32(n))  # __frcp_rn: correctly rounded
+def seed(n: int, ulps: int = 0) -> float:
+    """A float reciprocal seed: the correctly rounded 1/n moved by `ulps` floats
+    (the device seeds with the PTX fast reciprocal, within a couple of ulps;
+    the proof needs a seed within 2^-21, four ulps)."""
+    r = np.float32(1.0) / np.float32(n)
+    step = np.inf if ulps > 0 else -np.inf
+    for _ in range(abs(ulps)):
+        r = np.nextafter(r, np.float32(step))
+    return float(r)
+
+
+def recip_nr(n: int, ulps: int = 0) -> float:
+    r0 = seed(n, ulps)
     r1 = fma(r0, fma(-float(n), r0, 1.0), r0)
     return fma(r1, fma(-float(n), r1, 1.0), r1)
 
@@ -47,6 +58,15 @@ def test_reciprocal_error_bound_for_16_bit_counts():
     assert worst < Fraction(1, 2 ** 52)
     rel = np.abs(r * dens - 1.0)
     assert rel.max() <= 2.0 ** -51
+
+
+def test_reciprocal_error_bound_from_any_seed_within_four_ulps():
+    rng = np.random.default_rng(5)
+    dens = np.concatenate([np.arange(1, 300), rng.integers(300, 1 << 24, 400)])
+    for d in dens:
+        for u in (-4, -3, -2, -1, 1, 2, 3, 4):
+            x = recip_nr(int(d), u)
+            assert abs(Fraction(x) * int(d) - 1) < Fraction(1, 2 ** 52)
 
 
 def test_quotients_exhaustive_small_and_sampled_16_bit():
