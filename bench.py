@@ -513,10 +513,21 @@ def run_served(args, local_rank: int = 0, rate: float = 1000.0, seconds: float =
 
     # warm-up
     drive(pool_size, None)
+    # each request alone (submitted after the previous one completed): the
+    # latency it has without other requests in the server
+    alone = []
+    for seqs, typ, model in pool:
+        time.sleep(0.002)
+        rid = server.submit(seqs, model, typ)
+        server.wait(rid)
+        m, ms = server.result(ctx, rid)
+        m.close()
+        alone.append(ms)
     rng = np.random.default_rng(1)
     count = int(rate * seconds)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
     lat, work, wall = drive(count, arrivals)
+    slowdown = np.array([lat[k] / alone[k % pool_size] for k in range(count)])
     sat_lat, sat_work, sat_wall = drive(4 * pool_size, None)
     # plain per-request calls on the same requests
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -536,6 +547,13 @@ def run_served(args, local_rank: int = 0, rate: float = 1000.0, seconds: float =
     lat = np.array(lat)
     return {"rate_req_per_s": rate, "requests": count,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
+            "alone_p50_ms": float(np.percentile(alone, 50)),
+            "alone_p99_ms": float(np.percentile(np.array(alone)[[k % pool_size
+                                                                for k in range(count)]], 99)),
+            "slowdown_p50": float(np.percentile(slowdown, 50)),
+            "slowdown_p99": float(np.percentile(slowdown, 99)),
+            "slowdown_note": "a request's latency in the mix / its latency submitted alone",
             "mean_ms": float(lat.mean()), "throughput": work / wall,
             "saturation_throughput": sat_work / sat_wall,
             "saturation_p50_ms": float(np.percentile(sat_lat, 50)),

@@ -276,10 +276,8 @@ void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *k
   *kind = rank <= 4 ? KIND_MISM2 : (rank <= 32 ? KIND_MISM5 : KIND_MISM7);
 }
 
-// Allocation, pack kernel and TMA map of an alignment whose LUT is known; no
-// synchronisation.
-int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
-                  int flags, int kind, const uint8_t lut[256], rnj_aln **out);
+// (pack_prepared, declared in rnj_objects.h: allocation, pack kernel and TMA
+// map of an alignment whose LUT is known; no synchronisation.)
 
 namespace {
 
@@ -309,7 +307,9 @@ int pack_from_device_chars(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, s
 
 }  // namespace
 
-size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind, const uint8_t *lut) {
+size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind, const uint8_t *lut,
+                     bool tuned_kernel) {
+  const bool tc_choice = !tuned_kernel || tune_lookup(n, L, type, flags).dna_kernel == 0;
   p.n = n;
   p.L = L;
   p.type = type;
@@ -318,8 +318,7 @@ size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind, con
   p.W = (L + 31) / 32;
   p.Wp = std::max(kKW, (p.W + kKW - 1) / kKW * kKW);
   p.Np = std::max(kTile, (n + kTile - 1) / kTile * kTile);
-  if (kind == KIND_DNA && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns &&
-      tune_lookup(n, L, type, flags).dna_kernel == 0) {
+  if (kind == KIND_DNA && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns && tc_choice) {
     // FP4 feature rows for the tensor-core kernel instead of bit planes.
     p.kind = KIND_DNA_TC;
     p.NP = 0;
@@ -327,8 +326,7 @@ size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind, con
     p.Lk = std::max(256, (L + 255) / 256 * 256);
     return (size_t)p.Np * 4 * p.Lk / 2;
   }
-  if (type == RNJ_PROTEIN && lut && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns &&
-      tune_lookup(n, L, type, flags).dna_kernel == 0) {
+  if (type == RNJ_PROTEIN && lut && !(flags & RNJ_POPCOUNT) && L <= kMaxTcColumns && tc_choice) {
     // Protein on the tensor cores: a valid block and one one-hot block per
     // residue rank present, when there are at most kMaxTcRanks ranks.
     int ranks = 0;
@@ -347,11 +345,11 @@ size_t packed_layout(Packed &p, int n, int L, int type, int flags, int kind, con
 }
 
 int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
-                  int flags, int kind, const uint8_t lut[256], rnj_aln **out) {
+                  int flags, int kind, const uint8_t lut[256], rnj_aln **out, bool tuned_kernel) {
   rnj_aln *a = new rnj_aln();
   a->ctx = ctx;
   Packed &p = a->p;
-  const size_t pbytes = packed_layout(p, n, L, type, flags, kind, lut);
+  const size_t pbytes = packed_layout(p, n, L, type, flags, kind, lut, tuned_kernel);
   if (is_tc_kind(p.kind)) {
     const size_t fbytes = pbytes;
     cudaError_t e = cudaMallocAsync((void **)&p.feat, fbytes, ctx->stream);

@@ -280,7 +280,7 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
     rnj_aln *a = new rnj_aln();
     a->ctx = ctx;
     a->owns_mem = false;
-    const size_t bytes = packed_layout(a->p, n[k], L[k], type[k], flags, kind, lut);
+    const size_t bytes = packed_layout(a->p, n[k], L[k], type[k], flags, kind, lut, false);
     alns[k] = a;
     offs[k] = total;
     total += (bytes + 255) / 256 * 256;

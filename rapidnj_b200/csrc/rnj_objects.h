@@ -99,13 +99,18 @@ struct rnj_mat {
 // (protein needs its byte-presence mask), then allocation + pack kernel + map.
 void lut_for(int type, int flags, const uint32_t *mask, uint8_t lut[256], int *kind);
 int pack_prepared(rnj_ctx *ctx, const uint8_t *d_chars, int n, int L, size_t ld, int type,
-                  int flags, int kind, const uint8_t lut[256], rnj_aln **out);
+                  int flags, int kind, const uint8_t lut[256], rnj_aln **out,
+                  bool tuned_kernel = true);
 // The packed layout of an alignment (kind: from lut_for; a tensor-core layout
 // when DNA or protein takes one) without allocating; returns the bytes of its
 // planes or features.
 // lut (lut_for's table) decides the protein tensor-core layout (its ranks).
+// tuned_kernel: follow the tuner's choice of counting kernel for the bucket
+// (bit planes where they were faster for a single call); false for the work
+// lists of batches and of the server, whose bit-plane kernel has no K split,
+// so that every alignment the tensor cores can take goes to them.
 size_t packed_layout(rnj::Packed &p, int n, int L, int type, int flags, int kind,
-                     const uint8_t *lut);
+                     const uint8_t *lut, bool tuned_kernel = true);
 
 // Helpers of rnj_api.cu shared with the streamed host-to-host path
 // (rnj_stream.cu): grow the scratch words, transform parameters wired to the

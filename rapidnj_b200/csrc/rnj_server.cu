@@ -336,7 +336,7 @@ void prepare_all(rnj_server *s, const std::vector<Request *> &reqs) {
       lut_for(r->type, r->flags, r->type == RNJ_PROTEIN ? s->h_masks + 8 * k : nullptr, lut,
               &kind);
       rc[k] = pack_prepared(ctx, r->d_chars, r->n, r->L, (size_t)std::max(r->L, 1), r->type,
-                            r->flags, kind, lut, &r->aln);
+                            r->flags, kind, lut, &r->aln, false);
       if (rc[k] != RNJ_OK) err[k] = rnj_last_error();
     }
     s->t_pack += ms_since(t0);
