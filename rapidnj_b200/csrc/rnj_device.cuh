@@ -129,31 +129,37 @@ __device__ __forceinline__ double ln_table(double x) {
   return __fma_rn(dk, kLn2Hi, __dadd_rn(__fma_rn(dk, kLn2Lo, lnF), p));
 }
 
-// The same logarithm with the table read from `tab` (a copy of c_log_tab in
-// shared memory: a warp's 32 random entries are one shared-memory request
-// instead of up to 16 L1 lines) and k turned into a double by the 2^52 bias (an
-// integer add and a double subtraction, both exact, instead of a conversion):
-// the arithmetic, and so the result and its error bound, are ln_table's.
-__device__ __forceinline__ double ln_table_k(double x, const double2 *tab) {
+// -ln(x) / 4, the K2P fast path's logarithm, with the table read from `tab`
+// (a copy of c_log_tab in shared memory, each entry scaled by -1/4: a warp's
+// 32 random entries are one shared-memory request instead of up to 16 L1
+// lines) and k turned into a double by the 2^52 bias (an integer add and a
+// double subtraction, both exact, instead of a conversion).  The arithmetic
+// is ln_table's with every operand scaled by a power of two: r' = -r / 4 (the
+// table's -1/(4F)), Horner coefficients c_k (-4)^k, so the k-th Horner value
+// is (-4)^k times ln_table's and the product with r' is -1/4 of its; ln F and
+// ln 2 scaled by -1/4.  Rounding to nearest commutes with a power-of-two
+// scale (no operand comes near overflow or underflow), so the result is
+// exactly -ln_table(x) / 4, with ln_table's error bound divided by 4.
+constexpr double kNegQuarterLn2Hi = -0.25 * kLn2Hi, kNegQuarterLn2Lo = -0.25 * kLn2Lo;
+__device__ __forceinline__ double neg_quarter_ln_table_k(double x, const double2 *tabq) {
   const long long bits = __double_as_longlong(x);
   const int ebits = (int)((bits >> 52) & 0x7FF);  // k + 1023
   const int j = (int)((bits >> 45) & 127);
   const double m = __longlong_as_double((bits & 0x000FFFFFFFFFFFFFLL) | 0x3FF0000000000000LL);
   const double F = __longlong_as_double(0x3FF0000000000000LL | ((long long)j << 45));
-  const double2 e = tab[j];  // {ln F, 1 / F}
+  const double2 e = tabq[j];  // {-ln F / 4, -1 / (4 F)}
   const double r = __dmul_rn(__dsub_rn(m, F), e.y);
-  const double lnF = e.x;
-  double p = -1.0 / 6.0;
-  p = __fma_rn(p, r, 0.2);
-  p = __fma_rn(p, r, -0.25);
-  p = __fma_rn(p, r, 1.0 / 3.0);
-  p = __fma_rn(p, r, -0.5);
+  double p = (-1.0 / 6.0) * -1024.0;
+  p = __fma_rn(p, r, 0.2 * 256.0);
+  p = __fma_rn(p, r, -0.25 * -64.0);
+  p = __fma_rn(p, r, (1.0 / 3.0) * 16.0);
+  p = __fma_rn(p, r, -0.5 * -4.0);
   p = __fma_rn(p, r, 1.0);
   p = __dmul_rn(p, r);
   // 2^52 + ebits, exactly, minus 2^52 + 1023: the double k (|k| < 2^11).
   const double dk =
       __dsub_rn(__hiloint2double(0x43300000, ebits), 4503599627370496.0 + 1023.0);
-  return __fma_rn(dk, kLn2Hi, __dadd_rn(__fma_rn(dk, kLn2Lo, lnF), p));
+  return __fma_rn(dk, kNegQuarterLn2Hi, __dadd_rn(__fma_rn(dk, kNegQuarterLn2Lo, e.x), p));
 }
 
 // The double of an integer 0 <= v < 2^32: 2^52 + v has v in its low mantissa
@@ -360,7 +366,8 @@ __device__ __forceinline__ float k2p_decide(uint32_t P, uint32_t Q, uint32_t n, 
 //   * temp1 = (float)a <= 0 exactly when a <= 0: a and b are sums of doubles
 //     of floats in [0, 1] with at most 24 significant bits and exponents above
 //     -17, so a nonzero a or b exceeds 2^-70 in magnitude and its float is not 0;
-//   * ln_table_k for the logarithm (tab: the table in shared memory).
+//   * neg_quarter_ln_table_k for -ln(x) / 4 (tab: the table in shared memory,
+//     scaled by -1/4).
 __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n, bool &slow,
                                               const double2 *tab) {
   const uint32_t nn = n == 0 ? 1u : n;
@@ -371,13 +378,17 @@ __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n
   const double rn = __fma_rn(r1, __fma_rn(-dn, r1, 1.0), r1);
   const double ts = round_to_float_bits(__dmul_rn(u32_to_double(P), rn));
   const double tv = round_to_float_bits(__dmul_rn(u32_to_double(Q), rn));
-  const double a = __dsub_rn(__dsub_rn(1.0, __dmul_rn(2.0, ts)), tv);
-  const double b = __dsub_rn(1.0, __dmul_rn(2.0, tv));
+  // fl(1 - 2 ts) as one fused multiply-add: 2 ts is exact, so both forms are
+  // the exact 1 - 2 ts rounded once (the reference's double arithmetic).
+  const double a = __dsub_rn(__fma_rn(-2.0, ts, 1.0), tv);
+  const double b = __fma_rn(-2.0, tv, 1.0);
   const bool sat = (n == 0) | (a <= 0.0) | (b <= 0.0);
   const bool same = (P | Q) == 0;
   const double x = sat ? 1.0 : __dmul_rn(__dmul_rn(a, a), b);
-  const double dd = __dmul_rn(-0.25, ln_table_k(x, tab));
-  const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
+  const double dd = neg_quarter_ln_table_k(x, tab);  // -ln(x) / 4, exactly as scaled
+  // eps = 2^-49 (1 + 4 dd), one fused multiply-add (rounded once, as close to
+  // the bound as the three-operation form)
+  const double eps = __fma_rn(0x1p-47, dd, 0x1p-49);
   const float lo = __double2float_rn(__dsub_rn(dd, eps));
   const float hi = __double2float_rn(__dadd_rn(dd, eps));
   slow = !sat && !same && (__float_as_int(lo) != __float_as_int(hi));

@@ -52,7 +52,8 @@ static_assert(128 * kTcfRegsLow + 512 * kTcfRegsHigh <= kTcfThreads * kTcfRegsLa
               "the register split fits the launch's registers");
 // A ring of up to six stages (a seventh stage's 32 KB would leave no room; six
 // is the default, the tuner may choose fewer) and the logarithm table
-// (128 x {ln F, 1 / F}) after the barrier block.
+// (128 x {-ln F / 4, -1 / (4 F)}, the scaled table of neg_quarter_ln_table_k)
+// after the barrier block.
 constexpr int kTcfStages = 6;
 constexpr size_t kTcfTableBytes = 128 * 2 * sizeof(double);
 constexpr size_t kTcfSmemBytes = tc_smem_bytes(kTcfStages, kTcfTableBytes);
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
   if (it0 >= nitems) return;  // no item for this CTA (before any setup)
 
   for (int e = tid; e < 128; e += kTcfThreads)
-    tab[e] = make_double2(c_log_tab[e][0], c_log_tab[e][1]);
+    tab[e] = make_double2(-0.25 * c_log_tab[e][0], -0.25 * c_log_tab[e][1]);
   // tmem_empty: one arrival per epilogue warp; the scale factors by warps 0 .. 7
   const uint32_t tmem = tc_setup(sh, kTcfEpiWarps, 0, kTcfMmaWarp);
   uint32_t issued = 0;
@@ -577,7 +578,7 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   for (int e = tid; e < 128; e += kTcfThreads)
-    tab[e] = make_double2(c_log_tab[e][0], c_log_tab[e][1]);
+    tab[e] = make_double2(-0.25 * c_log_tab[e][0], -0.25 * c_log_tab[e][1]);
   if (tid == 0) {
     for (int k = 0; k < 2; ++k) {
       mbar_init(&lr->full[k], 1);

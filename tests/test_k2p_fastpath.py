@@ -59,7 +59,8 @@ def fast_k2p(a, b):
     with np.errstate(divide="ignore", invalid="ignore"):
         x = (a * a) * b
         dd = -0.25 * ln_table(x)
-        eps = 2.0 ** -49 * (1.0 + 4.0 * dd)
+        # fma(2^-47, dd, 2^-49): the product is exact, the sum rounded once
+        eps = dd * 2.0 ** -47 + 2.0 ** -49
         lo = (dd - eps).astype(np.float32)
         hi = (dd + eps).astype(np.float32)
     return lo.view(np.int32) == hi.view(np.int32), lo
