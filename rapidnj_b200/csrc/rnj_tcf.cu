@@ -302,7 +302,10 @@ __device__ __forceinline__ bool fused_tile(const TcShared &sh, uint32_t tmem, co
       !tc_wait(sh.acc_full, titer & 1, sh.abort_flag, limit))
     return false;
   tc_fence_after();
-  const bool prot = d.kind == KIND_PROT_TC;
+  // protein counts (V - M) or DNA (ts, tv): known at compile time for the
+  // single-model variants (K2P is DNA, protein Kimura is protein)
+  const bool prot = V == kFusedK2p ? false
+                                   : (V == kFusedProtein ? true : d.kind == KIND_PROT_TC);
   // Accumulators -> integer counts (DNA: transitions, transversions, valid;
   // protein: mismatches = V - M, 0, valid), 16 columns at a time, 16 bits
   // each (the fused form takes L < 65536): pq[k] = ts | tv << 16, and the

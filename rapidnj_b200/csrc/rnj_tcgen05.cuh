@@ -132,13 +132,17 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
 constexpr uint32_t kIdescFp4 = (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) | (1u << 23) |
                                ((uint32_t)(kTile >> 4) << 24);
 
-// A bounded wait (limit_ns) that also gives up early once another role has aborted.
+// A bounded wait (limit_ns) that also gives up early once another role has
+// aborted.  Between tests the thread sleeps until the phase completes, for at
+// most kTcWaitHintNs at a time (the limit and the abort flag are checked every
+// 256 tests, at most about 2.6 ms apart).
+constexpr uint32_t kTcWaitHintNs = 10000;
 __device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
                                         uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 0; it < kWaitIterCap; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_hint(bar, parity, kTcWaitHintNs)) return true;
     if ((it & 255u) == 255u) {
       if (*abort_flag) return false;
       if (global_timer_ns() - t0 > limit_ns) break;
