@@ -327,11 +327,13 @@ __device__ __forceinline__ bool fused_tile(const TcShared &sh, uint32_t tmem, co
     for (int k = 0; k < 16; ++k) {
       const float fv = __uint_as_float(av[k]), fr = __uint_as_float(ar[k]);
       const float ft = __uint_as_float(at[k]);
-      const float fp = prot ? __fsub_rn(fv, fr)
-                            : __fmul_rn(__fsub_rn(__fadd_rn(fv, fr), ft), 0.25f);
-      const float fq = prot ? 0.0f : __fmul_rn(__fsub_rn(fv, fr), 0.5f);
-      const uint32_t bp = __float_as_uint(__fadd_rn(fp, 8388608.0f));
-      const uint32_t bq = __float_as_uint(__fadd_rn(fq, 8388608.0f));
+      // DNA: 4P = V + R - T and 2Q = V - R are exact integers, so the scale and
+      // the bias fuse into one multiply-add with the same (exact) result.
+      const uint32_t bp = __float_as_uint(
+          prot ? __fadd_rn(__fsub_rn(fv, fr), 8388608.0f)
+               : __fmaf_rn(__fsub_rn(__fadd_rn(fv, fr), ft), 0.25f, 8388608.0f));
+      const uint32_t bq = __float_as_uint(
+          prot ? 8388608.0f : __fmaf_rn(__fsub_rn(fv, fr), 0.5f, 8388608.0f));
       const uint32_t bv = __float_as_uint(__fadd_rn(fv, 8388608.0f));
       pq[16 * h + k] = __byte_perm(bp, bq, 0x5410);  // P | Q << 16
       if (k & 1) pv[8 * h + (k >> 1)] = __byte_perm(pv[8 * h + (k >> 1)], bv, 0x5410);
