@@ -177,6 +177,18 @@ int rnj_distance_into(rnj_ctx *ctx, rnj_aln *aln, int model, float *d_out, size_
  * RNJ_FULL_ROWS; every other entry is set to zero).  The valid count is the
  * correct one; RNJ_COMPAT_PROTEIN_WRAP only changes distances. */
 int rnj_counts_into(rnj_ctx *ctx, rnj_aln *aln, unsigned int *d_counts);
+/* The distance matrix in double precision into d_out (device, n rows of stride
+ * ld doubles): each pair's value is the reference's double expression before
+ * its cast to distType (JCdistance.cpp:171-183, KimuraDistance.cpp:322-349),
+ * evaluated in the same order with CUDA's double log; then the post-process
+ * in double (KimuraDistance.cpp:366-395): saturated pairs (-1) become twice
+ * the maximum of the doubles, the lower triangle mirrors the upper (full rows
+ * with RNJ_FULL_ROWS), the diagonal is 0.  max_out (may be NULL) receives that
+ * maximum.  Synchronous.  Scratch: the n x n x 3 counts (12 n^2 bytes), freed
+ * before the call returns.  No counterpart in the reference, whose matrix is
+ * float; (float) of each value is the reference's entry. */
+int rnj_distance_f64(rnj_ctx *ctx, rnj_aln *aln, int model, double *d_out, size_t ld,
+                     double *max_out);
 
 int rnj_mat_info(rnj_mat *mat, int *n, float *max_distance);
 int rnj_mat_device_ptr(rnj_mat *mat, float **d_ptr, size_t *ld);

@@ -89,6 +89,15 @@ def lib():
         L.orc_protein_fast_valid.restype = ctypes.c_uint64
         L.orc_pam_value.argtypes = [ctypes.c_int]
         L.orc_pam_value.restype = ctypes.c_int
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        L.orc_matrix_d.argtypes = [u32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, f64p]
+        L.orc_matrix_d.restype = ctypes.c_double
+        for name in ("orc_jc_d", "orc_k2p_d", "orc_kimura_protein_d"):
+            getattr(L, name).restype = ctypes.c_double
+        L.orc_jc_d.argtypes = [ctypes.c_uint64] * 3 + [ctypes.c_int]
+        L.orc_k2p_d.argtypes = [ctypes.c_uint64] * 3
+        L.orc_kimura_protein_d.argtypes = [ctypes.c_uint64] * 2
         _lib = L
     return _lib
 
@@ -132,6 +141,17 @@ def matrix(cnt: np.ndarray, L: int, type_: int, model: int, naive: bool = False,
     fn = lib().orc_matrix_full if full else lib().orc_matrix
     mx = fn(np.ascontiguousarray(cnt, dtype=np.uint32).reshape(-1), n, L, type_, model,
             int(naive), int(compat_wrap), out.reshape(-1))
+    return out, float(mx)
+
+
+def matrix_f64(cnt: np.ndarray, L: int, type_: int, model: int, naive: bool = False,
+               compat_wrap: bool = False, full: bool = False):
+    """The double matrix (each pair's value before the reference's float cast,
+    post-processed in double) and its maximum from counts (orc_matrix_d)."""
+    n = cnt.shape[0]
+    out = np.zeros((n, n), dtype=np.float64)
+    mx = lib().orc_matrix_d(np.ascontiguousarray(cnt, dtype=np.uint32).reshape(-1), n, L, type_,
+                            model, int(naive), int(compat_wrap), int(full), out.reshape(-1))
     return out, float(mx)
 
 

@@ -234,6 +234,70 @@ float orc_distance(const uint32_t c[3], int L, int type, int model, int naive,
   return orc_k2p(c[0], c[1], valid);
 }
 
+/* The same three transforms returning the double each reference expression
+ * has before its (float) cast (the value of a saturated pair stays -1). */
+double orc_jc_d(uint64_t c0, uint64_t c1, uint64_t valid, int type) {
+  double alpha = (type == ORC_PROTEIN) ? 20.0 : 4.0;
+  long total = (long)(c0 + c1);
+  float distance;
+  if (valid == 0) distance = 0;
+  else distance = (float)total / (float)valid;
+  if (distance / ((alpha - 1) / alpha) >= 1.0) return -1.0;
+  return -((alpha - 1) / alpha) * log(1.0 - distance / ((alpha - 1) / alpha));
+}
+
+double orc_k2p_d(uint64_t ts_count, uint64_t tv_count, uint64_t valid) {
+  if (valid == 0) return -1.0;
+  float ts = (float)((double)ts_count / (double)valid);
+  float tv = (float)((double)tv_count / (double)valid);
+  float temp1 = (float)(1.0 - 2.0 * ts - tv);
+  float temp2 = (float)(1.0 - 2.0 * tv);
+  if (temp1 <= 0 || temp2 <= 0) return -1.0;
+  return -0.5 * log(1.0 - 2.0 * ts - tv) - 0.25 * log(1.0 - 2.0 * tv);
+}
+
+double orc_kimura_protein_d(uint64_t mism, uint64_t valid) {
+  long total = (long)mism;
+  float distance = -1.0f;
+  if (valid != 0) distance = ((float)total / (float)valid);
+  if (distance < 0.75) {
+    if (distance > 0.0) return -log(1.0 - distance - (double)(distance * distance) * 0.20);
+    return distance;
+  }
+  if (distance > 0.930) return 10.0;
+  int table_index = (int)((distance * 1000.0) - 750.0);
+  return kDayhoffPam[table_index] / 100.0;
+}
+
+/* The double matrix: raw doubles for i < j (every i != j with full), maximum
+ * over them, -1 -> 2 * max, mirror (unless full), diagonal 0. */
+double orc_matrix_d(const uint32_t *counts, int n, int L, int type, int model, int naive,
+                    int compat_wrap, int full, double *out) {
+  double maxd = 0.0;
+  for (int i = 0; i < n; i++) {
+    for (int j = full ? 0 : i + 1; j < n; j++) {
+      if (i == j) continue;
+      const uint32_t *c = counts + ((size_t)i * n + j) * 3;
+      uint64_t valid = c[2];
+      if (type == ORC_PROTEIN && !naive && compat_wrap) valid = orc_protein_fast_valid(valid, L);
+      double d = model == ORC_JC ? orc_jc_d(c[0], c[1], valid, type)
+                                 : (type == ORC_PROTEIN ? orc_kimura_protein_d(c[0], valid)
+                                                        : orc_k2p_d(c[0], c[1], valid));
+      if (d > maxd) maxd = d;
+      out[(size_t)i * n + j] = d;
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    double *row = out + (size_t)i * n;
+    for (int j = 0; j < n; j++) {
+      if (!full && j < i) row[j] = out[(size_t)j * n + i];
+      if (i == j) row[j] = 0.0;
+      if (row[j] == -1.0) row[j] = maxd * 2;
+    }
+  }
+  return maxd;
+}
+
 /* Raw (pre post-process) distances for i<j plus the running maximum, then the
  * post-process of KimuraDistance.cpp:366-395 / JCdistance.cpp:201-230:
  * mirror, zero diagonal, -1 -> 2*max. */

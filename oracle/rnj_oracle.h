@@ -25,6 +25,11 @@ void orc_counts_rows(const char *seqs, int n, int L, int type, int naive, int fu
 float orc_jc(uint64_t c0, uint64_t c1, uint64_t valid, int type);
 float orc_k2p(uint64_t ts, uint64_t tv, uint64_t valid);
 float orc_kimura_protein(uint64_t mism, uint64_t valid);
+double orc_jc_d(uint64_t c0, uint64_t c1, uint64_t valid, int type);
+double orc_k2p_d(uint64_t ts, uint64_t tv, uint64_t valid);
+double orc_kimura_protein_d(uint64_t mism, uint64_t valid);
+double orc_matrix_d(const uint32_t *counts, int n, int L, int type, int model, int naive,
+                    int compat_wrap, int full, double *out);
 float orc_distance(const uint32_t c[3], int L, int type, int model, int naive, int compat_wrap);
 
 /* Post-processed n*n float matrix from upper-triangle counts; returns the max. */

@@ -96,6 +96,8 @@ SIGNATURES = {
     "rnj_batch_take": (c_int, [c_void_p, c_int, P(c_void_p)]),
     "rnj_batch_size": (c_int, [c_void_p, P(c_int), P(ctypes.c_longlong)]),
     "rnj_batch_tuning": (c_int, [c_void_p, P(c_int), P(c_int)]),
+    "rnj_distance_f64": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_size_t,
+                                 P(ctypes.c_double)]),
     "rnj_batch_clear": (c_int, [c_void_p]),
     "rnj_batch_destroy": (c_int, [c_void_p]),
     "rnj_batch_poll": (c_int, [c_void_p, P(c_int)]),

@@ -196,6 +196,19 @@ class Context:
                                         ctypes.byref(m) if want_max else None))
         return m.value if want_max else None
 
+    def distance_f64(self, aln: Alignment, model, out=None):
+        """rnj_distance_f64: the matrix in double precision (each pair's value is
+        the reference's double before its float cast) into a CUDA float64 tensor
+        (n, >= n), allocated when out is None.  Returns (tensor, max)."""
+        import torch
+        if out is None:
+            out = torch.empty((aln.n, aln.n), dtype=torch.float64, device=f"cuda:{self.device}")
+        m = ctypes.c_double()
+        check(N.lib().rnj_distance_f64(self.handle, aln.handle, MODELS[model],
+                                       ctypes.c_void_p(out.data_ptr()), out.stride(0),
+                                       ctypes.byref(m)))
+        return out, m.value
+
     def distance_rows(self, aln: Alignment, model, on_rows, band_rows: int = 0):
         """The matrix in bands of full rows (rnj_distance_rows), for matrices larger
         than device memory: on_rows(row0, rows) receives each band as a float32
