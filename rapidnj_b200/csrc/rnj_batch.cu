@@ -243,7 +243,7 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
     j.n = n[k];
     j.L = L[k];
     j.unit0 = pres_units;
-    pres_units += (long long)n[k] * ((L[k] + 1023) / 1024);
+    pres_units += (long long)n[k] * ((L[k] + kPresenceSeg - 1) / kPresenceSeg);
     pres.push_back(j);
   }
   const int np = (int)pres.size();
@@ -298,6 +298,10 @@ int rnj_batch_add_many(rnj_batch *b, int count, const void *const *d_chars, cons
       memcpy(j.lut, lut, 256);
       j.unit0 = feat_units;
       feat_units += (long long)a->p.Np * (a->p.Lk / 32);
+      if (feat_units % 256 != 0) {  // Np is a multiple of 128 and Lk of 256
+        for (rnj_aln *x : alns) delete x;
+        return set_error(RNJ_ERR_UNSUPPORTED, "feature pack units not a multiple of 256");
+      }
       feats.push_back(j);
     } else {
       j.W = a->p.Wp;

@@ -172,9 +172,13 @@ cudaError_t launch_pack_chars(const uint8_t *d_chars, size_t ld, const Packed &p
                               const uint8_t lut[256], cudaStream_t s);
 cudaError_t launch_presence(const uint8_t *d_chars, size_t ld, int n, int L,
                             uint32_t *d_mask /*8 words*/, cudaStream_t s);
-// Many alignments in one launch each.  Presence: units = sum of n * ceil(L/1024)
-// (1 KB row segments), 8 mask words per job.  Planes: units = sum of
-// (Np/32) * (Wp/8) pack tiles.  Features (rnj_tc.cu): units = sum of Np * Lk/32.
+// Row segment of a presence-scan work unit (one warp), bytes.
+constexpr int kPresenceSeg = 4096;
+// Many alignments in one launch each.  Presence: units = sum of
+// n * ceil(L / kPresenceSeg) (row segments), 8 mask words per job.  Planes:
+// units = sum of (Np/32) * (Wp/8) pack tiles.  Features (rnj_tc.cu): units =
+// sum of Np * Lk/32, each job's a multiple of 256 (a block's 256 units share a
+// job).
 cudaError_t launch_presence_multi(const PackJob *d_jobs, int njobs, long long units,
                                   uint32_t *d_masks, cudaStream_t s);
 cudaError_t launch_pack_chars_multi(const PackJob *d_jobs, int njobs, long long units,

@@ -144,84 +144,108 @@ __global__ void __launch_bounds__(256) pack_chars_multi_kernel(const PackJob *__
 }
 
 // Byte-presence mask of an alignment (bit c of the 256-bit mask set when byte
-// c occurs), used to rank the residue alphabet on the host.  A warp walks a
-// row, 32 consecutive bytes per step; each lane keeps its own 256-bit mask in
-// registers and the warp merges them before one atomic per word.
-__device__ __forceinline__ void mask_set(uint32_t (&m)[8], uint32_t c) {
-  const uint32_t bit = 1u << (c & 31);
-  switch (c >> 5) {
-    case 0: m[0] |= bit; break;
-    case 1: m[1] |= bit; break;
-    case 2: m[2] |= bit; break;
-    case 3: m[3] |= bit; break;
-    case 4: m[4] |= bit; break;
-    case 5: m[5] |= bit; break;
-    case 6: m[6] |= bit; break;
-    default: m[7] |= bit; break;
+// c occurs), used to rank the residue alphabet on the host.  A warp scans row
+// segments of kPresenceSeg bytes, 16 bytes a lane from 16-byte aligned blocks
+// inside the row (single bytes at the row's unaligned ends, so nothing outside
+// the row is read), and marks each byte in its own 256 flags in shared memory
+// with a plain store of 1 (any number of lanes may mark the same byte).  The
+// flags then become eight mask words, merged into the result with one atomic OR
+// per word.
+constexpr int kPresenceWarps = 8;  // 256 threads
+
+__device__ __forceinline__ void mark_word(uint8_t *flags, uint32_t w) {
+  flags[w & 0xFFu] = 1;
+  flags[(w >> 8) & 0xFFu] = 1;
+  flags[(w >> 16) & 0xFFu] = 1;
+  flags[w >> 24] = 1;
+}
+
+// Marks the bytes p[0 .. len) (one warp, len >= 0).
+__device__ __forceinline__ void mark_span(const uint8_t *__restrict__ p, int len, uint8_t *flags,
+                                          int lane) {
+  const int head = min(len, (int)((16u - (uint32_t)(reinterpret_cast<uintptr_t>(p) & 15u)) & 15u));
+  if (lane < head) flags[p[lane]] = 1;
+  const uint4 *v = reinterpret_cast<const uint4 *>(p + head);
+  const int nv = (len - head) >> 4;
+#pragma unroll 4
+  for (int k = lane; k < nv; k += 32) {
+    const uint4 x = __ldg(v + k);
+    mark_word(flags, x.x);
+    mark_word(flags, x.y);
+    mark_word(flags, x.z);
+    mark_word(flags, x.w);
   }
+  const int tail = head + (nv << 4);
+  if (lane < len - tail) flags[p[tail + lane]] = 1;
+}
+
+// The warp's flags (one byte per byte value, 0 or 1) -> atomic OR into
+// mask[0 .. 8); the flags are cleared.  Lane l reads the flags of bytes 8l ..
+// 8l + 7, which are bits 8(l % 4) .. 8(l % 4) + 7 of mask word l / 4.
+__device__ __forceinline__ void flush_flags(uint8_t *flags, uint32_t *mask, int lane) {
+  __syncwarp();
+  uint2 *f2 = reinterpret_cast<uint2 *>(flags);
+  const uint2 f = f2[lane];
+  uint32_t lo = f.x, hi = f.y;  // a flag in bit 0 of each byte
+  lo = (lo | (lo >> 7)) & 0x00030003u;
+  lo = (lo | (lo >> 14)) & 0xFu;
+  hi = (hi | (hi >> 7)) & 0x00030003u;
+  hi = (hi | (hi >> 14)) & 0xFu;
+  uint32_t v = (lo | (hi << 4)) << ((lane & 3) * 8);
+  v |= __shfl_xor_sync(0xffffffffu, v, 1);
+  v |= __shfl_xor_sync(0xffffffffu, v, 2);
+  if ((lane & 3) == 0 && v) atomicOr(&mask[lane >> 2], v);
+  f2[lane] = make_uint2(0u, 0u);
+  __syncwarp();
 }
 
 __global__ void __launch_bounds__(256) presence_kernel(const uint8_t *__restrict__ chars,
                                                        size_t ld, int n, int L,
                                                        uint32_t *__restrict__ mask) {
-  uint32_t m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  __shared__ __align__(16) uint8_t s_flags[kPresenceWarps][256];
   const int lane = threadIdx.x & 31;
-  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  const int segs = (L + 1023) / 1024;  // 1 KB row segments
+  uint8_t *flags = s_flags[threadIdx.x >> 5];
+  reinterpret_cast<uint2 *>(flags)[lane] = make_uint2(0u, 0u);
+  __syncwarp();
+  const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int segs = (L + kPresenceSeg - 1) / kPresenceSeg;
   const long long units = (long long)n * segs;
   for (long long u = gwarp; u < units; u += nwarps) {
     const int i = (int)(u / segs), s = (int)(u % segs);
-    const uint8_t *row = chars + (size_t)i * ld;
-    const int k1 = min(L, (s + 1) * 1024);
-    for (int k = s * 1024 + lane; k < k1; k += 32) mask_set(m, row[k]);
+    const int k0 = s * kPresenceSeg;
+    mark_span(chars + (size_t)i * ld + k0, min(L - k0, kPresenceSeg), flags, lane);
   }
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    uint32_t v = m[q];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == 0 && v) atomicOr(&mask[q], v);
-  }
+  flush_flags(flags, mask, lane);
 }
 
-// Presence masks of many alignments: a warp per 1 KB row segment of any job,
-// its lane masks merged into the job's 8 words whenever the warp moves on to
-// another job.
-__device__ __forceinline__ void flush_mask(uint32_t (&m)[8], uint32_t *mask, int lane) {
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    uint32_t v = m[q];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == 0 && v) atomicOr(&mask[q], v);
-    m[q] = 0;
-  }
-}
-
+// Presence masks of many alignments: a warp per row segment of any job, its
+// flags merged into the job's 8 words whenever the warp moves on to another job.
 __global__ void __launch_bounds__(256) presence_multi_kernel(const PackJob *__restrict__ jobs,
                                                              int njobs, long long units,
                                                              uint32_t *__restrict__ masks) {
-  uint32_t m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  __shared__ __align__(16) uint8_t s_flags[kPresenceWarps][256];
   const int lane = threadIdx.x & 31;
+  uint8_t *flags = s_flags[threadIdx.x >> 5];
+  reinterpret_cast<uint2 *>(flags)[lane] = make_uint2(0u, 0u);
+  __syncwarp();
   const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   int cur = -1;
   for (long long u = gwarp; u < units; u += nwarps) {
     const int j = job_of(jobs, njobs, u);
     if (j != cur) {
-      if (cur >= 0) flush_mask(m, masks + 8 * cur, lane);
+      if (cur >= 0) flush_flags(flags, masks + 8 * cur, lane);
       cur = j;
     }
     const PackJob &jb = jobs[j];
-    const int segs = (jb.L + 1023) / 1024;
+    const int segs = (jb.L + kPresenceSeg - 1) / kPresenceSeg;
     const long long local = u - jb.unit0;
     const int i = (int)(local / segs), sg = (int)(local % segs);
-    const uint8_t *row = jb.chars + (size_t)i * jb.ld;
-    const int k1 = min(jb.L, (sg + 1) * 1024);
-    for (int k = sg * 1024 + lane; k < k1; k += 32) mask_set(m, row[k]);
+    const int k0 = sg * kPresenceSeg;
+    mark_span(jb.chars + (size_t)i * jb.ld + k0, min(jb.L - k0, kPresenceSeg), flags, lane);
   }
-  if (cur >= 0) flush_mask(m, masks + 8 * cur, lane);
+  if (cur >= 0) flush_flags(flags, masks + 8 * cur, lane);
 }
 
 __device__ __forceinline__ uint32_t compress_even_bits(uint32_t x) {
@@ -820,8 +844,8 @@ cudaError_t launch_pack_chars(const uint8_t *d_chars, size_t ld, const Packed &p
 
 cudaError_t launch_presence(const uint8_t *d_chars, size_t ld, int n, int L, uint32_t *d_mask,
                             cudaStream_t s) {
-  const long long work = (long long)n * L;
-  presence_kernel<<<grid_for(work, 256), 256, 0, s>>>(d_chars, ld, n, L, d_mask);
+  const long long units = (long long)n * ((L + kPresenceSeg - 1) / kPresenceSeg);  // a warp each
+  presence_kernel<<<grid_for(units * 32, 256), 256, 0, s>>>(d_chars, ld, n, L, d_mask);
   return cudaGetLastError();
 }
 

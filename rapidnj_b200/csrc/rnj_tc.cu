@@ -112,76 +112,161 @@ __device__ __forceinline__ void fill_feature_lut(uint16_t *lut) {
   lut[ch] = (uint16_t)(v[0] | (r[0] << 4) | (t[0] << 8) | (u[0] << 12));
 }
 
+// The 32 bytes of columns 32c .. 32c + 31 of a row as 8 little-endian words;
+// returns how many of them are the row's (0 .. 32; the rest are zero).  Each
+// 16-byte aligned block that lies inside the row is read with one 16-byte load,
+// a block that straddles an end of the row byte by byte within the chunk, and a
+// funnel shift brings the chunk's bytes to the start: nothing outside the row is
+// read, whatever the row's alignment (rows of stride L are rarely 16-byte
+// aligned).
+__device__ __forceinline__ int load_chunk(const uint8_t *__restrict__ row, int L, int c,
+                                          uint32_t (&q)[8]) {
+  const int len = min(32, L - 32 * c);
+  if (len <= 0) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) q[k] = 0u;
+    return 0;
+  }
+  const uintptr_t lo = reinterpret_cast<uintptr_t>(row), hi = lo + (uintptr_t)L;
+  const uintptr_t s = lo + (uintptr_t)c * 32u, e = s + (uintptr_t)len;
+  const int o = (int)(s & 15u);
+  if (o == 0 && len == 32) {
+    const uint4 x = __ldg(reinterpret_cast<const uint4 *>(s));
+    const uint4 y = __ldg(reinterpret_cast<const uint4 *>(s) + 1);
+    q[0] = x.x, q[1] = x.y, q[2] = x.z, q[3] = x.w;
+    q[4] = y.x, q[5] = y.y, q[6] = y.z, q[7] = y.w;
+    return 32;
+  }
+  uint32_t w[12];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const uintptr_t blk = s - (uintptr_t)o + 16u * b;
+    uint32_t x[4] = {0u, 0u, 0u, 0u};
+    if (blk >= lo && blk + 16u <= hi) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4 *>(blk));
+      x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w;
+    } else if (blk < e) {
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        const uintptr_t p = blk + (uintptr_t)m;
+        if (p >= s && p < e)
+          x[m >> 2] |= (uint32_t)(*reinterpret_cast<const uint8_t *>(p)) << (8 * (m & 3));
+      }
+    }
+    w[4 * b] = x[0], w[4 * b + 1] = x[1], w[4 * b + 2] = x[2], w[4 * b + 3] = x[3];
+  }
+  // bytes o .. o + 31 of the 48-byte window: whole words first, then the bytes
+  const int ow = o >> 2;
+  uint32_t u[10], v[9];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) u[k] = (ow & 2) ? w[k + 2] : w[k];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) v[k] = (ow & 1) ? u[k + 1] : u[k];
+  const uint32_t sh = 8u * (uint32_t)(o & 3);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) q[k] = __funnelshift_r(v[k], v[k + 1], sh);
+  return len;
+}
+
 // Row i, 32-column chunk c of the features (zeros for padding rows/columns).
+// The table gives each byte its four FP4 codes as two bytes, v | r << 4 and
+// t | u << 4 (byte 0, which pads a chunk past the row's end, has none).  Per 8
+// sites, byte permutes gather the codes of the even sites and of the odd sites
+// into words, whose nibbles interleave into the four feature words.
 __device__ __forceinline__ void pack_feature_chunk(const uint8_t *__restrict__ chars, size_t ld,
                                                    int n, int L, int Np, int Lk, int i, int c,
                                                    const uint16_t *lut, uint8_t *__restrict__ F) {
-  uint32_t v[4] = {0, 0, 0, 0}, r[4] = {0, 0, 0, 0}, tt[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
-  if (i < n) {
-    const bool aligned = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0;
-    const uint8_t *src = chars + (size_t)i * ld + c * 32;
-    // Two 16-byte loads when the rows are 16-byte aligned and the chunk is
-    // whole (a warp then reads 1 KB of a row contiguously).
-    uint4 q[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-    const bool vec = aligned && c * 32 + 32 <= L;
-    if (vec) {
-      q[0] = __ldg(reinterpret_cast<const uint4 *>(src));
-      q[1] = __ldg(reinterpret_cast<const uint4 *>(src) + 1);
-    }
-    const uint8_t *qb = reinterpret_cast<const uint8_t *>(q);
+  uint32_t q[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  if (i < n) load_chunk(chars + (size_t)i * ld, L, c, q);
+  uint32_t v[4], r[4], tt[4], u[4];
 #pragma unroll
-    for (int b = 0; b < 32; ++b) {
-      if (c * 32 + b >= L) break;
-      const uint32_t e = lut[vec ? qb[b] : src[b]];
-      const int w = b >> 3, sh = (b & 7) * 4;
-      v[w] |= (e & 0xFu) << sh;
-      r[w] |= ((e >> 4) & 0xFu) << sh;
-      tt[w] |= ((e >> 8) & 0xFu) << sh;
-      u[w] |= (e >> 12) << sh;
-    }
+  for (int g = 0; g < 4; ++g) {
+    const uint32_t a = q[2 * g], b = q[2 * g + 1];
+    const uint32_t e0 = lut[a & 0xFFu], e1 = lut[(a >> 8) & 0xFFu];
+    const uint32_t e2 = lut[(a >> 16) & 0xFFu], e3 = lut[a >> 24];
+    const uint32_t e4 = lut[b & 0xFFu], e5 = lut[(b >> 8) & 0xFFu];
+    const uint32_t e6 = lut[(b >> 16) & 0xFFu], e7 = lut[b >> 24];
+    // [lo0 lo2 hi0 hi2], [lo4 lo6 hi4 hi6] -> [lo0 lo2 lo4 lo6] and [hi0 hi2 hi4 hi6]
+    const uint32_t ea = __byte_perm(e0, e2, 0x5140), eb = __byte_perm(e4, e6, 0x5140);
+    const uint32_t oa = __byte_perm(e1, e3, 0x5140), ob = __byte_perm(e5, e7, 0x5140);
+    const uint32_t xe = __byte_perm(ea, eb, 0x5410), ze = __byte_perm(ea, eb, 0x7632);
+    const uint32_t xo = __byte_perm(oa, ob, 0x5410), zo = __byte_perm(oa, ob, 0x7632);
+    v[g] = (xe & 0x0F0F0F0Fu) | ((xo << 4) & 0xF0F0F0F0u);
+    r[g] = ((xe >> 4) & 0x0F0F0F0Fu) | (xo & 0xF0F0F0F0u);
+    tt[g] = (ze & 0x0F0F0F0Fu) | ((zo << 4) & 0xF0F0F0F0u);
+    u[g] = ((ze >> 4) & 0x0F0F0F0Fu) | (zo & 0xF0F0F0F0u);
   }
   store_chunk(F, Np, Lk, i, c, v, r, tt, u);
 }
 
+// The per-byte code of the protein feature pack: residue rank r (the host's
+// table, 0xFF for a gap) split as (r >> 2) | (r & 3) << 4; a gap as 0x40 (low
+// field 4, which no rank has); a rank above 30, which no feature block holds
+// (at most kMaxTcRanks + 1 blocks), as rank 31.
+__device__ __forceinline__ uint32_t prot_code(uint32_t r) {
+  if (r == 0xFFu) return 0x40u;
+  if (r > 30u) return 0x37u;
+  return (r >> 2) | ((r & 3u) << 4);
+}
+
 // Row i, 32-column chunk c of the protein features: block 0 is the valid
 // feature (+1 where the residue is not a gap), block 1 + r the one-hot feature
-// of residue rank r (lut: rank of each byte, 0xFF for a gap).  Then for two
-// sites, V = sum v v' counts the columns where both are residues and
-// M = sum over the rank blocks counts those where they are the same residue:
-// mismatches = V - M, the counts of bitDistanceProtein.cpp:31-61.
+// of residue rank r.  Then for two sites, V = sum v v' counts the columns where
+// both are residues and M = sum over the rank blocks counts those where they
+// are the same residue: mismatches = V - M, the counts of
+// bitDistanceProtein.cpp:31-61.
+// Per 8 sites the codes (prot_code) become two nibble words, hw (r >> 2) and lw
+// (r & 3, or 4 for a gap).  Site k has rank 4h + l exactly when nibble k of both
+// hw ^ h and lw ^ l is zero; adding 7 to every nibble (each is at most 7, so no
+// carry crosses nibbles) sets its bit 3 unless it was zero, which tests all
+// eight sites of a block word in a few instructions.
 __device__ __forceinline__ void pack_prot_chunk(const uint8_t *__restrict__ chars, size_t ld,
                                                 int n, int L, int Np, int Lk, int nfb,
-                                                const uint8_t *lut, int i, int c,
+                                                const uint8_t *code, int i, int c,
                                                 uint8_t *__restrict__ F) {
-  uint8_t rk[32];
+  uint32_t q[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  const int len = i < n ? load_chunk(chars + (size_t)i * ld, L, c, q) : 0;
+  uint32_t hw[4], lw[4];
 #pragma unroll
-  for (int b = 0; b < 32; ++b) rk[b] = 0xFF;
-  if (i < n) {
-    const bool aligned = ((reinterpret_cast<uintptr_t>(chars) | ld) & 15) == 0;
-    const uint8_t *src = chars + (size_t)i * ld + c * 32;
-    uint4 q[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
-    const bool vec = aligned && c * 32 + 32 <= L;
-    if (vec) {
-      q[0] = __ldg(reinterpret_cast<const uint4 *>(src));
-      q[1] = __ldg(reinterpret_cast<const uint4 *>(src) + 1);
+  for (int g = 0; g < 4; ++g) {
+    const uint32_t a = q[2 * g], b = q[2 * g + 1];
+    const uint32_t c0 = code[a & 0xFFu], c1 = code[(a >> 8) & 0xFFu];
+    const uint32_t c2 = code[(a >> 16) & 0xFFu], c3 = code[a >> 24];
+    const uint32_t c4 = code[b & 0xFFu], c5 = code[(b >> 8) & 0xFFu];
+    const uint32_t c6 = code[(b >> 16) & 0xFFu], c7 = code[b >> 24];
+    const uint32_t xe = __byte_perm(__byte_perm(c0, c2, 0x0040), __byte_perm(c4, c6, 0x0040), 0x5410);
+    const uint32_t xo = __byte_perm(__byte_perm(c1, c3, 0x0040), __byte_perm(c5, c7, 0x0040), 0x5410);
+    hw[g] = (xe & 0x0F0F0F0Fu) | ((xo << 4) & 0xF0F0F0F0u);
+    uint32_t l = ((xe >> 4) & 0x0F0F0F0Fu) | (xo & 0xF0F0F0F0u);
+    const int m = len - 8 * g;  // sites of this word inside the row
+    if (m < 8) {
+      const uint32_t keep = m <= 0 ? 0u : (1u << (4 * m)) - 1u;
+      l = (l & keep) | (0x44444444u & ~keep);  // the rest are gaps
     }
-    const uint8_t *qb = reinterpret_cast<const uint8_t *>(q);
-#pragma unroll
-    for (int b = 0; b < 32; ++b)
-      if (c * 32 + b < L) rk[b] = lut[vec ? qb[b] : src[b]];
+    lw[g] = l;
   }
-  uint32_t w[4] = {0, 0, 0, 0};
+  *feat_chunk(F, Np, Lk, 0, i, c) =
+      make_uint4((~lw[0] & 0x44444444u) >> 1, (~lw[1] & 0x44444444u) >> 1,
+                 (~lw[2] & 0x44444444u) >> 1, (~lw[3] & 0x44444444u) >> 1);
+  uint32_t tl[4][4];
 #pragma unroll
-  for (int b = 0; b < 32; ++b)
-    if (rk[b] != 0xFF) w[b >> 3] |= fp4_of(1) << ((b & 7) * 4);
-  *feat_chunk(F, Np, Lk, 0, i, c) = make_uint4(w[0], w[1], w[2], w[3]);
-  for (int f = 1; f < nfb; ++f) {
-    const uint8_t r = (uint8_t)(f - 1);
-    w[0] = w[1] = w[2] = w[3] = 0;
+  for (int l = 0; l < 4; ++l)
 #pragma unroll
-    for (int b = 0; b < 32; ++b)
-      if (rk[b] == r) w[b >> 3] |= fp4_of(1) << ((b & 7) * 4);
-    *feat_chunk(F, Np, Lk, f, i, c) = make_uint4(w[0], w[1], w[2], w[3]);
+    for (int g = 0; g < 4; ++g) tl[l][g] = (lw[g] ^ (0x11111111u * (uint32_t)l)) + 0x77777777u;
+  for (int h = 0; 4 * h + 1 < nfb; ++h) {
+    uint32_t th[4];
+#pragma unroll
+    for (int g = 0; g < 4; ++g) th[g] = (hw[g] ^ (0x11111111u * (uint32_t)h)) + 0x77777777u;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const int f = 4 * h + l + 1;
+      if (f < nfb)
+        *feat_chunk(F, Np, Lk, f, i, c) =
+            make_uint4((~(th[0] | tl[l][0]) & 0x88888888u) >> 2,
+                       (~(th[1] | tl[l][1]) & 0x88888888u) >> 2,
+                       (~(th[2] | tl[l][2]) & 0x88888888u) >> 2,
+                       (~(th[3] | tl[l][3]) & 0x88888888u) >> 2);
+    }
   }
 }
 
@@ -190,14 +275,14 @@ __global__ void __launch_bounds__(256) pack_features_prot_kernel(const uint8_t *
                                                                  int Lk, int nfb, Lut8 lut_in,
                                                                  int row0, int rows,
                                                                  uint8_t *__restrict__ F) {
-  __shared__ uint8_t lut[256];
-  lut[threadIdx.x] = lut_in.v[threadIdx.x];
+  __shared__ uint8_t code[256];
+  code[threadIdx.x] = (uint8_t)prot_code(lut_in.v[threadIdx.x]);
   __syncthreads();
   const int chunks = Lk / 32;
   const long long total = (long long)rows * chunks;
   for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x)
-    pack_prot_chunk(chars, ld, n, L, Np, Lk, nfb, lut, row0 + (int)(t / chunks),
+    pack_prot_chunk(chars, ld, n, L, Np, Lk, nfb, code, row0 + (int)(t / chunks),
                     (int)(t % chunks), F);
 }
 
@@ -217,24 +302,40 @@ __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__res
 }
 
 // Features of many alignments: a thread per (row, 32-column chunk) of any job.
+// A job's units (Np * Lk / 32, Np a multiple of 128 and Lk of 256) are a
+// multiple of 1024, so the 256 units a block takes at a time belong to one job;
+// a protein job's rank codes are staged in shared memory when the block moves
+// on to it.
 __global__ void __launch_bounds__(256) pack_features_multi_kernel(
     const PackJob *__restrict__ jobs, int njobs, long long units) {
   __shared__ uint16_t lut[256];
+  __shared__ uint8_t code[256];
   fill_feature_lut(lut);
   __syncthreads();
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < units;
-       t += (long long)gridDim.x * blockDim.x) {
+  int cur = -1;
+  for (long long base = (long long)blockIdx.x * 256; base < units;
+       base += (long long)gridDim.x * 256) {
     int lo = 0, hi = njobs - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (jobs[mid].unit0 <= t) lo = mid;
+      if (jobs[mid].unit0 <= base) lo = mid;
       else hi = mid - 1;
     }
     const PackJob &jb = jobs[lo];
+    if (lo != cur) {
+      if (jb.kind == KIND_PROT_TC) {
+        __syncthreads();
+        code[threadIdx.x] = (uint8_t)prot_code(jb.lut[threadIdx.x]);
+        __syncthreads();
+      }
+      cur = lo;
+    }
+    const long long t = base + threadIdx.x;
+    if (t >= units) continue;
     const int chunks = jb.W / 32;
     const long long local = t - jb.unit0;
     if (jb.kind == KIND_PROT_TC)
-      pack_prot_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, jb.nfb, jb.lut,
+      pack_prot_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, jb.nfb, code,
                       (int)(local / chunks), (int)(local % chunks), (uint8_t *)jb.dst);
     else
       pack_feature_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, (int)(local / chunks),
