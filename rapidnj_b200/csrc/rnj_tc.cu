@@ -270,6 +270,32 @@ __device__ __forceinline__ void pack_prot_chunk(const uint8_t *__restrict__ char
   }
 }
 
+// The (row, chunk) pairs of a grid-stride loop over rows x chunks work units:
+// one division at the start, then the stride added to the row and chunk.
+struct ChunkWalk {
+  long long t, total, stride;
+  int r, c, chunks, dr, dc;
+  __device__ ChunkWalk(int rows, int chunks_) : chunks(chunks_) {
+    t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    total = (long long)rows * chunks;
+    stride = (long long)gridDim.x * blockDim.x;
+    r = (int)(t / chunks);
+    c = (int)(t % chunks);
+    dr = (int)(stride / chunks);
+    dc = (int)(stride % chunks);
+  }
+  __device__ bool more() const { return t < total; }
+  __device__ void next() {
+    t += stride;
+    r += dr;
+    c += dc;
+    if (c >= chunks) {
+      c -= chunks;
+      ++r;
+    }
+  }
+};
+
 __global__ void __launch_bounds__(256) pack_features_prot_kernel(const uint8_t *__restrict__ chars,
                                                                  size_t ld, int n, int L, int Np,
                                                                  int Lk, int nfb, Lut8 lut_in,
@@ -278,12 +304,8 @@ __global__ void __launch_bounds__(256) pack_features_prot_kernel(const uint8_t *
   __shared__ uint8_t code[256];
   code[threadIdx.x] = (uint8_t)prot_code(lut_in.v[threadIdx.x]);
   __syncthreads();
-  const int chunks = Lk / 32;
-  const long long total = (long long)rows * chunks;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x)
-    pack_prot_chunk(chars, ld, n, L, Np, Lk, nfb, code, row0 + (int)(t / chunks),
-                    (int)(t % chunks), F);
+  ChunkWalk w(rows, Lk / 32);
+  for (; w.more(); w.next()) pack_prot_chunk(chars, ld, n, L, Np, Lk, nfb, code, row0 + w.r, w.c, F);
 }
 
 __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__restrict__ chars,
@@ -293,12 +315,8 @@ __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__res
   __shared__ uint16_t lut[256];
   fill_feature_lut(lut);
   __syncthreads();
-  const int chunks = Lk / 32;
-  const long long total = (long long)rows * chunks;
-  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x)
-    pack_feature_chunk(chars, ld, n, L, Np, Lk, row0 + (int)(t / chunks), (int)(t % chunks), lut,
-                       F);
+  ChunkWalk w(rows, Lk / 32);
+  for (; w.more(); w.next()) pack_feature_chunk(chars, ld, n, L, Np, Lk, row0 + w.r, w.c, lut, F);
 }
 
 // Features of many alignments: a thread per (row, 32-column chunk) of any job.
@@ -330,16 +348,23 @@ __global__ void __launch_bounds__(256) pack_features_multi_kernel(
       }
       cur = lo;
     }
-    const long long t = base + threadIdx.x;
-    if (t >= units) continue;
+    if (base + threadIdx.x >= units) continue;
     const int chunks = jb.W / 32;
-    const long long local = t - jb.unit0;
+    const long long local = base - jb.unit0 + threadIdx.x;
+    int r, c;
+    if (local < (1ll << 32)) {  // a 32-bit division (a job's units rarely exceed 2^32)
+      const uint32_t l = (uint32_t)local;
+      r = (int)(l / (uint32_t)chunks);
+      c = (int)(l - (uint32_t)r * (uint32_t)chunks);
+    } else {
+      r = (int)(local / chunks);
+      c = (int)(local % chunks);
+    }
     if (jb.kind == KIND_PROT_TC)
-      pack_prot_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, jb.nfb, code,
-                      (int)(local / chunks), (int)(local % chunks), (uint8_t *)jb.dst);
+      pack_prot_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, jb.nfb, code, r, c,
+                      (uint8_t *)jb.dst);
     else
-      pack_feature_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, (int)(local / chunks),
-                         (int)(local % chunks), lut, (uint8_t *)jb.dst);
+      pack_feature_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, r, c, lut, (uint8_t *)jb.dst);
   }
 }
 
