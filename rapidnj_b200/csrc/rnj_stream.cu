@@ -12,7 +12,8 @@
 //   rows r0 .. r1-1,  columns r0 .. n-1      (band rows, right of the band start)
 //   rows r1 .. n-1,   columns r0 .. r1-1     (the band's mirror image below it)
 // Each leaves as one 2-D copy into the caller's page-locked matrix while the
-// next band is uploaded (its own copy engine) and computed.  Saturated pairs
+// next bands are computed; every band's upload is enqueued at the start, on its
+// own copy engine.  Saturated pairs
 // (-1) can only take their final value, 2 x the global maximum, at the end:
 // their tiles are fixed on the device after the last band and copied again.
 // When the first band shows saturation in more than a quarter of its tiles,
@@ -49,18 +50,26 @@ int default_band_tiles(int nt) {
   return std::max(1, std::min(g, kTcChunkTiles / std::max(1, nt)));
 }
 
-// Tile-row boundaries of the bands, first band (the last rows) first: a short
-// first band (a quarter of the height) so that the first download starts early,
-// then bands of height g.  bounds[k] .. bounds[k + 1] - 1 are the tile rows of
-// band k in processing order, counted from the top (bounds decrease).
-std::vector<int> band_bounds(int nt, int g) {
+// Tile-row boundaries of the bands, first band (the last rows) first.
+// bounds[k] .. bounds[k + 1] - 1 are the tile rows of band k in processing
+// order, counted from the top (bounds decrease).  A band's download is about its
+// height times the rows below it and its upload its height times L, so the
+// bottom bands have little to download and the download engine waits for their
+// uploads: with `ramp` the first bands are short and grow (1/8, 1/4, 3/8, 1/2,
+// 3/4 of g, at least one tile row each) so that downloads start early, then
+// bands of g.  Without it (an alignment uploaded whole before the bands) only
+// the first band is short (g/4), for an early first download and the
+// saturation sample.
+std::vector<int> band_bounds(int nt, int g, bool ramp) {
+  static const int grow[5][2] = {{1, 8}, {1, 4}, {3, 8}, {1, 2}, {3, 4}};
   std::vector<int> b{nt};
-  int top = nt - std::max(1, g / 4);
-  while (true) {
-    top = std::max(top, 0);
+  int top = nt;
+  for (int k = 0; top > 0; ++k) {
+    int h = g;
+    if (ramp && k < 5) h = std::max(1, g * grow[k][0] / grow[k][1]);
+    else if (k == 0) h = std::max(1, g / 4);
+    top = std::max(0, top - h);
     b.push_back(top);
-    if (top == 0) break;
-    top -= g;
   }
   return b;
 }
@@ -144,7 +153,8 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   if (tp.dna_kernel != 0) return RNJ_ERR_UNSUPPORTED;  // this bucket counts on the bit planes
   const int g = band_tiles > 0 ? band_tiles
                                : (tp.stream_band > 0 ? tp.stream_band : default_band_tiles(nt));
-  const std::vector<int> bounds = band_bounds(nt, g);
+  // DNA uploads band by band (the ramp pays); protein is uploaded whole first.
+  const std::vector<int> bounds = band_bounds(nt, g, !prot);
   const int nbands = (int)bounds.size() - 1;
   if (nbands < 2) return RNJ_ERR_UNSUPPORTED;
   const long long ntiles = tri_tiles(nt);
@@ -263,16 +273,12 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
   RNJ_TRY(cudaEventRecord(ev_alloc, ctx->stream), "event");
   RNJ_TRY(cudaStreamWaitEvent(ctx->s_up, ev_alloc, 0), "upload wait");
 
-  // Band k: upload its sequences, pack them, count and transform its tiles,
-  // then (unless deferred) download what it finished.
-  bool deferred = false;
-  auto run_band = [&](int k) -> int {
-    const int r0 = bounds[k + 1] * kTile;
-    const int r1 = bounds[k] * kTile;                // packed rows (with padding)
-    const int rn1 = std::min(r1, n);                 // output rows
-    cudaEvent_t ev_up = ev.ev[1 + 2 * k], ev_done = ev.ev[2 + 2 * k];
-    // One contiguous upload when the host rows are packed: a 2-D upload
-    // running beside the downloads slows them down.  (Protein: uploaded above.)
+  // The uploads of every band, in band order, back to back on their own
+  // stream: none depends on a band's results, so they run ahead of the kernels
+  // and of the first band's saturation check.  One contiguous copy per band when
+  // the host rows are packed.  (Protein: uploaded above.)
+  for (int k = 0; k < nbands; ++k) {
+    const int r0 = bounds[k + 1] * kTile, rn1 = std::min(bounds[k] * kTile, n);
     if (prot) {
     } else if (ld == (size_t)L)
       RNJ_TRY(cudaMemcpyAsync(buf.chars + (size_t)r0 * L, chars + (size_t)r0 * L,
@@ -282,7 +288,17 @@ int distance_host_streamed(rnj_ctx *ctx, const char *chars, int n, int L, size_t
       RNJ_TRY(cudaMemcpy2DAsync(buf.chars + (size_t)r0 * L, (size_t)L, chars + (size_t)r0 * ld, ld,
                                 (size_t)L, (size_t)(rn1 - r0), cudaMemcpyHostToDevice, ctx->s_up),
               "alignment upload");
-    RNJ_TRY(cudaEventRecord(ev_up, ctx->s_up), "event");
+    RNJ_TRY(cudaEventRecord(ev.ev[1 + 2 * k], ctx->s_up), "event");
+  }
+
+  // Band k: once its sequences are up, pack them, count and transform its
+  // tiles, then (unless deferred) download what it finished.
+  bool deferred = false;
+  auto run_band = [&](int k) -> int {
+    const int r0 = bounds[k + 1] * kTile;
+    const int r1 = bounds[k] * kTile;                // packed rows (with padding)
+    const int rn1 = std::min(r1, n);                 // output rows
+    cudaEvent_t ev_up = ev.ev[1 + 2 * k], ev_done = ev.ev[2 + 2 * k];
     RNJ_TRY(cudaStreamWaitEvent(ctx->stream, ev_up, 0), "kernel wait");
     RNJ_TRY(prot ? launch_pack_features_prot(buf.chars, (size_t)L, n, L, p.Np, p.Lk, p.nfb, lut,
                                              p.feat, ctx->stream, r0, r1 - r0)
