@@ -40,10 +40,50 @@ __device__ __forceinline__ void tri_coords(int t, int nt, int &ti, int &tj) {
   tj = r + (int)(t - start(r));
 }
 
-// The saturation fix-up of one tile of d (-1 -> m2 = 2 x the alignment's
-// maximum; KimuraDistance.cpp:366-395, JCdistance.cpp:201-230), threads t0,
-// t0 + nthr, ... of its 128 x 128 entries: a triangle tile's pairs i < j and
-// their mirror entries, or every off-diagonal entry of a full-square tile.
+// -1 -> m2 in the rows x 128 block of rows r0 .. and columns c0 .. of the
+// matrix (rows and columns below n only; row i is out[(i - row0) * ld]), by
+// threads t0, t0 + nthr, ... of a block: consecutive threads take consecutive
+// columns, and each thread issues kBatch loads before it tests any (the
+// tiles are read at memory latency, not at one load's round trip each).  The
+// diagonal holds 0, never -1.  kBatch: loads in flight per thread (fewer where
+// registers are short).
+template <int kBatch = 16>
+__device__ __forceinline__ void fix_block(float *out, size_t ld, int n, int row0, int r0, int c0,
+                                          float m2, int t0, int nthr, int rows = kTile) {
+  for (int e0 = t0; e0 < rows * kTile; e0 += kBatch * nthr) {
+    float v[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const int e = e0 + k * nthr;
+      const int i = r0 + (e >> 7), j = c0 + (e & (kTile - 1));
+      v[k] = (e < rows * kTile && i < n && j < n) ? out[(size_t)(i - row0) * ld + j] : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      if (v[k] == -1.0f) {
+        const int e = e0 + k * nthr;
+        out[(size_t)(r0 + (e >> 7) - row0) * ld + c0 + (e & (kTile - 1))] = m2;
+      }
+    }
+  }
+}
+
+// The saturation fix-up of one tile (-1 -> m2 = 2 x the alignment's maximum;
+// KimuraDistance.cpp:366-395, JCdistance.cpp:201-230), threads t0, t0 + nthr,
+// ... of a block: a triangle tile and, off the diagonal, its mirror image (the
+// same -1 entries, transposed; each read row by row), or a full-square tile.
+// slice / slices: this block's share of the tile's rows (and of its mirror's).
+template <int kBatch = 16>
+__device__ __forceinline__ void fixup_tile_at(float *out, size_t ld, int n, int row0, bool full,
+                                              int ti, int tj, float m2, int t0, int nthr,
+                                              int slice = 0, int slices = 1) {
+  const int rows = kTile / slices, r = slice * rows;
+  fix_block<kBatch>(out, ld, n, row0, ti * kTile + r, tj * kTile, m2, t0, nthr, rows);
+  if (!full && ti != tj)
+    fix_block<kBatch>(out, ld, n, row0, tj * kTile + r, ti * kTile, m2, t0, nthr, rows);
+}
+
+template <int kBatch = 16>
 __device__ __forceinline__ void fixup_tile(const AlnDesc &d, int tile, float m2, int t0, int nthr) {
   int ti, tj;
   if (d.full) {
@@ -52,17 +92,7 @@ __device__ __forceinline__ void fixup_tile(const AlnDesc &d, int tile, float m2,
   } else {
     tri_coords(tile, d.nt, ti, tj);
   }
-  for (int e = t0; e < kTile * kTile; e += nthr) {
-    const int i = ti * kTile + e / kTile;
-    const int j = tj * kTile + e % kTile;
-    if (d.full) {
-      if (i < d.n && j < d.n && i != j && d.out[(size_t)(i - d.row0) * d.ld + j] == -1.0f)
-        d.out[(size_t)(i - d.row0) * d.ld + j] = m2;
-    } else if (i < j && j < d.n && d.out[(size_t)i * d.ld + j] == -1.0f) {
-      d.out[(size_t)i * d.ld + j] = m2;
-      d.out[(size_t)j * d.ld + i] = m2;
-    }
-  }
+  fixup_tile_at<kBatch>(d.out, d.ld, d.n, d.full ? d.row0 : 0, d.full != 0, ti, tj, m2, t0, nthr);
 }
 
 // Per-thread pair layout inside a 128 x 128 tile (256 threads = 4 x 2 warps, each

@@ -555,9 +555,11 @@ __global__ void __launch_bounds__(256) transform_counts_kernel(int nt, EpiParams
 
 // KimuraDistance.cpp:384-386 / JCdistance.cpp:219-221: every -1 becomes
 // maxDistance * 2, once the global maximum is known.  Only tiles flagged by the
-// epilogue are visited.
-__global__ void __launch_bounds__(256) fixup_kernel(int nt, EpiParams ep) {
-  const int tile_id = blockIdx.x;
+// epilogue are visited, each by `slices` blocks (a share of its rows each): one
+// block per tile when tiles are many (most blocks find no flag and end at
+// once), several when they are few.
+__global__ void __launch_bounds__(256, 8) fixup_kernel(int nt, EpiParams ep, int slices) {
+  const int tile_id = blockIdx.x / slices, slice = blockIdx.x % slices;
   if (ep.tile_flags[tile_id] == 0) return;
   int ti, tj;
   if (ep.full) {
@@ -567,17 +569,8 @@ __global__ void __launch_bounds__(256) fixup_kernel(int nt, EpiParams ep) {
     tri_coords(tile_id, nt, ti, tj);
   }
   const float m2 = __fmul_rn(__int_as_float(*ep.max_bits), 2.0f);
-  for (int e = threadIdx.x; e < kTile * kTile; e += blockDim.x) {
-    const int i = ti * kTile + e / kTile;
-    const int j = tj * kTile + e % kTile;
-    if (ep.full) {
-      if (i < ep.n && j < ep.n && i != j && ep.out[(size_t)i * ep.ld + j] == -1.0f)
-        ep.out[(size_t)i * ep.ld + j] = m2;
-    } else if (i < j && j < ep.n && ep.out[(size_t)i * ep.ld + j] == -1.0f) {
-      ep.out[(size_t)i * ep.ld + j] = m2;
-      ep.out[(size_t)j * ep.ld + i] = m2;
-    }
-  }
+  fixup_tile_at<4>(ep.out, ep.ld, ep.n, 0, ep.full != 0, ti, tj, m2, threadIdx.x, blockDim.x,
+                   slice, slices);
 }
 
 // ------------------------------------------------------- batched popcount path
@@ -794,7 +787,7 @@ __global__ void __launch_bounds__(256) fixup_batch_kernel(const AlnDesc *__restr
     const WorkItem w = it < na ? items_a[it] : items_b[it - na];
     const AlnDesc &d = descs[w.aln];
     if (d.out == nullptr || d.tile_flags[w.tile] == 0) continue;
-    fixup_tile(d, w.tile, __fmul_rn(__int_as_float(*d.max_bits), 2.0f), threadIdx.x, blockDim.x);
+    fixup_tile<4>(d, w.tile, __fmul_rn(__int_as_float(*d.max_bits), 2.0f), threadIdx.x, blockDim.x);
   }
 }
 
@@ -936,7 +929,8 @@ cudaError_t launch_count_tiles(const Packed &p, int count_kind, int epi_mode, co
 cudaError_t launch_fixup(const EpiParams &ep, int nt, cudaStream_t s) {
   const long long ntiles = ep.full ? (long long)nt * nt : tri_tiles(nt);
   if (ntiles == 0) return cudaSuccess;
-  fixup_kernel<<<(unsigned)ntiles, 256, 0, s>>>(nt, ep);
+  const int slices = ntiles <= 148 ? 16 : (ntiles <= 592 ? 4 : 1);
+  fixup_kernel<<<(unsigned)(ntiles * slices), 256, 0, s>>>(nt, ep, slices);
   return cudaGetLastError();
 }
 

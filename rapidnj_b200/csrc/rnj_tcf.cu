@@ -697,7 +697,7 @@ __global__ void __launch_bounds__(kTcfThreads, 1)
         // -------------------------------------------- a tile to fix up
         const float m2 = __fmul_rn(__int_as_float(*reinterpret_cast<volatile int *>(d.max_bits)),
                                    2.0f);
-        fixup_tile(d, tile, m2, tid, nthr);
+        fixup_tile<4>(d, tile, m2, tid, nthr);  // 4 loads in flight: registers are short here
         __threadfence();
         if (!live_epi_sync(sh, lr, ephase, limit)) {
           *sh.abort_flag = 1;
