@@ -56,6 +56,7 @@ SIGNATURES = {
     "rnj_ctx_stage_times": (c_int, [c_void_p, P(c_float)]),
     "rnj_probe_int_peaks": (c_int, [c_void_p, P(ctypes.c_double), P(ctypes.c_double)]),
     "rnj_probe_tc_peak": (c_int, [c_void_p, P(ctypes.c_double)]),
+    "rnj_check_quotient16": (c_int, [c_void_p, P(ctypes.c_ulonglong)]),
     "rnj_aln_from_host": (c_int, [c_void_p, P(c_char_p), c_int, c_int, c_int, c_int, P(c_void_p)]),
     "rnj_aln_from_host_buffer": (c_int, [c_void_p, c_void_p, c_int, c_int, c_size_t, c_int, c_int,
                                          P(c_void_p)]),

@@ -138,6 +138,13 @@ class Context:
         check(N.lib().rnj_probe_tc_peak(self.handle, ctypes.byref(x)))
         return x.value
 
+    def check_quotient16(self) -> int:
+        """Mismatches of the fused epilogue's float quotients num / n over every
+        0 <= num <= n < 2^16, checked on the device (0 on a sound build)."""
+        x = ctypes.c_ulonglong()
+        check(N.lib().rnj_check_quotient16(self.handle, ctypes.byref(x)))
+        return x.value
+
     # --- alignments
     def alignment(self, seqs, type_=None, fastdist: bool = True, compat_wrap: bool = False,
                   full_rows: bool = False, popcount: bool = False) -> Alignment:

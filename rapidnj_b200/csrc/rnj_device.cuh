@@ -274,6 +274,8 @@ static __device__ __noinline__ float k2p_two_logs(double a, double b) {
 
 // JCdistance.cpp:171-183.  b = (alpha - 1) / alpha in double, alpha 4 or 20.
 // rn: an approximate reciprocal of valid (recip_nr; see ratio_f32), or 0.
+__device__ __forceinline__ float jc_of_p(float distance, double b);
+
 __device__ __forceinline__ float jc_distance(unsigned long long total,
                                              unsigned long long valid, double b,
                                              double rn = 0.0) {
@@ -281,6 +283,11 @@ __device__ __forceinline__ float jc_distance(unsigned long long total,
   if (valid == 0) distance = 0.0f;
   else if (rn != 0.0) distance = ratio_f32(total, valid, rn);
   else distance = __fdiv_rn(__ll2float_rn((long long)total), __ull2float_rn(valid));
+  return jc_of_p(distance, b);
+}
+
+// JCdistance.cpp:177-183 from the float p (0 when valid is 0).
+__device__ __forceinline__ float jc_of_p(float distance, double b) {
   const double q = __ddiv_rn((double)distance, b);
   if (q >= 1.0) return -1.0f;
   const double arg = __dsub_rn(1.0, q);
@@ -369,17 +376,37 @@ __device__ __forceinline__ float k2p_decide(uint32_t P, uint32_t Q, uint32_t n, 
   return sat ? -1.0f : (same ? -0.0f : lo);
 }
 
+// 1 / d for an integer 1 <= d < 2^16 given as a float: one Newton-Raphson step
+// r0 + r0 (1 - d r0) from the fast reciprocal (|d r0 - 1| <= 2^-21).  1 - d r0
+// is exact as a fused multiply-add (d r0 has at most 40 significant bits and
+// lies within 2^-21 of 1; the difference is a multiple of 2^-39), so the
+// result has |d y - 1| <= 2^-42 + 2^-24 < 2^-23.9.
+__device__ __forceinline__ float recip16(float d) {
+  const float r0 = rcp_approx(d);
+  return __fmaf_rn(r0, __fmaf_rn(-d, r0, 1.0f), r0);
+}
+
+// fl32(num / d) for integers 0 <= num <= d < 2^16 (d as a float, y = recip16(d))
+// in float arithmetic.  q0 = fl(num y) is within 2^-22.9 (relative) of num / d;
+// the residual num - d q0 is a multiple of ulp(q0) with fewer than 2^17 of them,
+// so one fused multiply-add gives it exactly; q = fl(q0 + r y), one more fused
+// multiply-add, rounds num / d + (num / d - q0)(d y - 1), which is within
+// 2^-22 ulp of num / d.  num / d lies at least 2^-18 ulp from every float
+// midpoint (a midpoint is M 2^-e with M odd of 25 bits, and num / d = M 2^-e
+// would need M | num < 2^16), so q is the correctly rounded quotient: the
+// reference's (float)((double)num / (double)d) and (float)num / (float)d (the
+// double quotient is no midpoint either, so its float rounding agrees).
+__device__ __forceinline__ float quotient16(uint32_t num, float d, float y) {
+  const float fnum = __fsub_rn(__uint_as_float(0x4B000000u | num), 8388608.0f);
+  const float q0 = __fmul_rn(fnum, y);
+  return __fmaf_rn(__fmaf_rn(-q0, d, fnum), y, q0);
+}
+
 // k2p_decide for 16-bit counts (the fused kernel): P, Q, n < 2^16 given as
 // integers packed by the epilogue.  The same decision and result, computed
 // with fewer conversions:
-//   * the doubles of P, Q and n by the 2^52 bias (u32_to_double), the float of
-//     n by the 2^23 bias; the reciprocal as recip_nr from them;
-//   * ts, tv: y = fl(P rn) as in ratio_f32 is within 2^-50 of P / n, which lies
-//     at least 2^-49 (relative) from every float midpoint, so y is no midpoint
-//     and lies on the same side of each: its 24-bit rounding to nearest
-//     (round_to_float_bits, y in [2^-16, 1]) is (double)fl32(P / n), the
-//     reference's (double)ts, without a conversion to float and back (P = 0
-//     gives 0);
+//   * the floats of P, Q and n by the 2^23 bias; ts, tv = quotient16, the
+//     reference's float quotients, converted to double exactly;
 //   * temp1 = (float)a <= 0 exactly when a <= 0: a and b are sums of doubles
 //     of floats in [0, 1] with at most 24 significant bits and exponents above
 //     -17, so a nonzero a or b exceeds 2^-70 in magnitude and its float is not 0;
@@ -388,13 +415,10 @@ __device__ __forceinline__ float k2p_decide(uint32_t P, uint32_t Q, uint32_t n, 
 __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n, bool &slow,
                                               const double2 *tab) {
   const uint32_t nn = n == 0 ? 1u : n;
-  const double dn = u32_to_double(nn);
   const float fn = __fsub_rn(__uint_as_float(0x4B000000u | nn), 8388608.0f);
-  const double r0 = (double)rcp_approx(fn);
-  const double r1 = __fma_rn(r0, __fma_rn(-dn, r0, 1.0), r0);
-  const double rn = __fma_rn(r1, __fma_rn(-dn, r1, 1.0), r1);
-  const double ts = round_to_float_bits(__dmul_rn(u32_to_double(P), rn));
-  const double tv = round_to_float_bits(__dmul_rn(u32_to_double(Q), rn));
+  const float y = recip16(fn);
+  const double ts = (double)quotient16(P, fn, y);
+  const double tv = (double)quotient16(Q, fn, y);
   // fl(1 - 2 ts) as one fused multiply-add: 2 ts is exact, so both forms are
   // the exact 1 - 2 ts rounded once (the reference's double arithmetic).
   const double a = __dsub_rn(__fma_rn(-2.0, ts, 1.0), tv);
@@ -414,6 +438,8 @@ __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n
 
 // KimuraDistance.cpp:322-338 with the Dayhoff table of KimuraDistance.cpp:30-49.
 // rn: an approximate reciprocal of valid (recip_nr; see ratio_f32), or 0.
+__device__ __forceinline__ float kimura_protein_of_p(float distance, const int *pam);
+
 __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism,
                                                          unsigned long long valid,
                                                          const int *pam, double rn = 0.0) {
@@ -421,6 +447,11 @@ __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism
   if (valid != 0)
     distance = rn != 0.0 ? ratio_f32(mism, valid, rn)
                          : __fdiv_rn(__ll2float_rn((long long)mism), __ull2float_rn(valid));
+  return kimura_protein_of_p(distance, pam);
+}
+
+// KimuraDistance.cpp:325-338 from the float p (-1 when valid is 0).
+__device__ __forceinline__ float kimura_protein_of_p(float distance, const int *pam) {
   const double dd = (double)distance;
   if (dd < 0.75) {
     if (dd > 0.0) {

@@ -8,6 +8,7 @@
 #include <algorithm>
 
 #include "rnj.h"
+#include "rnj_device.cuh"
 #include "rnj_internal.h"
 
 namespace rnj {
@@ -131,5 +132,49 @@ extern "C" int rnj_probe_tc_peak(rnj_ctx *ctx, double *fp4_flops_per_s) {
   if (e != cudaSuccess) return cuda_error(e, "tensor-pipe probe");
   if (h_err) return set_error(RNJ_ERR_TIMEOUT, "tensor-pipe probe: a bounded wait ran out");
   *fp4_flops_per_s = best;
+  return RNJ_OK;
+}
+
+namespace rnj {
+
+// Every (num, d) with 1 <= d < 2^16 and 0 <= num <= d (block d, threads over
+// num): quotient16 against the correctly rounded float division and against
+// the reference's double division rounded to float; mismatches counted.
+__global__ void __launch_bounds__(256) quotient16_check_kernel(unsigned long long *mismatches) {
+  const uint32_t d = blockIdx.x + 1;
+  const float fd = (float)d, y = recip16(fd);
+  unsigned long long bad = 0;
+  for (uint32_t num = threadIdx.x; num <= d; num += blockDim.x) {
+    const float q = quotient16(num, fd, y);
+    const float f = __fdiv_rn((float)num, fd);
+    const float g = __double2float_rn(__ddiv_rn((double)num, (double)d));
+    bad += (__float_as_uint(q) != __float_as_uint(f)) + (__float_as_uint(q) != __float_as_uint(g));
+  }
+  if (bad) atomicAdd(mismatches, bad);
+}
+
+}  // namespace rnj
+
+// The fused epilogue's float quotients (quotient16) over their whole domain.
+extern "C" int rnj_check_quotient16(rnj_ctx *ctx, unsigned long long *mismatches) {
+  if (!ctx || !mismatches) return set_error(RNJ_ERR_INVALID, "null argument");
+  void *sv = nullptr;
+  int rc = rnj_ctx_stream(ctx, &sv);
+  if (rc != RNJ_OK) return rc;
+  cudaStream_t s = (cudaStream_t)sv;
+  unsigned long long *d_bad = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&d_bad, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return cuda_error(e, "check counter");
+  e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess) {
+    rnj::quotient16_check_kernel<<<(1u << 16) - 1, 256, 0, s>>>(d_bad);
+    e = cudaGetLastError();
+  }
+  unsigned long long h = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d_bad, sizeof(h), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFreeAsync(d_bad, s);
+  if (e != cudaSuccess) return cuda_error(e, "quotient check");
+  *mismatches = h;
   return RNJ_OK;
 }

@@ -71,11 +71,15 @@ enum {
 template <int M>
 __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint32_t tv,
                                             uint32_t vv) {
-  const double rn = vv ? recip_nr(vv) : 0.0;
-  if constexpr (M == kFusedJc) {
-    return jc_distance((unsigned long long)ts + tv, vv, d.jc_b, rn);
-  } else if constexpr (M == kFusedProtein) {
-    return kimura_protein_distance(ts, vv, c_pam, rn);
+  if constexpr (M == kFusedJc || M == kFusedProtein) {
+    // the float quotient by the valid count in float arithmetic (quotient16:
+    // counts below 2^16 here, the count of differences at most the valid count)
+    const float fv = __fsub_rn(__uint_as_float(0x4B000000u | (vv ? vv : 1u)), 8388608.0f);
+    const float y = recip16(fv);
+    if constexpr (M == kFusedJc)
+      return jc_of_p(vv ? quotient16(ts + tv, fv, y) : 0.0f, d.jc_b);
+    else
+      return kimura_protein_of_p(vv ? quotient16(ts, fv, y) : -1.0f, c_pam);
   } else {
     EpiParams ep;
     ep.n = d.n;

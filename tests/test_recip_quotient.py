@@ -128,3 +128,54 @@ def test_veltkamp_rounding_of_16_bit_quotients():
         check_k2p16(num, den, r)
     for edge in (np.zeros_like(den), np.ones_like(den), den - 1, den):
         check_k2p16(edge, den, r)
+
+
+# --- the fused epilogue's float quotients (rnj_device.cuh: recip16, quotient16)
+#
+# y = fma(r0, fma(-d, r0, 1), r0) from a seed r0 within four ulps of 1 / d, then
+# q0 = fl(num y), r = fma(-q0, d, num), q = fma(r, y, q0), all in float.  The
+# fused multiply-adds are restated exactly (Fraction) where rounding matters:
+# the Newton-Raphson step and the final correction.
+
+def f32(x) -> float:
+    return float(np.float32(x))
+
+
+def fma32(a: float, b: float, c: float) -> float:
+    """fma in float: the exact a * b + c rounded once to float (through a
+    correctly rounded double, exact here unless the sum needs more than 53 bits;
+    the rational is then rounded to float directly)."""
+    exact = Fraction(a) * Fraction(b) + Fraction(c)
+    d = float(exact)
+    if Fraction(d) == exact:
+        return f32(d)
+    lo = np.float32(d)
+    # round the rational to the nearest float, ties to even
+    cands = [np.nextafter(lo, np.float32(-np.inf)), lo, np.nextafter(lo, np.float32(np.inf))]
+    best = min(cands, key=lambda c: (abs(Fraction(float(c)) - exact),
+                                     int(np.array(c, np.float32).view(np.uint32)) & 1))
+    return float(best)
+
+
+def quotient16(num: int, d: int, ulps: int) -> float:
+    r0 = seed(d, ulps)
+    y = fma32(r0, fma32(-float(d), r0, 1.0), r0)
+    q0 = f32(np.float32(num) * np.float32(y))
+    return fma32(fma32(-q0, float(d), float(num)), y, q0)
+
+
+def test_float_quotient_of_16_bit_counts():
+    """Sampled restatement; the device checks every 0 <= num <= d < 2^16
+    itself (tests/test_gpu_quotient16.py)."""
+    rng = np.random.default_rng(16)
+    dens = np.concatenate([np.arange(1, 80), rng.integers(80, 1 << 16, 60), [65535, 65534, 49152]])
+    for d in dens:
+        d = int(d)
+        nums = set(range(min(d, 40) + 1)) | {d, d - 1, d // 2, d // 3} | set(
+            int(x) for x in rng.integers(0, d + 1, 25))
+        for ulps in (-4, -1, 0, 1, 4):
+            for num in nums:
+                if num < 0:
+                    continue
+                want = f32(Fraction(num, d))
+                assert quotient16(num, d, ulps) == want, (num, d, ulps)
