@@ -41,6 +41,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "rnj_device.cuh"
 #include "rnj_epilogue.cuh"
 #include "rnj_internal.h"
@@ -270,31 +272,18 @@ __device__ __forceinline__ void pack_prot_chunk(const uint8_t *__restrict__ char
   }
 }
 
-// The (row, chunk) pairs of a grid-stride loop over rows x chunks work units:
-// one division at the start, then the stride added to the row and chunk.
-struct ChunkWalk {
-  long long t, total, stride;
-  int r, c, chunks, dr, dc;
-  __device__ ChunkWalk(int rows, int chunks_) : chunks(chunks_) {
-    t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    total = (long long)rows * chunks;
-    stride = (long long)gridDim.x * blockDim.x;
-    r = (int)(t / chunks);
-    c = (int)(t % chunks);
-    dr = (int)(stride / chunks);
-    dc = (int)(stride % chunks);
+// The (row, chunk) of work unit t of rows x chunks: a 32-bit division below
+// 2^32 units (the launchers give one thread per unit, so the loop runs once).
+__device__ __forceinline__ void unit_rc(unsigned long long t, int chunks, int &r, int &c) {
+  if (t < (1ull << 32)) {
+    const uint32_t u = (uint32_t)t, q = u / (uint32_t)chunks;
+    r = (int)q;
+    c = (int)(u - q * (uint32_t)chunks);
+  } else {
+    r = (int)(t / (unsigned long long)chunks);
+    c = (int)(t % (unsigned long long)chunks);
   }
-  __device__ bool more() const { return t < total; }
-  __device__ void next() {
-    t += stride;
-    r += dr;
-    c += dc;
-    if (c >= chunks) {
-      c -= chunks;
-      ++r;
-    }
-  }
-};
+}
 
 __global__ void __launch_bounds__(256) pack_features_prot_kernel(const uint8_t *__restrict__ chars,
                                                                  size_t ld, int n, int L, int Np,
@@ -304,8 +293,14 @@ __global__ void __launch_bounds__(256) pack_features_prot_kernel(const uint8_t *
   __shared__ uint8_t code[256];
   code[threadIdx.x] = (uint8_t)prot_code(lut_in.v[threadIdx.x]);
   __syncthreads();
-  ChunkWalk w(rows, Lk / 32);
-  for (; w.more(); w.next()) pack_prot_chunk(chars, ld, n, L, Np, Lk, nfb, code, row0 + w.r, w.c, F);
+  const int chunks = Lk / 32;
+  const unsigned long long total = (unsigned long long)rows * chunks;
+  for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (unsigned long long)gridDim.x * blockDim.x) {
+    int r, c;
+    unit_rc(t, chunks, r, c);
+    pack_prot_chunk(chars, ld, n, L, Np, Lk, nfb, code, row0 + r, c, F);
+  }
 }
 
 __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__restrict__ chars,
@@ -315,8 +310,14 @@ __global__ void __launch_bounds__(256) pack_features_kernel(const uint8_t *__res
   __shared__ uint16_t lut[256];
   fill_feature_lut(lut);
   __syncthreads();
-  ChunkWalk w(rows, Lk / 32);
-  for (; w.more(); w.next()) pack_feature_chunk(chars, ld, n, L, Np, Lk, row0 + w.r, w.c, lut, F);
+  const int chunks = Lk / 32;
+  const unsigned long long total = (unsigned long long)rows * chunks;
+  for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (unsigned long long)gridDim.x * blockDim.x) {
+    int r, c;
+    unit_rc(t, chunks, r, c);
+    pack_feature_chunk(chars, ld, n, L, Np, Lk, row0 + r, c, lut, F);
+  }
 }
 
 // Features of many alignments: a thread per (row, 32-column chunk) of any job.
@@ -350,16 +351,8 @@ __global__ void __launch_bounds__(256) pack_features_multi_kernel(
     }
     if (base + threadIdx.x >= units) continue;
     const int chunks = jb.W / 32;
-    const long long local = base - jb.unit0 + threadIdx.x;
     int r, c;
-    if (local < (1ll << 32)) {  // a 32-bit division (a job's units rarely exceed 2^32)
-      const uint32_t l = (uint32_t)local;
-      r = (int)(l / (uint32_t)chunks);
-      c = (int)(l - (uint32_t)r * (uint32_t)chunks);
-    } else {
-      r = (int)(local / chunks);
-      c = (int)(local % chunks);
-    }
+    unit_rc((unsigned long long)(base - jb.unit0 + threadIdx.x), chunks, r, c);
     if (jb.kind == KIND_PROT_TC)
       pack_prot_chunk(jb.chars, jb.ld, jb.n, jb.L, jb.Np, jb.W, jb.nfb, code, r, c,
                       (uint8_t *)jb.dst);
@@ -407,9 +400,7 @@ cudaError_t launch_pack_features_prot(const uint8_t *d_chars, size_t ld, int n, 
   Lut8 l;
   for (int k = 0; k < 256; ++k) l.v[k] = lut[k];
   const long long work = (long long)rows * (Lk / 32);
-  long long g = (work + 255) / 256;
-  if (g > 148LL * 64) g = 148LL * 64;
-  if (g < 1) g = 1;
+  const long long g = std::max(1LL, std::min((work + 255) / 256, 0x7fffffffLL));  // a thread per unit
   pack_features_prot_kernel<<<(unsigned)g, 256, 0, s>>>(d_chars, ld, n, L, Np, Lk, nfb, l, row0,
                                                         rows, F);
   return cudaGetLastError();
@@ -632,9 +623,7 @@ cudaError_t launch_pack_features(const uint8_t *d_chars, size_t ld, int n, int L
   if (row0 < 0 || rows < 0 || row0 + rows > Np) return cudaErrorInvalidValue;
   if (rows == 0) return cudaSuccess;
   const long long work = (long long)rows * (Lk / 32);
-  long long g = (work + 255) / 256;
-  if (g > 148LL * 64) g = 148LL * 64;
-  if (g < 1) g = 1;
+  const long long g = std::max(1LL, std::min((work + 255) / 256, 0x7fffffffLL));  // a thread per unit
   pack_features_kernel<<<(unsigned)g, 256, 0, s>>>(d_chars, ld, n, L, Np, Lk, row0, rows, F);
   return cudaGetLastError();
 }
