@@ -261,15 +261,18 @@ int rnj_ctx_memory(rnj_ctx *ctx, size_t *free_bytes, size_t *total_bytes);
  * row-major).  max_out may be NULL.  This is what JCdistance::computeDistanceMatrix
  * (JCdistance.cpp:24-44) and KimuraDistance::computeDistances
  * (KimuraDistance.cpp:75-99) produce, from the loader's sequences to the filled
- * matrix.  For DNA on the tensor-core kernel with a page-locked `out`, the call
- * is streamed: bands of rows are computed last band first, and each band's
- * finished rows and columns are copied to `out` while the next band is uploaded
- * and computed (the n*n*4-byte download then bounds the call). */
+ * matrix.  For DNA and protein on the tensor-core kernel with a page-locked `out`
+ * and n above 1408 (12 tile rows; below that one upload, one launch sequence and
+ * one download are faster), the call is streamed: bands of rows are computed
+ * last band first, and each band's finished rows and columns are copied to `out`
+ * while later bands are uploaded and computed (the n*n*4-byte download then
+ * bounds the call). */
 int rnj_distance_matrix_host(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
                              int type, int model, int flags, float *out, float *max_out);
 /* The same with the band height of the streamed form in 128-row tiles:
- * 0 = the library's choice, > 0 = that many tile rows per band, < 0 = not
- * streamed (upload, compute, then one download). */
+ * 0 = the library's choice (not streamed below 12 tile rows), > 0 = that many
+ * tile rows per band (streamed at any size), < 0 = not streamed (upload,
+ * compute, then one download). */
 int rnj_distance_matrix_host_ex(rnj_ctx *ctx, const char *chars, int n, int L, size_t ld,
                                 int type, int model, int flags, int band_tiles, float *out,
                                 float *max_out);

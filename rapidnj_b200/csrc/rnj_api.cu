@@ -1093,6 +1093,23 @@ int rnj_distance_matrix_host_ex(rnj_ctx *ctx, const char *chars, int n, int L, s
   rc = rnj_distance(ctx, a, model, &m);
   rnj_aln_destroy(a);
   if (rc != RNJ_OK) return rc;
+  if (n > 0 && ctx_block_pinned(out, (size_t)n * n * sizeof(float))) {
+    // A page-locked output: the matrix as one 2-D download, the maximum and the
+    // error word behind it, and one synchronisation for all three.
+    cudaError_t e = cudaMemcpy2DAsync(out, (size_t)n * sizeof(float), m->d, m->ld * sizeof(float),
+                                      (size_t)n * sizeof(float), (size_t)n,
+                                      cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ctx->h_max, m->d_max, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ctx->h_max + 1, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    rc = e == cudaSuccess ? take_device_error(ctx) : cuda_error(e, "matrix download");
+    if (rc == RNJ_OK && max_out) memcpy(max_out, ctx->h_max, sizeof(float));
+    rnj_mat_destroy(m);
+    return rc;
+  }
   std::vector<float *> rows((size_t)n);
   for (int i = 0; i < n; ++i) rows[i] = out + (size_t)i * n;
   rc = rnj_mat_copy_rows(ctx, m, 0, n, rows.data(), 0);
