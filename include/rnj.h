@@ -124,10 +124,11 @@ int rnj_probe_int_peaks(rnj_ctx *ctx, double *popc_per_s, double *lop3_per_s);
  * counting kernel uses) with operands already in shared memory.  No counterpart
  * in the reference; the roofline of the tensor-core kernel is quoted against it. */
 int rnj_probe_tc_peak(rnj_ctx *ctx, double *fp4_flops_per_s);
-/* Self-check of the fused epilogue's float quotients by the valid count (the
- * reference's (float)((double)num / (double)n)): every 0 <= num <= n < 2^16 on
- * the device, against correctly rounded division; *mismatches is 0 on a sound
- * build.  No counterpart in the reference. */
+/* Self-check of the fused epilogue's quotients on the device, against
+ * correctly rounded division: the float quotients by the valid count (the
+ * reference's (float)((double)num / (double)n)) for every 0 <= num <= n < 2^16,
+ * and JC's (double)p / b for every float p in [0, 1] and b = 3/4, 19/20.
+ * *mismatches is 0 on a sound build.  No counterpart in the reference. */
 int rnj_check_quotient16(rnj_ctx *ctx, unsigned long long *mismatches);
 
 /* Sequence type of an alignment from its first sequence: any byte >= 65 outside

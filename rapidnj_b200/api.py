@@ -139,8 +139,10 @@ class Context:
         return x.value
 
     def check_quotient16(self) -> int:
-        """Mismatches of the fused epilogue's float quotients num / n over every
-        0 <= num <= n < 2^16, checked on the device (0 on a sound build)."""
+        """Mismatches of the fused epilogue's quotients, checked on the device over
+        their whole domains: the float quotients num / n (0 <= num <= n < 2^16)
+        and JC's double p / b (every float p in [0, 1], b = 3/4 and 19/20).  0 on
+        a sound build."""
         x = ctypes.c_ulonglong()
         check(N.lib().rnj_check_quotient16(self.handle, ctypes.byref(x)))
         return x.value

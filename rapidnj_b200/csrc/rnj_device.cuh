@@ -287,8 +287,25 @@ __device__ __forceinline__ float jc_distance(unsigned long long total,
 }
 
 // JCdistance.cpp:177-183 from the float p (0 when valid is 0).
+__device__ __forceinline__ float jc_of_q(double q, double b);
+
 __device__ __forceinline__ float jc_of_p(float distance, double b) {
-  const double q = __ddiv_rn((double)distance, b);
+  return jc_of_q(__ddiv_rn((double)distance, b), b);
+}
+
+// (double)p / b for a float p in [0, 1] from y = 1 / b correctly rounded
+// (b = 3/4 or 19/20, JCdistance.cpp:171-177): q0 = fl(p y) is within one ulp
+// of p / b, the residual p - b q0 is then exact as one fused multiply-add, and
+// fl(q0 + r y), one more, is the correctly rounded quotient (Markstein's
+// theorem for a correctly rounded reciprocal) -- checked on the device for
+// every float p in [0, 1] and both b (rnj_check_quotient16).
+__device__ __forceinline__ double div_by_b(double p, double b, double inv_b) {
+  const double q0 = __dmul_rn(p, inv_b);
+  return __fma_rn(__fma_rn(-q0, b, p), inv_b, q0);
+}
+
+// JCdistance.cpp:177-183 from q = (double)p / b.
+__device__ __forceinline__ float jc_of_q(double q, double b) {
   if (q >= 1.0) return -1.0f;
   const double arg = __dsub_rn(1.0, q);
   if (arg == 1.0) return __double2float_rn(__dmul_rn(-b, 0.0));  // -0.0, as the reference

@@ -153,9 +153,27 @@ __global__ void __launch_bounds__(256) quotient16_check_kernel(unsigned long lon
   if (bad) atomicAdd(mismatches, bad);
 }
 
+// Every float p in [0, 1] (2^30 + 1 values; thread t of the grid takes the
+// floats with bit patterns t, t + stride, ...): div_by_b against the correctly
+// rounded double division for b = 3/4 and b = 19/20, the two JC constants.
+__global__ void __launch_bounds__(256) jc_quotient_check_kernel(unsigned long long *mismatches) {
+  const double b4 = (4.0 - 1) / 4.0, b20 = (20.0 - 1) / 20.0;
+  const double y4 = __ddiv_rn(1.0, b4), y20 = __ddiv_rn(1.0, b20);
+  unsigned long long bad = 0;
+  const uint32_t one = 0x3F800000u;  // the bits of 1.0f: floats in [0, 1] are 0 .. one
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= one;
+       u += gridDim.x * blockDim.x) {
+    const double p = (double)__uint_as_float(u);
+    bad += __double_as_longlong(div_by_b(p, b4, y4)) != __double_as_longlong(__ddiv_rn(p, b4));
+    bad += __double_as_longlong(div_by_b(p, b20, y20)) != __double_as_longlong(__ddiv_rn(p, b20));
+  }
+  if (bad) atomicAdd(mismatches, bad);
+}
+
 }  // namespace rnj
 
-// The fused epilogue's float quotients (quotient16) over their whole domain.
+// The fused epilogue's quotients over their whole domain: the float quotients
+// (quotient16) and the JC double quotients (div_by_b).
 extern "C" int rnj_check_quotient16(rnj_ctx *ctx, unsigned long long *mismatches) {
   if (!ctx || !mismatches) return set_error(RNJ_ERR_INVALID, "null argument");
   void *sv = nullptr;
@@ -168,6 +186,10 @@ extern "C" int rnj_check_quotient16(rnj_ctx *ctx, unsigned long long *mismatches
   e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), s);
   if (e == cudaSuccess) {
     rnj::quotient16_check_kernel<<<(1u << 16) - 1, 256, 0, s>>>(d_bad);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    rnj::jc_quotient_check_kernel<<<148 * 16, 256, 0, s>>>(d_bad);
     e = cudaGetLastError();
   }
   unsigned long long h = 0;

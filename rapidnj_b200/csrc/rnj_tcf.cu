@@ -70,14 +70,15 @@ enum {
 
 template <int M>
 __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint32_t tv,
-                                            uint32_t vv) {
+                                            uint32_t vv, double jc_inv_b = 0.0) {
   if constexpr (M == kFusedJc || M == kFusedProtein) {
     // the float quotient by the valid count in float arithmetic (quotient16:
     // counts below 2^16 here, the count of differences at most the valid count)
     const float fv = __fsub_rn(__uint_as_float(0x4B000000u | (vv ? vv : 1u)), 8388608.0f);
     const float y = recip16(fv);
-    if constexpr (M == kFusedJc)
-      return jc_of_p(vv ? quotient16(ts + tv, fv, y) : 0.0f, d.jc_b);
+    if constexpr (M == kFusedJc)  // jc_inv_b: 1 / d.jc_b, correctly rounded
+      return jc_of_q(div_by_b(vv ? (double)quotient16(ts + tv, fv, y) : 0.0, d.jc_b, jc_inv_b),
+                     d.jc_b);
     else
       return kimura_protein_of_p(vv ? quotient16(ts, fv, y) : -1.0f, c_pam);
   } else {
@@ -109,6 +110,7 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
   const size_t ld = d.ld;
   const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
   float *const orow = out + (size_t)i * ld;  // dereferenced only for i < n
+  const double jc_inv_b = M == kFusedJc ? __ddiv_rn(1.0, d.jc_b) : 0.0;  // once per row
 #pragma unroll 1
   for (int g = 0; g < 32 / kTcfGroup; ++g) {
     const int j0 = jb + kTcfGroup * g;
@@ -120,7 +122,7 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
         x[k] = 0.0f;
         if (i < j && j < n) {
           const uint32_t vv = (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
-          x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv);
+          x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv, jc_inv_b);
           tmax = fmaxf(tmax, x[k]);
           sat |= (x[k] == -1.0f);
           __stcs(out + (size_t)j * ld + i, x[k]);  // mirror: consecutive i across lanes
