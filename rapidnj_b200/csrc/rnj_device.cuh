@@ -455,20 +455,21 @@ __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n
 
 // KimuraDistance.cpp:322-338 with the Dayhoff table of KimuraDistance.cpp:30-49.
 // rn: an approximate reciprocal of valid (recip_nr; see ratio_f32), or 0.
-__device__ __forceinline__ float kimura_protein_of_p(float distance, const int *pam);
+__device__ __forceinline__ float kimura_protein_of_p(float distance, const float *pam_dist);
 
 __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism,
                                                          unsigned long long valid,
-                                                         const int *pam, double rn = 0.0) {
+                                                         const float *pam_dist, double rn = 0.0) {
   float distance = -1.0f;
   if (valid != 0)
     distance = rn != 0.0 ? ratio_f32(mism, valid, rn)
                          : __fdiv_rn(__ll2float_rn((long long)mism), __ull2float_rn(valid));
-  return kimura_protein_of_p(distance, pam);
+  return kimura_protein_of_p(distance, pam_dist);
 }
 
-// KimuraDistance.cpp:325-338 from the float p (-1 when valid is 0).
-__device__ __forceinline__ float kimura_protein_of_p(float distance, const int *pam) {
+// KimuraDistance.cpp:325-338 from the float p (-1 when valid is 0).  pam_dist:
+// the Dayhoff table's distances, (float)(PAM / 100.0) per entry.
+__device__ __forceinline__ float kimura_protein_of_p(float distance, const float *pam_dist) {
   const double dd = (double)distance;
   if (dd < 0.75) {
     if (dd > 0.0) {
@@ -482,7 +483,7 @@ __device__ __forceinline__ float kimura_protein_of_p(float distance, const int *
       distance = 10.0f;
     } else {
       const int idx = (int)__dsub_rn(__dmul_rn(dd, 1000.0), 750.0);
-      distance = __double2float_rn(__ddiv_rn((double)pam[idx], 100.0));
+      distance = __ldg(pam_dist + idx);
     }
   }
   return distance;

@@ -12,7 +12,7 @@ namespace rnj {
 
 // Dayhoff PAM distances (x100) for p = 0.750 .. 0.930, the table that defines the
 // protein Kimura distance above p = 0.75 (rapidNJ KimuraDistance.cpp:30-49).
-static __constant__ int c_pam[181] = {
+constexpr int kPamX100[181] = {
     195, 196, 197, 198, 199, 200, 200, 201, 202, 203, 204, 205, 206, 207, 208,
     209, 209, 210, 211, 212, 213, 214, 215, 216, 217, 218, 219, 220, 221, 222,
     223, 224, 226, 227, 228, 229, 230, 231, 232, 233, 234, 236, 237, 238, 239,
@@ -26,6 +26,25 @@ static __constant__ int c_pam[181] = {
     517, 524, 531, 538, 545, 553, 560, 569, 577, 586, 595, 605, 615, 626, 637,
     649, 661, 675, 688, 703, 719, 736, 754, 775, 796, 819, 845, 874, 907, 945,
     988};
+
+// The table on the device: the integers, and the distances the reference
+// returns from them, (float)(PAM / 100.0) (KimuraDistance.cpp:336), rounded at
+// compile time (a double division and a float conversion, both correctly
+// rounded).  In global memory, read through L1: the lanes of a warp read
+// different entries, which the constant cache would serialise.
+struct PamTables {
+  int x100[181];
+  float dist[181];
+};
+constexpr PamTables pam_tables() {
+  PamTables t{};
+  for (int k = 0; k < 181; ++k) {
+    t.x100[k] = kPamX100[k];
+    t.dist[k] = (float)((double)kPamX100[k] / 100.0);
+  }
+  return t;
+}
+static __device__ const PamTables c_pam = pam_tables();
 
 // Upper-triangle tile t -> (ti, tj), ti <= tj, row-major over the triangle.
 __device__ __forceinline__ void tri_coords(int t, int nt, int &ti, int &tj) {
@@ -113,7 +132,7 @@ __device__ __forceinline__ float pair_distance(const EpiParams &ep, uint32_t c0,
   if (ep.compat_wrap) v = protein_fast_valid(v, ep.L);
   else if (nr_quotients && valid != 0 && valid < (1u << 24)) rn = recip_nr(valid);
   if (ep.model == RNJ_JC) return jc_distance((unsigned long long)c0 + c1, v, ep.jc_b, rn);
-  if (ep.type == RNJ_PROTEIN) return kimura_protein_distance(c0, v, c_pam, rn);
+  if (ep.type == RNJ_PROTEIN) return kimura_protein_distance(c0, v, c_pam.dist, rn);
   return k2p_distance(c0, c1, v, rn);
 }
 

@@ -64,7 +64,7 @@ __device__ double kimura_protein_double(unsigned long long mism, unsigned long l
   }
   if (dp > 0.930) return 10.0;
   const int idx = (int)__dsub_rn(__dmul_rn(dp, 1000.0), 750.0);
-  return __ddiv_rn((double)c_pam[idx], 100.0);
+  return __ddiv_rn((double)c_pam.x100[idx], 100.0);
 }
 
 struct F64Params {

@@ -80,7 +80,7 @@ __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint3
       return jc_of_q(div_by_b(vv ? (double)quotient16(ts + tv, fv, y) : 0.0, d.jc_b, jc_inv_b),
                      d.jc_b);
     else
-      return kimura_protein_of_p(vv ? quotient16(ts, fv, y) : -1.0f, c_pam);
+      return kimura_protein_of_p(vv ? quotient16(ts, fv, y) : -1.0f, c_pam.dist);
   } else {
     EpiParams ep;
     ep.n = d.n;
