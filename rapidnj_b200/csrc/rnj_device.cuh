@@ -220,6 +220,18 @@ __device__ __forceinline__ float neg_log_checked(double c, double arg) {
   return __float_as_int(lo) == __float_as_int(hi) ? lo : __int_as_float(0x7fc00000);
 }
 
+// neg_log_checked with the table read from `tabq`, the shared-memory copy scaled
+// by -1/4 (neg_quarter_ln_table_k): ln_table(arg) is exactly -4 times that value
+// (a power-of-two scale), so dd, the check and the result are neg_log_checked's
+// bit for bit.
+__device__ __forceinline__ float neg_log_checked_tab(double c, double arg, const double2 *tabq) {
+  const double dd = __dmul_rn(c, __dmul_rn(4.0, neg_quarter_ln_table_k(arg, tabq)));
+  const double eps = __dmul_rn(0x1p-49, __dadd_rn(1.0, __dmul_rn(4.0, dd)));
+  const float lo = __double2float_rn(__dsub_rn(dd, eps));
+  const float hi = __double2float_rn(__dadd_rn(dd, eps));
+  return __float_as_int(lo) == __float_as_int(hi) ? lo : __int_as_float(0x7fc00000);
+}
+
 // The float quotient fl32(num / den) of integers 0 <= num <= den < 2^24, the
 // value of both (float)num / (float)den and (float)((double)num / (double)den)
 // in the reference.  Given rn within 2^-51 (relative) of 1 / den (recip_nr),
@@ -287,7 +299,7 @@ __device__ __forceinline__ float jc_distance(unsigned long long total,
 }
 
 // JCdistance.cpp:177-183 from the float p (0 when valid is 0).
-__device__ __forceinline__ float jc_of_q(double q, double b);
+__device__ __forceinline__ float jc_of_q(double q, double b, const double2 *tabq = nullptr);
 
 __device__ __forceinline__ float jc_of_p(float distance, double b) {
   return jc_of_q(__ddiv_rn((double)distance, b), b);
@@ -304,12 +316,13 @@ __device__ __forceinline__ double div_by_b(double p, double b, double inv_b) {
   return __fma_rn(__fma_rn(-q0, b, p), inv_b, q0);
 }
 
-// JCdistance.cpp:177-183 from q = (double)p / b.
-__device__ __forceinline__ float jc_of_q(double q, double b) {
+// JCdistance.cpp:177-183 from q = (double)p / b.  tabq: the logarithm table in
+// shared memory (neg_log_checked_tab), or null for the global one.
+__device__ __forceinline__ float jc_of_q(double q, double b, const double2 *tabq) {
   if (q >= 1.0) return -1.0f;
   const double arg = __dsub_rn(1.0, q);
   if (arg == 1.0) return __double2float_rn(__dmul_rn(-b, 0.0));  // -0.0, as the reference
-  const float fast = neg_log_checked(b, arg);
+  const float fast = tabq ? neg_log_checked_tab(b, arg, tabq) : neg_log_checked(b, arg);
   if (fast == fast) return fast;
   return neg_log_slow(b, arg);
 }
@@ -455,7 +468,8 @@ __device__ __forceinline__ float k2p_decide16(uint32_t P, uint32_t Q, uint32_t n
 
 // KimuraDistance.cpp:322-338 with the Dayhoff table of KimuraDistance.cpp:30-49.
 // rn: an approximate reciprocal of valid (recip_nr; see ratio_f32), or 0.
-__device__ __forceinline__ float kimura_protein_of_p(float distance, const float *pam_dist);
+__device__ __forceinline__ float kimura_protein_of_p(float distance, const float *pam_dist,
+                                                     const double2 *tabq = nullptr);
 
 __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism,
                                                          unsigned long long valid,
@@ -468,14 +482,15 @@ __device__ __forceinline__ float kimura_protein_distance(unsigned long long mism
 }
 
 // KimuraDistance.cpp:325-338 from the float p (-1 when valid is 0).  pam_dist:
-// the Dayhoff table's distances, (float)(PAM / 100.0) per entry.
-__device__ __forceinline__ float kimura_protein_of_p(float distance, const float *pam_dist) {
+// the Dayhoff table's distances, (float)(PAM / 100.0) per entry; tabq: as jc_of_q.
+__device__ __forceinline__ float kimura_protein_of_p(float distance, const float *pam_dist,
+                                                     const double2 *tabq) {
   const double dd = (double)distance;
   if (dd < 0.75) {
     if (dd > 0.0) {
       const double sq = (double)__fmul_rn(distance, distance);
       const double arg = __dsub_rn(__dsub_rn(1.0, dd), __dmul_rn(sq, 0.20));
-      const float fast = neg_log_checked(1.0, arg);
+      const float fast = tabq ? neg_log_checked_tab(1.0, arg, tabq) : neg_log_checked(1.0, arg);
       distance = fast == fast ? fast : neg_log_slow(1.0, arg);
     }
   } else {

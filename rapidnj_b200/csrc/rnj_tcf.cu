@@ -70,7 +70,8 @@ enum {
 
 template <int M>
 __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint32_t tv,
-                                            uint32_t vv, double jc_inv_b = 0.0) {
+                                            uint32_t vv, double jc_inv_b = 0.0,
+                                            const double2 *tab = nullptr) {
   if constexpr (M == kFusedJc || M == kFusedProtein) {
     // the float quotient by the valid count in float arithmetic (quotient16:
     // counts below 2^16 here, the count of differences at most the valid count)
@@ -78,9 +79,9 @@ __device__ __forceinline__ float fused_pair(const AlnDesc &d, uint32_t ts, uint3
     const float y = recip16(fv);
     if constexpr (M == kFusedJc)  // jc_inv_b: 1 / d.jc_b, correctly rounded
       return jc_of_q(div_by_b(vv ? (double)quotient16(ts + tv, fv, y) : 0.0, d.jc_b, jc_inv_b),
-                     d.jc_b);
+                     d.jc_b, tab);
     else
-      return kimura_protein_of_p(vv ? quotient16(ts, fv, y) : -1.0f, c_pam.dist);
+      return kimura_protein_of_p(vv ? quotient16(ts, fv, y) : -1.0f, c_pam.dist, tab);
   } else {
     EpiParams ep;
     ep.n = d.n;
@@ -102,9 +103,11 @@ static __device__ __noinline__ float k2p_undecided(uint32_t P, uint32_t Q, uint3
 // The 32 distances of row i, columns jb .. jb + 31 (counts pq / pv, see the
 // epilogue): the mirror entries out[j][i], the row entries out[i][j] for j >= i
 // (0 on the diagonal), the running maximum and whether a pair saturated.
+// tab: the logarithm table in shared memory, scaled by -1/4.
 template <int M>
 __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint32_t (&pq)[32],
-                                           uint32_t (&pv)[16], float &tmax, bool &sat) {
+                                           uint32_t (&pv)[16], float &tmax, bool &sat,
+                                           const double2 *tab) {
   const int n = d.n;
   float *const out = d.out;
   const size_t ld = d.ld;
@@ -122,7 +125,7 @@ __device__ __forceinline__ void fused_rows(const AlnDesc &d, int i, int jb, uint
         x[k] = 0.0f;
         if (i < j && j < n) {
           const uint32_t vv = (pv[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
-          x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv, jc_inv_b);
+          x[k] = fused_pair<M>(d, pq[k] & 0xFFFFu, pq[k] >> 16, vv, jc_inv_b, tab);
           tmax = fmaxf(tmax, x[k]);
           sat |= (x[k] == -1.0f);
           __stcs(out + (size_t)j * ld + i, x[k]);  // mirror: consecutive i across lanes
@@ -361,13 +364,13 @@ __device__ __forceinline__ bool fused_tile(const TcShared &sh, uint32_t tmem, co
   } else if constexpr (V == kFusedK2p) {
     fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat, tab);
   } else if constexpr (V != kFusedAny) {
-    fused_rows<V>(d, i, jb, pq, pv, tmax, sat);
+    fused_rows<V>(d, i, jb, pq, pv, tmax, sat, tab);
   } else if (d.compat) {
-    fused_rows<kFusedGeneric>(d, i, jb, pq, pv, tmax, sat);
+    fused_rows<kFusedGeneric>(d, i, jb, pq, pv, tmax, sat, tab);
   } else if (d.model == RNJ_JC) {
-    fused_rows<kFusedJc>(d, i, jb, pq, pv, tmax, sat);
+    fused_rows<kFusedJc>(d, i, jb, pq, pv, tmax, sat, tab);
   } else if (d.type == RNJ_PROTEIN) {
-    fused_rows<kFusedProtein>(d, i, jb, pq, pv, tmax, sat);
+    fused_rows<kFusedProtein>(d, i, jb, pq, pv, tmax, sat, tab);
   } else {
     fused_rows_k2p(d, i, jb, ti < tj && (tj + 1) * kTile <= d.n, pq, pv, tmax, sat, tab);
   }
