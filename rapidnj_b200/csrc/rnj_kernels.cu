@@ -557,7 +557,8 @@ __global__ void __launch_bounds__(256) transform_counts_kernel(int nt, EpiParams
 // maxDistance * 2, once the global maximum is known.  Only tiles flagged by the
 // epilogue are visited, each by `slices` blocks (a share of its rows each): one
 // block per tile when tiles are many (most blocks find no flag and end at
-// once), several when they are few.
+// once; grouping tiles per block serialises the flagged ones and measured
+// slower), several when they are few.
 __global__ void __launch_bounds__(256, 8) fixup_kernel(int nt, EpiParams ep, int slices) {
   const int tile_id = blockIdx.x / slices, slice = blockIdx.x % slices;
   if (ep.tile_flags[tile_id] == 0) return;

@@ -167,6 +167,32 @@ def test_saturation_fixup(ctx):
         assert_matrix_parity(got, ref)
 
 
+@pytest.mark.parametrize("model,mo", [("kim", oracle.KIMURA), ("jc", oracle.JC)])
+def test_saturation_fixup_of_a_large_triangle(ctx, model, mo):
+    """A triangle of 4,465 tiles, about half its pairs saturated: no -1 is
+    left, saturated cells hold 2 x the global maximum, the others the
+    reference's value (cells among 240 random sequences, against the oracle's
+    counts)."""
+    n, L = 12000, 48
+    rng = np.random.default_rng(31)
+    seqs = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, (n, L))]
+    aln = ctx.alignment(torch.from_numpy(seqs).cuda(), oracle.DNA)
+    out = torch.empty((n, n), dtype=torch.float32, device="cuda")
+    mx = ctx.distance_into(aln, model, out, want_max=True)
+    aln.close()
+    rows = np.sort(rng.choice(n, 240, replace=False))
+    got = out[torch.from_numpy(rows).cuda()][:, torch.from_numpy(rows).cuda()].cpu().numpy()
+    assert not bool((out == -1.0).any())
+    del out
+    ref, rmx = oracle.matrix(oracle.counts(seqs[rows], oracle.DNA), L, oracle.DNA, mo)
+    off = ~np.eye(len(rows), dtype=bool)
+    sat = (ref == np.float32(2.0) * np.float32(rmx)) & off
+    assert sat.sum() > 1000
+    assert (got[sat] == np.float32(2.0) * np.float32(mx)).all()
+    d = ulp_diff(got[~sat], ref[~sat])
+    assert d.max() <= 1 and (d == 1).sum() <= 2
+
+
 def test_all_saturated_gives_zero_matrix(ctx):
     seqs = np.array([list(b"AAAA"), list(b"TTTT"), list(b"CCCC")], np.uint8)
     got, mx = gpu_matrix(ctx, seqs, oracle.DNA, "kim")
